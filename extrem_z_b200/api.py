@@ -1,0 +1,243 @@
+"""Python host side of the ExtreM correction, over the C ABI of libextremz.so.
+
+Mirrors the reference's correction call (src/ExtreM_cuda.cu main(), and the
+host API include/api/ExtreM.h used by main.cpp): an original field, its
+decompressed copy and the absolute bound go in; the decompressed copy comes
+back corrected in place.  Status codes of the C ABI become exceptions, except
+``EXTREMZ_ROUND_CAP``, which is reported in the returned report.
+
+There is no CPU fallback: if the CUDA library is missing or no device is
+present, these functions raise.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+import threading
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+_lock = threading.Lock()
+
+OK, ROUND_CAP, BAD_ARG, OOM, CUDA_ERR, DEVICE_TIMEOUT, NO_DEVICE = range(7)
+F32, F64 = 0, 1
+
+# Every entry point declared in include/extremz.h.
+EXPORTS = ("extremz_version", "extremz_default_params", "extremz_ctx_create",
+           "extremz_ctx_destroy", "extremz_correct_device", "extremz_correct_host",
+           "extremz_lut", "extremz_status_string", "extremz_last_cuda_error")
+
+
+class ExtremzError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"extremz status {status}: {msg}")
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("bound", ctypes.c_double), ("thr", ctypes.c_double),
+                ("q", ctypes.c_int), ("edit_type", ctypes.c_int),
+                ("max_outer", ctypes.c_int), ("max_cloop_rounds", ctypes.c_int),
+                ("final_join", ctypes.c_int), ("preserve_join", ctypes.c_int),
+                ("flags", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+
+
+class Report(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("outer_iters", ctypes.c_int),
+                ("cloop_rounds", ctypes.c_int), ("manifold_rounds", ctypes.c_int),
+                ("counters", ctypes.c_int * 11), ("error_bits", ctypes.c_int),
+                ("kernel_launches", ctypes.c_longlong),
+                ("prof_ms", ctypes.c_float * 10), ("prof_launches", ctypes.c_int * 10),
+                ("reserved", ctypes.c_int * 8)]
+
+FLAG_PROFILE = 1
+KCLASS_NAMES = ("setup_classify", "classify_detect", "direction", "jump", "propose", "apply",
+                "rows", "wrong_nbr", "fixpath", "other")
+
+
+@dataclasses.dataclass
+class CorrectionReport:
+    status: int
+    outer_iters: int
+    cloop_rounds: int
+    manifold_rounds: int
+    counters: list
+    error_bits: int
+    kernel_launches: int = 0
+    prof_ms: dict = None
+    prof_launches: dict = None
+
+    @staticmethod
+    def of(r: Report) -> "CorrectionReport":
+        return CorrectionReport(r.status, r.outer_iters, r.cloop_rounds, r.manifold_rounds,
+                                list(r.counters), r.error_bits, int(r.kernel_launches),
+                                dict(zip(KCLASS_NAMES, [float(x) for x in r.prof_ms])),
+                                dict(zip(KCLASS_NAMES, [int(x) for x in r.prof_launches])))
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load libextremz.so (building it first if it is absent or stale)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = _build.LIB
+        if build_if_missing and (not os.path.exists(path) or _build._stale()):
+            try:
+                _build.build()
+            except Exception:
+                if not os.path.exists(path):
+                    raise
+        if not os.path.exists(path):
+            raise ExtremzError(NO_DEVICE, f"CUDA library missing: {path}")
+        L = ctypes.CDLL(path)
+        vp, i32 = ctypes.c_void_p, ctypes.c_int
+        L.extremz_version.restype = i32
+        L.extremz_default_params.argtypes = [ctypes.POINTER(Params)]
+        L.extremz_ctx_create.argtypes = [i32, ctypes.POINTER(vp)]
+        L.extremz_ctx_create.restype = i32
+        L.extremz_ctx_destroy.argtypes = [vp]
+        L.extremz_correct_device.argtypes = [vp, vp, vp, i32, i32, i32, i32,
+                                             ctypes.POINTER(Params), ctypes.POINTER(Report),
+                                             vp, vp, i32]
+        L.extremz_correct_device.restype = i32
+        L.extremz_correct_host.argtypes = [vp, vp, vp, i32, i32, i32, i32,
+                                           ctypes.POINTER(Params), ctypes.POINTER(Report), vp]
+        L.extremz_correct_host.restype = i32
+        L.extremz_lut.argtypes = [vp, i32]
+        L.extremz_lut.restype = i32
+        L.extremz_status_string.argtypes = [i32]
+        L.extremz_status_string.restype = ctypes.c_char_p
+        L.extremz_last_cuda_error.restype = ctypes.c_char_p
+        _lib = L
+        return L
+
+
+def status_string(st: int) -> str:
+    return load().extremz_status_string(st).decode()
+
+
+def _check(st: int, allow_cap: bool = True):
+    if st == OK or (allow_cap and st == ROUND_CAP):
+        return
+    msg = status_string(st)
+    if st == CUDA_ERR:
+        msg += ": " + load().extremz_last_cuda_error().decode()
+    raise ExtremzError(st, msg)
+
+
+def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 1,
+                max_outer: int = 1000, max_cloop_rounds: int = 100000,
+                final_join: bool = True, preserve_join: bool = False,
+                profile: bool = False) -> Params:
+    p = Params()
+    load().extremz_default_params(ctypes.byref(p))
+    p.bound, p.thr, p.q, p.edit_type = float(bound), float(thr), int(q), int(edit_type)
+    p.max_outer, p.max_cloop_rounds = int(max_outer), int(max_cloop_rounds)
+    p.final_join, p.preserve_join = int(bool(final_join)), int(bool(preserve_join))
+    p.flags = FLAG_PROFILE if profile else 0
+    return p
+
+
+class Context:
+    """One device workspace.  Not thread-safe: one correction at a time."""
+
+    def __init__(self, device: int = 0):
+        L = load()
+        h = ctypes.c_void_p()
+        _check(L.extremz_ctx_create(int(device), ctypes.byref(h)), allow_cap=False)
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if self._h:
+            load().extremz_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- device tensors -----------------------------------------------------
+    def correct_device(self, f, decp, bound: float, *, stream=None, trace_cap: int = 0,
+                       **kw):
+        """Correct the CUDA tensor ``decp`` in place; ``f`` is the original.
+
+        Both are contiguous float32/float64 CUDA tensors of shape (D, H, W) or
+        (H, W).  Returns (CorrectionReport, trace array or None).
+        """
+        import torch
+        assert f.is_cuda and decp.is_cuda and f.dtype == decp.dtype and f.shape == decp.shape
+        assert f.is_contiguous() and decp.is_contiguous()
+        dt = {torch.float32: F32, torch.float64: F64}[f.dtype]
+        w, h, d = _whd(tuple(f.shape))
+        if stream is None:
+            stream = torch.cuda.current_stream(f.device).cuda_stream
+        p = make_params(bound, **kw)
+        r = Report()
+        tr = np.zeros(max(trace_cap, 1) * 4, dtype=np.int32)
+        st = load().extremz_correct_device(self._h, f.data_ptr(), decp.data_ptr(), dt, w, h, d,
+                                           ctypes.byref(p), ctypes.byref(r), stream,
+                                           tr.ctypes.data if trace_cap else None, trace_cap * 4)
+        _check(st)
+        trace = None
+        if trace_cap:
+            trace = tr.reshape(-1, 4)
+            trace = trace[trace[:, 0] != 0]
+        return CorrectionReport.of(r), trace
+
+    # -- host arrays ----------------------------------------------------------
+    def correct_host(self, f: np.ndarray, decp: np.ndarray, bound: float, *, stream=None, **kw):
+        """Correct the numpy array ``decp`` in place through host buffers."""
+        assert f.dtype == decp.dtype and f.shape == decp.shape
+        assert f.flags.c_contiguous and decp.flags.c_contiguous
+        dt = {np.dtype(np.float32): F32, np.dtype(np.float64): F64}[f.dtype]
+        w, h, d = _whd(f.shape)
+        p = make_params(bound, **kw)
+        r = Report()
+        st = load().extremz_correct_host(self._h, f.ctypes.data, decp.ctypes.data, dt, w, h, d,
+                                         ctypes.byref(p), ctypes.byref(r), stream)
+        _check(st)
+        return CorrectionReport.of(r)
+
+
+def _whd(shape):
+    if len(shape) == 2:
+        return shape[1], shape[0], 1
+    if len(shape) == 3:
+        return shape[2], shape[1], shape[0]
+    raise ValueError(f"field must be 2-D or 3-D, got shape {shape}")
+
+
+_default_ctx = {}
+
+
+def context(device: int = 0) -> Context:
+    if device not in _default_ctx:
+        _default_ctx[device] = Context(device)
+    return _default_ctx[device]
+
+
+def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, device: int = 0, **kw):
+    """Host-array correction call: returns (corrected copy, report)."""
+    out = np.ascontiguousarray(decp).copy()
+    rep = context(device).correct_host(np.ascontiguousarray(f), out, bound, **kw)
+    return out, rep
+
+
+def lut() -> np.ndarray:
+    out = np.zeros(24800, dtype=np.int32)
+    n = load().extremz_lut(out.ctypes.data, out.size)
+    assert n == 24800
+    return out

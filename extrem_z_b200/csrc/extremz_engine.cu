@@ -1,0 +1,846 @@
+// Host engine of the ExtreM correction and its C ABI (include/extremz.h).
+//
+// The engine runs the reference GPU driver's control flow (src/ExtreM_cuda.cu
+// main() :5508-5997) on one CUDA stream: setup, hot loop #1 (c_loops), the
+// outer loop of three blocks and the final join-saddle pass.  Every kernel is a
+// grid-stride loop over a device-resident count, so no launch shape depends on
+// a host copy of a counter; the host reads the counter block only where the
+// reference's control flow branches on it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/extremz.h"
+#include "extremz_kernels.cuh"
+#include "extremz_lut.h"
+
+namespace extremz {
+
+#define EZ_CHECK(call)                                  \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) {                            \
+      last_cuda_error() = e_;                           \
+      return EXTREMZ_CUDA_ERR;                          \
+    }                                                   \
+  } while (0)
+
+cudaError_t& last_cuda_error() {
+  static thread_local cudaError_t e = cudaSuccess;
+  return e;
+}
+
+// Device copies of the lookup tables, one per device, built on first use.
+struct DeviceLut {
+  int8_t* lut = nullptr;
+  int* key_offset = nullptr;
+  bool ready = false;
+};
+
+static std::mutex g_lut_mu;
+static DeviceLut g_lut[64];
+
+static int device_tables(DeviceTables* out) {
+  int dev = 0;
+  EZ_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return EXTREMZ_BAD_ARG;
+  std::lock_guard<std::mutex> lk(g_lut_mu);
+  DeviceLut& d = g_lut[dev];
+  if (!d.ready) {
+    static HostTables* host = [] {
+      HostTables* t = new HostTables;
+      build_tables(*t);
+      return t;
+    }();
+    EZ_CHECK(cudaMalloc(&d.lut, kLutSize));
+    EZ_CHECK(cudaMalloc(&d.key_offset, 64 * sizeof(int)));
+    EZ_CHECK(cudaMemcpy(d.lut, host->lut, kLutSize, cudaMemcpyHostToDevice));
+    EZ_CHECK(cudaMemcpy(d.key_offset, host->key_offset, 64 * sizeof(int), cudaMemcpyHostToDevice));
+    d.ready = true;
+  }
+  out->lut = d.lut;
+  out->key_offset = d.key_offset;
+  return EXTREMZ_OK;
+}
+
+const HostTables& host_tables() {
+  static HostTables* t = [] {
+    HostTables* p = new HostTables;
+    build_tables(*p);
+    return p;
+  }();
+  return *t;
+}
+
+// ---------------------------------------------------------------------------
+// Workspace: one device arena per context, grown on demand.
+// ---------------------------------------------------------------------------
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, used = 0;
+  int reserve(size_t bytes) {
+    if (bytes <= cap) return EXTREMZ_OK;
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&base, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return EXTREMZ_OOM;
+    }
+    cap = bytes;
+    return EXTREMZ_OK;
+  }
+  template <class P>
+  P* take(size_t count) {
+    size_t bytes = (count * sizeof(P) + 255) & ~size_t(255);
+    if (used + bytes > cap) return nullptr;
+    P* p = reinterpret_cast<P*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+struct Context {
+  int device = 0;
+  Arena arena;
+  int* h_ctr = nullptr;  // pinned copy of the counter block
+  unsigned long long wn_round = 0;
+  int wn_stamp = 0;
+  ~Context() {
+    if (arena.base) cudaFree(arena.base);
+    if (h_ctr) cudaFreeHost(h_ctr);
+  }
+};
+
+// Kernel classes for the optional per-class timing (extremz_report.prof_*).
+enum KClass : int {
+  K_SETUP = 0, K_DETECT, K_DIRECTION, K_JUMP, K_PROPOSE, K_APPLY, K_ROWS, K_WRONG_NBR,
+  K_FIXPATH, K_OTHER, K_NUM
+};
+
+// Phases of the trace (same records as the oracle's trace).
+enum Phase : int {
+  PH_CLOOP_DETECT = 1, PH_WRONG_NBR = 2, PH_SLOOPS = 3, PH_SADDLE = 4, PH_DETECT3 = 5,
+  PH_SLOOPS_JOIN = 6, PH_SADDLE_JOIN = 7, PH_OUTER = 8, PH_CHECKSUM = 9
+};
+
+template <class T>
+__global__ void k_checksum(const T* __restrict__ a, int N, unsigned long long* out) {
+  unsigned long long acc = 0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
+    unsigned long long bits = 0;
+    if (sizeof(T) == 8) bits = (unsigned long long)__double_as_longlong((double)a[v]);
+    else bits = (unsigned long long)__float_as_uint((float)a[v]);
+    unsigned long long z = bits + 0x9e3779b97f4a7c15ull * (unsigned long long)(v + 1);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    acc += z ^ (z >> 31);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+template <class T>
+class Corrector {
+ public:
+  using K = typename KeyOf<T>::K;
+
+  Corrector(Context& ctx, const T* f, T* g, int W, int H, int D, const extremz_params& p,
+            cudaStream_t st, int32_t* trace, int trace_cap)
+      : ctx_(ctx), p_(p), st_(st), trace_(trace), trace_cap_(trace_cap) {
+    std::memset(&J, 0, sizeof(J));
+    J.dim = Dims{W, H, D, W * H * D};
+    J.f = f;
+    J.g = g;
+    J.bound = (T)p.bound;
+    J.thr = (T)p.thr;
+    J.sentinel = T(-4.0) * J.bound;  // init_delta (:2572)
+    J.sentinel_key = KeyOf<T>::enc(J.sentinel);
+    J.q = p.q;
+    J.edit_type = p.edit_type;
+    profile_ = (p.flags & EXTREMZ_FLAG_PROFILE) != 0;
+  }
+
+  int run(extremz_report* rep) {
+    int rc = setup();
+    if (rc != EXTREMZ_OK) return rc;
+    rc = main_loop();
+    if (rep) {
+      rep->status = rc;
+      rep->outer_iters = outer_;
+      rep->cloop_rounds = cloop_rounds_;
+      rep->manifold_rounds = manifold_rounds_;
+      std::memcpy(rep->counters, hc_, sizeof(hc_));
+      rep->error_bits = ctx_.h_ctr[C_ERROR];
+      rep->kernel_launches = launches_;
+    }
+    finish_profile(rep);
+    return rc;
+  }
+
+ private:
+  Context& ctx_;
+  extremz_params p_;
+  cudaStream_t st_;
+  int32_t* trace_;
+  int trace_cap_, trace_len_ = 0;
+  Job<T> J;
+  int grid_ = 0;
+  int outer_ = 0, cloop_rounds_ = 0, manifold_rounds_ = 0;
+  bool capped_ = false;
+  int hc_[11] = {0};
+  int* ctr_ = nullptr;
+
+  long long launches_ = 0;
+  bool profile_ = false;
+  struct Rec { int cls; cudaEvent_t a, b; };
+  std::vector<Rec> recs_;
+  std::vector<cudaEvent_t> pool_;
+
+  cudaEvent_t event() {
+    if (!pool_.empty()) {
+      cudaEvent_t e = pool_.back();
+      pool_.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+
+  // Every kernel goes through here: counted, and bracketed by events when
+  // per-class timing is on.
+  template <class... KArgs, class... Args>
+  void launch(int cls, void (*kern)(KArgs...), dim3 grid, dim3 block, Args... args) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (profile_) {
+      a = event();
+      b = event();
+      cudaEventRecord(a, st_);
+    }
+    kern<<<grid, block, 0, st_>>>(args...);
+    ++launches_;
+    if (profile_) {
+      cudaEventRecord(b, st_);
+      recs_.push_back({cls, a, b});
+    }
+  }
+
+  void finish_profile(extremz_report* rep) {
+    if (!profile_) return;
+    cudaStreamSynchronize(st_);
+    for (const Rec& r : recs_) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      if (rep) {
+        rep->prof_ms[r.cls] += ms;
+        rep->prof_launches[r.cls] += 1;
+      }
+      pool_.push_back(r.a);
+      pool_.push_back(r.b);
+    }
+    recs_.clear();
+    for (cudaEvent_t e : pool_) cudaEventDestroy(e);
+    pool_.clear();
+  }
+
+  int sm_count() {
+    int dev = 0, n = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+  }
+
+  void emit(int phase, int a = 0, int b = 0, int c = 0) {
+    if (!trace_ || trace_len_ + 4 > trace_cap_) return;
+    trace_[trace_len_++] = phase;
+    trace_[trace_len_++] = a;
+    trace_[trace_len_++] = b;
+    trace_[trace_len_++] = c;
+  }
+
+  int zero(int slot, int n = 1) {
+    EZ_CHECK(cudaMemsetAsync(ctr_ + slot, 0, n * sizeof(int), st_));
+    return EXTREMZ_OK;
+  }
+  int read_ctr() {
+    EZ_CHECK(cudaMemcpyAsync(ctx_.h_ctr, ctr_, C_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st_));
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    if (ctx_.h_ctr[C_ERROR]) return EXTREMZ_DEVICE_TIMEOUT;
+    return EXTREMZ_OK;
+  }
+  int h(int slot) const { return ctx_.h_ctr[slot]; }
+  int launched() {
+    EZ_CHECK(cudaGetLastError());
+    return EXTREMZ_OK;
+  }
+  dim3 tile_grid() const {
+    return dim3((J.dim.W + TX - 1) / TX, (J.dim.H + TY - 1) / TY, (J.dim.D + TZ - 1) / TZ);
+  }
+
+#define EZ_RUN(expr)               \
+  do {                             \
+    int rc_ = (expr);              \
+    if (rc_ != EXTREMZ_OK) return rc_; \
+  } while (0)
+
+  // ---------------------------------------------------------------- setup --
+  int setup() {
+    const int N = J.dim.N;
+    EZ_RUN(device_tables(&J.tb));
+    if (!ctx_.h_ctr) EZ_CHECK(cudaMallocHost(&ctx_.h_ctr, C_COUNT * sizeof(int)));
+    grid_ = sm_count() * 8;
+    const int nb = (N + kCpBlock - 1) / kCpBlock;
+    // Phase-1 arena: per-voxel arrays and the CP block counts.  The per-CP
+    // arrays are carved after the counts are known.
+    auto bytes_for = [&](long long ns2, long long ns1, long long nmax, long long nmin) {
+      long long b = 0;
+      auto add = [&](long long count, long long sz) { b += (count * sz + 255) & ~255ll; };
+      add(C_COUNT, 4);
+      add(N, 1); add(N, 2); add(N, 1);         // otype, olm, gate
+      for (int i = 0; i < 5; ++i) add(N, 4);   // ds, as, dds, das, ext
+      add(N, sizeof(K)); add(N, 4); add(N, 4); add(N, 4);  // delta, counter, touched, mm
+      add(N, 8); add(N, 4); add(N, 4);         // claim, taken, taken1
+      for (int i = 0; i < 4; ++i) add(N, 4);   // cand, cand_next, flagged, flagged1
+      add(4ll * nb, 4);                        // cp block counts
+      add(ns2, 4); add(ns1, 4); add(nmax, 4); add(nmin, 4);
+      add(ns2 * kRowStride, 4); add(ns2 * kRowStride, 4);
+      add(ns1 * kRowStride, 4); add(ns1 * kRowStride, 4);
+      for (int i = 0; i < 4; ++i) add(nmax, 4);  // largest, first1, flag2, first_s
+      for (int i = 0; i < 4; ++i) add(nmin, 4);  // smallest, first_min1, flag_min2, first_sj
+      long long ne = std::max(nmax, nmin);
+      add(ne, sizeof(K)); add(ne, 4);
+      add(8, 8);  // checksum
+      return b;
+    };
+    // Worst case for the CP lists is N each; reserve that up front so the
+    // arena is never re-allocated between the two phases.
+    long long worst = bytes_for(N, N, N, N);
+    int rc = ctx_.arena.reserve((size_t)worst);
+    if (rc != EXTREMZ_OK) return rc;
+    Arena& A = ctx_.arena;
+    A.used = 0;
+    ctr_ = J.ctr = A.take<int>(C_COUNT);
+    J.otype = A.take<int8_t>(N);
+    J.olm = A.take<uint16_t>(N);
+    J.gate = A.take<uint8_t>(N);
+    J.ds = A.take<int>(N); J.as = A.take<int>(N);
+    J.dds = A.take<int>(N); J.das = A.take<int>(N);
+    J.ext = A.take<int>(N);
+    J.delta = A.take<K>(N);
+    J.counter = A.take<int>(N);
+    J.touched = A.take<int>(N);
+    J.mm = A.take<int>(N);
+    J.claim = A.take<unsigned long long>(N);
+    J.taken = A.take<int>(N); J.taken1 = A.take<int>(N);
+    J.cand = A.take<int>(N); J.cand_next = A.take<int>(N);
+    J.flagged = A.take<int>(N); J.flagged1 = A.take<int>(N);
+    int* bcount = A.take<int>(4ll * nb);
+    EZ_CHECK(cudaMemsetAsync(ctr_, 0, C_COUNT * sizeof(int), st_));
+
+    // Original classification, gates and manifolds.
+    launch(K_SETUP, k_classify<T, false>, tile_grid(), 256, J, J.f);
+    launch(K_OTHER, k_gate<T>, grid_, 256, J);
+    launch(K_DIRECTION, k_direction<T>, tile_grid(), 256, J, J.f, J.ds, J.as);
+    launch(K_JUMP, k_jump, grid_, 256, J.ds, J.gate, 1, N, N, ctr_ + C_ERROR);
+    launch(K_JUMP, k_jump, grid_, 256, J.as, J.gate, 2, N, N, ctr_ + C_ERROR);
+    EZ_RUN(launched());
+    // Critical-point lists in ascending id.
+    launch(K_OTHER, k_cp_count, nb, kCpBlock, J.otype, N, bcount);
+    launch(K_OTHER, k_cp_scan, 1, 1024, bcount, nb, ctr_);
+    EZ_RUN(launched());
+    EZ_RUN(read_ctr());
+    const int ns2 = h(C_NS2), ns1 = h(C_NS1), nmax = h(C_NMAX), nmin = h(C_NMIN);
+    J.sad2 = A.take<int>(ns2); J.sad1 = A.take<int>(ns1);
+    J.maxima = A.take<int>(nmax); J.minima = A.take<int>(nmin);
+    J.orow2 = A.take<int>((long long)ns2 * kRowStride);
+    J.drow2 = A.take<int>((long long)ns2 * kRowStride);
+    J.orow1 = A.take<int>((long long)ns1 * kRowStride);
+    J.drow1 = A.take<int>((long long)ns1 * kRowStride);
+    J.largest = A.take<int>(nmax); J.first1 = A.take<int>(nmax);
+    J.flag2 = A.take<int>(nmax); J.first_s = A.take<int>(nmax);
+    J.smallest = A.take<int>(nmin); J.first_min1 = A.take<int>(nmin);
+    J.flag_min2 = A.take<int>(nmin); J.first_sj = A.take<int>(nmin);
+    const int ne = std::max(nmax, nmin);
+    J.ext_key = A.take<K>(ne);
+    J.ext_id = A.take<int>(ne);
+    checksum_ = A.take<unsigned long long>(8);
+    launch(K_OTHER, k_cp_write, nb, kCpBlock, J.otype, N, bcount, J.sad2, J.sad1, J.maxima, J.minima);
+    launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
+    launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.f, J.ds, J.sad2, C_NS2, J.orow2);
+    launch(K_ROWS, k_rows<T, false>, grid_, 256, J, J.f, J.as, J.sad1, C_NS1, J.orow1);
+    EZ_RUN(launched());
+    if (ns2) EZ_CHECK(cudaMemsetAsync(J.drow2, 0, (size_t)ns2 * kRowStride * 4, st_));
+    if (ns1) EZ_CHECK(cudaMemsetAsync(J.drow1, 0, (size_t)ns1 * kRowStride * 4, st_));
+    // Largest saddle per maximum, smallest per minimum (original field).
+    if (nmax) {
+      launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, K(0), nmax);
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, -1, nmax);
+      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 0);
+      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 1);
+      EZ_CHECK(cudaMemcpyAsync(J.largest, J.ext_id, nmax * 4, cudaMemcpyDeviceToDevice, st_));
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.first1, kInf, nmax);
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_s, kInf, nmax);
+      EZ_CHECK(cudaMemsetAsync(J.flag2, 0, nmax * 4, st_));
+    }
+    if (nmin) {
+      launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, ~K(0), nmin);
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, kInf, nmin);
+      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 0);
+      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 1);
+      EZ_CHECK(cudaMemcpyAsync(J.smallest, J.ext_id, nmin * 4, cudaMemcpyDeviceToDevice, st_));
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_min1, kInf, nmin);
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_sj, kInf, nmin);
+      EZ_CHECK(cudaMemsetAsync(J.flag_min2, 0, nmin * 4, st_));
+    }
+    // Proposal buffer at the sentinel, counters at -1 (:5082), stamps at 0.
+    launch(K_OTHER, k_fill<K>, grid_, 256, J.delta, J.sentinel_key, N);
+    launch(K_OTHER, k_fill<int>, grid_, 256, J.counter, -1, N);
+    EZ_CHECK(cudaMemsetAsync(J.claim, 0, (size_t)N * 8, st_));
+    EZ_CHECK(cudaMemsetAsync(J.taken, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.taken1, 0, (size_t)N * 4, st_));
+    EZ_RUN(launched());
+    return EXTREMZ_OK;
+  }
+
+  unsigned long long* checksum_ = nullptr;
+
+  int checksum_emit() {
+    if (!trace_) return EXTREMZ_OK;
+    EZ_CHECK(cudaMemsetAsync(checksum_, 0, 8, st_));
+    launch(K_OTHER, k_checksum<T>, grid_, 256, J.g, J.dim.N, checksum_);
+    unsigned long long hsum = 0;
+    EZ_CHECK(cudaMemcpyAsync(&hsum, checksum_, 8, cudaMemcpyDeviceToHost, st_));
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    emit(PH_CHECKSUM, (int)(hsum & 0x7fffffff), (int)((hsum >> 31) & 0x7fffffff));
+    return EXTREMZ_OK;
+  }
+
+  // ------------------------------------------------------------- c_loops --
+  int detect() {
+    EZ_RUN(zero(C_MM, 4));
+    launch(K_DETECT, k_classify<T, true>, tile_grid(), 256, J, J.g);
+    EZ_RUN(launched());
+    EZ_RUN(read_ctr());
+    emit(PH_CLOOP_DETECT, h(C_CMAX), h(C_CMIN), h(C_CSAD));
+    return EXTREMZ_OK;
+  }
+
+  int apply() {
+    launch(K_APPLY, k_apply<T>, grid_, 256, J);
+    return launched();
+  }
+
+  // c_loops (:3913-4044).
+  int c_loops() {
+    EZ_RUN(detect());
+    int rounds = 0;
+    while (h(C_MM) > 0) {
+      if (rounds >= p_.max_cloop_rounds) {
+        capped_ = true;
+        return EXTREMZ_OK;
+      }
+      ++rounds;
+      ++cloop_rounds_;
+      EZ_RUN(zero(C_TOUCHED));
+      launch(K_PROPOSE, k_propose_cp<T>, grid_, 256, J);
+      EZ_RUN(launched());
+      EZ_RUN(apply());
+      EZ_RUN(detect());
+    }
+    return EXTREMZ_OK;
+  }
+
+  // ----------------------------------------------------------- manifolds --
+  int manifolds() {
+    ++manifold_rounds_;
+    const int N = J.dim.N;
+    launch(K_DIRECTION, k_direction<T>, tile_grid(), 256, J, J.g, J.dds, J.das);
+    launch(K_JUMP, k_jump, grid_, 256, J.dds, J.gate, 1, N, N, ctr_ + C_ERROR);
+    launch(K_JUMP, k_jump, grid_, 256, J.das, J.gate, 2, N, N, ctr_ + C_ERROR);
+    launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.g, J.dds, J.sad2, C_NS2, J.drow2);
+    launch(K_ROWS, k_rows<T, false>, grid_, 256, J, J.g, J.das, J.sad1, C_NS1, J.drow1);
+    return launched();
+  }
+
+  template <bool kSplit>
+  int resolve_side(int stamp) {
+    EZ_RUN(zero(C_CAND));
+    launch(K_WRONG_NBR, k_wn_seed<T, kSplit>, grid_, 256, J);
+    EZ_RUN(launched());
+    const int kRounds = 16;
+    for (int r = 0; r < kRounds; ++r) {
+      EZ_RUN(read_ctr());
+      if (h(C_CAND) == 0) return EXTREMZ_OK;
+      const unsigned long long round = ++ctx_.wn_round;
+      EZ_RUN(zero(C_CAND_NEXT));
+      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, J, round, stamp);
+      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, J, round, stamp);
+      EZ_RUN(launched());
+      std::swap(J.cand, J.cand_next);
+      EZ_CHECK(cudaMemcpyAsync(ctr_ + C_CAND, ctr_ + C_CAND_NEXT, 4, cudaMemcpyDeviceToDevice, st_));
+    }
+    launch(K_WRONG_NBR, k_wn_sequential<T, kSplit>, 1, 1, J, stamp);
+    return launched();
+  }
+
+  // get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513).
+  int wrong_neighbors() {
+    const int stamp = ++ctx_.wn_stamp;
+    EZ_RUN(zero(C_NFC, 2));
+    EZ_RUN(resolve_side<true>(stamp));
+    EZ_RUN(resolve_side<false>(stamp));
+    EZ_RUN(read_ctr());
+    emit(PH_WRONG_NBR, h(C_NFC), h(C_NFC1));
+    return EXTREMZ_OK;
+  }
+
+  int manifold_block() {
+    EZ_RUN(manifolds());
+    return wrong_neighbors();
+  }
+
+  // r_loops (:4210-4227).
+  int r_loops() {
+    EZ_RUN(zero(C_TOUCHED));
+    launch(K_FIXPATH, k_fixpath<T, true>, grid_, 256, J);
+    launch(K_FIXPATH, k_fixpath<T, false>, grid_, 256, J);
+    EZ_RUN(launched());
+    return apply();
+  }
+
+  // s_loops (:3465-3487).
+  int s_loops() {
+    EZ_RUN(zero(C_WMC, 2));
+    EZ_RUN(zero(C_TOUCHED));
+    launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, J);
+    launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, J, 1);
+    EZ_RUN(launched());
+    EZ_RUN(apply());
+    if (trace_) {
+      EZ_RUN(read_ctr());
+      emit(PH_SLOOPS, h(C_WMC), h(C_WMC2));
+    }
+    return EXTREMZ_OK;
+  }
+
+  // saddle_loops (:4229-4243).
+  int saddle_loops() {
+    EZ_RUN(zero(C_WSC));
+    EZ_RUN(zero(C_TOUCHED));
+    launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, J);
+    launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, J, 1);
+    EZ_RUN(launched());
+    EZ_RUN(apply());
+    if (trace_) {
+      EZ_RUN(read_ctr());
+      emit(PH_SADDLE, h(C_WSC));
+    }
+    return EXTREMZ_OK;
+  }
+
+  // s_loops_join (:3489-3512).
+  int s_loops_join() {
+    EZ_RUN(zero(C_WMIN, 2));
+    EZ_RUN(zero(C_TOUCHED));
+    launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, J);
+    launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, J, 1);
+    launch(K_OTHER, k_wim_min2_scan<T>, grid_, 256, J);
+    launch(K_OTHER, k_wim_min2_collect<T>, grid_, 256, J);
+    EZ_RUN(launched());
+    EZ_RUN(apply());
+    if (trace_) {
+      EZ_RUN(read_ctr());
+      emit(PH_SLOOPS_JOIN, h(C_WMIN), h(C_WMIN2));
+    }
+    return EXTREMZ_OK;
+  }
+
+  // saddle_loops_join (:4245-4261).
+  int saddle_loops_join() {
+    EZ_RUN(zero(C_WSCJ));
+    EZ_RUN(zero(C_TOUCHED));
+    launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, J);
+    launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, J, 1);
+    EZ_RUN(launched());
+    EZ_RUN(apply());
+    if (trace_) {
+      EZ_RUN(read_ctr());
+      emit(PH_SADDLE_JOIN, h(C_WSCJ));
+    }
+    return EXTREMZ_OK;
+  }
+
+  // --------------------------------------------------------------- main --
+  int main_loop() {
+    const bool join = p_.preserve_join != 0;
+    EZ_RUN(c_loops());
+    if (capped_) return EXTREMZ_ROUND_CAP;
+    EZ_RUN(manifold_block());
+    int nfc = h(C_NFC), nfc1 = h(C_NFC1);
+    int h_wmc = 0, h_wmin = 0;
+    if (nfc == 0) {
+      EZ_RUN(s_loops());
+      EZ_RUN(read_ctr());
+      h_wmc = h(C_WMC);
+      if (h_wmc == 0) EZ_RUN(saddle_loops());
+    }
+    if (nfc1 == 0 && join) {
+      EZ_RUN(s_loops_join());
+      EZ_RUN(read_ctr());
+      h_wmin = h(C_WMIN);
+      if (h_wmin == 0) EZ_RUN(saddle_loops_join());
+    }
+    EZ_RUN(read_ctr());
+    nfc = h(C_NFC);
+    nfc1 = h(C_NFC1);
+    int cfmax = h(C_CMAX), cfmin = h(C_CMIN), cfsad = h(C_CSAD);
+    h_wmin = h(C_WMIN);
+    h_wmc = h(C_WMC);
+    int h_wmin2 = h(C_WMIN2), h_wmc2 = h(C_WMC2), h_wsc = h(C_WSC), h_wscj = h(C_WSCJ);
+    auto any = [&] {
+      return nfc > 0 || nfc1 > 0 || cfmax > 0 || cfmin > 0 || cfsad > 0 || h_wmc > 0 ||
+             h_wmc2 > 0 || h_wsc > 0 || h_wmin > 0 || h_wmin2 > 0 || h_wscj > 0;
+    };
+    while (any()) {
+      if (outer_ >= p_.max_outer) {
+        capped_ = true;
+        break;
+      }
+      ++outer_;
+      // Block 1 (:5622-5747).
+      EZ_RUN(c_loops());
+      if (capped_) break;
+      EZ_RUN(r_loops());
+      EZ_RUN(manifold_block());
+      nfc = h(C_NFC);
+      nfc1 = h(C_NFC1);
+      if (nfc == 0) {
+        EZ_RUN(s_loops());
+        if (h_wmc == 0) EZ_RUN(saddle_loops());  // stale host copy (:5712)
+      }
+      if (nfc1 == 0 && join) {
+        EZ_RUN(s_loops_join());
+        EZ_RUN(read_ctr());
+        h_wmin = h(C_WMIN);
+        if (h_wmin == 0) EZ_RUN(saddle_loops_join());
+      }
+      // Block 2 (:5749-5870).
+      EZ_RUN(c_loops());
+      if (capped_) break;
+      EZ_RUN(manifold_block());
+      nfc = h(C_NFC);
+      nfc1 = h(C_NFC1);
+      if (nfc == 0) {
+        EZ_RUN(s_loops());
+        EZ_RUN(read_ctr());
+        h_wmc = h(C_WMC);
+        if (h_wmc == 0) EZ_RUN(saddle_loops());
+      }
+      if (nfc1 == 0 && join) {
+        EZ_RUN(s_loops_join());
+        EZ_RUN(read_ctr());
+        h_wmin = h(C_WMIN);
+        if (h_wmin == 0) EZ_RUN(saddle_loops_join());
+      }
+      // Block 3 (:5872-5979): detection only.
+      EZ_RUN(c_loops());
+      if (capped_) break;
+      EZ_RUN(manifold_block());
+      nfc = h(C_NFC);
+      nfc1 = h(C_NFC1);
+      if (nfc == 0) {
+        EZ_RUN(zero(C_WMC, 2));
+        EZ_RUN(zero(C_WSC));
+        launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, J);
+        launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, J, 0);
+        launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, J);
+        launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, J, 0);
+        EZ_RUN(launched());
+        EZ_RUN(read_ctr());
+        h_wsc = h(C_WSC);
+        h_wmc = h(C_WMC);
+        h_wmc2 = h(C_WMC2);
+        emit(PH_DETECT3, h_wsc, h_wmc, h_wmc2);
+      }
+      if (nfc1 == 0 && join) {
+        EZ_RUN(zero(C_WMIN, 2));
+        EZ_RUN(zero(C_WSCJ));
+        launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, J);
+        launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, J, 0);
+        launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, J);
+        launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, J, 0);
+        EZ_RUN(launched());
+        EZ_RUN(read_ctr());
+        h_wscj = h(C_WSCJ);
+        h_wmin2 = h(C_WMIN2);
+        h_wmin = h(C_WMIN);
+      }
+      EZ_RUN(detect());
+      cfmax = h(C_CMAX);
+      cfmin = h(C_CMIN);
+      cfsad = h(C_CSAD);
+      emit(PH_OUTER, outer_);
+      EZ_RUN(checksum_emit());
+    }
+    if (!capped_ && p_.final_join) EZ_RUN(saddle_loops_join());  // unconditional (:5997)
+    EZ_RUN(read_ctr());
+    int c[11] = {nfc, nfc1, cfmax, cfmin, cfsad, h_wmc, h_wmc2, h_wsc, h_wmin, h_wmin2, h_wscj};
+    std::memcpy(hc_, c, sizeof(c));
+    return capped_ ? EXTREMZ_ROUND_CAP : EXTREMZ_OK;
+  }
+#undef EZ_RUN
+};
+
+static int check_args(int dtype, long long W, long long H, long long D, const extremz_params* p) {
+  if (!p || (dtype != EXTREMZ_F32 && dtype != EXTREMZ_F64)) return EXTREMZ_BAD_ARG;
+  if (W <= 0 || H <= 0 || D <= 0) return EXTREMZ_BAD_ARG;
+  if (W * H * D >= (1ll << kCatShift)) return EXTREMZ_BAD_ARG;
+  if (p->q <= 0 || (p->edit_type != 0 && p->edit_type != 1)) return EXTREMZ_BAD_ARG;
+  if (p->max_outer < 0 || p->max_cloop_rounds < 0) return EXTREMZ_BAD_ARG;
+  return EXTREMZ_OK;
+}
+
+}  // namespace extremz
+
+using namespace extremz;
+
+struct extremz_ctx_s {
+  Context c;
+};
+
+extern "C" {
+
+int extremz_version(void) { return EXTREMZ_ABI_VERSION; }
+
+void extremz_default_params(extremz_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->bound = 0.0;
+  p->thr = 0.0;
+  p->q = 4;
+  p->edit_type = 1;
+  p->max_outer = 1000;
+  p->max_cloop_rounds = 100000;
+  p->final_join = 1;
+  p->preserve_join = 0;
+  p->flags = 0;
+}
+
+extremz_status extremz_ctx_create(int device, extremz_ctx** out) {
+  if (!out) return EXTREMZ_BAD_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return EXTREMZ_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) return EXTREMZ_BAD_ARG;
+  extremz_ctx* c = new (std::nothrow) extremz_ctx;
+  if (!c) return EXTREMZ_OOM;
+  c->c.device = device;
+  *out = c;
+  return EXTREMZ_OK;
+}
+
+void extremz_ctx_destroy(extremz_ctx* ctx) {
+  if (!ctx) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ctx->c.device);
+  delete ctx;
+  cudaSetDevice(prev);
+}
+
+extremz_status extremz_correct_device(extremz_ctx* ctx, const void* d_orig, void* d_decp, int dtype,
+                                      int width, int height, int depth, const extremz_params* params,
+                                      extremz_report* report, void* stream, int32_t* trace,
+                                      int trace_cap) {
+  if (!ctx || !d_orig || !d_decp) return EXTREMZ_BAD_ARG;
+  int rc = check_args(dtype, width, height, depth, params);
+  if (rc != EXTREMZ_OK) return (extremz_status)rc;
+  if (report) std::memset(report, 0, sizeof(*report));
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == EXTREMZ_F32) {
+    Corrector<float> c(ctx->c, (const float*)d_orig, (float*)d_decp, width, height, depth, *params,
+                       st, trace, trace_cap);
+    rc = c.run(report);
+  } else {
+    Corrector<double> c(ctx->c, (const double*)d_orig, (double*)d_decp, width, height, depth,
+                        *params, st, trace, trace_cap);
+    rc = c.run(report);
+  }
+  if (report) report->status = rc;
+  if (prev != ctx->c.device) cudaSetDevice(prev);
+  return (extremz_status)rc;
+}
+
+extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* h_decp, int dtype,
+                                    int width, int height, int depth, const extremz_params* params,
+                                    extremz_report* report, void* stream) {
+  if (!ctx || !h_orig || !h_decp) return EXTREMZ_BAD_ARG;
+  int rc = check_args(dtype, width, height, depth, params);
+  if (rc != EXTREMZ_OK) return (extremz_status)rc;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
+  const size_t bytes = (size_t)width * height * depth * (dtype == EXTREMZ_F32 ? 4 : 8);
+  cudaStream_t st = (cudaStream_t)stream;
+  void* d = nullptr;
+  if (cudaMalloc(&d, 2 * bytes) != cudaSuccess) {
+    cudaGetLastError();
+    if (prev != ctx->c.device) cudaSetDevice(prev);
+    return EXTREMZ_OOM;
+  }
+  char* df = (char*)d;
+  char* dg = df + bytes;
+  rc = EXTREMZ_OK;
+  if (cudaMemcpyAsync(df, h_orig, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(dg, h_decp, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    rc = EXTREMZ_CUDA_ERR;
+  if (rc == EXTREMZ_OK)
+    rc = extremz_correct_device(ctx, df, dg, dtype, width, height, depth, params, report, stream,
+                                nullptr, 0);
+  if (rc == EXTREMZ_OK || rc == EXTREMZ_ROUND_CAP) {
+    if (cudaMemcpyAsync(h_decp, dg, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      rc = EXTREMZ_CUDA_ERR;
+  }
+  cudaFree(d);
+  if (prev != ctx->c.device) cudaSetDevice(prev);
+  return (extremz_status)rc;
+}
+
+int extremz_lut(int32_t* out, int n) {
+  if (!out || n < kLutSize) return -1;
+  const HostTables& t = host_tables();
+  for (int i = 0; i < kLutSize; ++i) out[i] = t.lut[i];
+  return kLutSize;
+}
+
+const char* extremz_status_string(int status) {
+  switch (status) {
+    case EXTREMZ_OK: return "ok";
+    case EXTREMZ_ROUND_CAP: return "round cap reached before zero mismatch";
+    case EXTREMZ_BAD_ARG: return "bad argument";
+    case EXTREMZ_OOM: return "out of device memory";
+    case EXTREMZ_CUDA_ERR: return "CUDA error";
+    case EXTREMZ_DEVICE_TIMEOUT: return "device-side iteration limit reached";
+    case EXTREMZ_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* extremz_last_cuda_error(void) { return cudaGetErrorString(last_cuda_error()); }
+
+}  // extern "C"

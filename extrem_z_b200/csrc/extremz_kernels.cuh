@@ -1,0 +1,919 @@
+// ExtreM correction kernels for sm_100a.
+//
+// Each kernel replaces one or more kernels of the reference GPU path
+// (src/ExtreM_cuda.cu); the comment on each names them.  Integer, label and
+// comparison work is exact; floating-point updates repeat the reference's
+// operations in the field type T (build with -fmad=false).
+#pragma once
+
+#include "extremz_common.cuh"
+
+namespace extremz {
+
+// ---------------------------------------------------------------------------
+// Per-job device state passed by value to every kernel.
+// ---------------------------------------------------------------------------
+template <class T>
+struct Job {
+  using K = typename KeyOf<T>::K;
+  Dims dim;
+  const T* f;  // original field
+  T* g;        // decompressed field, corrected in place
+  T bound, thr, sentinel;
+  K sentinel_key;
+  int q, edit_type;
+
+  int8_t* otype;      // original vertex type (-1, 0..5)
+  uint16_t* olm;      // original lower-star direction mask
+  uint8_t* gate;      // bit0: next to an original 2-saddle; bit1: next to a 1-saddle
+  int* ds; int* as;   // original steepest ascent / descent roots
+  int* dds; int* das; // decompressed roots
+  int* ext;           // vertex -> index in the maxima / minima list
+
+  K* delta;           // proposal buffer (order-preserving keys), sentinel between phases
+  int* counter;       // delta_counter of the reference (starts at -1)
+  int* touched;       // vertices whose delta left the sentinel in this phase
+  int* mm;            // mismatch list: v | cat << 29
+  unsigned long long* claim;  // wrong-neighbour arbitration, (round << 32) | ~saddle
+  int* taken;         // wrong-neighbour flag stamps (== call id when flagged)
+  int* taken1;
+  int* cand; int* cand_next;  // wrong-neighbour candidate saddles
+  int* flagged; int* flagged1;  // flagged neighbours (split / join)
+
+  int* sad2; int* sad1; int* maxima; int* minima;
+  int* orow2; int* orow1; int* drow2; int* drow1;  // rows of kRowStride ints
+  int* largest; int* smallest;  // per maximum / minimum
+  int* first1; int* flag2;      // per maximum: wrong_index_max arbitration
+  int* first_min1; int* flag_min2;
+  int* first_s; int* first_sj;  // per extremum: wrong_index_saddles arbitration
+  K* ext_key; int* ext_id;      // largest / smallest saddle selection scratch
+
+  int* ctr;  // device counters, see Ctr
+  DeviceTables tb;
+};
+
+// Indices into the device counter block.
+enum Ctr : int {
+  C_MM = 0, C_CMAX, C_CMIN, C_CSAD, C_TOUCHED, C_NFC, C_NFC1, C_CAND, C_CAND_NEXT,
+  C_WMC, C_WMC2, C_WSC, C_WMIN, C_WMIN2, C_WSCJ, C_NS2, C_NS1, C_NMAX, C_NMIN,
+  C_ERROR, C_CHANGED, C_COUNT
+};
+// Error bits in ctr[C_ERROR].
+constexpr int kErrJump = 1, kErrPath = 2, kErrTile = 4, kErrResolve = 8;
+
+template <class T>
+__device__ __forceinline__ T tabs(T v) { return v < T(0) ? -v : v; }
+
+// ---------------------------------------------------------------------------
+// Classification over a shared-memory halo tile.
+//
+// Replaces classifyVertex_CUDA (:3720-3911).  kDetect = false writes the
+// original type and lower-star mask (type=0 call, :5289); kDetect = true is the
+// fused mismatch detection of the type=1 call (:3856-3910), appending each
+// mismatching vertex once with its categories (max, min, saddle) through
+// warp ballots.
+// ---------------------------------------------------------------------------
+constexpr int TX = 32, TY = 8, TZ = 4;
+constexpr int HX = TX + 2, HY = TY + 2, HZ = TZ + 2;
+
+template <class T>
+__device__ __forceinline__ void load_tile(T (*s)[HY][HX], const T* __restrict__ a, const Dims& g,
+                                          int bx, int by, int bz) {
+  for (int i = threadIdx.x; i < HX * HY * HZ; i += blockDim.x) {
+    int lx = i % HX, t = i / HX, ly = t % HY, lz = t / HY;
+    int gx = bx + lx - 1, gy = by + ly - 1, gz = bz + lz - 1;
+    if (gx >= 0 && gx < g.W && gy >= 0 && gy < g.H && gz >= 0 && gz < g.D)
+      s[lz][ly][lx] = a[gx + (long long)gy * g.W + (long long)gz * g.W * g.H];
+  }
+}
+
+// Type of the tile voxel at (lx, ly, lz) (1-based tile coordinates).
+template <class T>
+__device__ __forceinline__ int tile_type(const T (*s)[HY][HX], int lx, int ly, int lz, int bc,
+                                         const DeviceTables& tb, int& lmask) {
+  const T c = s[lz][ly][lx];
+  int lm = 0, up = 0, k = 0, nl = 0, nu = 0;
+#pragma unroll
+  for (int d = 0; d < kNumDirs; ++d) {
+    if (!dir_valid(d, bc)) continue;
+    const T nv = s[lz + dir_z(d)][ly + dir_y(d)][lx + dir_x(d)];
+    const bool before = dir_neighbour_is_before(d);
+    if (nv < c || (nv == c && before)) {
+      lm |= 1 << d;
+      ++nl;
+    } else if (nv > c || (nv == c && !before)) {
+      up |= 1 << k;
+      ++nu;
+    }
+    ++k;
+  }
+  lmask = lm;
+  if (nu == 0) return 4;
+  if (nl == 0) return 0;
+  const int off = tb.key_offset[bc];
+  if (off < 0) return -1;
+  return __ldg(tb.lut + off + up);
+}
+
+__device__ __forceinline__ int mismatch_cats(int t, int o, int lm, int olm) {
+  int cat = 0;
+  if (t != o) {
+    if ((t == 4) != (o == 4)) cat |= kCatMax;
+    if ((t == 0) != (o == 0)) cat |= kCatMin;
+    if ((t == 2) != (o == 2) || (t == 1) != (o == 1) || (t == 3) != (o == 3)) cat |= kCatSaddle;
+  } else if ((t == 1 || t == 2 || t == 3) && lm != olm) {
+    cat |= kCatSaddle;  // areVectorsDifferent_local (:909-921) on direction masks
+  }
+  return cat;
+}
+
+template <class T, bool kDetect>
+__global__ void __launch_bounds__(256) k_classify(Job<T> J, const T* __restrict__ a) {
+  __shared__ T s[HZ][HY][HX];
+  const Dims g = J.dim;
+  const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
+  load_tile(s, a, g, bx, by, bz);
+  __syncthreads();
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  for (int tz = 0; tz < TZ; ++tz) {
+    const int x = bx + tx, y = by + ty, z = bz + tz;
+    const bool in = x < g.W && y < g.H && z < g.D;
+    int cat = 0, v = 0;
+    if (in) {
+      v = x + y * g.W + z * g.W * g.H;
+      const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
+      int lm;
+      const int t = tile_type(s, tx + 1, ty + 1, tz + 1, bc, J.tb, lm);
+      if (!kDetect) {
+        J.otype[v] = (int8_t)t;
+        J.olm[v] = (uint16_t)lm;
+      } else {
+        cat = mismatch_cats(t, J.otype[v], lm, J.olm[v]);
+      }
+    }
+    if (kDetect) {
+      const int slot = warp_append(J.ctr + C_MM, cat != 0, 0xffffffffu);
+      if (slot >= 0) J.mm[slot] = v | (cat << kCatShift);
+      if (cat & kCatMax) atomicAdd(J.ctr + C_CMAX, 1);
+      if (cat & kCatMin) atomicAdd(J.ctr + C_CMIN, 1);
+      if (cat & kCatSaddle) atomicAdd(J.ctr + C_CSAD, 1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Steepest directions with tile-local path compression.
+//
+// Replaces ComputeDirection (:1464-1512) and the first steps of the pointer
+// jumping (:1514-1611): each voxel's steepest-ascent (descent) pointer is
+// followed inside the tile in shared memory until it leaves the tile or stops
+// at a root, so the global jump that follows moves a tile per hop.
+// Output: ds/as = first vertex outside the tile on the path, or the root.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_direction(Job<T> J, const T* __restrict__ a,
+                                                   int* __restrict__ ds, int* __restrict__ as) {
+  __shared__ T s[HZ][HY][HX];
+  __shared__ int phi[TZ * TY * TX], plo[TZ * TY * TX];
+  const Dims g = J.dim;
+  const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
+  load_tile(s, a, g, bx, by, bz);
+  __syncthreads();
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  const int WH = g.W * g.H;
+  for (int tz = 0; tz < TZ; ++tz) {
+    const int li = (tz * TY + ty) * TX + tx;
+    const int x = bx + tx, y = by + ty, z = bz + tz;
+    if (!(x < g.W && y < g.H && z < g.D)) {
+      phi[li] = -1;
+      plo[li] = -1;
+      continue;
+    }
+    const int v = x + y * g.W + z * WH;
+    const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
+    const T c = s[tz + 1][ty + 1][tx + 1];
+    int hd = -1, ld = -1;
+    T hv = c, lv = c;
+    int hid = v, lid = v;
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d) {
+      if (!dir_valid(d, bc)) continue;
+      const T nv = s[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + 1 + dir_x(d)];
+      const int r = v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+      if (hv < nv || (hv == nv && hid < r)) { hv = nv; hid = r; hd = d; }
+      if (lv > nv || (lv == nv && lid > r)) { lv = nv; lid = r; ld = d; }
+    }
+    // Encode: local index (>= 0) when the target lies in this tile, else
+    // -(global id) - 1; a root points to itself and is stored resolved.
+    auto enc = [&](int d, int gid) {
+      if (d < 0) return -gid - 1;
+      const int ltx = tx + dir_x(d), lty = ty + dir_y(d), ltz = tz + dir_z(d);
+      if (ltx < 0 || ltx >= TX || lty < 0 || lty >= TY || ltz < 0 || ltz >= TZ) return -gid - 1;
+      return (ltz * TY + lty) * TX + ltx;
+    };
+    phi[li] = enc(hd, hid);
+    plo[li] = enc(ld, lid);
+  }
+  __syncthreads();
+  // In-place pointer jumping inside the tile; each step advances along the
+  // path, so it converges in O(log tile) steps.
+  for (int it = 0; it < 64; ++it) {
+    int changed = 0;
+    for (int tz = 0; tz < TZ; ++tz) {
+      const int li = (tz * TY + ty) * TX + tx;
+      int p = phi[li];
+      if (p >= 0) { phi[li] = phi[p]; changed = 1; }
+      p = plo[li];
+      if (p >= 0) { plo[li] = plo[p]; changed = 1; }
+    }
+    if (!__syncthreads_or(changed)) break;
+    if (it == 63 && threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
+  }
+  for (int tz = 0; tz < TZ; ++tz) {
+    const int li = (tz * TY + ty) * TX + tx;
+    const int x = bx + tx, y = by + ty, z = bz + tz;
+    if (!(x < g.W && y < g.H && z < g.D)) continue;
+    const int v = x + y * g.W + z * WH;
+    const int ph = phi[li], pl = plo[li];
+    ds[v] = ph < 0 ? -ph - 1 : v;  // ph >= 0 cannot remain; guard anyway
+    as[v] = pl < 0 ? -pl - 1 : v;
+  }
+}
+
+// Global pointer jumping for gated vertices (ComputeDescendingManifold /
+// ComputeAscendingManifold, :1514-1611): in place, with an iteration cap
+// after which the error word is set instead of spinning.
+__global__ void __launch_bounds__(256) k_jump(int* __restrict__ lab, const uint8_t* __restrict__ gate,
+                                              int bit, int N, int cap, int* err) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
+    if (gate && !(gate[v] & bit)) continue;
+    int u = lab[v];
+    int it = 0;
+    for (; it < cap; ++it) {
+      const int w = lab[u];
+      if (w == u) break;
+      lab[v] = w;
+      u = w;
+    }
+    if (it == cap) atomicOr(err, kErrJump);
+  }
+}
+
+// Gate bits from the original types: bit0 when a neighbour is an original
+// 2-saddle (type 2 or 3), bit1 when one is a 1-saddle (type 1 or 3)
+// (the is_saddle_neighbor tests at :1530-1548 and :1584-1601).
+template <class T>
+__global__ void k_gate(Job<T> J) {
+  const Dims g = J.dim;
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < g.N; v += stride) {
+    int ids[kNumDirs];
+    const int n = neighbours(v, g, ids, nullptr);
+    uint8_t gb = 0;
+    for (int j = 0; j < n; ++j) {
+      const int t = J.otype[ids[j]];
+      if (t == 2 || t == 3) gb |= 1;
+      if (t == 1 || t == 3) gb |= 2;
+    }
+    J.gate[v] = gb;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ordered compaction of the critical-point lists (ExtractCP :1694-1741, here in
+// ascending vertex id).  Pass 1 counts per 1024-vertex block, pass 2 scans the
+// block counts, pass 3 writes.
+// ---------------------------------------------------------------------------
+constexpr int kCpBlock = 1024;
+
+__device__ __forceinline__ int cp_bits(int t) {
+  return ((t == 2 || t == 3) ? 1 : 0) | ((t == 1 || t == 3) ? 2 : 0) | (t == 4 ? 4 : 0) |
+         (t == 0 ? 8 : 0);
+}
+
+__global__ void __launch_bounds__(kCpBlock) k_cp_count(const int8_t* __restrict__ otype, int N,
+                                                       int* __restrict__ bcount) {
+  __shared__ int cnt[4];
+  if (threadIdx.x < 4) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int v = blockIdx.x * kCpBlock + threadIdx.x;
+  const int b = v < N ? cp_bits(otype[v]) : 0;
+  for (int l = 0; l < 4; ++l) {
+    const unsigned m = __ballot_sync(0xffffffffu, (b >> l) & 1);
+    if (lane_id() == 0 && m) atomicAdd(&cnt[l], __popc(m));
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) bcount[threadIdx.x * gridDim.x + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// Single block: exclusive scan of the 4 x nb block counts in place, totals to
+// ctr[C_NS2 .. C_NMIN].
+__global__ void __launch_bounds__(1024) k_cp_scan(int* __restrict__ bcount, int nb, int* ctr) {
+  __shared__ int carry;
+  __shared__ int warp_sums[32];
+  for (int l = 0; l < 4; ++l) {
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += 1024) {
+      const int i = base + threadIdx.x;
+      const int x = i < nb ? bcount[l * nb + i] : 0;
+      int incl = x;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane_id() >= (unsigned)o) incl += y;
+      }
+      if (lane_id() == 31) warp_sums[threadIdx.x / 32] = incl;
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        int w = warp_sums[threadIdx.x], wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, wi, o);
+          if (lane_id() >= (unsigned)o) wi += y;
+        }
+        warp_sums[threadIdx.x] = wi - w;
+      }
+      __syncthreads();
+      const int excl = carry + warp_sums[threadIdx.x / 32] + incl - x;
+      if (i < nb) bcount[l * nb + i] = excl;
+      __syncthreads();
+      if (threadIdx.x == 1023) carry = excl + x;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) ctr[C_NS2 + l] = carry;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kCpBlock) k_cp_write(const int8_t* __restrict__ otype, int N,
+                                                       const int* __restrict__ boff, int* sad2,
+                                                       int* sad1, int* maxima, int* minima) {
+  __shared__ int wcnt[4][32];
+  const int v = blockIdx.x * kCpBlock + threadIdx.x;
+  const int b = v < N ? cp_bits(otype[v]) : 0;
+  const unsigned lt = (1u << lane_id()) - 1u;
+  unsigned m[4];
+  for (int l = 0; l < 4; ++l) {
+    m[l] = __ballot_sync(0xffffffffu, (b >> l) & 1);
+    if (lane_id() == 0) wcnt[l][threadIdx.x / 32] = __popc(m[l]);
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int l = 0; l < 4; ++l) {
+      const int w = wcnt[l][threadIdx.x];
+      int wi = w;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane_id() >= (unsigned)o) wi += y;
+      }
+      wcnt[l][threadIdx.x] = wi - w;
+    }
+  }
+  __syncthreads();
+  int* outs[4] = {sad2, sad1, maxima, minima};
+  for (int l = 0; l < 4; ++l) {
+    if ((b >> l) & 1) {
+      const int pos = boff[l * gridDim.x + blockIdx.x] + wcnt[l][threadIdx.x / 32] + __popc(m[l] & lt);
+      outs[l][pos] = v;
+    }
+  }
+}
+
+// ext[maxima[i]] = i and ext[minima[i]] = i (computeMaxIndex / computeMinIndex
+// :1928-1939 share one array).
+template <class T>
+__global__ void k_ext_index(Job<T> J) {
+  const int nmax = J.ctr[C_NMAX], nmin = J.ctr[C_NMIN];
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nmax + nmin; i += stride) {
+    if (i < nmax) J.ext[J.maxima[i]] = i;
+    else J.ext[J.minima[i - nmax]] = i - nmax;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Saddle rows: findAscPaths (:1832-1926) and findDescPaths (:1956-2049).
+// Row i belongs to the i-th ORIGINAL saddle for both fields.  Only [0, count)
+// and the count are written, so entries past a shorter row keep their last
+// value, as in the reference.
+// ---------------------------------------------------------------------------
+template <class T, bool kAsc>
+__global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
+                                              const int* __restrict__ lab, const int* __restrict__ sad,
+                                              int ns_slot, int* __restrict__ rows) {
+  const int ns = J.ctr[ns_slot];
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+    const int s = sad[i];
+    int ids[kNumDirs];
+    const int n = neighbours(s, J.dim, ids, nullptr);
+    const T sv = a[s];
+    int row[kNumDirs];
+    int cnt = 0;
+    for (int j = 0; j < n; ++j) {
+      const int r = ids[j];
+      const T rv = a[r];
+      if (kAsc) {
+        const int m = lab[r];
+        if (above(rv, r, sv, s) && tabs(T(a[m] - sv)) >= J.thr) row[cnt++] = m;
+      } else {
+        if (below(rv, r, sv, s)) row[cnt++] = lab[r];
+      }
+    }
+    // Insertion sort: descending (insertionSort :1795-1811) for ascending
+    // rows, ascending (reversed_insertionSort :1813-1829) for descending rows.
+    for (int p = 1; p < cnt; ++p) {
+      const int key = row[p];
+      const T kv = a[key];
+      int q = p - 1;
+      while (q >= 0) {
+        const int rq = row[q];
+        const bool move = kAsc ? below(a[rq], rq, kv, key) : above(a[rq], rq, kv, key);
+        if (!move) break;
+        row[q + 1] = rq;
+        --q;
+      }
+      row[q + 1] = key;
+    }
+    int* out = rows + (long long)i * kRowStride;
+    for (int p = 0; p < cnt; ++p) out[p] = row[p];
+    out[14] = cnt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Largest saddle per maximum / smallest per minimum on the ORIGINAL field
+// (findLargestSaddlePerMax / findSmallestSaddlePerMin :4890-4940): the CSR
+// max->saddle table is never materialised; every (row, entry) pair votes.
+// Pass 1 selects the extreme value key, pass 2 the extreme id at that value.
+// ---------------------------------------------------------------------------
+template <class T, bool kMax>
+__global__ void k_extreme_saddle(Job<T> J, int pass) {
+  using K = typename KeyOf<T>::K;
+  const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
+  const int* sad = kMax ? J.sad2 : J.sad1;
+  const int* rows = kMax ? J.orow2 : J.orow1;
+  const long long total = (long long)ns * kNumDirs;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += stride) {
+    const int i = (int)(e / kNumDirs), p = (int)(e % kNumDirs);
+    const int* row = rows + (long long)i * kRowStride;
+    if (p >= row[14]) continue;
+    const int m = J.ext[row[p]];
+    const int s = sad[i];
+    const K key = KeyOf<T>::enc(J.f[s] + T(0));  // -0 and +0 compare equal
+    if (pass == 0) {
+      if (kMax) atomicMax(J.ext_key + m, key);
+      else atomicMin(J.ext_key + m, key);
+    } else if (J.ext_key[m] == key) {
+      if (kMax) atomicMax(J.ext_id + m, s);
+      else atomicMin(J.ext_id + m, s);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Proposals and their application.
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ T midpoint_delta(const Job<T>& J, int i) {
+  const T gi = J.g[i];
+  return ((J.f[i] - J.bound) + gi) / T(2) - gi;
+}
+template <class T>
+__device__ __forceinline__ T step_delta(const Job<T>& J, int i) {
+  return J.edit_type == 1 ? midpoint_delta(J, i) : -J.bound / T(J.q);
+}
+
+// Atomic max into the proposal buffer (swap / swap1 / atomicCASDouble
+// :2643-2691).  The thread that lifts a vertex off the sentinel records it.
+template <class T>
+__device__ __forceinline__ void propose(const Job<T>& J, int i, T d) {
+  using K = typename KeyOf<T>::K;
+  const K k = KeyOf<T>::enc(d);
+  const K old = atomicMax(J.delta + i, k);
+  if (old == J.sentinel_key && k > old) {
+    const int slot = atomicAdd(J.ctr + C_TOUCHED, 1);
+    J.touched[slot] = i;
+  }
+}
+
+// c_loop(0..2) (:2887-3055) over the mismatch list.
+template <class T>
+__global__ void __launch_bounds__(256) k_propose_cp(Job<T> J) {
+  const int n = J.ctr[C_MM];
+  const int stride = gridDim.x * blockDim.x;
+  const Dims g = J.dim;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    const int ent = J.mm[e];
+    const int v = ent & ((1 << kCatShift) - 1);
+    const int cat = (unsigned)ent >> kCatShift;
+    int ids[kNumDirs], dirs[kNumDirs];
+    const int nn = neighbours(v, g, ids, dirs);
+    const int ot = J.otype[v];
+    const T gv = J.g[v];
+    if (cat & kCatMin) {  // c_loop(1) (:2965-3039)
+      if (ot != 0) {
+        int S = v;
+        T sval = J.f[v];
+        for (int j = 0; j < nn; ++j) {
+          const T nv = J.f[ids[j]];
+          if (below(nv, ids[j], sval, S)) { S = ids[j]; sval = nv; }
+        }
+        const T gs = J.g[S];
+        const T d = J.edit_type == 1 ? ((sval - J.bound) + gs) / T(2) - gs : -J.bound / T(J.q);
+        if (!(gv > gs || (gv == gs && v > S))) propose(J, S, d);
+      } else {
+        propose(J, v, step_delta(J, v));
+      }
+    }
+    if (cat & kCatSaddle) {  // c_loop(2) -> fix_saddle_local (:2804-2884)
+      int dm = 0;
+      for (int j = 0; j < nn; ++j) {
+        const T nv = J.g[ids[j]];
+        if (nv < gv || (nv == gv && ids[j] < v)) dm |= 1 << dirs[j];
+      }
+      const int om = J.olm[v];
+      for (int j = 0; j < nn; ++j)
+        if ((om >> dirs[j] & 1) && !(dm >> dirs[j] & 1)) propose(J, ids[j], step_delta(J, ids[j]));
+      if (dm & ~om) propose(J, v, step_delta(J, v));
+    }
+    if (cat & kCatMax) {  // c_loop(0) (:2890-2963)
+      if (ot != 4) {
+        propose(J, v, step_delta(J, v));
+      } else {
+        int L = v;
+        T lval = gv;
+        for (int j = 0; j < nn; ++j) {
+          const T nv = J.g[ids[j]];
+          if (above(nv, ids[j], lval, L)) { L = ids[j]; lval = nv; }
+        }
+        if (L != v) propose(J, L, step_delta(J, L));
+      }
+    }
+  }
+}
+
+// applyDeltaBuffer (:3061-3111) over the vertices that received a proposal;
+// the proposal buffer is reset to the sentinel on the way (init_delta).
+template <class T>
+__global__ void __launch_bounds__(256) k_apply(Job<T> J) {
+  const int n = J.ctr[C_TOUCHED];
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    const int v = J.touched[e];
+    const T d = KeyOf<T>::dec(J.delta[v]);
+    J.delta[v] = J.sentinel_key;
+    if (d == J.sentinel) continue;
+    const T fv = J.f[v];
+    T gv = J.g[v];
+    if (J.edit_type == 0) {
+      const int c = J.counter[v];
+      if (c < J.q - 1 && tabs(T(fv - (gv + d))) <= J.bound) {
+        gv += d;
+        J.counter[v] = c + 1;
+      } else {
+        J.counter[v] = J.q;
+        gv = fv - J.bound;
+      }
+    } else {
+      if (tabs(T(fv - (gv + d))) <= J.bound) gv += d;
+      else gv = fv - J.bound;
+    }
+    J.g[v] = gv;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wrong manifold neighbours (get_wrong_split_neighbors / get_wrong_join_neighbors
+// :2400-2513) in the canonical order "saddles in ascending id": saddle s flags
+// its first candidate neighbour not flagged by a smaller saddle.
+//
+// Candidates of s: valid neighbours r (direction order) with r above s in the
+// decompressed field and dds[r] != ds[r] (split), or below and das[r] != as[r]
+// (join).  Resolution runs in rounds: every unresolved saddle votes (atomic
+// max of (round << 32) | ~s) on each of its remaining candidates; a saddle
+// commits its first remaining candidate when its own vote won, i.e. no smaller
+// unresolved saddle can still take it.  The smallest unresolved saddle always
+// commits, and a larger one never takes what a smaller one could still take,
+// so the result equals the sequential greedy.
+// ---------------------------------------------------------------------------
+template <class T, bool kSplit>
+__device__ __forceinline__ int wn_candidates(const Job<T>& J, int s, int* ids) {
+  const int n = neighbours(s, J.dim, ids, nullptr);
+  const T sv = J.g[s];
+  int k = 0;
+  for (int j = 0; j < n; ++j) {
+    const int r = ids[j];
+    const T rv = J.g[r];
+    const bool side = kSplit ? above(rv, r, sv, s) : below(rv, r, sv, s);
+    const bool wrong = kSplit ? (J.dds[r] != J.ds[r]) : (J.das[r] != J.as[r]);
+    if (side && wrong) ids[k++] = r;
+  }
+  return k;
+}
+
+template <class T, bool kSplit>
+__global__ void __launch_bounds__(256) k_wn_seed(Job<T> J) {
+  const int ns = J.ctr[kSplit ? C_NS2 : C_NS1];
+  const int* sad = kSplit ? J.sad2 : J.sad1;
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < ns; base += stride) {
+    const int i = base + threadIdx.x;
+    bool has = false;
+    int s = 0;
+    if (i < ns) {
+      s = sad[i];
+      int ids[kNumDirs];
+      has = wn_candidates<T, kSplit>(J, s, ids) > 0;
+    }
+    const int slot = warp_append(J.ctr + C_CAND, has, 0xffffffffu);
+    if (slot >= 0) J.cand[slot] = s;
+  }
+}
+
+template <class T, bool kSplit>
+__global__ void __launch_bounds__(256) k_wn_vote(Job<T> J, unsigned long long round, int stamp) {
+  const int n = J.ctr[C_CAND];
+  const int* taken = kSplit ? J.taken : J.taken1;
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    const int s = J.cand[e];
+    int ids[kNumDirs];
+    const int k = wn_candidates<T, kSplit>(J, s, ids);
+    const unsigned long long vote = (round << 32) | (unsigned)(~s);
+    for (int j = 0; j < k; ++j)
+      if (taken[ids[j]] != stamp) atomicMax(J.claim + ids[j], vote);
+  }
+}
+
+template <class T, bool kSplit>
+__global__ void __launch_bounds__(256) k_wn_commit(Job<T> J, unsigned long long round, int stamp) {
+  const int n = J.ctr[C_CAND];
+  int* taken = kSplit ? J.taken : J.taken1;
+  int* flagged = kSplit ? J.flagged : J.flagged1;
+  int* nflag = J.ctr + (kSplit ? C_NFC : C_NFC1);
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    const int s = J.cand[e];
+    int ids[kNumDirs];
+    const int k = wn_candidates<T, kSplit>(J, s, ids);
+    int first = -1;
+    for (int j = 0; j < k; ++j)
+      if (taken[ids[j]] != stamp) { first = ids[j]; break; }
+    if (first < 0) continue;  // every candidate already flagged: resolved
+    const unsigned long long vote = (round << 32) | (unsigned)(~s);
+    if (J.claim[first] == vote) {
+      taken[first] = stamp;
+      flagged[atomicAdd(nflag, 1)] = first;
+    } else {
+      J.cand_next[atomicAdd(J.ctr + C_CAND_NEXT, 1)] = s;
+    }
+  }
+}
+
+// Sequential completion for whatever the bounded rounds left unresolved:
+// one thread takes the remaining saddles in ascending id.
+template <class T, bool kSplit>
+__global__ void k_wn_sequential(Job<T> J, int stamp) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int n = J.ctr[C_CAND];
+  int* taken = kSplit ? J.taken : J.taken1;
+  int* flagged = kSplit ? J.flagged : J.flagged1;
+  int* nflag = J.ctr + (kSplit ? C_NFC : C_NFC1);
+  while (n > 0) {
+    int bi = 0;
+    for (int e = 1; e < n; ++e)
+      if (J.cand[e] < J.cand[bi]) bi = e;
+    const int s = J.cand[bi];
+    J.cand[bi] = J.cand[n - 1];
+    --n;
+    int ids[kNumDirs];
+    const int k = wn_candidates<T, kSplit>(J, s, ids);
+    for (int j = 0; j < k; ++j)
+      if (taken[ids[j]] != stamp) {
+        taken[ids[j]] = stamp;
+        flagged[(*nflag)++] = ids[j];
+        break;
+      }
+  }
+  J.ctr[C_CAND] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// fixpath (:4046-4206): walk the steepest ascent (descent) of both fields from a
+// flagged vertex until they diverge; lower the decompressed choice (split) or
+// the original choice (join).
+// ---------------------------------------------------------------------------
+template <class T, bool kSplit>
+__global__ void __launch_bounds__(256) k_fixpath(Job<T> J) {
+  const int n = J.ctr[kSplit ? C_NFC : C_NFC1];
+  const int* list = kSplit ? J.flagged : J.flagged1;
+  const int stride = gridDim.x * blockDim.x;
+  const Dims g = J.dim;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    int cur = list[e];
+    int t = -1, fl = -1;
+    long long steps = 0;
+    for (; steps <= (long long)g.N; ++steps) {
+      int ids[kNumDirs];
+      const int nn = neighbours(cur, g, ids, nullptr);
+      int ni = cur, nd = cur;
+      T fi = J.f[cur], gd = J.g[cur];
+      for (int j = 0; j < nn; ++j) {
+        const int r = ids[j];
+        const T fr = J.f[r], gr = J.g[r];
+        if (kSplit) {
+          if (fi < fr || (fi == fr && ni < r)) { ni = r; fi = fr; }
+          if (gd < gr || (gd == gr && nd < r)) { nd = r; gd = gr; }
+        } else {
+          if (fi > fr || (fi == fr && ni > r)) { ni = r; fi = fr; }
+          if (gd > gr || (gd == gr && nd > r)) { nd = r; gd = gr; }
+        }
+      }
+      if (ni != nd) { t = ni; fl = nd; break; }
+      if (ni == cur) break;
+      cur = ni;
+    }
+    if (steps > (long long)g.N) atomicOr(J.ctr + C_ERROR, kErrPath);
+    if (fl == t) continue;
+    const int target = kSplit ? fl : t;
+    propose(J, target, step_delta(J, target));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// s_loops (:3465-3487) / s_loops_join (:3489-3512): get_wrong_index_max
+// (:3113-3141) and get_wrong_index_min (:3143-3171) with the lowest saddle row
+// winning per extremum, followed by the fixes (:3320-3413).
+// ---------------------------------------------------------------------------
+template <class T, bool kMax>
+__global__ void __launch_bounds__(256) k_wim_scan(Job<T> J) {
+  const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
+  const int* orow = kMax ? J.orow2 : J.orow1;
+  const int* drow = kMax ? J.drow2 : J.drow1;
+  int* first = kMax ? J.first1 : J.first_min1;
+  int* flag = kMax ? J.flag2 : J.flag_min2;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+    const int* o = orow + (long long)i * kRowStride;
+    const int* d = drow + (long long)i * kRowStride;
+    const int cnt = o[14];
+    if (cnt == 0) continue;
+    if (o[0] != d[0]) atomicMin(first + J.ext[o[0]], i);
+    const int k = cnt - 1;
+    if (o[k] != d[k]) flag[J.ext[o[k]]] = 1;
+  }
+}
+
+// Collect per extremum, count, propose the fix and reset the arbitration slots.
+// fix = false: detection only (the third block of the outer loop, :5932-5951).
+template <class T, bool kMax>
+__global__ void __launch_bounds__(256) k_wim_collect(Job<T> J, int fix) {
+  const int next = J.ctr[kMax ? C_NMAX : C_NMIN];
+  const int* ext_list = kMax ? J.maxima : J.minima;
+  const int* drow = kMax ? J.drow2 : J.drow1;
+  int* first = kMax ? J.first1 : J.first_min1;
+  int* flag = kMax ? J.flag2 : J.flag_min2;
+  int* c1 = J.ctr + (kMax ? C_WMC : C_WMIN);
+  int* c2 = J.ctr + (kMax ? C_WMC2 : C_WMIN2);
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < next; base += stride) {
+    const int m = base + threadIdx.x;
+    bool h1 = false, h2 = false;
+    if (m < next) {
+      const int row = first[m];
+      if (row != kInf) {
+        h1 = true;
+        first[m] = kInf;
+        if (fix) {
+          const int* d = drow + (long long)row * kRowStride;
+          // split: lower the false maximum d[0] (:3326-3344); join: lower the
+          // true minimum itself (:3375-3391).
+          const int target = kMax ? d[0] : ext_list[m];
+          propose(J, target, step_delta(J, target));
+        }
+      }
+      if (flag[m]) {
+        h2 = true;
+        flag[m] = 0;
+        if (fix) {
+          if (kMax) {
+            // lower the true maximum (:3346-3364)
+            propose(J, ext_list[m], step_delta(J, ext_list[m]));
+          }
+        }
+      }
+    }
+    const unsigned mask = 0xffffffffu;
+    const unsigned b1 = __ballot_sync(mask, h1), b2 = __ballot_sync(mask, h2);
+    if (lane_id() == 0) {
+      if (b1) atomicAdd(c1, __popc(b1));
+      if (b2) atomicAdd(c2, __popc(b2));
+    }
+  }
+}
+
+// get_wrong_index_min direction 1 (:3157-3168, fix :3393-3410) keeps the pair of
+// the lowest row per minimum and lowers the row's FALSE last entry, so it needs
+// the winning row: one more scan, arbitrating through first_sj as scratch.
+template <class T>
+__global__ void __launch_bounds__(256) k_wim_min2_scan(Job<T> J) {
+  const int ns = J.ctr[C_NS1];
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+    const int* o = J.orow1 + (long long)i * kRowStride;
+    const int* d = J.drow1 + (long long)i * kRowStride;
+    const int cnt = o[14];
+    if (cnt == 0) continue;
+    const int k = cnt - 1;
+    if (o[k] != d[k]) atomicMin(J.first_sj + J.ext[o[k]], i);
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(256) k_wim_min2_collect(Job<T> J) {
+  const int next = J.ctr[C_NMIN];
+  const int stride = gridDim.x * blockDim.x;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < next; m += stride) {
+    const int row = J.first_sj[m];
+    if (row == kInf) continue;
+    J.first_sj[m] = kInf;
+    const int* o = J.orow1 + (long long)row * kRowStride;
+    const int* d = J.drow1 + (long long)row * kRowStride;
+    const int target = d[o[14] - 1];
+    propose(J, target, step_delta(J, target));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// saddle_loops (:4229-4243) / saddle_loops_join (:4245-4261):
+// get_wrong_index_saddles(_join) (:3173-3270) -- the first saddle in an
+// extremum's CSR list (row order, then entry order) that outranks the true
+// largest (smallest) saddle in the decompressed field -- and
+// fix_wrong_index_saddle (:3415-3463).
+// ---------------------------------------------------------------------------
+template <class T, bool kMax>
+__global__ void __launch_bounds__(256) k_wis_scan(Job<T> J) {
+  const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
+  const int* sad = kMax ? J.sad2 : J.sad1;
+  const int* rows = kMax ? J.orow2 : J.orow1;
+  const int* best = kMax ? J.largest : J.smallest;
+  int* first = kMax ? J.first_s : J.first_sj;
+  const long long total = (long long)ns * kNumDirs;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += stride) {
+    const int i = (int)(e / kNumDirs), p = (int)(e % kNumDirs);
+    const int* row = rows + (long long)i * kRowStride;
+    if (p >= row[14]) continue;
+    const int m = J.ext[row[p]];
+    const int tb = best[m];
+    const int s = sad[i];
+    const T gs = J.g[s], gt = J.g[tb];
+    const bool wrong = kMax ? above(gs, s, gt, tb) : below(gs, s, gt, tb);
+    if (wrong) atomicMin(first + m, i * kRowStride + p);
+  }
+}
+
+template <class T, bool kMax>
+__global__ void __launch_bounds__(256) k_wis_collect(Job<T> J, int fix) {
+  const int next = J.ctr[kMax ? C_NMAX : C_NMIN];
+  const int* sad = kMax ? J.sad2 : J.sad1;
+  const int* best = kMax ? J.largest : J.smallest;
+  int* first = kMax ? J.first_s : J.first_sj;
+  int* cnt = J.ctr + (kMax ? C_WSC : C_WSCJ);
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < next; base += stride) {
+    const int m = base + threadIdx.x;
+    bool hit = false;
+    if (m < next && first[m] != kInf) {
+      hit = true;
+      const int s = sad[first[m] / kRowStride];
+      first[m] = kInf;
+      const int t = best[m];
+      if (fix) {
+        const T gt = J.g[t], gs = J.g[s];
+        if (kMax) {
+          if (!(gt > gs || (gt == gs && t > s))) propose(J, s, step_delta(J, s));
+        } else if (!(gt < gs || (gt == gs && t < s))) {
+          // store -bound/q, then (edit_type 1) atomic max with the midpoint:
+          // max(-bound/q, midpoint) whatever the interleaving (:3447-3458).
+          propose(J, t, -J.bound / T(J.q));
+          if (J.edit_type == 1) propose(J, t, midpoint_delta(J, t));
+        }
+      }
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, hit);
+    if (lane_id() == 0 && b) atomicAdd(cnt, __popc(b));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Small helpers.
+// ---------------------------------------------------------------------------
+template <class K>
+__global__ void k_fill(K* p, K v, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
+}
+
+}  // namespace extremz

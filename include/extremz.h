@@ -1,0 +1,147 @@
+/*
+ * extremz.h -- C ABI of the B200 ExtreM correction library (libextremz.so).
+ *
+ * The library corrects a lossy-decompressed scalar field so that its critical
+ * points and its ascending / descending manifold labels match the original,
+ * by lowering values within the absolute error bound.  It is the drop-in for
+ * the reference's correction call:
+ *   - the GPU correction driver, main() of src/ExtreM_cuda.cu:4954-6078
+ *     (classification, manifolds, c_loops / r_loops / s_loops / saddle_loops
+ *     and the outer loop), and
+ *   - the CPU correction sequence of main.cpp:65-446 over the host API
+ *     include/api/ExtreM.h:43-123 (getdata, classifyAllVertices,
+ *     ComputeDescendingManifold / ComputeAscendingManifold, c_loops, r_loops,
+ *     s_loops, saddle_loops).
+ * Buffers are caller-owned plain pointers; no C++ or torch types cross this
+ * boundary.  Every entry point returns a status code instead of exiting.
+ */
+#ifndef EXTREMZ_H
+#define EXTREMZ_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EXTREMZ_ABI_VERSION 1
+
+typedef enum {
+  EXTREMZ_OK = 0,
+  EXTREMZ_ROUND_CAP = 1,      /* a round cap was hit before zero mismatch */
+  EXTREMZ_BAD_ARG = 2,
+  EXTREMZ_OOM = 3,
+  EXTREMZ_CUDA_ERR = 4,
+  EXTREMZ_DEVICE_TIMEOUT = 5, /* a device-side iteration limit was hit */
+  EXTREMZ_NO_DEVICE = 6
+} extremz_status;
+
+typedef enum { EXTREMZ_F32 = 0, EXTREMZ_F64 = 1 } extremz_dtype;
+
+/*
+ * Correction parameters.  The reference takes them on the command line of
+ * src/ExtreM_cuda.cu (:4958-4963, :5015-5018) and hard-codes the rest:
+ *   bound      absolute error bound; the reference computes
+ *              (max - min) * er of the original field (:229-232)
+ *   thr        persistence filter of the ascending rows, sim * (max - min) (:231)
+ *   q          step divisor and edit-counter threshold (:4962, :5015)
+ *   edit_type  0: fixed step -bound/q gated by the edit counter;
+ *              1: midpoint step toward input - bound (:4963, :3061-3111)
+ *   max_outer, max_cloop_rounds
+ *              caps the reference does not have (its loops at :3961 and
+ *              :5603 are unbounded); hitting one returns EXTREMZ_ROUND_CAP
+ *   final_join run the unconditional saddle_loops_join after the loop (:5997)
+ *   preserve_join
+ *              preserve_join_tree of the reference (:4969, false there)
+ */
+typedef struct {
+  double bound;
+  double thr;
+  int q;
+  int edit_type;
+  int max_outer;
+  int max_cloop_rounds;
+  int final_join;
+  int preserve_join;
+  int flags;          /* EXTREMZ_FLAG_* */
+  int reserved[5];
+} extremz_params;
+
+/* flags: time every kernel launch with CUDA events, per kernel class, into
+ * extremz_report.prof_ms / prof_launches. */
+#define EXTREMZ_FLAG_PROFILE 1
+
+/* Kernel classes of extremz_report.prof_*: 0 setup classification, 1 fused
+ * classification + mismatch detection, 2 steepest directions, 3 pointer
+ * jumping, 4 proposals, 5 apply, 6 saddle rows, 7 wrong-neighbour resolution,
+ * 8 path walks, 9 everything else. */
+#define EXTREMZ_NUM_KCLASS 10
+
+/* Outcome of one correction. counters[] are the eleven host counters of the
+ * reference's loop test (:5603-5605) at exit: wrong split / join neighbours,
+ * false max / min / saddle counts, wrong_max(2), wrong saddle, wrong_min(2),
+ * wrong join saddle. */
+typedef struct {
+  int status;
+  int outer_iters;
+  int cloop_rounds;
+  int manifold_rounds;
+  int counters[11];
+  int error_bits;
+  long long kernel_launches;          /* kernels this call launched */
+  float prof_ms[EXTREMZ_NUM_KCLASS];  /* with EXTREMZ_FLAG_PROFILE */
+  int prof_launches[EXTREMZ_NUM_KCLASS];
+  int reserved[8];
+} extremz_report;
+
+typedef struct extremz_ctx_s extremz_ctx;
+
+/* ABI version of the loaded library (EXTREMZ_ABI_VERSION). */
+int extremz_version(void);
+
+/* Reference defaults: q = 4, edit_type = 1, thr = 0, final join on. */
+void extremz_default_params(extremz_params* p);
+
+/* A context owns the device workspace (grown on demand, reused across calls)
+ * for one device.  Calls on one context must not overlap. */
+extremz_status extremz_ctx_create(int device, extremz_ctx** out);
+void extremz_ctx_destroy(extremz_ctx* ctx);
+
+/*
+ * Correct d_decp in place.  d_orig and d_decp are device pointers to
+ * width*height*depth values of dtype (x fastest).  stream is a cudaStream_t
+ * (NULL = legacy default stream).  trace (host, optional) receives records of
+ * four int32 (phase, counter, counter, counter) for debugging; trace_cap is its
+ * length in int32.
+ * Replaces: main() of src/ExtreM_cuda.cu:5508-5997 (the correction proper, with
+ * input and decompressed field already resident on the device).
+ */
+extremz_status extremz_correct_device(extremz_ctx* ctx, const void* d_orig, void* d_decp,
+                                      int dtype, int width, int height, int depth,
+                                      const extremz_params* params, extremz_report* report,
+                                      void* stream, int32_t* trace, int trace_cap);
+
+/*
+ * Same with host buffers: copies both fields to the device, corrects, copies
+ * the corrected field back into h_decp.
+ * Replaces: the correction sequence of main.cpp:65-446 (host arrays in,
+ * corrected decp_data out, saved by saveArrayToBin at main.cpp:507).
+ */
+extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* h_decp,
+                                    int dtype, int width, int height, int depth,
+                                    const extremz_params* params, extremz_report* report,
+                                    void* stream);
+
+/* The critical-point lookup table in the layout of the reference's
+ * src/LUT.bin (24 800 int32, read by loadLUTToGPU, src/ExtreM_cuda.cu:244-260).
+ * Returns the number of entries written or -1. */
+int extremz_lut(int32_t* out, int n);
+
+const char* extremz_status_string(int status);
+const char* extremz_last_cuda_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EXTREMZ_H */

@@ -1,0 +1,1026 @@
+// ExtreM correction oracle -- TEST INFRASTRUCTURE ONLY.
+//
+// A single-threaded CPU restatement of the reference GPU correction
+// (src/ExtreM_cuda.cu, main() at :4954-6078 and the kernels it launches).  It
+// is the checker for this repository's CUDA path: only tests, the smoke check
+// and the CPU-baseline leg of bench.py load it.  The product never links it.
+//
+// Canonical order.  Three sites of the reference GPU path are racy; this
+// restatement resolves them sequentially, which the CUDA path reproduces:
+//   * ExtractCP (:1694-1741) appends with atomicAdd; here every CP list is in
+//     ascending vertex id, which fixes the triplet row order and the
+//     max->saddle CSR order (:4806-4888).
+//   * get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513) flag a
+//     neighbour with check-then-set; here saddles are visited in ascending id.
+//   * get_wrong_index_max / _min (:3113-3171) keep one (true, false) pair per
+//     extremum with check-then-set; here the lowest saddle row wins.
+// The stale read in get_wrong_index_max (:3128-3130: the decompressed row is
+// read at the ORIGINAL row's last position even when the decompressed row is
+// shorter) is reproduced by keeping decompressed rows persistent across
+// rounds, zero-initialised, and rewriting only [0, count) each time, exactly as
+// the reference's findAscPaths/findDescPaths do (:1892-1918, :2026-2047).
+//
+// Manifold labels are full roots for every vertex.  The reference jumps
+// descending labels only next to original 2-saddles (:1514-1557) but every
+// consumer reads labels only there, so consumed values are identical.
+//
+// Arithmetic follows the reference operation by operation in the field type T
+// (double as in the reference; float keeps data, bound and deltas in float as
+// the reference's float variant does, src/ExtreM_cuda_f.cu:124).  Build with
+// -ffp-contract=off so that no multiply-add is fused.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+// The 14 Freudenthal directions in the reference's order
+// (src/ExtreM_cuda.cu:155-162, src/ExtreM.cpp:16-21).  Star lists and LUT bit
+// positions follow this order.
+const int kDir[14][3] = {
+    {1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 0, 1},
+    {0, 0, -1}, {-1, 1, 0}, {1, -1, 0}, {0, 1, 1},  {0, -1, -1},
+    {-1, 0, 1}, {1, 0, -1}, {-1, 1, 1}, {1, -1, -1}};
+
+constexpr int kLutSize = 24800;
+constexpr int kNumKeys = 27;
+
+// ---------------------------------------------------------------------------
+// Lookup table (src/ExtreM_cuda.cu:263-467 calculateLUT, :3280-3318
+// generateLookupTable, :84-113 keys/lutOffsets, :5233-5266 representatives).
+// ---------------------------------------------------------------------------
+struct Lut {
+  int8_t table[kLutSize];
+  int key_mask[kNumKeys];
+  int offset[kNumKeys];
+  int16_t key_of_valid[1 << 14];  // valid-direction mask -> key index or -1
+};
+
+bool is_direction(int dx, int dy, int dz) {
+  for (int d = 0; d < 14; ++d)
+    if (kDir[d][0] == dx && kDir[d][1] == dy && kDir[d][2] == dz) return true;
+  return false;
+}
+
+int count_components(const std::vector<int>& nodes, const int adj[14][14]) {
+  int n = (int)nodes.size();
+  std::vector<int> seen(n, 0);
+  int comps = 0;
+  for (int s = 0; s < n; ++s) {
+    if (seen[s]) continue;
+    ++comps;
+    std::vector<int> stack{s};
+    seen[s] = 1;
+    while (!stack.empty()) {
+      int u = stack.back();
+      stack.pop_back();
+      for (int t = 0; t < n; ++t)
+        if (!seen[t] && adj[nodes[u]][nodes[t]]) {
+          seen[t] = 1;
+          stack.push_back(t);
+        }
+    }
+  }
+  return comps;
+}
+
+void build_lut(Lut& L) {
+  // Boundary classes: each axis is low (0), interior (1) or high (3) in a
+  // 4x4x4 grid.  Keys are grouped by neighbour count, then ordered by the
+  // representative vertex id -- the layout of the reference's LUT.bin.
+  struct Rep { int id, mask, count; };
+  std::vector<Rep> reps;
+  const int cls[3] = {0, 1, 3};
+  for (int cz : cls)
+    for (int cy : cls)
+      for (int cx : cls) {
+        int mask = 0;
+        for (int d = 0; d < 14; ++d) {
+          int nx = cx + kDir[d][0], ny = cy + kDir[d][1], nz = cz + kDir[d][2];
+          if (nx >= 0 && nx < 4 && ny >= 0 && ny < 4 && nz >= 0 && nz < 4) mask |= 1 << d;
+        }
+        reps.push_back({cx + 4 * cy + 16 * cz, mask, __builtin_popcount(mask)});
+      }
+  std::sort(reps.begin(), reps.end(), [](const Rep& a, const Rep& b) {
+    return a.count != b.count ? a.count < b.count : a.id < b.id;
+  });
+  int adj[14][14];
+  for (int a = 0; a < 14; ++a)
+    for (int b = 0; b < 14; ++b)
+      adj[a][b] = a != b && is_direction(kDir[b][0] - kDir[a][0], kDir[b][1] - kDir[a][1],
+                                         kDir[b][2] - kDir[a][2]);
+  for (int i = 0; i < (1 << 14); ++i) L.key_of_valid[i] = -1;
+  std::memset(L.table, 0, sizeof(L.table));
+  int off = 0;
+  for (int k = 0; k < kNumKeys; ++k) {
+    const Rep& r = reps[k];
+    L.key_mask[k] = r.mask;
+    L.offset[k] = off;
+    L.key_of_valid[r.mask] = (int16_t)k;
+    std::vector<int> valid;
+    for (int d = 0; d < 14; ++d)
+      if (r.mask >> d & 1) valid.push_back(d);
+    int n = (int)valid.size();
+    for (int cfg = 0; cfg < (1 << n); ++cfg) {
+      std::vector<int> lower, upper;
+      for (int j = 0; j < n; ++j) ((cfg >> j & 1) ? upper : lower).push_back(valid[j]);
+      int lc = count_components(lower, adj), uc = count_components(upper, adj);
+      int t = 0;  // lc == uc == 0 cannot occur (>= 4 valid neighbours)
+      if (lc == 0 && uc == 1) t = 0;
+      else if (lc == 1 && uc == 0) t = 4;
+      else if (lc == 1 && uc == 1) t = 5;
+      else if (lc > 1 && uc > 1) t = 3;
+      else if (lc > 1) t = 1;
+      else if (uc > 1) t = 2;
+      L.table[off + cfg] = (int8_t)t;
+    }
+    off += 1 << n;
+  }
+}
+
+const Lut& lut() {
+  static Lut* L = [] {
+    Lut* p = new Lut;
+    build_lut(*p);
+    return p;
+  }();
+  return *L;
+}
+
+// ---------------------------------------------------------------------------
+// Grid and total order.
+// ---------------------------------------------------------------------------
+struct Grid {
+  int W, H, D, N;
+  // Valid neighbours of v in direction order; returns the count.  dirs (if
+  // given) receives the direction index of each.
+  int nbrs(int v, int* out, int* dirs = nullptr) const {
+    int x = v % W, y = (v / W) % H, z = (v / (W * H)) % D;
+    int k = 0;
+    for (int d = 0; d < 14; ++d) {
+      int nx = x + kDir[d][0], ny = y + kDir[d][1], nz = z + kDir[d][2];
+      if (nx < 0 || nx >= W || ny < 0 || ny >= H || nz < 0 || nz >= D) continue;
+      if (dirs) dirs[k] = d;
+      out[k++] = nx + (ny + nz * H) * W;
+    }
+    return k;
+  }
+};
+
+// u above v in the total order (value, then id): islarger (:1779-1781).
+template <class T>
+inline bool above(const T* a, int u, int v) {
+  return a[u] > a[v] || (a[u] == a[v] && u > v);
+}
+// u below v: isless (:1787-1789).
+template <class T>
+inline bool below(const T* a, int u, int v) {
+  return a[u] < a[v] || (a[u] == a[v] && u < v);
+}
+
+// classifyVertex_CUDA (:3720-3911): type of v and its lower-star mask (bit d
+// set when the neighbour in direction d exists and is below v).
+template <class T>
+int classify(const T* a, const Grid& g, int v, uint16_t* lmask_out) {
+  const Lut& L = lut();
+  int x = v % g.W, y = (v / g.W) % g.H, z = (v / (g.W * g.H)) % g.D;
+  int valid = 0, lmask = 0, upbits = 0, k = 0, lower = 0, upper = 0;
+  T c = a[v];
+  for (int d = 0; d < 14; ++d) {
+    int nx = x + kDir[d][0], ny = y + kDir[d][1], nz = z + kDir[d][2];
+    if (nx < 0 || nx >= g.W || ny < 0 || ny >= g.H || nz < 0 || nz >= g.D) continue;
+    int r = nx + (ny + nz * g.H) * g.W;
+    T nv = a[r];
+    if (nv < c || (nv == c && r < v)) {
+      lmask |= 1 << d;
+      ++lower;
+    } else if (nv > c || (nv == c && r > v)) {
+      upbits |= 1 << k;
+      ++upper;
+    }
+    valid |= 1 << d;
+    ++k;
+  }
+  if (lmask_out) *lmask_out = (uint16_t)lmask;
+  if (upper == 0) return 4;
+  if (lower == 0) return 0;
+  int key = L.key_of_valid[valid];
+  if (key < 0) return -1;
+  return L.table[L.offset[key] + upbits];
+}
+
+// ComputeDirection + pointer jumping (:1464-1611): full roots of the steepest
+// ascent (ds) and descent (as) graphs.
+template <class T>
+void roots(const T* a, const Grid& g, int* ds, int* as) {
+  int nb[14];
+  for (int v = 0; v < g.N; ++v) {
+    int hi = v, lo = v;
+    int n = g.nbrs(v, nb);
+    for (int j = 0; j < n; ++j) {
+      int r = nb[j];
+      if (a[hi] < a[r] || (a[hi] == a[r] && hi < r)) hi = r;
+      if (a[lo] > a[r] || (a[lo] == a[r] && lo > r)) lo = r;
+    }
+    ds[v] = hi;
+    as[v] = lo;
+  }
+  for (int* m : {ds, as}) {
+    std::vector<int> path;
+    for (int v = 0; v < g.N; ++v) {
+      int u = v;
+      path.clear();
+      while (m[u] != u && m[m[u]] != m[u]) {
+        path.push_back(u);
+        u = m[u];
+      }
+      int root = m[u];
+      for (int p : path) m[p] = root;
+      m[v] = root;
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Parameters, report and trace (mirrored by tests/oracle_ffi.py).
+// ---------------------------------------------------------------------------
+extern "C" {
+struct oracle_params {
+  double bound;          // absolute error bound (cast to T)
+  double thr;            // persistence filter thr = sim * range (:231)
+  int q;                 // step divisor / counter threshold (:4962, :5015)
+  int edit_type;         // 0: fixed step with counter; 1: midpoint (:4963)
+  int max_outer;         // cap on outer iterations (the reference has none)
+  int max_cloop_rounds;  // cap on rounds of one c_loops call
+  int final_join;        // run the final saddle_loops_join (:5997)
+  int preserve_join;     // preserve_join_tree (:4969, false in the reference)
+};
+struct oracle_report {
+  int status;        // 0 ok, 1 round cap hit
+  int outer_iters;
+  int cloop_rounds;  // total c_loops correction rounds
+  int manifold_rounds;
+  long long edited;  // voxels whose value differs from the input decp
+  int counters[11];  // final host counters (order of the loop test :5603)
+};
+}
+
+namespace {
+
+enum Phase : int {
+  PH_CLOOP_DETECT = 1,  // counts: max, min, saddle
+  PH_WRONG_NBR = 2,     // nfc, nfc1
+  PH_SLOOPS = 3,        // wmc, wmc2
+  PH_SADDLE = 4,        // wsc
+  PH_DETECT3 = 5,       // wsc, wmc, wmc2
+  PH_SLOOPS_JOIN = 6,   // wmin, wmin2
+  PH_SADDLE_JOIN = 7,   // wscj
+  PH_OUTER = 8,         // 11 counters
+  PH_CHECKSUM = 9,      // running value checksum after a phase (lo, hi)
+};
+
+template <class T>
+struct Corrector {
+  Grid g;
+  const T* f;
+  T* a;  // decompressed field, corrected in place
+  T bound, thr;
+  int q, edit_type;
+  T sentinel;
+
+  std::vector<int8_t> otype;
+  std::vector<uint16_t> olmask;
+  std::vector<int> DS, AS, dDS, dAS;
+  std::vector<int> sad2, sad1, maxima, minima, ext_index;
+  // Rows of 14 labels + count.
+  std::vector<int> orow2, orow1, drow2, drow1;
+  std::vector<int> max_off, max_sad, min_off, min_sad;
+  std::vector<int> largest, smallest;
+
+  std::vector<T> delta;
+  std::vector<int> touched;
+  std::vector<int> counter;
+
+  std::vector<int> lmax, lmin, lsad;
+  std::vector<uint8_t> wn_ds, wn_as, wr_max, wr_max2, wr_min, wr_min2;
+  std::vector<int> wn_ds_list, wn_as_list;
+  std::vector<int> pmax1, pmax2, pmin1, pmin2, psad, psadj;
+
+  // Device-side counters of the reference (:133, :150-152).
+  int d_nfc = 0, d_nfc1 = 0, d_cfmax = 0, d_cfmin = 0, d_cfsad = 0;
+  int d_wmc = 0, d_wmc2 = 0, d_wsc = 0, d_wmin = 0, d_wmin2 = 0, d_wscj = 0;
+
+  int cloop_rounds = 0, manifold_rounds = 0, max_cloop_rounds = 0;
+  bool capped = false;
+  int* trace;
+  int trace_cap, trace_len = 0;
+
+  static constexpr int kRow = 15;  // 14 labels + count
+
+  void emit(int phase, int c0 = 0, int c1 = 0, int c2 = 0) {
+    if (!trace || trace_len + 4 > trace_cap) return;
+    trace[trace_len++] = phase;
+    trace[trace_len++] = c0;
+    trace[trace_len++] = c1;
+    trace[trace_len++] = c2;
+  }
+
+  void amax(int i, T d) {
+    if (delta[i] == sentinel) touched.push_back(i);
+    if (d > delta[i]) delta[i] = d;
+  }
+
+  T midpoint_delta(int i) const {  // e.g. :2906, :3334-3337, :3433
+    return ((f[i] - bound) + a[i]) / T(2) - a[i];
+  }
+  T step_delta(int i) const { return edit_type == 1 ? midpoint_delta(i) : -bound / T(q); }
+
+  void init_delta() {  // init_delta (:2569-2577), sparse form
+    for (int i : touched) delta[i] = sentinel;
+    touched.clear();
+  }
+
+  // applyDeltaBuffer (:3061-3111).
+  void apply() {
+    std::sort(touched.begin(), touched.end());
+    for (int i : touched) {
+      T d = delta[i];
+      if (d == sentinel) continue;
+      if (edit_type == 0) {
+        if (counter[i] < q - 1 && std::fabs(f[i] - (a[i] + d)) <= bound) {
+          a[i] += d;
+          counter[i] += 1;
+        } else {
+          counter[i] = q;
+          a[i] = f[i] - bound;
+        }
+      } else {
+        if (std::fabs(f[i] - (a[i] + d)) <= bound) a[i] += d;
+        else a[i] = f[i] - bound;
+      }
+    }
+  }
+
+  // classifyVertex_CUDA(type=1) fused detection (:3856-3910).
+  void detect() {
+    lmax.clear();
+    lmin.clear();
+    lsad.clear();
+    for (int v = 0; v < g.N; ++v) {
+      uint16_t lm;
+      int t = classify(a, g, v, &lm);
+      int o = otype[v];
+      if (t != o) {
+        if ((t == 4) != (o == 4)) lmax.push_back(v);
+        if ((t == 0) != (o == 0)) lmin.push_back(v);
+        if ((t == 2) != (o == 2) || (t == 1) != (o == 1) || (t == 3) != (o == 3))
+          lsad.push_back(v);
+      } else if (t == 1 || t == 2 || t == 3) {
+        if (lm != olmask[v]) lsad.push_back(v);  // areVectorsDifferent_local (:909-921)
+      }
+    }
+    d_cfmax = (int)lmax.size();
+    d_cfmin = (int)lmin.size();
+    d_cfsad = (int)lsad.size();
+    emit(PH_CLOOP_DETECT, d_cfmax, d_cfmin, d_cfsad);
+  }
+
+  // c_loop(0) (:2890-2963).
+  void propose_max(int v) {
+    if (otype[v] != 4) {
+      amax(v, step_delta(v));
+      return;
+    }
+    int nb[14];
+    int n = g.nbrs(v, nb);
+    int L = v;
+    for (int j = 0; j < n; ++j)
+      if (above(a, nb[j], L)) L = nb[j];
+    if (L == v) return;
+    amax(L, step_delta(L));
+  }
+
+  // c_loop(1) (:2965-3039).
+  void propose_min(int v) {
+    if (otype[v] != 0) {
+      int nb[14];
+      int n = g.nbrs(v, nb);
+      int S = v;
+      for (int j = 0; j < n; ++j)
+        if (below(f, nb[j], S)) S = nb[j];
+      T d = edit_type == 1 ? ((f[S] - bound) + a[S]) / T(2) - a[S] : -bound / T(q);
+      if (a[v] > a[S] || (a[v] == a[S] && v > S)) return;
+      amax(S, d);
+      return;
+    }
+    amax(v, step_delta(v));
+  }
+
+  // c_loop(2) -> fix_saddle_local (:2804-2884).
+  void propose_saddle(int v) {
+    int nb[14], dirs[14];
+    int n = g.nbrs(v, nb, dirs);
+    int dmask = 0;
+    for (int j = 0; j < n; ++j)
+      if (a[nb[j]] < a[v] || (a[nb[j]] == a[v] && nb[j] < v)) dmask |= 1 << dirs[j];
+    int om = olmask[v];
+    for (int j = 0; j < n; ++j)
+      if ((om >> dirs[j] & 1) && !(dmask >> dirs[j] & 1)) amax(nb[j], step_delta(nb[j]));
+    if (dmask & ~om) amax(v, step_delta(v));
+  }
+
+  // c_loops host driver (:3913-4044).
+  void c_loops() {
+    init_delta();
+    detect();
+    int rounds = 0;
+    while (!lmax.empty() || !lmin.empty() || !lsad.empty()) {
+      if (rounds >= max_cloop_rounds) {
+        capped = true;
+        return;
+      }
+      ++rounds;
+      ++cloop_rounds;
+      init_delta();
+      for (int v : lmin) propose_min(v);
+      for (int v : lsad) propose_saddle(v);
+      for (int v : lmax) propose_max(v);
+      apply();
+      detect();
+    }
+  }
+
+  // Row of a 2-saddle (findAscPaths :1832-1926) or 1-saddle (findDescPaths
+  // :1956-2049) into row[0..14].
+  void asc_row(const T* val, const int* dsm, int s, int* row) const {
+    int nb[14], cnt = 0;
+    int n = g.nbrs(s, nb);
+    T sv = val[s];
+    for (int j = 0; j < n; ++j) {
+      int r = nb[j];
+      int m = dsm[r];
+      if (above(val, r, s) && std::fabs(val[m] - sv) >= thr) row[cnt++] = m;
+    }
+    // insertionSort (:1795-1811): descending in the total order.
+    for (int i = 1; i < cnt; ++i) {
+      int key = row[i], j = i - 1;
+      while (j >= 0 && below(val, row[j], key)) {
+        row[j + 1] = row[j];
+        --j;
+      }
+      row[j + 1] = key;
+    }
+    row[14] = cnt;
+  }
+  void desc_row(const T* val, const int* asm_, int s, int* row) const {
+    int nb[14], cnt = 0;
+    int n = g.nbrs(s, nb);
+    for (int j = 0; j < n; ++j) {
+      int r = nb[j];
+      if (below(val, r, s)) row[cnt++] = asm_[r];
+    }
+    // reversed_insertionSort (:1813-1829): ascending.
+    for (int i = 1; i < cnt; ++i) {
+      int key = row[i], j = i - 1;
+      while (j >= 0 && above(val, row[j], key)) {
+        row[j + 1] = row[j];
+        --j;
+      }
+      row[j + 1] = key;
+    }
+    row[14] = cnt;
+  }
+
+  // Decompressed rows: only [0, count) and the count are rewritten.
+  void dec_rows() {
+    int tmp[kRow];
+    for (size_t i = 0; i < sad2.size(); ++i) {
+      asc_row(a, dDS.data(), sad2[i], tmp);
+      int* r = &drow2[i * kRow];
+      for (int k = 0; k < tmp[14]; ++k) r[k] = tmp[k];
+      r[14] = tmp[14];
+    }
+    for (size_t i = 0; i < sad1.size(); ++i) {
+      desc_row(a, dAS.data(), sad1[i], tmp);
+      int* r = &drow1[i * kRow];
+      for (int k = 0; k < tmp[14]; ++k) r[k] = tmp[k];
+      r[14] = tmp[14];
+    }
+  }
+
+  void manifolds() {
+    ++manifold_rounds;
+    roots(a, g, dDS.data(), dAS.data());
+    dec_rows();
+  }
+
+  // get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513), with
+  // saddles visited in ascending id.
+  void wrong_neighbors() {
+    for (int v : wn_ds_list) wn_ds[v] = 0;
+    for (int v : wn_as_list) wn_as[v] = 0;
+    wn_ds_list.clear();
+    wn_as_list.clear();
+    int nb[14];
+    for (int s : sad2) {
+      int n = g.nbrs(s, nb);
+      for (int j = 0; j < n; ++j) {
+        int r = nb[j];
+        if (above(a, r, s) && dDS[r] != DS[r] && !wn_ds[r]) {
+          wn_ds[r] = 1;
+          wn_ds_list.push_back(r);
+          break;
+        }
+      }
+    }
+    for (int s : sad1) {
+      int n = g.nbrs(s, nb);
+      for (int j = 0; j < n; ++j) {
+        int r = nb[j];
+        if (below(a, r, s) && dAS[r] != AS[r] && !wn_as[r]) {
+          wn_as[r] = 1;
+          wn_as_list.push_back(r);
+          break;
+        }
+      }
+    }
+    d_nfc = (int)wn_ds_list.size();
+    d_nfc1 = (int)wn_as_list.size();
+    emit(PH_WRONG_NBR, d_nfc, d_nfc1);
+  }
+
+  // fixpath (:4046-4206).
+  void fixpath(int start, int direction) {
+    int nb[14];
+    int cur = start, t = -1, fl = -1;
+    for (long long steps = 0; steps <= (long long)g.N; ++steps) {
+      int ni = cur, nd = cur;
+      int n = g.nbrs(cur, nb);
+      for (int j = 0; j < n; ++j) {
+        int r = nb[j];
+        if (direction == 0) {
+          if (f[ni] < f[r] || (f[ni] == f[r] && ni < r)) ni = r;
+          if (a[nd] < a[r] || (a[nd] == a[r] && nd < r)) nd = r;
+        } else {
+          if (f[ni] > f[r] || (f[ni] == f[r] && ni > r)) ni = r;
+          if (a[nd] > a[r] || (a[nd] == a[r] && nd > r)) nd = r;
+        }
+      }
+      if (ni != nd) {
+        t = ni;
+        fl = nd;
+        break;
+      }
+      if (ni == cur) break;
+      cur = ni;
+    }
+    if (fl == t) return;
+    int target = direction == 0 ? fl : t;
+    amax(target, step_delta(target));
+  }
+
+  // r_loops (:4210-4227).
+  void r_loops() {
+    init_delta();
+    for (int v : wn_ds_list) fixpath(v, 0);
+    for (int v : wn_as_list) fixpath(v, 1);
+    apply();
+  }
+
+  // get_wrong_index_max (:3113-3141).
+  void wrong_index_max() {
+    std::fill(wr_max.begin(), wr_max.end(), 0);
+    std::fill(wr_max2.begin(), wr_max2.end(), 0);
+    pmax1.clear();
+    pmax2.clear();
+    for (size_t i = 0; i < sad2.size(); ++i) {
+      const int* o = &orow2[i * kRow];
+      const int* d = &drow2[i * kRow];
+      if (o[14] == 0) continue;
+      if (o[0] != d[0] && !wr_max[o[0]]) {
+        wr_max[o[0]] = 1;
+        pmax1.push_back(o[0]);
+        pmax1.push_back(d[0]);
+      }
+      int k = o[14] - 1;
+      if (o[k] != d[k] && !wr_max2[o[k]]) {
+        wr_max2[o[k]] = 1;
+        pmax2.push_back(o[k]);
+        pmax2.push_back(d[k]);
+      }
+    }
+    d_wmc = (int)pmax1.size() / 2;
+    d_wmc2 = (int)pmax2.size() / 2;
+  }
+
+  // get_wrong_index_min (:3143-3171).
+  void wrong_index_min() {
+    std::fill(wr_min.begin(), wr_min.end(), 0);
+    std::fill(wr_min2.begin(), wr_min2.end(), 0);
+    pmin1.clear();
+    pmin2.clear();
+    for (size_t i = 0; i < sad1.size(); ++i) {
+      const int* o = &orow1[i * kRow];
+      const int* d = &drow1[i * kRow];
+      if (o[14] == 0) continue;
+      if (o[0] != d[0] && !wr_min[o[0]]) {
+        wr_min[o[0]] = 1;
+        pmin1.push_back(o[0]);
+        pmin1.push_back(d[0]);
+      }
+      int k = o[14] - 1;
+      if (o[k] != d[k] && !wr_min2[o[k]]) {
+        wr_min2[o[k]] = 1;
+        pmin2.push_back(o[k]);
+        pmin2.push_back(d[k]);
+      }
+    }
+    d_wmin = (int)pmin1.size() / 2;
+    d_wmin2 = (int)pmin2.size() / 2;
+  }
+
+  // s_loops (:3465-3487).
+  void s_loops() {
+    wrong_index_max();
+    init_delta();
+    for (size_t p = 0; p < pmax1.size(); p += 2) {
+      int fl = pmax1[p + 1];
+      amax(fl, step_delta(fl));  // fix_wrong_index_max(0) (:3326-3344)
+    }
+    for (size_t p = 0; p < pmax2.size(); p += 2) {
+      int t = pmax2[p];
+      amax(t, step_delta(t));  // fix_wrong_index_max(1) (:3346-3364)
+    }
+    apply();
+    emit(PH_SLOOPS, d_wmc, d_wmc2);
+  }
+
+  // s_loops_join (:3489-3512).
+  void s_loops_join() {
+    wrong_index_min();
+    init_delta();
+    for (size_t p = 0; p < pmin1.size(); p += 2) {
+      int t = pmin1[p];
+      amax(t, step_delta(t));  // fix_wrong_index_min(0) (:3375-3391)
+    }
+    for (size_t p = 0; p < pmin2.size(); p += 2) {
+      int fl = pmin2[p + 1];
+      amax(fl, step_delta(fl));  // fix_wrong_index_min(1) (:3393-3410)
+    }
+    apply();
+    emit(PH_SLOOPS_JOIN, d_wmin, d_wmin2);
+  }
+
+  // get_wrong_index_saddles (:3173-3218).
+  void wrong_index_saddles() {
+    psad.clear();
+    for (size_t m = 0; m < maxima.size(); ++m) {
+      int tl = largest[m];
+      for (int i = max_off[m]; i < max_off[m + 1]; ++i) {
+        int s = max_sad[i];
+        if (a[s] > a[tl] || (a[s] == a[tl] && s > tl)) {
+          psad.push_back(tl);
+          psad.push_back(s);
+          break;
+        }
+      }
+    }
+    d_wsc = (int)psad.size() / 2;
+  }
+
+  // get_wrong_index_saddles_join (:3220-3270).
+  void wrong_index_saddles_join() {
+    psadj.clear();
+    for (size_t m = 0; m < minima.size(); ++m) {
+      int ts = smallest[m];
+      for (int i = min_off[m]; i < min_off[m + 1]; ++i) {
+        int s = min_sad[i];
+        if (a[s] < a[ts] || (a[s] == a[ts] && s < ts)) {
+          psadj.push_back(ts);
+          psadj.push_back(s);
+          break;
+        }
+      }
+    }
+    d_wscj = (int)psadj.size() / 2;
+  }
+
+  // saddle_loops (:4229-4243).
+  void saddle_loops() {
+    wrong_index_saddles();
+    init_delta();
+    for (size_t p = 0; p < psad.size(); p += 2) {  // fix_wrong_index_saddle(0)
+      int t = psad[p], fl = psad[p + 1];
+      if (a[t] > a[fl] || (a[t] == a[fl] && t > fl)) continue;
+      amax(fl, step_delta(fl));
+    }
+    apply();
+    emit(PH_SADDLE, d_wsc);
+  }
+
+  // saddle_loops_join (:4245-4261).  fix_wrong_index_saddle(1) first stores
+  // -bound/q non-atomically, then (edit_type 1) takes the atomic max with the
+  // midpoint step (:3447-3458); the store-then-max sequence leaves
+  // max(-bound/q, midpoint) whatever the interleaving, since every pair that
+  // targets one vertex proposes the same midpoint.
+  void saddle_loops_join() {
+    wrong_index_saddles_join();
+    init_delta();
+    emit(PH_SADDLE_JOIN, d_wscj);
+    if (d_wscj > 0) {
+      for (size_t p = 0; p < psadj.size(); p += 2) {
+        int t = psadj[p], fl = psadj[p + 1];
+        if (a[t] < a[fl] || (a[t] == a[fl] && t < fl)) continue;
+        if (delta[t] == sentinel) touched.push_back(t);
+        T s = -bound / T(q);
+        delta[t] = s;
+        if (edit_type == 1) {
+          T d = midpoint_delta(t);
+          if (d > delta[t]) delta[t] = d;
+        }
+      }
+      apply();
+    }
+  }
+
+  void setup() {
+    int N = g.N;
+    otype.resize(N);
+    olmask.resize(N);
+    for (int v = 0; v < N; ++v) otype[v] = (int8_t)classify(f, g, v, &olmask[v]);
+    DS.resize(N);
+    AS.resize(N);
+    dDS.resize(N);
+    dAS.resize(N);
+    roots(f, g, DS.data(), AS.data());
+    ext_index.assign(N, 0);
+    for (int v = 0; v < N; ++v) {
+      int t = otype[v];
+      if (t == 2 || t == 3) sad2.push_back(v);
+      if (t == 1 || t == 3) sad1.push_back(v);
+      if (t == 4) maxima.push_back(v);
+      if (t == 0) minima.push_back(v);
+    }
+    // computeMaxIndex then computeMinIndex share one array (:1928-1939).
+    for (size_t i = 0; i < maxima.size(); ++i) ext_index[maxima[i]] = (int)i;
+    for (size_t i = 0; i < minima.size(); ++i) ext_index[minima[i]] = (int)i;
+    orow2.assign(sad2.size() * kRow, 0);
+    orow1.assign(sad1.size() * kRow, 0);
+    drow2.assign(sad2.size() * kRow, 0);
+    drow1.assign(sad1.size() * kRow, 0);
+    for (size_t i = 0; i < sad2.size(); ++i) asc_row(f, DS.data(), sad2[i], &orow2[i * kRow]);
+    for (size_t i = 0; i < sad1.size(); ++i) desc_row(f, AS.data(), sad1[i], &orow1[i * kRow]);
+    // computeMax_saddle_table / computeMin_saddle_table (:4806-4888).
+    auto csr = [&](const std::vector<int>& sad, const std::vector<int>& rows, size_t next,
+                   std::vector<int>& off, std::vector<int>& lst) {
+      std::vector<int> cnt(next + 1, 0);
+      for (size_t i = 0; i < sad.size(); ++i)
+        for (int p = 0; p < rows[i * kRow + 14]; ++p) cnt[ext_index[rows[i * kRow + p]] + 1]++;
+      off.assign(next + 1, 0);
+      for (size_t m = 0; m < next; ++m) off[m + 1] = off[m] + cnt[m + 1];
+      lst.assign(off[next], 0);
+      std::vector<int> fill(off.begin(), off.end() - 1);
+      for (size_t i = 0; i < sad.size(); ++i)
+        for (int p = 0; p < rows[i * kRow + 14]; ++p)
+          lst[fill[ext_index[rows[i * kRow + p]]]++] = sad[i];
+    };
+    csr(sad2, orow2, maxima.size(), max_off, max_sad);
+    csr(sad1, orow1, minima.size(), min_off, min_sad);
+    // findLargestSaddlePerMax / findSmallestSaddlePerMin (:4890-4940).
+    largest.assign(maxima.size(), -1);
+    for (size_t m = 0; m < maxima.size(); ++m) {
+      int best = -1;
+      for (int i = max_off[m]; i < max_off[m + 1]; ++i) {
+        int s = max_sad[i];
+        if (best < 0 || f[s] > f[best] || (f[s] == f[best] && s > best)) best = s;
+      }
+      largest[m] = best;
+    }
+    smallest.assign(minima.size(), -1);
+    for (size_t m = 0; m < minima.size(); ++m) {
+      int best = -1;
+      for (int i = min_off[m]; i < min_off[m + 1]; ++i) {
+        int s = min_sad[i];
+        if (best < 0 || f[s] < f[best] || (f[s] == f[best] && s < best)) best = s;
+      }
+      smallest[m] = best;
+    }
+    delta.assign(N, sentinel);
+    counter.assign(N, -1);
+    wn_ds.assign(N, 0);
+    wn_as.assign(N, 0);
+    wr_max.assign(N, 0);
+    wr_max2.assign(N, 0);
+    wr_min.assign(N, 0);
+    wr_min2.assign(N, 0);
+  }
+
+  // Order-independent value checksum (sum of mixed (bits, id) words), the same
+  // on the CPU and in the CUDA trace.
+  void checksum_emit() {
+    uint64_t acc = 0;
+    for (int v = 0; v < g.N; ++v) {
+      uint64_t bits = 0;
+      std::memcpy(&bits, &a[v], sizeof(T));
+      uint64_t z = bits + 0x9e3779b97f4a7c15ull * (uint64_t)(v + 1);
+      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+      z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+      acc += z ^ (z >> 31);
+    }
+    emit(PH_CHECKSUM, (int)(acc & 0x7fffffff), (int)((acc >> 31) & 0x7fffffff));
+  }
+
+  // One "manifold block" of the outer loop: manifolds, rows, wrong neighbours.
+  void manifold_block() {
+    manifolds();
+    wrong_neighbors();
+  }
+
+  // main() (:5508-5997), preserve_join_tree as configured.
+  int run(int max_outer, bool final_join, bool preserve_join, int* outer_out, int* counters) {
+    setup();
+    c_loops();
+    if (capped) return 1;
+    manifold_block();
+    int h_nfc = d_nfc, h_nfc1 = d_nfc1;
+    int h_wmc = 0, h_wmin = 0;
+    if (h_nfc == 0) {
+      s_loops();
+      h_wmc = d_wmc;
+      if (h_wmc == 0) saddle_loops();
+    }
+    if (h_nfc1 == 0 && preserve_join) {
+      s_loops_join();
+      h_wmin = d_wmin;
+      if (h_wmin == 0) saddle_loops_join();
+    }
+    h_nfc = d_nfc;
+    h_nfc1 = d_nfc1;
+    int h_cfmax = d_cfmax, h_cfmin = d_cfmin, h_cfsad = d_cfsad;
+    h_wmin = d_wmin;
+    h_wmc = d_wmc;
+    int h_wmin2 = d_wmin2, h_wmc2 = d_wmc2, h_wsc = d_wsc, h_wscj = d_wscj;
+    int outer = 0;
+    auto any = [&] {
+      return h_nfc > 0 || h_nfc1 > 0 || h_cfmax > 0 || h_cfmin > 0 || h_cfsad > 0 ||
+             h_wmc > 0 || h_wmc2 > 0 || h_wsc > 0 || h_wmin > 0 || h_wmin2 > 0 || h_wscj > 0;
+    };
+    while (any()) {
+      if (outer >= max_outer) {
+        capped = true;
+        break;
+      }
+      ++outer;
+      // Block 1 (:5622-5747).
+      c_loops();
+      if (capped) break;
+      r_loops();
+      manifold_block();
+      h_nfc = d_nfc;
+      h_nfc1 = d_nfc1;
+      if (h_nfc == 0) {
+        s_loops();
+        if (h_wmc == 0) saddle_loops();  // stale host copy (:5712)
+      }
+      if (h_nfc1 == 0 && preserve_join) {
+        s_loops_join();
+        h_wmin = d_wmin;
+        if (h_wmin == 0) saddle_loops_join();
+      }
+      // Block 2 (:5749-5870).
+      c_loops();
+      if (capped) break;
+      manifold_block();
+      h_nfc = d_nfc;
+      h_nfc1 = d_nfc1;
+      if (h_nfc == 0) {
+        s_loops();
+        h_wmc = d_wmc;
+        if (h_wmc == 0) saddle_loops();
+      }
+      if (h_nfc1 == 0 && preserve_join) {
+        s_loops_join();
+        h_wmin = d_wmin;
+        if (h_wmin == 0) saddle_loops_join();
+      }
+      // Block 3 (:5872-5979): detection only.
+      c_loops();
+      if (capped) break;
+      manifold_block();
+      h_nfc = d_nfc;
+      h_nfc1 = d_nfc1;
+      if (h_nfc == 0) {
+        wrong_index_max();
+        wrong_index_saddles();
+        h_wsc = d_wsc;
+        h_wmc = d_wmc;
+        h_wmc2 = d_wmc2;
+        emit(PH_DETECT3, h_wsc, h_wmc, h_wmc2);
+      }
+      if (h_nfc1 == 0 && preserve_join) {
+        wrong_index_min();
+        wrong_index_saddles_join();
+        h_wscj = d_wscj;
+        h_wmin2 = d_wmin2;
+        h_wmin = d_wmin;
+      }
+      detect();
+      h_cfmax = d_cfmax;
+      h_cfmin = d_cfmin;
+      h_cfsad = d_cfsad;
+      emit(PH_OUTER, outer);
+      checksum_emit();
+    }
+    if (!capped && final_join) saddle_loops_join();  // unconditional (:5997)
+    if (outer_out) *outer_out = outer;
+    if (counters) {
+      int c[11] = {h_nfc, h_nfc1, h_cfmax, h_cfmin, h_cfsad, h_wmc,
+                   h_wmc2, h_wsc, h_wmin, h_wmin2, h_wscj};
+      std::memcpy(counters, c, sizeof(c));
+    }
+    return capped ? 1 : 0;
+  }
+};
+
+template <class T>
+int correct_t(const T* f, T* a, int W, int H, int D, const oracle_params* p, oracle_report* rep,
+              int* trace, int trace_cap) {
+  Corrector<T> c;
+  c.g = {W, H, D, W * H * D};
+  c.f = f;
+  c.a = a;
+  c.bound = (T)p->bound;
+  c.thr = (T)p->thr;
+  c.q = p->q;
+  c.edit_type = p->edit_type;
+  c.sentinel = T(-4.0) * c.bound;  // init_delta (:2572)
+  c.max_cloop_rounds = p->max_cloop_rounds;
+  c.trace = trace;
+  c.trace_cap = trace_cap;
+  std::vector<T> a0(a, a + c.g.N);
+  int outer = 0;
+  int counters[11] = {0};
+  int st = c.run(p->max_outer, p->final_join != 0, p->preserve_join != 0, &outer, counters);
+  if (rep) {
+    rep->status = st;
+    rep->outer_iters = outer;
+    rep->cloop_rounds = c.cloop_rounds;
+    rep->manifold_rounds = c.manifold_rounds;
+    long long e = 0;
+    for (int v = 0; v < c.g.N; ++v) e += std::memcmp(&a0[v], &a[v], sizeof(T)) != 0;
+    rep->edited = e;
+    std::memcpy(rep->counters, counters, sizeof(counters));
+  }
+  return st;
+}
+
+bool dims_ok(int W, int H, int D) {
+  return W > 0 && H > 0 && D > 0 && (long long)W * H * D < (1ll << 31) / 16;
+}
+
+}  // namespace
+
+extern "C" {
+
+// LUT in the reference's LUT.bin layout (24 800 int32).
+int oracle_lut(int32_t* out, int n) {
+  if (n < kLutSize) return -1;
+  const Lut& L = lut();
+  for (int i = 0; i < kLutSize; ++i) out[i] = L.table[i];
+  return kLutSize;
+}
+
+// Per-vertex type and lower-star mask of a field.  dtype 0 = float32, 1 = float64.
+int oracle_classify(const void* f, int dtype, int W, int H, int D, int8_t* type, uint16_t* lmask) {
+  if (!dims_ok(W, H, D)) return -1;
+  Grid g{W, H, D, W * H * D};
+  for (int v = 0; v < g.N; ++v)
+    type[v] = (int8_t)(dtype == 0 ? classify((const float*)f, g, v, &lmask[v])
+                                  : classify((const double*)f, g, v, &lmask[v]));
+  return 0;
+}
+
+// Full steepest-ascent / steepest-descent roots of every vertex.
+int oracle_roots(const void* f, int dtype, int W, int H, int D, int32_t* ds, int32_t* as) {
+  if (!dims_ok(W, H, D)) return -1;
+  Grid g{W, H, D, W * H * D};
+  if (dtype == 0) roots((const float*)f, g, ds, as);
+  else roots((const double*)f, g, ds, as);
+  return 0;
+}
+
+// Full correction, in place on decp.  trace (optional) receives 4-int records.
+int oracle_correct(const void* f, void* decp, int dtype, int W, int H, int D,
+                   const oracle_params* p, oracle_report* rep, int32_t* trace, int trace_cap) {
+  if (!dims_ok(W, H, D) || !p || p->q <= 0) return -1;
+  if (dtype == 0)
+    return correct_t((const float*)f, (float*)decp, W, H, D, p, rep, trace, trace_cap);
+  return correct_t((const double*)f, (double*)decp, W, H, D, p, rep, trace, trace_cap);
+}
+
+}  // extern "C"

@@ -1,0 +1,126 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` use this module; the product path never imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+PHASES = {1: "cloop_detect", 2: "wrong_nbr", 3: "s_loops", 4: "saddle_loops",
+          5: "detect3", 6: "s_loops_join", 7: "saddle_loops_join", 8: "outer",
+          9: "checksum"}
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("bound", ctypes.c_double), ("thr", ctypes.c_double),
+                ("q", ctypes.c_int), ("edit_type", ctypes.c_int),
+                ("max_outer", ctypes.c_int), ("max_cloop_rounds", ctypes.c_int),
+                ("final_join", ctypes.c_int), ("preserve_join", ctypes.c_int)]
+
+
+class Report(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("outer_iters", ctypes.c_int),
+                ("cloop_rounds", ctypes.c_int), ("manifold_rounds", ctypes.c_int),
+                ("edited", ctypes.c_longlong), ("counters", ctypes.c_int * 11)]
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the Makefile next to this file."""
+    src = os.path.join(_HERE, "extremz_oracle.cpp")
+    if force or not os.path.exists(_LIB_PATH) or \
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", _HERE, "liboracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp, i32 = ctypes.c_void_p, ctypes.c_int
+        L.oracle_lut.argtypes = [vp, i32]
+        L.oracle_classify.argtypes = [vp, i32, i32, i32, i32, vp, vp]
+        L.oracle_roots.argtypes = [vp, i32, i32, i32, i32, vp, vp]
+        L.oracle_correct.argtypes = [vp, vp, i32, i32, i32, i32,
+                                     ctypes.POINTER(Params), ctypes.POINTER(Report), vp, i32]
+        _lib = L
+    return _lib
+
+
+def _dtype_code(a: np.ndarray) -> int:
+    if a.dtype == np.float32:
+        return 0
+    if a.dtype == np.float64:
+        return 1
+    raise TypeError(f"unsupported dtype {a.dtype}")
+
+
+def _dims(a: np.ndarray):
+    if a.ndim == 2:
+        return a.shape[1], a.shape[0], 1
+    d, h, w = a.shape
+    return w, h, d
+
+
+def lut() -> np.ndarray:
+    out = np.zeros(24800, dtype=np.int32)
+    n = lib().oracle_lut(out.ctypes.data, out.size)
+    assert n == 24800
+    return out
+
+
+def classify(f: np.ndarray):
+    f = np.ascontiguousarray(f)
+    w, h, d = _dims(f)
+    t = np.zeros(f.size, dtype=np.int8)
+    m = np.zeros(f.size, dtype=np.uint16)
+    rc = lib().oracle_classify(f.ctypes.data, _dtype_code(f), w, h, d, t.ctypes.data, m.ctypes.data)
+    assert rc == 0
+    return t, m
+
+
+def roots(f: np.ndarray):
+    f = np.ascontiguousarray(f)
+    w, h, d = _dims(f)
+    ds = np.zeros(f.size, dtype=np.int32)
+    a_s = np.zeros(f.size, dtype=np.int32)
+    rc = lib().oracle_roots(f.ctypes.data, _dtype_code(f), w, h, d, ds.ctypes.data, a_s.ctypes.data)
+    assert rc == 0
+    return ds, a_s
+
+
+def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, q: int = 4,
+            edit_type: int = 0, max_outer: int = 500, max_cloop_rounds: int = 100000,
+            final_join: bool = True, preserve_join: bool = False, trace_cap: int = 0):
+    """Run the oracle correction; returns (corrected copy, report dict, trace)."""
+    f = np.ascontiguousarray(f)
+    out = np.ascontiguousarray(decp).copy()
+    assert f.dtype == out.dtype and f.shape == out.shape
+    w, h, d = _dims(f)
+    p = Params(bound, thr, q, edit_type, max_outer, max_cloop_rounds,
+               int(final_join), int(preserve_join))
+    r = Report()
+    tr = np.zeros(max(trace_cap, 1) * 4, dtype=np.int32)
+    rc = lib().oracle_correct(f.ctypes.data, out.ctypes.data, _dtype_code(f), w, h, d,
+                              ctypes.byref(p), ctypes.byref(r), tr.ctypes.data, trace_cap * 4)
+    if rc < 0:
+        raise ValueError("oracle rejected the arguments")
+    rep = dict(status=r.status, outer_iters=r.outer_iters, cloop_rounds=r.cloop_rounds,
+               manifold_rounds=r.manifold_rounds, edited=int(r.edited),
+               counters=list(r.counters))
+    trace = tr.reshape(-1, 4)
+    if trace_cap:
+        trace = trace[trace[:, 0] != 0]
+    return out, rep, trace

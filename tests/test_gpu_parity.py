@@ -1,0 +1,94 @@
+"""CUDA path against the oracle: bit-exact corrected fields and equal traces.
+
+Every comparison is exact (byte equality of the corrected field); the trace
+records the per-phase counters (mismatch counts, wrong neighbours, wrong
+extremum / saddle pairs) and a checksum of the field after each outer
+iteration, so a divergence is located to the phase where it starts.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from extrem_z_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = np.load(os.path.join(HERE, "golden", "oracle_cases.npz"))
+CASES = sorted({k.split("/")[0] for k in GOLDEN.files})
+KW = dict(q=4, max_outer=500, max_cloop_rounds=100000, final_join=True)
+
+
+def gpu_correct(f, decp, eb, trace_cap=200000, **kw):
+    import torch
+    from extrem_z_b200 import api
+    tf = torch.from_numpy(np.ascontiguousarray(f)).cuda()
+    tg = torch.from_numpy(np.ascontiguousarray(decp)).cuda()
+    rep, trace = api.context(0).correct_device(tf, tg, eb, trace_cap=trace_cap, **kw)
+    torch.cuda.synchronize()
+    return tg.cpu().numpy(), rep, trace
+
+
+def first_divergence(a, b):
+    n = min(len(a), len(b))
+    for i in range(n):
+        if not np.array_equal(a[i], b[i]):
+            return i, a[i].tolist(), b[i].tolist()
+    return n, None, None
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_golden_cases_bit_exact(name):
+    f, decp = GOLDEN[f"{name}/f"], GOLDEN[f"{name}/decp"]
+    eb, et = GOLDEN[f"{name}/meta"][:2]
+    out, rep, trace = gpu_correct(f, decp, eb, edit_type=int(et), **KW)
+    ref_trace = GOLDEN[f"{name}/trace"]
+    assert np.array_equal(trace, ref_trace), first_divergence(trace, ref_trace)
+    assert np.array_equal(out.view(np.uint8), GOLDEN[f"{name}/fixed"].view(np.uint8))
+    assert rep.status == 0 and rep.error_bits == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("edit_type", [1, 0])
+def test_plain_64_bit_exact(dtype, edit_type):
+    from oracle import ffi
+    fld = synth.plain_64(dtype)
+    ref, rrep, rtrace = ffi.correct(fld.f, fld.decp, fld.eb, edit_type=edit_type,
+                                    trace_cap=400000, **KW)
+    out, rep, trace = gpu_correct(fld.f, fld.decp, fld.eb, trace_cap=400000,
+                                  edit_type=edit_type, **KW)
+    assert np.array_equal(trace, rtrace), first_divergence(trace, rtrace)
+    assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+    assert rep.status == rrep["status"] == 0
+    assert rep.counters == rrep["counters"] == [0] * 11
+
+
+@pytest.mark.parametrize("seed", [3, 17])
+def test_uneven_shapes_bit_exact(seed):
+    from oracle import ffi
+    rng = np.random.default_rng(seed)
+    w, h, d = (int(x) for x in rng.integers(5, 40, size=3))
+    dt = np.float32 if seed % 2 else np.float64
+    fld = synth.make_field(w, h, d, n_gauss=12, seed=seed, rel=3e-3, dtype=dt)
+    ref, rrep, rtrace = ffi.correct(fld.f, fld.decp, fld.eb, trace_cap=200000, **KW)
+    out, rep, trace = gpu_correct(fld.f, fld.decp, fld.eb, **KW)
+    assert np.array_equal(trace, rtrace), first_divergence(trace, rtrace)
+    assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+
+
+def test_host_entry_point_equals_device_entry_point():
+    from extrem_z_b200 import api
+    fld = synth.make_field(33, 17, 9, n_gauss=8, seed=8, rel=2e-3)
+    dev, _, _ = gpu_correct(fld.f, fld.decp, fld.eb, trace_cap=0, **KW)
+    host, rep = api.correct(fld.f, fld.decp, fld.eb, **KW)
+    assert np.array_equal(dev.view(np.uint8), host.view(np.uint8))
+    assert rep.status == 0
+
+
+def test_repeated_calls_on_one_context_are_identical():
+    fld = synth.make_field(20, 20, 20, n_gauss=10, seed=4, rel=1e-3)
+    a, _, _ = gpu_correct(fld.f, fld.decp, fld.eb, **KW)
+    b, _, _ = gpu_correct(fld.f, fld.decp, fld.eb, **KW)
+    assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
