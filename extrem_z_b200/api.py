@@ -56,6 +56,8 @@ class Report(ctypes.Structure):
                 ("reserved", ctypes.c_int * 8)]
 
 FLAG_PROFILE = 1
+FLAG_NO_TMA = 2
+PROFILE_CLASS_SHIFT = 8
 KCLASS_NAMES = ("setup_classify", "classify_detect", "direction", "jump", "propose", "apply",
                 "rows", "wrong_nbr", "fixpath", "other")
 
@@ -138,13 +140,20 @@ def _check(st: int, allow_cap: bool = True):
 def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 1,
                 max_outer: int = 1000, max_cloop_rounds: int = 100000,
                 final_join: bool = True, preserve_join: bool = False,
-                profile: bool = False) -> Params:
+                profile=False, tma: bool = True) -> Params:
+    """profile: False, True (time every kernel class) or an iterable of class
+    names from KCLASS_NAMES to time only those."""
     p = Params()
     load().extremz_default_params(ctypes.byref(p))
     p.bound, p.thr, p.q, p.edit_type = float(bound), float(thr), int(q), int(edit_type)
     p.max_outer, p.max_cloop_rounds = int(max_outer), int(max_cloop_rounds)
     p.final_join, p.preserve_join = int(bool(final_join)), int(bool(preserve_join))
-    p.flags = FLAG_PROFILE if profile else 0
+    p.flags = 0 if tma else FLAG_NO_TMA
+    if profile:
+        p.flags |= FLAG_PROFILE
+        if profile is not True:
+            for name in profile:
+                p.flags |= 1 << (PROFILE_CLASS_SHIFT + KCLASS_NAMES.index(name))
     return p
 
 

@@ -8,6 +8,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace extremz {
@@ -36,6 +37,21 @@ __host__ __device__ constexpr int dir_z(int d) {
 // an index tie-break "r < v" is "d is odd".
 __host__ __device__ constexpr bool dir_neighbour_is_before(int d) { return (d & 1) != 0; }
 
+// Neighbour ids in ascending order, by rank j = 0..13: the centre falls
+// between ranks 6 and 7.  Among the valid neighbours of any vertex the offsets
+// dx + dy*W + dz*W*H are distinct and ordered as (dz, dy, dx) lexicographically
+// (the ones that would tie are never valid together), so comparing ids of
+// neighbours is comparing these static ranks.
+__host__ __device__ constexpr int rank_dir(int j) {
+  return j == 0 ? 9 : j == 1 ? 13 : j == 2 ? 5 : j == 3 ? 11 : j == 4 ? 3 : j == 5 ? 7
+       : j == 6 ? 1 : j == 7 ? 0 : j == 8 ? 6 : j == 9 ? 2 : j == 10 ? 10 : j == 11 ? 4
+       : j == 12 ? 12 : 8;
+}
+constexpr int kRankCentre = 7;  // the centre comes before rank_dir(7)
+
+// Bit mask of the valid directions for boundary code bc (0x3fff inside).
+__host__ __device__ __forceinline__ int valid_mask(int bc);
+
 // Device tables: LUT entries (int8), key index / LUT offset per boundary code.
 struct DeviceTables {
   const int8_t* lut;      // 24 800 entries, the reference's LUT.bin layout
@@ -59,6 +75,55 @@ __host__ __device__ __forceinline__ bool dir_valid(int d, int bc) {
   if (dz < 0 && (bc & 16)) return false;
   if (dz > 0 && (bc & 32)) return false;
   return true;
+}
+
+__host__ __device__ __forceinline__ int valid_mask(int bc) {
+  if (bc == 0) return (1 << kNumDirs) - 1;
+  int m = 0;
+#pragma unroll
+  for (int d = 0; d < kNumDirs; ++d) m |= dir_valid(d, bc) << d;
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// TMA (bulk tensor copy) with an mbarrier, for halo tiles.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
+               : "memory");
+}
+// Bounded wait for phase `parity`; returns false when the limit is reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long long limit) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  for (long long it = 0; it < limit; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// 3-D tiled bulk copy global -> shared.  x must be a multiple of 16 bytes
+// (callers start boxes 4 elements left of a 32-aligned tile origin).
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(d),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(b)
+      : "memory");
 }
 
 // ---------------------------------------------------------------------------

@@ -6,6 +6,8 @@
 // grid-stride loop over a device-resident count, so no launch shape depends on
 // a host copy of a counter; the host reads the counter block only where the
 // reference's control flow branches on it.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -78,6 +80,44 @@ const HostTables& host_tables() {
 }
 
 // ---------------------------------------------------------------------------
+// Tensor maps for the TMA halo tiles.  The encoder comes from the driver
+// through the runtime, so the library does not link libcuda directly.
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }();
+  return fn;
+}
+
+// A 3-D map of the field with the halo-tile box; false when TMA cannot be
+// used (base not 16-byte aligned, or a row stride that is not a multiple of
+// 16 bytes), in which case the kernels load tiles with plain loads.
+template <class T>
+static bool make_tile_map(CUtensorMap* m, const T* ptr, const Dims& g) {
+  std::memset(m, 0, sizeof(*m));
+  if ((reinterpret_cast<uintptr_t>(ptr) & 15) || ((size_t)g.W * sizeof(T)) % 16) return false;
+  auto fn = tensor_map_encoder();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)g.W, (cuuint64_t)g.H, (cuuint64_t)g.D};
+  cuuint64_t strides[2] = {(cuuint64_t)g.W * sizeof(T), (cuuint64_t)g.W * g.H * sizeof(T)};
+  cuuint32_t box[3] = {(cuuint32_t)SX, (cuuint32_t)SY, (cuuint32_t)SZ};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                  3, const_cast<T*>(ptr), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
 // Workspace: one device arena per context, grown on demand.
 // ---------------------------------------------------------------------------
 struct Arena {
@@ -109,11 +149,13 @@ struct Arena {
 struct Context {
   int device = 0;
   Arena arena;
+  Arena stage;           // device copies of host fields (extremz_correct_host)
   int* h_ctr = nullptr;  // pinned copy of the counter block
   unsigned long long wn_round = 0;
   int wn_stamp = 0;
   ~Context() {
     if (arena.base) cudaFree(arena.base);
+    if (stage.base) cudaFree(stage.base);
     if (h_ctr) cudaFreeHost(h_ctr);
   }
 };
@@ -166,6 +208,10 @@ class Corrector {
     J.q = p.q;
     J.edit_type = p.edit_type;
     profile_ = (p.flags & EXTREMZ_FLAG_PROFILE) != 0;
+    const bool tma_ok = (p.flags & EXTREMZ_FLAG_NO_TMA) == 0;
+    tma_f_ = tma_ok && make_tile_map(&map_f_, f, J.dim);
+    tma_g_ = tma_ok && make_tile_map(&map_g_, (const T*)g, J.dim);
+    profile_mask_ = (p.flags >> EXTREMZ_PROFILE_CLASS_SHIFT) & ((1 << K_NUM) - 1);
   }
 
   int run(extremz_report* rep) {
@@ -198,8 +244,22 @@ class Corrector {
   int hc_[11] = {0};
   int* ctr_ = nullptr;
 
+  CUtensorMap map_f_, map_g_;
+  bool tma_f_ = false, tma_g_ = false;
+
+  template <bool kDetect>
+  void launch_classify(int cls, const T* a, bool tma, const CUtensorMap& m) {
+    if (tma) launch(cls, k_classify<T, kDetect, true>, tile_grid(), 256, J, m, a);
+    else launch(cls, k_classify<T, kDetect, false>, tile_grid(), 256, J, m, a);
+  }
+  void launch_direction(const T* a, bool tma, const CUtensorMap& m, int* ds, int* as) {
+    if (tma) launch(K_DIRECTION, k_direction<T, true>, tile_grid(), 256, J, m, a, ds, as);
+    else launch(K_DIRECTION, k_direction<T, false>, tile_grid(), 256, J, m, a, ds, as);
+  }
+
   long long launches_ = 0;
   bool profile_ = false;
+  int profile_mask_ = 0;
   struct Rec { int cls; cudaEvent_t a, b; };
   std::vector<Rec> recs_;
   std::vector<cudaEvent_t> pool_;
@@ -220,14 +280,15 @@ class Corrector {
   template <class... KArgs, class... Args>
   void launch(int cls, void (*kern)(KArgs...), dim3 grid, dim3 block, Args... args) {
     cudaEvent_t a = nullptr, b = nullptr;
-    if (profile_) {
+    const bool timed = profile_ && (profile_mask_ == 0 || (profile_mask_ >> cls & 1));
+    if (timed) {
       a = event();
       b = event();
       cudaEventRecord(a, st_);
     }
     kern<<<grid, block, 0, st_>>>(args...);
     ++launches_;
-    if (profile_) {
+    if (timed) {
       cudaEventRecord(b, st_);
       recs_.push_back({cls, a, b});
     }
@@ -307,12 +368,13 @@ class Corrector {
       add(N, 1); add(N, 2); add(N, 1);         // otype, olm, gate
       for (int i = 0; i < 5; ++i) add(N, 4);   // ds, as, dds, das, ext
       add(N, sizeof(K)); add(N, 4); add(N, 4); add(N, 4);  // delta, counter, touched, mm
+      add(N, 4); add(N, 1); add(N, 4); add(N, 4); add(N, 4);  // mm_next, mstat, dirty, dstamp, rstamp
       add(N, 8); add(N, 4); add(N, 4);         // claim, taken, taken1
       for (int i = 0; i < 4; ++i) add(N, 4);   // cand, cand_next, flagged, flagged1
       add(4ll * nb, 4);                        // cp block counts
       add(ns2, 4); add(ns1, 4); add(nmax, 4); add(nmin, 4);
-      add(ns2 * kRowStride, 4); add(ns2 * kRowStride, 4);
-      add(ns1 * kRowStride, 4); add(ns1 * kRowStride, 4);
+      add(ns2 * kRowStride, 4); add(ns2 * 2, 4);
+      add(ns1 * kRowStride, 4); add(ns1 * 2, 4);
       for (int i = 0; i < 4; ++i) add(nmax, 4);  // largest, first1, flag2, first_s
       for (int i = 0; i < 4; ++i) add(nmin, 4);  // smallest, first_min1, flag_min2, first_sj
       long long ne = std::max(nmax, nmin);
@@ -338,6 +400,11 @@ class Corrector {
     J.counter = A.take<int>(N);
     J.touched = A.take<int>(N);
     J.mm = A.take<int>(N);
+    J.mm_next = A.take<int>(N);
+    J.mstat = A.take<uint8_t>(N);
+    J.dirty = A.take<int>(N);
+    J.dstamp = A.take<int>(N);
+    J.rstamp = A.take<int>(N);
     J.claim = A.take<unsigned long long>(N);
     J.taken = A.take<int>(N); J.taken1 = A.take<int>(N);
     J.cand = A.take<int>(N); J.cand_next = A.take<int>(N);
@@ -346,9 +413,9 @@ class Corrector {
     EZ_CHECK(cudaMemsetAsync(ctr_, 0, C_COUNT * sizeof(int), st_));
 
     // Original classification, gates and manifolds.
-    launch(K_SETUP, k_classify<T, false>, tile_grid(), 256, J, J.f);
+    launch_classify<false>(K_SETUP, J.f, tma_f_, map_f_);
     launch(K_OTHER, k_gate<T>, grid_, 256, J);
-    launch(K_DIRECTION, k_direction<T>, tile_grid(), 256, J, J.f, J.ds, J.as);
+    launch_direction(J.f, tma_f_, map_f_, J.ds, J.as);
     launch(K_JUMP, k_jump, grid_, 256, J.ds, J.gate, 1, N, N, ctr_ + C_ERROR);
     launch(K_JUMP, k_jump, grid_, 256, J.as, J.gate, 2, N, N, ctr_ + C_ERROR);
     EZ_RUN(launched());
@@ -361,9 +428,9 @@ class Corrector {
     J.sad2 = A.take<int>(ns2); J.sad1 = A.take<int>(ns1);
     J.maxima = A.take<int>(nmax); J.minima = A.take<int>(nmin);
     J.orow2 = A.take<int>((long long)ns2 * kRowStride);
-    J.drow2 = A.take<int>((long long)ns2 * kRowStride);
+    J.drow2 = A.take<int>((long long)ns2 * 2);
     J.orow1 = A.take<int>((long long)ns1 * kRowStride);
-    J.drow1 = A.take<int>((long long)ns1 * kRowStride);
+    J.drow1 = A.take<int>((long long)ns1 * 2);
     J.largest = A.take<int>(nmax); J.first1 = A.take<int>(nmax);
     J.flag2 = A.take<int>(nmax); J.first_s = A.take<int>(nmax);
     J.smallest = A.take<int>(nmin); J.first_min1 = A.take<int>(nmin);
@@ -377,8 +444,10 @@ class Corrector {
     launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.f, J.ds, J.sad2, C_NS2, J.orow2);
     launch(K_ROWS, k_rows<T, false>, grid_, 256, J, J.f, J.as, J.sad1, C_NS1, J.orow1);
     EZ_RUN(launched());
-    if (ns2) EZ_CHECK(cudaMemsetAsync(J.drow2, 0, (size_t)ns2 * kRowStride * 4, st_));
-    if (ns1) EZ_CHECK(cudaMemsetAsync(J.drow1, 0, (size_t)ns1 * kRowStride * 4, st_));
+    // Decompressed row slots start at zero: the reference's rows are fresh
+    // cudaMalloc memory read before first written (:5338-5341, :3128-3130).
+    if (ns2) EZ_CHECK(cudaMemsetAsync(J.drow2, 0, (size_t)ns2 * 2 * 4, st_));
+    if (ns1) EZ_CHECK(cudaMemsetAsync(J.drow1, 0, (size_t)ns1 * 2 * 4, st_));
     // Largest saddle per maximum, smallest per minimum (original field).
     if (nmax) {
       launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, K(0), nmax);
@@ -406,9 +475,14 @@ class Corrector {
     EZ_CHECK(cudaMemsetAsync(J.claim, 0, (size_t)N * 8, st_));
     EZ_CHECK(cudaMemsetAsync(J.taken, 0, (size_t)N * 4, st_));
     EZ_CHECK(cudaMemsetAsync(J.taken1, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.dstamp, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.rstamp, 0, (size_t)N * 4, st_));
     EZ_RUN(launched());
     return EXTREMZ_OK;
   }
+
+  int dirty_epoch_ = 1, detect_epoch_ = 0;
+  bool dense_done_ = false;
 
   unsigned long long* checksum_ = nullptr;
 
@@ -424,9 +498,24 @@ class Corrector {
   }
 
   // ------------------------------------------------------------- c_loops --
+  // Mismatch detection: dense the first time, then incremental over the
+  // neighbourhoods of the vertices changed since the previous detection.
   int detect() {
-    EZ_RUN(zero(C_MM, 4));
-    launch(K_DETECT, k_classify<T, true>, tile_grid(), 256, J, J.g);
+    if (!dense_done_) {
+      EZ_RUN(zero(C_MM, 4));
+      launch_classify<true>(K_DETECT, J.g, tma_g_, map_g_);
+      dense_done_ = true;
+    } else {
+      ++detect_epoch_;
+      EZ_RUN(zero(C_MM_NEXT));
+      EZ_RUN(zero(C_CMAX, 3));
+      launch(K_DETECT, k_redetect<T>, grid_, 256, J, detect_epoch_);
+      launch(K_DETECT, k_keep<T>, grid_, 256, J, detect_epoch_);
+      std::swap(J.mm, J.mm_next);
+      EZ_CHECK(cudaMemcpyAsync(ctr_ + C_MM, ctr_ + C_MM_NEXT, 4, cudaMemcpyDeviceToDevice, st_));
+    }
+    EZ_RUN(zero(C_DIRTY));
+    ++dirty_epoch_;
     EZ_RUN(launched());
     EZ_RUN(read_ctr());
     emit(PH_CLOOP_DETECT, h(C_CMAX), h(C_CMIN), h(C_CSAD));
@@ -434,7 +523,7 @@ class Corrector {
   }
 
   int apply() {
-    launch(K_APPLY, k_apply<T>, grid_, 256, J);
+    launch(K_APPLY, k_apply<T>, grid_, 256, J, dirty_epoch_);
     return launched();
   }
 
@@ -459,40 +548,16 @@ class Corrector {
   }
 
   // ----------------------------------------------------------- manifolds --
-  int manifolds() {
+  // One manifold round: decompressed steepest roots, then per saddle side the
+  // fused row-slot / candidate pass and the wrong-neighbour arbitration
+  // (ComputeDirection + Compute*Manifold, findAscPaths / findDescPaths,
+  // get_wrong_split_neighbors / get_wrong_join_neighbors).
+  int manifold_block() {
     ++manifold_rounds_;
     const int N = J.dim.N;
-    launch(K_DIRECTION, k_direction<T>, tile_grid(), 256, J, J.g, J.dds, J.das);
-    launch(K_JUMP, k_jump, grid_, 256, J.dds, J.gate, 1, N, N, ctr_ + C_ERROR);
-    launch(K_JUMP, k_jump, grid_, 256, J.das, J.gate, 2, N, N, ctr_ + C_ERROR);
-    launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.g, J.dds, J.sad2, C_NS2, J.drow2);
-    launch(K_ROWS, k_rows<T, false>, grid_, 256, J, J.g, J.das, J.sad1, C_NS1, J.drow1);
-    return launched();
-  }
-
-  template <bool kSplit>
-  int resolve_side(int stamp) {
-    EZ_RUN(zero(C_CAND));
-    launch(K_WRONG_NBR, k_wn_seed<T, kSplit>, grid_, 256, J);
-    EZ_RUN(launched());
-    const int kRounds = 16;
-    for (int r = 0; r < kRounds; ++r) {
-      EZ_RUN(read_ctr());
-      if (h(C_CAND) == 0) return EXTREMZ_OK;
-      const unsigned long long round = ++ctx_.wn_round;
-      EZ_RUN(zero(C_CAND_NEXT));
-      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, J, round, stamp);
-      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, J, round, stamp);
-      EZ_RUN(launched());
-      std::swap(J.cand, J.cand_next);
-      EZ_CHECK(cudaMemcpyAsync(ctr_ + C_CAND, ctr_ + C_CAND_NEXT, 4, cudaMemcpyDeviceToDevice, st_));
-    }
-    launch(K_WRONG_NBR, k_wn_sequential<T, kSplit>, 1, 1, J, stamp);
-    return launched();
-  }
-
-  // get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513).
-  int wrong_neighbors() {
+    launch_direction(J.g, tma_g_, map_g_, J.dds, J.das);
+    launch(K_JUMP, k_jump, grid_, 256, J.dds, (const uint8_t*)J.gate, 1, N, N, ctr_ + C_ERROR);
+    launch(K_JUMP, k_jump, grid_, 256, J.das, (const uint8_t*)J.gate, 2, N, N, ctr_ + C_ERROR);
     const int stamp = ++ctx_.wn_stamp;
     EZ_RUN(zero(C_NFC, 2));
     EZ_RUN(resolve_side<true>(stamp));
@@ -502,9 +567,23 @@ class Corrector {
     return EXTREMZ_OK;
   }
 
-  int manifold_block() {
-    EZ_RUN(manifolds());
-    return wrong_neighbors();
+  // Bounded device rounds of vote / commit, then the sequential completion
+  // for whatever is left; no host round trip.
+  template <bool kSplit>
+  int resolve_side(int stamp) {
+    EZ_RUN(zero(C_CAND));
+    launch(K_ROWS, k_saddle_pass<T, kSplit>, grid_, 256, J);
+    const int kRounds = 3;
+    for (int r = 0; r < kRounds; ++r) {
+      const unsigned long long round = ++ctx_.wn_round;
+      EZ_RUN(zero(C_CAND_NEXT));
+      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, J, round, stamp);
+      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, J, round, stamp);
+      std::swap(J.cand, J.cand_next);
+      EZ_CHECK(cudaMemcpyAsync(ctr_ + C_CAND, ctr_ + C_CAND_NEXT, 4, cudaMemcpyDeviceToDevice, st_));
+    }
+    launch(K_WRONG_NBR, k_wn_sequential<T, kSplit>, 1, 1, J, stamp);
+    return launched();
   }
 
   // r_loops (:4210-4227).
@@ -796,15 +875,14 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
   if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
   const size_t bytes = (size_t)width * height * depth * (dtype == EXTREMZ_F32 ? 4 : 8);
   cudaStream_t st = (cudaStream_t)stream;
-  void* d = nullptr;
-  if (cudaMalloc(&d, 2 * bytes) != cudaSuccess) {
-    cudaGetLastError();
+  rc = ctx->c.stage.reserve(2 * bytes + 512);
+  if (rc != EXTREMZ_OK) {
     if (prev != ctx->c.device) cudaSetDevice(prev);
-    return EXTREMZ_OOM;
+    return (extremz_status)rc;
   }
-  char* df = (char*)d;
-  char* dg = df + bytes;
-  rc = EXTREMZ_OK;
+  ctx->c.stage.used = 0;
+  char* df = ctx->c.stage.take<char>(bytes);
+  char* dg = ctx->c.stage.take<char>(bytes);
   if (cudaMemcpyAsync(df, h_orig, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(dg, h_decp, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
     rc = EXTREMZ_CUDA_ERR;
@@ -816,7 +894,6 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
         cudaStreamSynchronize(st) != cudaSuccess)
       rc = EXTREMZ_CUDA_ERR;
   }
-  cudaFree(d);
   if (prev != ctx->c.device) cudaSetDevice(prev);
   return (extremz_status)rc;
 }

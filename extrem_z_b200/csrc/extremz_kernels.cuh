@@ -34,6 +34,11 @@ struct Job {
   int* counter;       // delta_counter of the reference (starts at -1)
   int* touched;       // vertices whose delta left the sentinel in this phase
   int* mm;            // mismatch list: v | cat << 29
+  int* mm_next;       // the list being rebuilt by the incremental detection
+  uint8_t* mstat;     // current mismatch categories of every vertex
+  int* dirty;         // vertices whose value changed since the last detection
+  int* dstamp;        // dirty-list membership stamps (== dirty epoch)
+  int* rstamp;        // re-evaluation stamps (== detection epoch)
   unsigned long long* claim;  // wrong-neighbour arbitration, (round << 32) | ~saddle
   int* taken;         // wrong-neighbour flag stamps (== call id when flagged)
   int* taken1;
@@ -41,7 +46,8 @@ struct Job {
   int* flagged; int* flagged1;  // flagged neighbours (split / join)
 
   int* sad2; int* sad1; int* maxima; int* minima;
-  int* orow2; int* orow1; int* drow2; int* drow1;  // rows of kRowStride ints
+  int* orow2; int* orow1;  // original rows of kRowStride ints
+  int* drow2; int* drow1;  // decompressed rows: 2 persistent slots per row, see k_saddle_pass
   int* largest; int* smallest;  // per maximum / minimum
   int* first1; int* flag2;      // per maximum: wrong_index_max arbitration
   int* first_min1; int* flag_min2;
@@ -56,7 +62,7 @@ struct Job {
 enum Ctr : int {
   C_MM = 0, C_CMAX, C_CMIN, C_CSAD, C_TOUCHED, C_NFC, C_NFC1, C_CAND, C_CAND_NEXT,
   C_WMC, C_WMC2, C_WSC, C_WMIN, C_WMIN2, C_WSCJ, C_NS2, C_NS1, C_NMAX, C_NMIN,
-  C_ERROR, C_CHANGED, C_COUNT
+  C_ERROR, C_CHANGED, C_DIRTY, C_MM_NEXT, C_COUNT
 };
 // Error bits in ctr[C_ERROR].
 constexpr int kErrJump = 1, kErrPath = 2, kErrTile = 4, kErrResolve = 8;
@@ -74,45 +80,95 @@ __device__ __forceinline__ T tabs(T v) { return v < T(0) ? -v : v; }
 // warp ballots.
 // ---------------------------------------------------------------------------
 constexpr int TX = 32, TY = 8, TZ = 4;
-constexpr int HX = TX + 2, HY = TY + 2, HZ = TZ + 2;
+// Shared tile rows start 4 elements left of the tile origin so that the TMA
+// box origin x = bx - 4 is 16-byte aligned; the tile's x = 0 sits at kXOff.
+constexpr int SX = TX + 8, SY = TY + 2, SZ = TZ + 2, kXOff = 4;
 
 template <class T>
-__device__ __forceinline__ void load_tile(T (*s)[HY][HX], const T* __restrict__ a, const Dims& g,
-                                          int bx, int by, int bz) {
-  for (int i = threadIdx.x; i < HX * HY * HZ; i += blockDim.x) {
-    int lx = i % HX, t = i / HX, ly = t % HY, lz = t / HY;
-    int gx = bx + lx - 1, gy = by + ly - 1, gz = bz + lz - 1;
-    if (gx >= 0 && gx < g.W && gy >= 0 && gy < g.H && gz >= 0 && gz < g.D)
-      s[lz][ly][lx] = a[gx + (long long)gy * g.W + (long long)gz * g.W * g.H];
+struct alignas(128) Tile {
+  T v[SZ][SY][SX];
+};
+
+// Halo tile: TMA box (one bulk tensor copy, zero fill outside the grid) when
+// the field's row stride allows it, else plain loads with every thread's loads
+// issued before its first shared store.  Outside-grid entries are never read.
+template <class T, bool kTma>
+__device__ __forceinline__ bool load_tile(Tile<T>& s, uint64_t* bar, const CUtensorMap* map,
+                                          const T* __restrict__ a, const Dims& g, int bx, int by,
+                                          int bz) {
+  if (kTma) {
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      mbar_expect_tx(bar, (unsigned)sizeof(Tile<T>));
+      tma_load_3d(&s.v[0][0][0], map, bx - kXOff, by - 1, bz - 1, bar);
+    }
+    __syncthreads();
+    return mbar_wait(bar, 0, 1ll << 26);
   }
+  constexpr int HX = TX + 2;
+  constexpr int kTotal = HX * SY * SZ;
+  constexpr int kPer = (kTotal + 255) / 256;
+  T v[kPer];
+  int off[kPer];
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const int i = threadIdx.x + k * 256;
+    const int lx = i % HX, t = i / HX, ly = t % SY, lz = t / SY;
+    const int gx = bx + lx - 1, gy = by + ly - 1, gz = bz + lz - 1;
+    const bool ok = i < kTotal && gx >= 0 && gx < g.W && gy >= 0 && gy < g.H && gz >= 0 && gz < g.D;
+    off[k] = ok ? (lz * SY + ly) * SX + lx + kXOff - 1 : -1;
+    v[k] = ok ? __ldg(a + gx + (long long)gy * g.W + (long long)gz * g.W * g.H) : T(0);
+  }
+#pragma unroll
+  for (int k = 0; k < kPer; ++k)
+    if (off[k] >= 0) (&s.v[0][0][0])[off[k]] = v[k];
+  __syncthreads();
+  return true;
 }
 
-// Type of the tile voxel at (lx, ly, lz) (1-based tile coordinates).
+// Lower-star direction mask and upper mask of the tile voxel at tile
+// coordinates (tx, ty, tz).  A tie goes to the lower side exactly when the
+// neighbour's id is smaller, i.e. for odd directions.
 template <class T>
-__device__ __forceinline__ int tile_type(const T (*s)[HY][HX], int lx, int ly, int lz, int bc,
-                                         const DeviceTables& tb, int& lmask) {
-  const T c = s[lz][ly][lx];
-  int lm = 0, up = 0, k = 0, nl = 0, nu = 0;
+__device__ __forceinline__ void tile_masks(const Tile<T>& s, int tx, int ty, int tz, int valid,
+                                           int& lm, int& um) {
+  const T c = s.v[tz + 1][ty + 1][tx + kXOff];
+  lm = 0;
+  um = 0;
 #pragma unroll
   for (int d = 0; d < kNumDirs; ++d) {
-    if (!dir_valid(d, bc)) continue;
-    const T nv = s[lz + dir_z(d)][ly + dir_y(d)][lx + dir_x(d)];
-    const bool before = dir_neighbour_is_before(d);
-    if (nv < c || (nv == c && before)) {
-      lm |= 1 << d;
-      ++nl;
-    } else if (nv > c || (nv == c && !before)) {
-      up |= 1 << k;
-      ++nu;
-    }
-    ++k;
+    const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
+    const bool lower = dir_neighbour_is_before(d) ? (nv <= c) : (nv < c);
+    const bool upper = dir_neighbour_is_before(d) ? (nv > c) : (nv >= c);
+    lm |= (int)lower << d;
+    um |= (int)upper << d;
   }
-  lmask = lm;
-  if (nu == 0) return 4;
-  if (nl == 0) return 0;
+  lm &= valid;
+  um &= valid;
+}
+
+// Vertex type from the masks (classifyVertex_CUDA :3835-3853): maximum when no
+// upper neighbour, minimum when no lower one, else the LUT entry of the
+// boundary configuration, or -1 for a configuration the LUT has no key for.
+__device__ __forceinline__ int type_from_masks(int lm, int um, int valid, int bc,
+                                               const DeviceTables& tb) {
+  if (um == 0) return 4;
+  if (lm == 0) return 0;
   const int off = tb.key_offset[bc];
   if (off < 0) return -1;
-  return __ldg(tb.lut + off + up);
+  int idx = um;
+  if (bc != 0) {  // index bits follow the valid neighbours' order
+    idx = 0;
+    int k = 0;
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d) {
+      if (valid >> d & 1) {
+        idx |= (um >> d & 1) << k;
+        ++k;
+      }
+    }
+  }
+  return __ldg(tb.lut + off + idx);
 }
 
 __device__ __forceinline__ int mismatch_cats(int t, int o, int lm, int olm) {
@@ -127,13 +183,29 @@ __device__ __forceinline__ int mismatch_cats(int t, int o, int lm, int olm) {
   return cat;
 }
 
-template <class T, bool kDetect>
-__global__ void __launch_bounds__(256) k_classify(Job<T> J, const T* __restrict__ a) {
-  __shared__ T s[HZ][HY][HX];
+// Per-category counts of mismatching vertices, one atomic per warp and category.
+__device__ __forceinline__ void count_cats(int* ctr, int cat) {
+  const unsigned bm = __ballot_sync(0xffffffffu, cat & kCatMax);
+  const unsigned bn = __ballot_sync(0xffffffffu, cat & kCatMin);
+  const unsigned bs = __ballot_sync(0xffffffffu, cat & kCatSaddle);
+  if (lane_id() == 0) {
+    if (bm) atomicAdd(ctr + C_CMAX, __popc(bm));
+    if (bn) atomicAdd(ctr + C_CMIN, __popc(bn));
+    if (bs) atomicAdd(ctr + C_CSAD, __popc(bs));
+  }
+}
+
+template <class T, bool kDetect, bool kTma>
+__global__ void __launch_bounds__(256) k_classify(Job<T> J, const __grid_constant__ CUtensorMap map,
+                                                  const T* __restrict__ a) {
+  __shared__ Tile<T> s;
+  __shared__ uint64_t bar;
   const Dims g = J.dim;
   const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
-  load_tile(s, a, g, bx, by, bz);
-  __syncthreads();
+  if (!load_tile<T, kTma>(s, &bar, &map, a, g, bx, by, bz)) {
+    if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
+    return;
+  }
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   for (int tz = 0; tz < TZ; ++tz) {
     const int x = bx + tx, y = by + ty, z = bz + tz;
@@ -142,22 +214,115 @@ __global__ void __launch_bounds__(256) k_classify(Job<T> J, const T* __restrict_
     if (in) {
       v = x + y * g.W + z * g.W * g.H;
       const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
-      int lm;
-      const int t = tile_type(s, tx + 1, ty + 1, tz + 1, bc, J.tb, lm);
+      const int valid = valid_mask(bc);
+      int lm, um;
+      tile_masks(s, tx, ty, tz, valid, lm, um);
+      const int t = type_from_masks(lm, um, valid, bc, J.tb);
       if (!kDetect) {
         J.otype[v] = (int8_t)t;
         J.olm[v] = (uint16_t)lm;
       } else {
         cat = mismatch_cats(t, J.otype[v], lm, J.olm[v]);
+        J.mstat[v] = (uint8_t)cat;
       }
     }
     if (kDetect) {
       const int slot = warp_append(J.ctr + C_MM, cat != 0, 0xffffffffu);
       if (slot >= 0) J.mm[slot] = v | (cat << kCatShift);
-      if (cat & kCatMax) atomicAdd(J.ctr + C_CMAX, 1);
-      if (cat & kCatMin) atomicAdd(J.ctr + C_CMIN, 1);
-      if (cat & kCatSaddle) atomicAdd(J.ctr + C_CSAD, 1);
+      count_cats(J.ctr, cat);
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Incremental mismatch detection.
+//
+// The type of v depends only on the values of v and its 14 neighbours, so after
+// the first dense detection only the closed neighbourhoods of vertices whose
+// value changed can change status.  k_redetect re-evaluates them (once each,
+// by stamp) and appends the mismatching ones to the next list; k_keep carries
+// over the entries of the previous list that were not re-evaluated.  The
+// resulting set equals a dense re-detection (the lists are unordered; every
+// consumer merges by atomic max).
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ int global_type(const Job<T>& J, int v, int& lmask) {
+  const Dims g = J.dim;
+  int x, y, z;
+  coords(v, g, x, y, z);
+  const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
+  const T c = J.g[v];
+  int lm = 0, up = 0, k = 0, nl = 0, nu = 0;
+#pragma unroll
+  for (int d = 0; d < kNumDirs; ++d) {
+    if (!dir_valid(d, bc)) continue;
+    const T nv = J.g[v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * g.W * g.H];
+    const bool before = dir_neighbour_is_before(d);
+    if (nv < c || (nv == c && before)) {
+      lm |= 1 << d;
+      ++nl;
+    } else if (nv > c || (nv == c && !before)) {
+      up |= 1 << k;
+      ++nu;
+    }
+    ++k;
+  }
+  lmask = lm;
+  if (nu == 0) return 4;
+  if (nl == 0) return 0;
+  const int off = J.tb.key_offset[bc];
+  if (off < 0) return -1;
+  return __ldg(J.tb.lut + off + up);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_redetect(Job<T> J, int epoch) {
+  const int n = J.ctr[C_DIRTY];
+  const long long total = (long long)n * (kNumDirs + 1);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const Dims g = J.dim;
+  for (long long base = blockIdx.x * (long long)blockDim.x; base < total; base += stride) {
+    const long long e = base + threadIdx.x;
+    int cat = 0, v = -1;
+    if (e < total) {
+      const int c = J.dirty[e / (kNumDirs + 1)];
+      const int d = (int)(e % (kNumDirs + 1)) - 1;  // -1: the vertex itself
+      v = c;
+      if (d >= 0) {
+        int x, y, z;
+        coords(c, g, x, y, z);
+        v = dir_valid(d, boundary_code(x, y, z, g.W, g.H, g.D))
+                ? c + dir_x(d) + dir_y(d) * g.W + dir_z(d) * g.W * g.H
+                : -1;
+      }
+      if (v >= 0 && atomicExch(J.rstamp + v, epoch) != epoch) {
+        int lm;
+        const int t = global_type(J, v, lm);
+        cat = mismatch_cats(t, J.otype[v], lm, J.olm[v]);
+        J.mstat[v] = (uint8_t)cat;
+      }
+    }
+    const int slot = warp_append(J.ctr + C_MM_NEXT, cat != 0, 0xffffffffu);
+    if (slot >= 0) J.mm_next[slot] = v | (cat << kCatShift);
+    count_cats(J.ctr, cat);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_keep(Job<T> J, int epoch) {
+  const int n = J.ctr[C_MM];
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int e = base + threadIdx.x;
+    int ent = 0, cat = 0;
+    if (e < n) {
+      ent = J.mm[e];
+      const int v = ent & ((1 << kCatShift) - 1);
+      if (J.rstamp[v] != epoch) cat = (unsigned)ent >> kCatShift;
+    }
+    const int slot = warp_append(J.ctr + C_MM_NEXT, cat != 0, 0xffffffffu);
+    if (slot >= 0) J.mm_next[slot] = ent;
+    count_cats(J.ctr, cat);
   }
 }
 
@@ -170,17 +335,21 @@ __global__ void __launch_bounds__(256) k_classify(Job<T> J, const T* __restrict_
 // at a root, so the global jump that follows moves a tile per hop.
 // Output: ds/as = first vertex outside the tile on the path, or the root.
 // ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(256) k_direction(Job<T> J, const T* __restrict__ a,
-                                                   int* __restrict__ ds, int* __restrict__ as) {
-  __shared__ T s[HZ][HY][HX];
+template <class T, bool kTma>
+__global__ void __launch_bounds__(256) k_direction(Job<T> J, const __grid_constant__ CUtensorMap map,
+                                                   const T* __restrict__ a, int* __restrict__ ds,
+                                                   int* __restrict__ as) {
+  __shared__ Tile<T> s;
+  __shared__ uint64_t bar;
   __shared__ int phi[TZ * TY * TX], plo[TZ * TY * TX];
   const Dims g = J.dim;
-  const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
-  load_tile(s, a, g, bx, by, bz);
-  __syncthreads();
-  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   const int WH = g.W * g.H;
+  const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
+  if (!load_tile<T, kTma>(s, &bar, &map, a, g, bx, by, bz)) {
+    if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
+    return;
+  }
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   for (int tz = 0; tz < TZ; ++tz) {
     const int li = (tz * TY + ty) * TX + tx;
     const int x = bx + tx, y = by + ty, z = bz + tz;
@@ -190,33 +359,45 @@ __global__ void __launch_bounds__(256) k_direction(Job<T> J, const T* __restrict
       continue;
     }
     const int v = x + y * g.W + z * WH;
-    const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
-    const T c = s[tz + 1][ty + 1][tx + 1];
+    const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
+    const T c = s.v[tz + 1][ty + 1][tx + kXOff];
+    // Steepest ascent: maximum of (value, id) over {v} and its neighbours,
+    // scanning ids in ascending order so that ">=" keeps the larger id on a
+    // tie; steepest descent scans in descending order with "<=".
+    // (Finite inputs: the scans start from -inf / +inf and always meet the
+    // centre, so no "first element" flag is needed.)
+    T hv = -T(INFINITY), lv = T(INFINITY);
     int hd = -1, ld = -1;
-    T hv = c, lv = c;
-    int hid = v, lid = v;
 #pragma unroll
-    for (int d = 0; d < kNumDirs; ++d) {
-      if (!dir_valid(d, bc)) continue;
-      const T nv = s[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + 1 + dir_x(d)];
-      const int r = v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
-      if (hv < nv || (hv == nv && hid < r)) { hv = nv; hid = r; hd = d; }
-      if (lv > nv || (lv == nv && lid > r)) { lv = nv; lid = r; ld = d; }
+    for (int j = 0; j < kNumDirs; ++j) {
+      const int d = rank_dir(j);
+      if (j == kRankCentre && c >= hv) { hv = c; hd = -1; }
+      const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
+      if ((valid >> d & 1) && nv >= hv) { hv = nv; hd = d; }
     }
-    // Encode: local index (>= 0) when the target lies in this tile, else
-    // -(global id) - 1; a root points to itself and is stored resolved.
-    auto enc = [&](int d, int gid) {
-      if (d < 0) return -gid - 1;
+#pragma unroll
+    for (int j = kNumDirs - 1; j >= 0; --j) {
+      const int d = rank_dir(j);
+      const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
+      if ((valid >> d & 1) && nv <= lv) { lv = nv; ld = d; }
+      if (j == kRankCentre && c <= lv) { lv = c; ld = -1; }
+    }
+    // Local index when the target lies in this tile, else -(global id) - 1;
+    // a root (no steeper neighbour) is stored resolved.
+    auto enc = [&](int d) {
+      if (d < 0) return -v - 1;
       const int ltx = tx + dir_x(d), lty = ty + dir_y(d), ltz = tz + dir_z(d);
-      if (ltx < 0 || ltx >= TX || lty < 0 || lty >= TY || ltz < 0 || ltz >= TZ) return -gid - 1;
+      const int gid = v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+      if ((unsigned)ltx >= (unsigned)TX || (unsigned)lty >= (unsigned)TY || (unsigned)ltz >= (unsigned)TZ)
+        return -gid - 1;
       return (ltz * TY + lty) * TX + ltx;
     };
-    phi[li] = enc(hd, hid);
-    plo[li] = enc(ld, lid);
+    phi[li] = enc(hd);
+    plo[li] = enc(ld);
   }
   __syncthreads();
-  // In-place pointer jumping inside the tile; each step advances along the
-  // path, so it converges in O(log tile) steps.
+  // In-place pointer jumping inside the tile; every step moves along the path,
+  // so it ends in O(log tile) steps.
   for (int it = 0; it < 64; ++it) {
     int changed = 0;
     for (int tz = 0; tz < TZ; ++tz) {
@@ -235,7 +416,7 @@ __global__ void __launch_bounds__(256) k_direction(Job<T> J, const T* __restrict
     if (!(x < g.W && y < g.H && z < g.D)) continue;
     const int v = x + y * g.W + z * WH;
     const int ph = phi[li], pl = plo[li];
-    ds[v] = ph < 0 ? -ph - 1 : v;  // ph >= 0 cannot remain; guard anyway
+    ds[v] = ph < 0 ? -ph - 1 : v;
     as[v] = pl < 0 ? -pl - 1 : v;
   }
 }
@@ -557,7 +738,7 @@ __global__ void __launch_bounds__(256) k_propose_cp(Job<T> J) {
 // applyDeltaBuffer (:3061-3111) over the vertices that received a proposal;
 // the proposal buffer is reset to the sentinel on the way (init_delta).
 template <class T>
-__global__ void __launch_bounds__(256) k_apply(Job<T> J) {
+__global__ void __launch_bounds__(256) k_apply(Job<T> J, int dirty_epoch) {
   const int n = J.ctr[C_TOUCHED];
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
@@ -566,7 +747,8 @@ __global__ void __launch_bounds__(256) k_apply(Job<T> J) {
     J.delta[v] = J.sentinel_key;
     if (d == J.sentinel) continue;
     const T fv = J.f[v];
-    T gv = J.g[v];
+    const T g0 = J.g[v];
+    T gv = g0;
     if (J.edit_type == 0) {
       const int c = J.counter[v];
       if (c < J.q - 1 && tabs(T(fv - (gv + d))) <= J.bound) {
@@ -581,6 +763,8 @@ __global__ void __launch_bounds__(256) k_apply(Job<T> J) {
       else gv = fv - J.bound;
     }
     J.g[v] = gv;
+    if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0) && atomicExch(J.dstamp + v, dirty_epoch) != dirty_epoch)
+      J.dirty[atomicAdd(J.ctr + C_DIRTY, 1)] = v;
   }
 }
 
@@ -613,10 +797,25 @@ __device__ __forceinline__ int wn_candidates(const Job<T>& J, int s, int* ids) {
   return k;
 }
 
+// Fused pass over the original saddles after a manifold round:
+//  * decompressed row slots.  The reference rewrites row i (findAscPaths /
+//    findDescPaths, :1832-2049) in place each round, and its only reader,
+//    get_wrong_index_max / _min (:3113-3171), reads entry 0 and entry k =
+//    (original count - 1), possibly stale when the new row is shorter.  So two
+//    persistent slots per row reproduce it: slot 0 takes the new entry 0 when
+//    the new row is non-empty, slot 1 takes the new entry k when the new row
+//    has more than k entries.  Entry k of the sorted row is found by counting
+//    (rank of each candidate), without materialising the sort.
+//  * wrong-neighbour seeds: saddles with at least one candidate.
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_wn_seed(Job<T> J) {
+__global__ void __launch_bounds__(256) k_saddle_pass(Job<T> J) {
   const int ns = J.ctr[kSplit ? C_NS2 : C_NS1];
   const int* sad = kSplit ? J.sad2 : J.sad1;
+  const int* orow = kSplit ? J.orow2 : J.orow1;
+  int* slots = kSplit ? J.drow2 : J.drow1;
+  const int* lab = kSplit ? J.dds : J.das;
+  const int* olab = kSplit ? J.ds : J.as;
+  const Dims g = J.dim;
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < ns; base += stride) {
     const int i = base + threadIdx.x;
@@ -624,8 +823,54 @@ __global__ void __launch_bounds__(256) k_wn_seed(Job<T> J) {
     int s = 0;
     if (i < ns) {
       s = sad[i];
-      int ids[kNumDirs];
-      has = wn_candidates<T, kSplit>(J, s, ids) > 0;
+      int x, y, z;
+      coords(s, g, x, y, z);
+      const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
+      const T sv = J.g[s];
+      int ml[kNumDirs];
+      T mv[kNumDirs];
+      int valid = 0;
+#pragma unroll
+      for (int d = 0; d < kNumDirs; ++d) {
+        ml[d] = 0;
+        mv[d] = T(0);
+        if (!dir_valid(d, bc)) continue;
+        const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * g.W * g.H;
+        const T rv = J.g[r];
+        if (kSplit ? above(rv, r, sv, s) : below(rv, r, sv, s)) {
+          const int m = lab[r];
+          if (m != olab[r]) has = true;
+          const T v = J.g[m];
+          if (!kSplit || tabs(T(v - sv)) >= J.thr) {
+            ml[d] = m;
+            mv[d] = v;
+            valid |= 1 << d;
+          }
+        }
+      }
+      const int ocnt = orow[(long long)i * kRowStride + 14];
+      if (ocnt > 0 && valid) {
+        const int k = ocnt - 1;
+        int first = -1, kth = -1;
+        const int cnt = __popc(valid);
+#pragma unroll
+        for (int d = 0; d < kNumDirs; ++d) {
+          if (!(valid >> d & 1)) continue;
+          int gt = 0, eq = 0;
+#pragma unroll
+          for (int e = 0; e < kNumDirs; ++e) {
+            if (!(valid >> e & 1)) continue;
+            const bool before = kSplit ? above(mv[e], ml[e], mv[d], ml[d])
+                                       : below(mv[e], ml[e], mv[d], ml[d]);
+            gt += before;
+            eq += ml[e] == ml[d];
+          }
+          if (gt == 0) first = ml[d];
+          if (gt <= k && k < gt + eq) kth = ml[d];
+        }
+        slots[2ll * i] = first;
+        if (cnt > k) slots[2ll * i + 1] = kth;
+      }
     }
     const int slot = warp_append(J.ctr + C_CAND, has, 0xffffffffu);
     if (slot >= 0) J.cand[slot] = s;
@@ -757,12 +1002,12 @@ __global__ void __launch_bounds__(256) k_wim_scan(Job<T> J) {
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
     const int* o = orow + (long long)i * kRowStride;
-    const int* d = drow + (long long)i * kRowStride;
+    const int* d = drow + 2ll * i;  // slots: entry 0, entry (count - 1)
     const int cnt = o[14];
     if (cnt == 0) continue;
     if (o[0] != d[0]) atomicMin(first + J.ext[o[0]], i);
     const int k = cnt - 1;
-    if (o[k] != d[k]) flag[J.ext[o[k]]] = 1;
+    if (o[k] != d[1]) flag[J.ext[o[k]]] = 1;
   }
 }
 
@@ -787,10 +1032,10 @@ __global__ void __launch_bounds__(256) k_wim_collect(Job<T> J, int fix) {
         h1 = true;
         first[m] = kInf;
         if (fix) {
-          const int* d = drow + (long long)row * kRowStride;
-          // split: lower the false maximum d[0] (:3326-3344); join: lower the
-          // true minimum itself (:3375-3391).
-          const int target = kMax ? d[0] : ext_list[m];
+          // split: lower the false maximum, entry 0 of the winning
+          // decompressed row (:3326-3344); join: lower the true minimum
+          // itself (:3375-3391).
+          const int target = kMax ? drow[2ll * row] : ext_list[m];
           propose(J, target, step_delta(J, target));
         }
       }
@@ -823,11 +1068,10 @@ __global__ void __launch_bounds__(256) k_wim_min2_scan(Job<T> J) {
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
     const int* o = J.orow1 + (long long)i * kRowStride;
-    const int* d = J.drow1 + (long long)i * kRowStride;
     const int cnt = o[14];
     if (cnt == 0) continue;
     const int k = cnt - 1;
-    if (o[k] != d[k]) atomicMin(J.first_sj + J.ext[o[k]], i);
+    if (o[k] != J.drow1[2ll * i + 1]) atomicMin(J.first_sj + J.ext[o[k]], i);
   }
 }
 template <class T>
@@ -838,9 +1082,7 @@ __global__ void __launch_bounds__(256) k_wim_min2_collect(Job<T> J) {
     const int row = J.first_sj[m];
     if (row == kInf) continue;
     J.first_sj[m] = kInf;
-    const int* o = J.orow1 + (long long)row * kRowStride;
-    const int* d = J.drow1 + (long long)row * kRowStride;
-    const int target = d[o[14] - 1];
+    const int target = J.drow1[2ll * row + 1];
     propose(J, target, step_delta(J, target));
   }
 }

@@ -67,9 +67,16 @@ typedef struct {
   int reserved[5];
 } extremz_params;
 
-/* flags: time every kernel launch with CUDA events, per kernel class, into
- * extremz_report.prof_ms / prof_launches. */
+/* flags: time kernel launches with CUDA events, per kernel class, into
+ * extremz_report.prof_ms / prof_launches.  Bits from
+ * EXTREMZ_PROFILE_CLASS_SHIFT up select the classes to time (none set = all),
+ * so that a benchmark can time only its dominant kernel. */
 #define EXTREMZ_FLAG_PROFILE 1
+#define EXTREMZ_PROFILE_CLASS_SHIFT 8
+/* flags: load halo tiles with plain loads instead of TMA bulk tensor copies
+ * (TMA is used whenever the field's base is 16-byte aligned and its row stride
+ * W * sizeof(value) is a multiple of 16 bytes). */
+#define EXTREMZ_FLAG_NO_TMA 2
 
 /* Kernel classes of extremz_report.prof_*: 0 setup classification, 1 fused
  * classification + mismatch detection, 2 steepest directions, 3 pointer

@@ -35,6 +35,10 @@
 #include <cstring>
 #include <vector>
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 namespace {
 
 // The 14 Freudenthal directions in the reference's order
@@ -216,8 +220,9 @@ int classify(const T* a, const Grid& g, int v, uint16_t* lmask_out) {
 // ascent (ds) and descent (as) graphs.
 template <class T>
 void roots(const T* a, const Grid& g, int* ds, int* as) {
-  int nb[14];
+#pragma omp parallel for schedule(static)
   for (int v = 0; v < g.N; ++v) {
+    int nb[14];
     int hi = v, lo = v;
     int n = g.nbrs(v, nb);
     for (int j = 0; j < n; ++j) {
@@ -228,18 +233,19 @@ void roots(const T* a, const Grid& g, int* ds, int* as) {
     ds[v] = hi;
     as[v] = lo;
   }
+  // Synchronous pointer doubling until every label is a root.
+  std::vector<int> tmp(g.N);
   for (int* m : {ds, as}) {
-    std::vector<int> path;
-    for (int v = 0; v < g.N; ++v) {
-      int u = v;
-      path.clear();
-      while (m[u] != u && m[m[u]] != m[u]) {
-        path.push_back(u);
-        u = m[u];
+    for (;;) {
+      int changed = 0;
+#pragma omp parallel for schedule(static) reduction(| : changed)
+      for (int v = 0; v < g.N; ++v) {
+        int w = m[m[v]];
+        tmp[v] = w;
+        changed |= (w != m[v]);
       }
-      int root = m[u];
-      for (int p : path) m[p] = root;
-      m[v] = root;
+      std::memcpy(m, tmp.data(), sizeof(int) * (size_t)g.N);
+      if (!changed) break;
     }
   }
 }
@@ -366,23 +372,43 @@ struct Corrector {
     }
   }
 
-  // classifyVertex_CUDA(type=1) fused detection (:3856-3910).
+  // classifyVertex_CUDA(type=1) fused detection (:3856-3910).  Threads take
+  // contiguous ranges and their lists are joined in order, so the lists are in
+  // ascending id whatever the thread count.
   void detect() {
     lmax.clear();
     lmin.clear();
     lsad.clear();
-    for (int v = 0; v < g.N; ++v) {
-      uint16_t lm;
-      int t = classify(a, g, v, &lm);
-      int o = otype[v];
-      if (t != o) {
-        if ((t == 4) != (o == 4)) lmax.push_back(v);
-        if ((t == 0) != (o == 0)) lmin.push_back(v);
-        if ((t == 2) != (o == 2) || (t == 1) != (o == 1) || (t == 3) != (o == 3))
-          lsad.push_back(v);
-      } else if (t == 1 || t == 2 || t == 3) {
-        if (lm != olmask[v]) lsad.push_back(v);  // areVectorsDifferent_local (:909-921)
+    int nt = 1;
+#ifdef _OPENMP
+    nt = omp_get_max_threads();
+#endif
+    std::vector<std::vector<int>> pmax(nt), pmin(nt), psad_(nt);
+#pragma omp parallel num_threads(nt)
+    {
+      int t = 0;
+#ifdef _OPENMP
+      t = omp_get_thread_num();
+#endif
+      long long lo = (long long)g.N * t / nt, hi = (long long)g.N * (t + 1) / nt;
+      for (int v = (int)lo; v < (int)hi; ++v) {
+        uint16_t lm;
+        int ty = classify(a, g, v, &lm);
+        int o = otype[v];
+        if (ty != o) {
+          if ((ty == 4) != (o == 4)) pmax[t].push_back(v);
+          if ((ty == 0) != (o == 0)) pmin[t].push_back(v);
+          if ((ty == 2) != (o == 2) || (ty == 1) != (o == 1) || (ty == 3) != (o == 3))
+            psad_[t].push_back(v);
+        } else if (ty == 1 || ty == 2 || ty == 3) {
+          if (lm != olmask[v]) psad_[t].push_back(v);  // areVectorsDifferent_local (:909-921)
+        }
       }
+    }
+    for (int t = 0; t < nt; ++t) {
+      lmax.insert(lmax.end(), pmax[t].begin(), pmax[t].end());
+      lmin.insert(lmin.end(), pmin[t].begin(), pmin[t].end());
+      lsad.insert(lsad.end(), psad_[t].begin(), psad_[t].end());
     }
     d_cfmax = (int)lmax.size();
     d_cfmin = (int)lmin.size();
@@ -498,14 +524,17 @@ struct Corrector {
 
   // Decompressed rows: only [0, count) and the count are rewritten.
   void dec_rows() {
-    int tmp[kRow];
-    for (size_t i = 0; i < sad2.size(); ++i) {
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)sad2.size(); ++i) {
+      int tmp[kRow];
       asc_row(a, dDS.data(), sad2[i], tmp);
       int* r = &drow2[i * kRow];
       for (int k = 0; k < tmp[14]; ++k) r[k] = tmp[k];
       r[14] = tmp[14];
     }
-    for (size_t i = 0; i < sad1.size(); ++i) {
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)sad1.size(); ++i) {
+      int tmp[kRow];
       desc_row(a, dAS.data(), sad1[i], tmp);
       int* r = &drow1[i * kRow];
       for (int k = 0; k < tmp[14]; ++k) r[k] = tmp[k];
@@ -752,6 +781,7 @@ struct Corrector {
     int N = g.N;
     otype.resize(N);
     olmask.resize(N);
+#pragma omp parallel for schedule(static)
     for (int v = 0; v < N; ++v) otype[v] = (int8_t)classify(f, g, v, &olmask[v]);
     DS.resize(N);
     AS.resize(N);
@@ -986,6 +1016,18 @@ bool dims_ok(int W, int H, int D) {
 }  // namespace
 
 extern "C" {
+
+// Threads of the dense passes (detection, manifolds, rows); results do not
+// depend on it.
+int oracle_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
 
 // LUT in the reference's LUT.bin layout (24 800 int32).
 int oracle_lut(int32_t* out, int n) {

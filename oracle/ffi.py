@@ -50,6 +50,8 @@ def lib():
         build()
         L = ctypes.CDLL(_LIB_PATH)
         vp, i32 = ctypes.c_void_p, ctypes.c_int
+        L.oracle_set_threads.argtypes = [i32]
+        L.oracle_set_threads.restype = i32
         L.oracle_lut.argtypes = [vp, i32]
         L.oracle_classify.argtypes = [vp, i32, i32, i32, i32, vp, vp]
         L.oracle_roots.argtypes = [vp, i32, i32, i32, i32, vp, vp]
@@ -57,6 +59,11 @@ def lib():
                                      ctypes.POINTER(Params), ctypes.POINTER(Report), vp, i32]
         _lib = L
     return _lib
+
+
+def set_threads(n: int) -> int:
+    """Threads of the oracle's dense passes (results do not depend on it)."""
+    return lib().oracle_set_threads(int(n))
 
 
 def _dtype_code(a: np.ndarray) -> int:
@@ -102,7 +109,7 @@ def roots(f: np.ndarray):
 
 
 def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, q: int = 4,
-            edit_type: int = 0, max_outer: int = 500, max_cloop_rounds: int = 100000,
+            edit_type: int = 1, max_outer: int = 500, max_cloop_rounds: int = 100000,
             final_join: bool = True, preserve_join: bool = False, trace_cap: int = 0):
     """Run the oracle correction; returns (corrected copy, report dict, trace)."""
     f = np.ascontiguousarray(f)

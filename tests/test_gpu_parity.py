@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = np.load(os.path.join(HERE, "golden", "oracle_cases.npz"))
 CASES = sorted({k.split("/")[0] for k in GOLDEN.files})
-KW = dict(q=4, max_outer=500, max_cloop_rounds=100000, final_join=True)
+KW = dict(q=4, edit_type=1, max_outer=500, max_cloop_rounds=100000, final_join=True)
 
 
 def gpu_correct(f, decp, eb, trace_cap=200000, **kw):
@@ -43,7 +43,8 @@ def first_divergence(a, b):
 def test_golden_cases_bit_exact(name):
     f, decp = GOLDEN[f"{name}/f"], GOLDEN[f"{name}/decp"]
     eb, et = GOLDEN[f"{name}/meta"][:2]
-    out, rep, trace = gpu_correct(f, decp, eb, edit_type=int(et), **KW)
+    kw = dict(KW, edit_type=int(et))
+    out, rep, trace = gpu_correct(f, decp, eb, **kw)
     ref_trace = GOLDEN[f"{name}/trace"]
     assert np.array_equal(trace, ref_trace), first_divergence(trace, ref_trace)
     assert np.array_equal(out.view(np.uint8), GOLDEN[f"{name}/fixed"].view(np.uint8))
@@ -55,10 +56,9 @@ def test_golden_cases_bit_exact(name):
 def test_plain_64_bit_exact(dtype, edit_type):
     from oracle import ffi
     fld = synth.plain_64(dtype)
-    ref, rrep, rtrace = ffi.correct(fld.f, fld.decp, fld.eb, edit_type=edit_type,
-                                    trace_cap=400000, **KW)
-    out, rep, trace = gpu_correct(fld.f, fld.decp, fld.eb, trace_cap=400000,
-                                  edit_type=edit_type, **KW)
+    kw = dict(KW, edit_type=edit_type)
+    ref, rrep, rtrace = ffi.correct(fld.f, fld.decp, fld.eb, trace_cap=400000, **kw)
+    out, rep, trace = gpu_correct(fld.f, fld.decp, fld.eb, trace_cap=400000, **kw)
     assert np.array_equal(trace, rtrace), first_divergence(trace, rtrace)
     assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
     assert rep.status == rrep["status"] == 0
@@ -92,3 +92,14 @@ def test_repeated_calls_on_one_context_are_identical():
     a, _, _ = gpu_correct(fld.f, fld.decp, fld.eb, **KW)
     b, _, _ = gpu_correct(fld.f, fld.decp, fld.eb, **KW)
     assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+@pytest.mark.parametrize("tma", [True, False])
+def test_tile_load_paths_agree(tma):
+    """TMA halo tiles and plain-load tiles give the same bytes (64^3 f32)."""
+    from oracle import ffi
+    fld = synth.plain_64(np.float32)
+    ref, _, _ = ffi.correct(fld.f, fld.decp, fld.eb, **KW)
+    out, rep, _ = gpu_correct(fld.f, fld.decp, fld.eb, trace_cap=0, tma=tma, **KW)
+    assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+    assert rep.error_bits == 0
