@@ -365,7 +365,7 @@ class Corrector {
       long long b = 0;
       auto add = [&](long long count, long long sz) { b += (count * sz + 255) & ~255ll; };
       add(C_COUNT, 4);
-      add(N, 1); add(N, 2); add(N, 1);         // otype, olm, gate
+      add(N, 1); add(N, 2);                    // otype, olm
       for (int i = 0; i < 5; ++i) add(N, 4);   // ds, as, dds, das, ext
       add(N, sizeof(K)); add(N, 4); add(N, 4); add(N, 4);  // delta, counter, touched, mm
       add(N, 4); add(N, 1); add(N, 4); add(N, 4); add(N, 4);  // mm_next, mstat, dirty, dstamp, rstamp
@@ -373,8 +373,8 @@ class Corrector {
       for (int i = 0; i < 4; ++i) add(N, 4);   // cand, cand_next, flagged, flagged1
       add(4ll * nb, 4);                        // cp block counts
       add(ns2, 4); add(ns1, 4); add(nmax, 4); add(nmin, 4);
-      add(ns2 * kRowStride, 4); add(ns2 * 2, 4);
-      add(ns1 * kRowStride, 4); add(ns1 * 2, 4);
+      add(ns2 * kRowStride, 4); add(ns2 * 2, 4); add(ns2, 1);
+      add(ns1 * kRowStride, 4); add(ns1 * 2, 4); add(ns1, 1);
       for (int i = 0; i < 4; ++i) add(nmax, 4);  // largest, first1, flag2, first_s
       for (int i = 0; i < 4; ++i) add(nmin, 4);  // smallest, first_min1, flag_min2, first_sj
       long long ne = std::max(nmax, nmin);
@@ -392,7 +392,6 @@ class Corrector {
     ctr_ = J.ctr = A.take<int>(C_COUNT);
     J.otype = A.take<int8_t>(N);
     J.olm = A.take<uint16_t>(N);
-    J.gate = A.take<uint8_t>(N);
     J.ds = A.take<int>(N); J.as = A.take<int>(N);
     J.dds = A.take<int>(N); J.das = A.take<int>(N);
     J.ext = A.take<int>(N);
@@ -412,12 +411,10 @@ class Corrector {
     int* bcount = A.take<int>(4ll * nb);
     EZ_CHECK(cudaMemsetAsync(ctr_, 0, C_COUNT * sizeof(int), st_));
 
-    // Original classification, gates and manifolds.
+    // Original classification and manifolds.
     launch_classify<false>(K_SETUP, J.f, tma_f_, map_f_);
-    launch(K_OTHER, k_gate<T>, grid_, 256, J);
     launch_direction(J.f, tma_f_, map_f_, J.ds, J.as);
-    launch(K_JUMP, k_jump, grid_, 256, J.ds, J.gate, 1, N, N, ctr_ + C_ERROR);
-    launch(K_JUMP, k_jump, grid_, 256, J.as, J.gate, 2, N, N, ctr_ + C_ERROR);
+    launch(K_JUMP, k_jump2, grid_, 256, J.ds, J.as, N, N, ctr_ + C_ERROR);
     EZ_RUN(launched());
     // Critical-point lists in ascending id.
     launch(K_OTHER, k_cp_count, nb, kCpBlock, J.otype, N, bcount);
@@ -429,8 +426,10 @@ class Corrector {
     J.maxima = A.take<int>(nmax); J.minima = A.take<int>(nmin);
     J.orow2 = A.take<int>((long long)ns2 * kRowStride);
     J.drow2 = A.take<int>((long long)ns2 * 2);
+    J.ocnt2 = A.take<uint8_t>(ns2);
     J.orow1 = A.take<int>((long long)ns1 * kRowStride);
     J.drow1 = A.take<int>((long long)ns1 * 2);
+    J.ocnt1 = A.take<uint8_t>(ns1);
     J.largest = A.take<int>(nmax); J.first1 = A.take<int>(nmax);
     J.flag2 = A.take<int>(nmax); J.first_s = A.take<int>(nmax);
     J.smallest = A.take<int>(nmin); J.first_min1 = A.take<int>(nmin);
@@ -443,6 +442,7 @@ class Corrector {
     launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
     launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.f, J.ds, J.sad2, C_NS2, J.orow2);
     launch(K_ROWS, k_rows<T, false>, grid_, 256, J, J.f, J.as, J.sad1, C_NS1, J.orow1);
+    launch(K_SETUP, k_row_counts<T>, grid_, 256, J);
     EZ_RUN(launched());
     // Decompressed row slots start at zero: the reference's rows are fresh
     // cudaMalloc memory read before first written (:5338-5341, :3128-3130).
@@ -556,8 +556,7 @@ class Corrector {
     ++manifold_rounds_;
     const int N = J.dim.N;
     launch_direction(J.g, tma_g_, map_g_, J.dds, J.das);
-    launch(K_JUMP, k_jump, grid_, 256, J.dds, (const uint8_t*)J.gate, 1, N, N, ctr_ + C_ERROR);
-    launch(K_JUMP, k_jump, grid_, 256, J.das, (const uint8_t*)J.gate, 2, N, N, ctr_ + C_ERROR);
+    launch(K_JUMP, k_jump2, grid_, 256, J.dds, J.das, N, N, ctr_ + C_ERROR);
     const int stamp = ++ctx_.wn_stamp;
     EZ_RUN(zero(C_NFC, 2));
     EZ_RUN(resolve_side<true>(stamp));
@@ -603,10 +602,10 @@ class Corrector {
     launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, J, 1);
     EZ_RUN(launched());
     EZ_RUN(apply());
-    if (trace_) {
-      EZ_RUN(read_ctr());
-      emit(PH_SLOOPS, h(C_WMC), h(C_WMC2));
-    }
+    // s_loops refreshes the reference's file-scope host copies (:3473-3476);
+    // the first block branches on them right away.
+    EZ_RUN(read_ctr());
+    emit(PH_SLOOPS, h(C_WMC), h(C_WMC2));
     return EXTREMZ_OK;
   }
 
@@ -658,35 +657,42 @@ class Corrector {
   }
 
   // --------------------------------------------------------------- main --
+  // main() (:5508-5997).  The reference's host counters: c_loops and r_loops
+  // take them by value (main's copies unchanged); s_loops, saddle_loops and
+  // the join variants refresh the file-scope copies of wrong_max(_2),
+  // wrong_saddle, wrong_min(_2) and wrong_saddle_join (:62, :3473-3476,
+  // :4236, :3498-3501, :4252).  Each device counter changes only in the call
+  // that refreshes its host copy, so reading the counter block at the end of
+  // an iteration yields exactly those copies.
   int main_loop() {
     const bool join = p_.preserve_join != 0;
     EZ_RUN(c_loops());
     if (capped_) return EXTREMZ_ROUND_CAP;
     EZ_RUN(manifold_block());
     int nfc = h(C_NFC), nfc1 = h(C_NFC1);
-    int h_wmc = 0, h_wmin = 0;
     if (nfc == 0) {
       EZ_RUN(s_loops());
-      EZ_RUN(read_ctr());
-      h_wmc = h(C_WMC);
-      if (h_wmc == 0) EZ_RUN(saddle_loops());
+      if (h(C_WMC) == 0) EZ_RUN(saddle_loops());
     }
     if (nfc1 == 0 && join) {
       EZ_RUN(s_loops_join());
       EZ_RUN(read_ctr());
-      h_wmin = h(C_WMIN);
-      if (h_wmin == 0) EZ_RUN(saddle_loops_join());
+      if (h(C_WMIN) == 0) EZ_RUN(saddle_loops_join());
     }
-    EZ_RUN(read_ctr());
+    EZ_RUN(read_ctr());  // :5589-5599
+    auto snapshot = [&](int* c) {
+      const int v[11] = {nfc, nfc1, h(C_CMAX), h(C_CMIN), h(C_CSAD), h(C_WMC),
+                         h(C_WMC2), h(C_WSC), h(C_WMIN), h(C_WMIN2), h(C_WSCJ)};
+      std::memcpy(c, v, sizeof(v));
+    };
     nfc = h(C_NFC);
     nfc1 = h(C_NFC1);
-    int cfmax = h(C_CMAX), cfmin = h(C_CMIN), cfsad = h(C_CSAD);
-    h_wmin = h(C_WMIN);
-    h_wmc = h(C_WMC);
-    int h_wmin2 = h(C_WMIN2), h_wmc2 = h(C_WMC2), h_wsc = h(C_WSC), h_wscj = h(C_WSCJ);
+    int c[11];
+    snapshot(c);
     auto any = [&] {
-      return nfc > 0 || nfc1 > 0 || cfmax > 0 || cfmin > 0 || cfsad > 0 || h_wmc > 0 ||
-             h_wmc2 > 0 || h_wsc > 0 || h_wmin > 0 || h_wmin2 > 0 || h_wscj > 0;
+      for (int i = 0; i < 11; ++i)
+        if (c[i] > 0) return true;
+      return false;
     };
     while (any()) {
       if (outer_ >= p_.max_outer) {
@@ -703,13 +709,12 @@ class Corrector {
       nfc1 = h(C_NFC1);
       if (nfc == 0) {
         EZ_RUN(s_loops());
-        if (h_wmc == 0) EZ_RUN(saddle_loops());  // stale host copy (:5712)
+        if (h(C_WMC) == 0) EZ_RUN(saddle_loops());
       }
       if (nfc1 == 0 && join) {
         EZ_RUN(s_loops_join());
         EZ_RUN(read_ctr());
-        h_wmin = h(C_WMIN);
-        if (h_wmin == 0) EZ_RUN(saddle_loops_join());
+        if (h(C_WMIN) == 0) EZ_RUN(saddle_loops_join());
       }
       // Block 2 (:5749-5870).
       EZ_RUN(c_loops());
@@ -719,15 +724,12 @@ class Corrector {
       nfc1 = h(C_NFC1);
       if (nfc == 0) {
         EZ_RUN(s_loops());
-        EZ_RUN(read_ctr());
-        h_wmc = h(C_WMC);
-        if (h_wmc == 0) EZ_RUN(saddle_loops());
+        if (h(C_WMC) == 0) EZ_RUN(saddle_loops());
       }
       if (nfc1 == 0 && join) {
         EZ_RUN(s_loops_join());
         EZ_RUN(read_ctr());
-        h_wmin = h(C_WMIN);
-        if (h_wmin == 0) EZ_RUN(saddle_loops_join());
+        if (h(C_WMIN) == 0) EZ_RUN(saddle_loops_join());
       }
       // Block 3 (:5872-5979): detection only.
       EZ_RUN(c_loops());
@@ -743,11 +745,10 @@ class Corrector {
         launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, J);
         launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, J, 0);
         EZ_RUN(launched());
-        EZ_RUN(read_ctr());
-        h_wsc = h(C_WSC);
-        h_wmc = h(C_WMC);
-        h_wmc2 = h(C_WMC2);
-        emit(PH_DETECT3, h_wsc, h_wmc, h_wmc2);
+        if (trace_) {
+          EZ_RUN(read_ctr());
+          emit(PH_DETECT3, h(C_WSC), h(C_WMC), h(C_WMC2));
+        }
       }
       if (nfc1 == 0 && join) {
         EZ_RUN(zero(C_WMIN, 2));
@@ -757,22 +758,15 @@ class Corrector {
         launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, J);
         launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, J, 0);
         EZ_RUN(launched());
-        EZ_RUN(read_ctr());
-        h_wscj = h(C_WSCJ);
-        h_wmin2 = h(C_WMIN2);
-        h_wmin = h(C_WMIN);
       }
-      EZ_RUN(detect());
-      cfmax = h(C_CMAX);
-      cfmin = h(C_CMIN);
-      cfsad = h(C_CSAD);
+      EZ_RUN(detect());  // reads the whole counter block
+      snapshot(c);
       emit(PH_OUTER, outer_);
       EZ_RUN(checksum_emit());
     }
+    std::memcpy(hc_, c, sizeof(c));  // counters at loop exit
     if (!capped_ && p_.final_join) EZ_RUN(saddle_loops_join());  // unconditional (:5997)
     EZ_RUN(read_ctr());
-    int c[11] = {nfc, nfc1, cfmax, cfmin, cfsad, h_wmc, h_wmc2, h_wsc, h_wmin, h_wmin2, h_wscj};
-    std::memcpy(hc_, c, sizeof(c));
     return capped_ ? EXTREMZ_ROUND_CAP : EXTREMZ_OK;
   }
 #undef EZ_RUN

@@ -25,7 +25,7 @@ struct Job {
 
   int8_t* otype;      // original vertex type (-1, 0..5)
   uint16_t* olm;      // original lower-star direction mask
-  uint8_t* gate;      // bit0: next to an original 2-saddle; bit1: next to a 1-saddle
+  uint8_t* ocnt2; uint8_t* ocnt1;  // original row counts (compact copy of row[14])
   int* ds; int* as;   // original steepest ascent / descent roots
   int* dds; int* das; // decompressed roots
   int* ext;           // vertex -> index in the maxima / minima list
@@ -335,13 +335,47 @@ __global__ void __launch_bounds__(256) k_keep(Job<T> J, int epoch) {
 // at a root, so the global jump that follows moves a tile per hop.
 // Output: ds/as = first vertex outside the tile on the path, or the root.
 // ---------------------------------------------------------------------------
+// Direction components packed two bits per direction (component + 1), so a
+// runtime direction index decodes with a shift and a mask.
+__host__ __device__ constexpr unsigned pack_dir(int axis) {
+  unsigned p = 0;
+  for (int d = 0; d < kNumDirs; ++d)
+    p |= (unsigned)((axis == 0 ? dir_x(d) : axis == 1 ? dir_y(d) : dir_z(d)) + 1) << (2 * d);
+  return p;
+}
+__device__ __forceinline__ int ddx(int d) { return (int)((pack_dir(0) >> (2 * d)) & 3u) - 1; }
+__device__ __forceinline__ int ddy(int d) { return (int)((pack_dir(1) >> (2 * d)) & 3u) - 1; }
+__device__ __forceinline__ int ddz(int d) { return (int)((pack_dir(2) >> (2 * d)) & 3u) - 1; }
+
+// Follows a steepest path inside the tile from (cx, cy, cz) until it leaves
+// the tile or stops at a root; returns the global id of the first vertex
+// outside the tile, or of the root.
+__device__ __forceinline__ int follow_in_tile(const int8_t* dir, int cx, int cy, int cz, int bx,
+                                              int by, int bz, int W, int WH, int* err) {
+  int d = dir[(cz * TY + cy) * TX + cx];
+  for (int step = 0; d >= 0; ++step) {
+    const int nx = cx + ddx(d), ny = cy + ddy(d), nz = cz + ddz(d);
+    if ((unsigned)nx >= (unsigned)TX || (unsigned)ny >= (unsigned)TY || (unsigned)nz >= (unsigned)TZ)
+      return (bx + nx) + (by + ny) * W + (bz + nz) * WH;
+    cx = nx;
+    cy = ny;
+    cz = nz;
+    d = dir[(cz * TY + cy) * TX + cx];
+    if (step >= TX * TY * TZ) {  // a path cannot revisit a vertex; guard anyway
+      atomicOr(err, kErrTile);
+      break;
+    }
+  }
+  return (bx + cx) + (by + cy) * W + (bz + cz) * WH;
+}
+
 template <class T, bool kTma>
 __global__ void __launch_bounds__(256) k_direction(Job<T> J, const __grid_constant__ CUtensorMap map,
                                                    const T* __restrict__ a, int* __restrict__ ds,
                                                    int* __restrict__ as) {
   __shared__ Tile<T> s;
   __shared__ uint64_t bar;
-  __shared__ int phi[TZ * TY * TX], plo[TZ * TY * TX];
+  __shared__ int8_t hdir[TZ * TY * TX], ldir[TZ * TY * TX];
   const Dims g = J.dim;
   const int WH = g.W * g.H;
   const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
@@ -353,111 +387,72 @@ __global__ void __launch_bounds__(256) k_direction(Job<T> J, const __grid_consta
   for (int tz = 0; tz < TZ; ++tz) {
     const int li = (tz * TY + ty) * TX + tx;
     const int x = bx + tx, y = by + ty, z = bz + tz;
-    if (!(x < g.W && y < g.H && z < g.D)) {
-      phi[li] = -1;
-      plo[li] = -1;
-      continue;
-    }
-    const int v = x + y * g.W + z * WH;
-    const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
-    const T c = s.v[tz + 1][ty + 1][tx + kXOff];
-    // Steepest ascent: maximum of (value, id) over {v} and its neighbours,
-    // scanning ids in ascending order so that ">=" keeps the larger id on a
-    // tie; steepest descent scans in descending order with "<=".
-    // (Finite inputs: the scans start from -inf / +inf and always meet the
-    // centre, so no "first element" flag is needed.)
-    T hv = -T(INFINITY), lv = T(INFINITY);
     int hd = -1, ld = -1;
+    if (x < g.W && y < g.H && z < g.D) {
+      const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
+      const T c = s.v[tz + 1][ty + 1][tx + kXOff];
+      // Steepest ascent: maximum of (value, id) over {v} and its neighbours,
+      // scanning ids in ascending order so that ">=" keeps the larger id on a
+      // tie; steepest descent scans in descending order with "<=" (finite
+      // inputs: the scans start from -inf / +inf and always meet the centre).
+      T hv = -T(INFINITY), lv = T(INFINITY);
 #pragma unroll
-    for (int j = 0; j < kNumDirs; ++j) {
-      const int d = rank_dir(j);
-      if (j == kRankCentre && c >= hv) { hv = c; hd = -1; }
-      const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
-      if ((valid >> d & 1) && nv >= hv) { hv = nv; hd = d; }
-    }
+      for (int j = 0; j < kNumDirs; ++j) {
+        const int d = rank_dir(j);
+        if (j == kRankCentre && c >= hv) { hv = c; hd = -1; }
+        const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
+        if ((valid >> d & 1) && nv >= hv) { hv = nv; hd = d; }
+      }
 #pragma unroll
-    for (int j = kNumDirs - 1; j >= 0; --j) {
-      const int d = rank_dir(j);
-      const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
-      if ((valid >> d & 1) && nv <= lv) { lv = nv; ld = d; }
-      if (j == kRankCentre && c <= lv) { lv = c; ld = -1; }
+      for (int j = kNumDirs - 1; j >= 0; --j) {
+        const int d = rank_dir(j);
+        const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
+        if ((valid >> d & 1) && nv <= lv) { lv = nv; ld = d; }
+        if (j == kRankCentre && c <= lv) { lv = c; ld = -1; }
+      }
     }
-    // Local index when the target lies in this tile, else -(global id) - 1;
-    // a root (no steeper neighbour) is stored resolved.
-    auto enc = [&](int d) {
-      if (d < 0) return -v - 1;
-      const int ltx = tx + dir_x(d), lty = ty + dir_y(d), ltz = tz + dir_z(d);
-      const int gid = v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
-      if ((unsigned)ltx >= (unsigned)TX || (unsigned)lty >= (unsigned)TY || (unsigned)ltz >= (unsigned)TZ)
-        return -gid - 1;
-      return (ltz * TY + lty) * TX + ltx;
-    };
-    phi[li] = enc(hd);
-    plo[li] = enc(ld);
+    hdir[li] = (int8_t)hd;
+    ldir[li] = (int8_t)ld;
   }
   __syncthreads();
-  // In-place pointer jumping inside the tile; every step moves along the path,
-  // so it ends in O(log tile) steps.
-  for (int it = 0; it < 64; ++it) {
-    int changed = 0;
-    for (int tz = 0; tz < TZ; ++tz) {
-      const int li = (tz * TY + ty) * TX + tx;
-      int p = phi[li];
-      if (p >= 0) { phi[li] = phi[p]; changed = 1; }
-      p = plo[li];
-      if (p >= 0) { plo[li] = plo[p]; changed = 1; }
-    }
-    if (!__syncthreads_or(changed)) break;
-    if (it == 63 && threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
-  }
   for (int tz = 0; tz < TZ; ++tz) {
-    const int li = (tz * TY + ty) * TX + tx;
     const int x = bx + tx, y = by + ty, z = bz + tz;
     if (!(x < g.W && y < g.H && z < g.D)) continue;
     const int v = x + y * g.W + z * WH;
-    const int ph = phi[li], pl = plo[li];
-    ds[v] = ph < 0 ? -ph - 1 : v;
-    as[v] = pl < 0 ? -pl - 1 : v;
+    ds[v] = follow_in_tile(hdir, tx, ty, tz, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
+    as[v] = follow_in_tile(ldir, tx, ty, tz, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
   }
 }
 
-// Global pointer jumping for gated vertices (ComputeDescendingManifold /
-// ComputeAscendingManifold, :1514-1611): in place, with an iteration cap
-// after which the error word is set instead of spinning.
-__global__ void __launch_bounds__(256) k_jump(int* __restrict__ lab, const uint8_t* __restrict__ gate,
-                                              int bit, int N, int cap, int* err) {
+// Global pointer jumping of both label arrays (ComputeDescendingManifold /
+// ComputeAscendingManifold, :1514-1611), the two chains interleaved for
+// memory-level parallelism.  Labels always point further along the path, so
+// concurrent readers of a label being finalised see either value correctly.
+// Every vertex is resolved (the reference resolves descending labels only next
+// to original 2-saddles, the only places they are read).  Iterations are
+// capped; hitting the cap sets the error word instead of spinning.
+__global__ void __launch_bounds__(256) k_jump2(int* __restrict__ a, int* __restrict__ b, int N,
+                                               int cap, int* err) {
   const int stride = gridDim.x * blockDim.x;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
-    if (gate && !(gate[v] & bit)) continue;
-    int u = lab[v];
+    int u1 = a[v], u2 = b[v];
+    bool d1 = false, d2 = false;
     int it = 0;
-    for (; it < cap; ++it) {
-      const int w = lab[u];
-      if (w == u) break;
-      lab[v] = w;
-      u = w;
+    for (; it < cap && !(d1 && d2); ++it) {
+      if (!d1) {
+        const int w = a[u1];
+        if (w == u1) d1 = true;
+        else u1 = w;
+      }
+      if (!d2) {
+        const int w = b[u2];
+        if (w == u2) d2 = true;
+        else u2 = w;
+      }
     }
     if (it == cap) atomicOr(err, kErrJump);
-  }
-}
-
-// Gate bits from the original types: bit0 when a neighbour is an original
-// 2-saddle (type 2 or 3), bit1 when one is a 1-saddle (type 1 or 3)
-// (the is_saddle_neighbor tests at :1530-1548 and :1584-1601).
-template <class T>
-__global__ void k_gate(Job<T> J) {
-  const Dims g = J.dim;
-  const int stride = gridDim.x * blockDim.x;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < g.N; v += stride) {
-    int ids[kNumDirs];
-    const int n = neighbours(v, g, ids, nullptr);
-    uint8_t gb = 0;
-    for (int j = 0; j < n; ++j) {
-      const int t = J.otype[ids[j]];
-      if (t == 2 || t == 3) gb |= 1;
-      if (t == 1 || t == 3) gb |= 2;
-    }
-    J.gate[v] = gb;
+    a[v] = u1;
+    b[v] = u2;
   }
 }
 
@@ -634,21 +629,23 @@ __global__ void k_extreme_saddle(Job<T> J, int pass) {
   const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
   const int* sad = kMax ? J.sad2 : J.sad1;
   const int* rows = kMax ? J.orow2 : J.orow1;
-  const long long total = (long long)ns * kNumDirs;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += stride) {
-    const int i = (int)(e / kNumDirs), p = (int)(e % kNumDirs);
-    const int* row = rows + (long long)i * kRowStride;
-    if (p >= row[14]) continue;
-    const int m = J.ext[row[p]];
+  const uint8_t* ocnt = kMax ? J.ocnt2 : J.ocnt1;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+    const int cnt = ocnt[i];
+    if (cnt == 0) continue;
     const int s = sad[i];
     const K key = KeyOf<T>::enc(J.f[s] + T(0));  // -0 and +0 compare equal
-    if (pass == 0) {
-      if (kMax) atomicMax(J.ext_key + m, key);
-      else atomicMin(J.ext_key + m, key);
-    } else if (J.ext_key[m] == key) {
-      if (kMax) atomicMax(J.ext_id + m, s);
-      else atomicMin(J.ext_id + m, s);
+    const int* row = rows + (long long)i * kRowStride;
+    for (int p = 0; p < cnt; ++p) {
+      const int m = J.ext[row[p]];
+      if (pass == 0) {
+        if (kMax) atomicMax(J.ext_key + m, key);
+        else atomicMin(J.ext_key + m, key);
+      } else if (J.ext_key[m] == key) {
+        if (kMax) atomicMax(J.ext_id + m, s);
+        else atomicMin(J.ext_id + m, s);
+      }
     }
   }
 }
@@ -804,18 +801,60 @@ __device__ __forceinline__ int wn_candidates(const Job<T>& J, int s, int* ids) {
 //    (original count - 1), possibly stale when the new row is shorter.  So two
 //    persistent slots per row reproduce it: slot 0 takes the new entry 0 when
 //    the new row is non-empty, slot 1 takes the new entry k when the new row
-//    has more than k entries.  Entry k of the sorted row is found by counting
-//    (rank of each candidate), without materialising the sort.
+//    has more than k entries.  Entry 0 is the row's extreme label in the sort
+//    order and entry count-1 the opposite extreme, found in one pass; any other
+//    entry k is found by ranking the candidates (rare: the rows of both fields
+//    usually have the same length).
 //  * wrong-neighbour seeds: saddles with at least one candidate.
+template <class T, bool kSplit>
+__device__ __forceinline__ bool row_first(T v, int m, T bv, int bm) {
+  // "comes first in the row": descending for ascending rows, ascending else.
+  return kSplit ? above(v, m, bv, bm) : below(v, m, bv, bm);
+}
+
+template <class T, bool kSplit>
+__device__ __noinline__ int row_entry_k(const Job<T>& J, int s, int k) {
+  const int* lab = kSplit ? J.dds : J.das;
+  int ids[kNumDirs];
+  const int n = neighbours(s, J.dim, ids, nullptr);
+  const T sv = J.g[s];
+  int ml[kNumDirs];
+  T mv[kNumDirs];
+  int cnt = 0;
+  for (int j = 0; j < n; ++j) {
+    const int r = ids[j];
+    const T rv = J.g[r];
+    if (kSplit ? above(rv, r, sv, s) : below(rv, r, sv, s)) {
+      const int m = lab[r];
+      const T v = J.g[m];
+      if (!kSplit || tabs(T(v - sv)) >= J.thr) {
+        ml[cnt] = m;
+        mv[cnt] = v;
+        ++cnt;
+      }
+    }
+  }
+  for (int a = 0; a < cnt; ++a) {
+    int before = 0, same = 0;
+    for (int b = 0; b < cnt; ++b) {
+      before += row_first<T, kSplit>(mv[b], ml[b], mv[a], ml[a]);
+      same += ml[b] == ml[a];
+    }
+    if (before <= k && k < before + same) return ml[a];
+  }
+  return -1;
+}
+
 template <class T, bool kSplit>
 __global__ void __launch_bounds__(256) k_saddle_pass(Job<T> J) {
   const int ns = J.ctr[kSplit ? C_NS2 : C_NS1];
   const int* sad = kSplit ? J.sad2 : J.sad1;
-  const int* orow = kSplit ? J.orow2 : J.orow1;
+  const uint8_t* ocnt = kSplit ? J.ocnt2 : J.ocnt1;
   int* slots = kSplit ? J.drow2 : J.drow1;
   const int* lab = kSplit ? J.dds : J.das;
   const int* olab = kSplit ? J.ds : J.as;
   const Dims g = J.dim;
+  const int WH = g.W * g.H;
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < ns; base += stride) {
     const int i = base + threadIdx.x;
@@ -825,55 +864,53 @@ __global__ void __launch_bounds__(256) k_saddle_pass(Job<T> J) {
       s = sad[i];
       int x, y, z;
       coords(s, g, x, y, z);
-      const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
+      const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
       const T sv = J.g[s];
-      int ml[kNumDirs];
-      T mv[kNumDirs];
-      int valid = 0;
+      int cnt = 0, fm = -1, lm = -1;
+      T fv = T(0), lv = T(0);
 #pragma unroll
       for (int d = 0; d < kNumDirs; ++d) {
-        ml[d] = 0;
-        mv[d] = T(0);
-        if (!dir_valid(d, bc)) continue;
-        const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * g.W * g.H;
+        if (!(valid >> d & 1)) continue;
+        const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
         const T rv = J.g[r];
         if (kSplit ? above(rv, r, sv, s) : below(rv, r, sv, s)) {
           const int m = lab[r];
           if (m != olab[r]) has = true;
           const T v = J.g[m];
           if (!kSplit || tabs(T(v - sv)) >= J.thr) {
-            ml[d] = m;
-            mv[d] = v;
-            valid |= 1 << d;
+            if (cnt == 0 || row_first<T, kSplit>(v, m, fv, fm)) { fv = v; fm = m; }
+            if (cnt == 0 || row_first<T, kSplit>(lv, lm, v, m)) { lv = v; lm = m; }
+            ++cnt;
           }
         }
       }
-      const int ocnt = orow[(long long)i * kRowStride + 14];
-      if (ocnt > 0 && valid) {
-        const int k = ocnt - 1;
-        int first = -1, kth = -1;
-        const int cnt = __popc(valid);
-#pragma unroll
-        for (int d = 0; d < kNumDirs; ++d) {
-          if (!(valid >> d & 1)) continue;
-          int gt = 0, eq = 0;
-#pragma unroll
-          for (int e = 0; e < kNumDirs; ++e) {
-            if (!(valid >> e & 1)) continue;
-            const bool before = kSplit ? above(mv[e], ml[e], mv[d], ml[d])
-                                       : below(mv[e], ml[e], mv[d], ml[d]);
-            gt += before;
-            eq += ml[e] == ml[d];
-          }
-          if (gt == 0) first = ml[d];
-          if (gt <= k && k < gt + eq) kth = ml[d];
+      const int oc = ocnt[i];
+      if (oc > 0 && cnt > 0) {
+        const int k = oc - 1;
+        slots[2ll * i] = fm;
+        if (cnt > k) {
+          int kth;
+          if (k == cnt - 1) kth = lm;
+          else if (k == 0) kth = fm;
+          else kth = row_entry_k<T, kSplit>(J, s, k);
+          slots[2ll * i + 1] = kth;
         }
-        slots[2ll * i] = first;
-        if (cnt > k) slots[2ll * i + 1] = kth;
       }
     }
     const int slot = warp_append(J.ctr + C_CAND, has, 0xffffffffu);
     if (slot >= 0) J.cand[slot] = s;
+  }
+}
+
+// Compact copy of the original rows' counts (the only field of a row most
+// passes need).
+template <class T>
+__global__ void k_row_counts(Job<T> J) {
+  const int n2 = J.ctr[C_NS2], n1 = J.ctr[C_NS1];
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2 + n1; i += stride) {
+    if (i < n2) J.ocnt2[i] = (uint8_t)J.orow2[(long long)i * kRowStride + 14];
+    else J.ocnt1[i - n2] = (uint8_t)J.orow1[(long long)(i - n2) * kRowStride + 14];
   }
 }
 
@@ -1001,10 +1038,10 @@ __global__ void __launch_bounds__(256) k_wim_scan(Job<T> J) {
   int* flag = kMax ? J.flag2 : J.flag_min2;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+    const int cnt = (kMax ? J.ocnt2 : J.ocnt1)[i];
+    if (cnt == 0) continue;
     const int* o = orow + (long long)i * kRowStride;
     const int* d = drow + 2ll * i;  // slots: entry 0, entry (count - 1)
-    const int cnt = o[14];
-    if (cnt == 0) continue;
     if (o[0] != d[0]) atomicMin(first + J.ext[o[0]], i);
     const int k = cnt - 1;
     if (o[k] != d[1]) flag[J.ext[o[k]]] = 1;
@@ -1067,9 +1104,9 @@ __global__ void __launch_bounds__(256) k_wim_min2_scan(Job<T> J) {
   const int ns = J.ctr[C_NS1];
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
-    const int* o = J.orow1 + (long long)i * kRowStride;
-    const int cnt = o[14];
+    const int cnt = J.ocnt1[i];
     if (cnt == 0) continue;
+    const int* o = J.orow1 + (long long)i * kRowStride;
     const int k = cnt - 1;
     if (o[k] != J.drow1[2ll * i + 1]) atomicMin(J.first_sj + J.ext[o[k]], i);
   }
@@ -1099,20 +1136,31 @@ __global__ void __launch_bounds__(256) k_wis_scan(Job<T> J) {
   const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
   const int* sad = kMax ? J.sad2 : J.sad1;
   const int* rows = kMax ? J.orow2 : J.orow1;
+  const uint8_t* ocnt = kMax ? J.ocnt2 : J.ocnt1;
   const int* best = kMax ? J.largest : J.smallest;
   int* first = kMax ? J.first_s : J.first_sj;
-  const long long total = (long long)ns * kNumDirs;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += stride) {
-    const int i = (int)(e / kNumDirs), p = (int)(e % kNumDirs);
-    const int* row = rows + (long long)i * kRowStride;
-    if (p >= row[14]) continue;
-    const int m = J.ext[row[p]];
-    const int tb = best[m];
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+    const int cnt = ocnt[i];
+    if (cnt == 0) continue;
     const int s = sad[i];
-    const T gs = J.g[s], gt = J.g[tb];
-    const bool wrong = kMax ? above(gs, s, gt, tb) : below(gs, s, gt, tb);
-    if (wrong) atomicMin(first + m, i * kRowStride + p);
+    const T gs = J.g[s];
+    const int4* row4 = reinterpret_cast<const int4*>(rows + (long long)i * kRowStride);
+    int row[kRowStride];
+#pragma unroll
+    for (int q = 0; q < kRowStride / 4; ++q) {
+      const int4 t = row4[q];
+      row[4 * q] = t.x; row[4 * q + 1] = t.y; row[4 * q + 2] = t.z; row[4 * q + 3] = t.w;
+    }
+#pragma unroll
+    for (int p = 0; p < kNumDirs; ++p) {
+      if (p >= cnt) break;
+      const int m = J.ext[row[p]];
+      const int tb = best[m];
+      const T gt = J.g[tb];
+      const bool wrong = kMax ? above(gs, s, gt, tb) : below(gs, s, gt, tb);
+      if (wrong) atomicMin(first + m, i * kRowStride + p);
+    }
   }
 }
 

@@ -320,6 +320,10 @@ struct Corrector {
   // Device-side counters of the reference (:133, :150-152).
   int d_nfc = 0, d_nfc1 = 0, d_cfmax = 0, d_cfmin = 0, d_cfsad = 0;
   int d_wmc = 0, d_wmc2 = 0, d_wsc = 0, d_wmin = 0, d_wmin2 = 0, d_wscj = 0;
+  // File-scope host copies (:62): s_loops, saddle_loops and their join
+  // variants refresh them as a side effect (:3473-3476, :4236, :3498-3501,
+  // :4252); c_loops and r_loops take counters by value and refresh nothing.
+  int h_wmc = 0, h_wmc2 = 0, h_wsc = 0, h_wmin = 0, h_wmin2 = 0, h_wscj = 0;
 
   int cloop_rounds = 0, manifold_rounds = 0, max_cloop_rounds = 0;
   bool capped = false;
@@ -677,6 +681,8 @@ struct Corrector {
   void s_loops() {
     wrong_index_max();
     init_delta();
+    h_wmc = d_wmc;
+    h_wmc2 = d_wmc2;
     for (size_t p = 0; p < pmax1.size(); p += 2) {
       int fl = pmax1[p + 1];
       amax(fl, step_delta(fl));  // fix_wrong_index_max(0) (:3326-3344)
@@ -693,6 +699,8 @@ struct Corrector {
   void s_loops_join() {
     wrong_index_min();
     init_delta();
+    h_wmin = d_wmin;
+    h_wmin2 = d_wmin2;
     for (size_t p = 0; p < pmin1.size(); p += 2) {
       int t = pmin1[p];
       amax(t, step_delta(t));  // fix_wrong_index_min(0) (:3375-3391)
@@ -743,6 +751,7 @@ struct Corrector {
   void saddle_loops() {
     wrong_index_saddles();
     init_delta();
+    h_wsc = d_wsc;
     for (size_t p = 0; p < psad.size(); p += 2) {  // fix_wrong_index_saddle(0)
       int t = psad[p], fl = psad[p + 1];
       if (a[t] > a[fl] || (a[t] == a[fl] && t > fl)) continue;
@@ -760,6 +769,7 @@ struct Corrector {
   void saddle_loops_join() {
     wrong_index_saddles_join();
     init_delta();
+    h_wscj = d_wscj;
     emit(PH_SADDLE_JOIN, d_wscj);
     if (d_wscj > 0) {
       for (size_t p = 0; p < psadj.size(); p += 2) {
@@ -878,10 +888,11 @@ struct Corrector {
     if (capped) return 1;
     manifold_block();
     int h_nfc = d_nfc, h_nfc1 = d_nfc1;
-    int h_wmc = 0, h_wmin = 0;
+    h_wmc = 0;  // :5562-5563
+    h_wmc2 = 0;
     if (h_nfc == 0) {
       s_loops();
-      h_wmc = d_wmc;
+      h_wmc = d_wmc;  // :5570
       if (h_wmc == 0) saddle_loops();
     }
     if (h_nfc1 == 0 && preserve_join) {
@@ -889,12 +900,16 @@ struct Corrector {
       h_wmin = d_wmin;
       if (h_wmin == 0) saddle_loops_join();
     }
+    // :5589-5599: every host counter re-read.
     h_nfc = d_nfc;
     h_nfc1 = d_nfc1;
     int h_cfmax = d_cfmax, h_cfmin = d_cfmin, h_cfsad = d_cfsad;
     h_wmin = d_wmin;
     h_wmc = d_wmc;
-    int h_wmin2 = d_wmin2, h_wmc2 = d_wmc2, h_wsc = d_wsc, h_wscj = d_wscj;
+    h_wmin2 = d_wmin2;
+    h_wmc2 = d_wmc2;
+    h_wsc = d_wsc;
+    h_wscj = d_wscj;
     int outer = 0;
     auto any = [&] {
       return h_nfc > 0 || h_nfc1 > 0 || h_cfmax > 0 || h_cfmin > 0 || h_cfsad > 0 ||
@@ -915,7 +930,7 @@ struct Corrector {
       h_nfc1 = d_nfc1;
       if (h_nfc == 0) {
         s_loops();
-        if (h_wmc == 0) saddle_loops();  // stale host copy (:5712)
+        if (h_wmc == 0) saddle_loops();
       }
       if (h_nfc1 == 0 && preserve_join) {
         s_loops_join();
@@ -966,13 +981,14 @@ struct Corrector {
       emit(PH_OUTER, outer);
       checksum_emit();
     }
-    if (!capped && final_join) saddle_loops_join();  // unconditional (:5997)
-    if (outer_out) *outer_out = outer;
+    // Counters at loop exit (the loop test :5603-5605).
     if (counters) {
       int c[11] = {h_nfc, h_nfc1, h_cfmax, h_cfmin, h_cfsad, h_wmc,
                    h_wmc2, h_wsc, h_wmin, h_wmin2, h_wscj};
       std::memcpy(counters, c, sizeof(c));
     }
+    if (!capped && final_join) saddle_loops_join();  // unconditional (:5997)
+    if (outer_out) *outer_out = outer;
     return capped ? 1 : 0;
   }
 };
