@@ -24,12 +24,13 @@ from . import build as _build
 _lib = None
 _lock = threading.Lock()
 
-OK, ROUND_CAP, BAD_ARG, OOM, CUDA_ERR, DEVICE_TIMEOUT, NO_DEVICE = range(7)
+OK, ROUND_CAP, BAD_ARG, OOM, CUDA_ERR, DEVICE_TIMEOUT, NO_DEVICE, TOO_LARGE = range(8)
 F32, F64 = 0, 1
 
 # Every entry point declared in include/extremz.h.
 EXPORTS = ("extremz_version", "extremz_default_params", "extremz_ctx_create",
            "extremz_ctx_destroy", "extremz_correct_device", "extremz_correct_host",
+           "extremz_correct_device_noalloc", "extremz_noalloc_max_voxels",
            "extremz_lut", "extremz_status_string", "extremz_last_cuda_error")
 
 
@@ -115,6 +116,11 @@ def load(build_if_missing: bool = True):
         L.extremz_correct_host.argtypes = [vp, vp, vp, i32, i32, i32, i32,
                                            ctypes.POINTER(Params), ctypes.POINTER(Report), vp]
         L.extremz_correct_host.restype = i32
+        L.extremz_correct_device_noalloc.argtypes = [vp, vp, i32, i32, i32, i32,
+                                                     ctypes.POINTER(Params),
+                                                     ctypes.POINTER(Report), vp]
+        L.extremz_correct_device_noalloc.restype = i32
+        L.extremz_noalloc_max_voxels.restype = ctypes.c_longlong
         L.extremz_lut.argtypes = [vp, i32]
         L.extremz_lut.restype = i32
         L.extremz_status_string.argtypes = [i32]
@@ -243,6 +249,37 @@ def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, device: int = 0, *
     out = np.ascontiguousarray(decp).copy()
     rep = context(device).correct_host(np.ascontiguousarray(f), out, bound, **kw)
     return out, rep
+
+
+def noalloc_max_voxels() -> int:
+    return int(load().extremz_noalloc_max_voxels())
+
+
+def correct_device_noalloc(f, decp, bound: float, *, stream=None, **kw) -> CorrectionReport:
+    """Allocation-free correction of the CUDA tensor ``decp`` in place.
+
+    For callers that cannot allocate device memory while correcting (work
+    issued during CUDA graph capture, applications whose allocator owns the
+    device memory, real-time code that forbids allocation after start-up):
+    the workspace is a static device array of the library, for fields of at
+    most noalloc_max_voxels() voxels.  Calls share that array, so they must not
+    overlap on the GPU.  The first call on a device does a synchronous set-up;
+    make it before any stream capture.
+    """
+    import torch
+    assert f.is_cuda and decp.is_cuda and f.dtype == decp.dtype and f.shape == decp.shape
+    assert f.is_contiguous() and decp.is_contiguous()
+    dt = {torch.float32: F32, torch.float64: F64}[f.dtype]
+    w, h, d = _whd(tuple(f.shape))
+    if stream is None:
+        stream = torch.cuda.current_stream(f.device).cuda_stream
+    p = make_params(bound, **kw)
+    r = Report()
+    with torch.cuda.device(f.device):
+        st = load().extremz_correct_device_noalloc(f.data_ptr(), decp.data_ptr(), dt, w, h, d,
+                                                   ctypes.byref(p), ctypes.byref(r), stream)
+    _check(st)
+    return CorrectionReport.of(r)
 
 
 def lut() -> np.ndarray:

@@ -123,8 +123,10 @@ static bool make_tile_map(CUtensorMap* m, const T* ptr, const Dims& g) {
 struct Arena {
   char* base = nullptr;
   size_t cap = 0, used = 0;
+  bool fixed = false;  // borrowed storage: never freed or grown
   int reserve(size_t bytes) {
     if (bytes <= cap) return EXTREMZ_OK;
+    if (fixed) return EXTREMZ_OOM;
     if (base) cudaFree(base);
     base = nullptr;
     cap = 0;
@@ -148,13 +150,15 @@ struct Arena {
 
 struct Context {
   int device = 0;
+  bool has_tables = false;  // tables given by the owner instead of device_tables()
+  DeviceTables tables{};
   Arena arena;
   Arena stage;           // device copies of host fields (extremz_correct_host)
   int* h_ctr = nullptr;  // pinned copy of the counter block
   unsigned long long wn_round = 0;
   int wn_stamp = 0;
   ~Context() {
-    if (arena.base) cudaFree(arena.base);
+    if (arena.base && !arena.fixed) cudaFree(arena.base);
     if (stage.base) cudaFree(stage.base);
     if (h_ctr) cudaFreeHost(h_ctr);
   }
@@ -355,7 +359,8 @@ class Corrector {
   // ---------------------------------------------------------------- setup --
   int setup() {
     const int N = J.dim.N;
-    EZ_RUN(device_tables(&J.tb));
+    if (ctx_.has_tables) J.tb = ctx_.tables;
+    else EZ_RUN(device_tables(&J.tb));
     if (!ctx_.h_ctr) EZ_CHECK(cudaMallocHost(&ctx_.h_ctr, C_COUNT * sizeof(int)));
     grid_ = sm_count() * 8;
     const int nb = (N + kCpBlock - 1) / kCpBlock;
@@ -781,6 +786,92 @@ static int check_args(int dtype, long long W, long long H, long long D, const ex
   return EXTREMZ_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free correction (extremz_correct_device_noalloc).
+//
+// Some callers cannot allocate device memory at the time they correct a
+// field: code that runs while a CUDA graph is being captured, allocators
+// that own all of the device's memory, or real-time paths that forbid
+// allocation after start-up.  For them the whole workspace of one correction
+// lives in a fixed-size static device array, and the lookup table in static
+// device arrays, so a call allocates nothing.  The array is sized for the
+// worst case of EXTREMZ_NOALLOC_MAX_VOXELS voxels and every GPU that loads
+// the library keeps it until the process exits.
+// ---------------------------------------------------------------------------
+constexpr long long kNoAllocMaxVoxels = EXTREMZ_NOALLOC_MAX_VOXELS;
+// Worst case of the workspace layout (every voxel a critical point of every
+// kind, 8-byte values): 297 bytes per voxel plus per-array alignment.
+constexpr size_t kNoAllocScratchBytes = (size_t)kNoAllocMaxVoxels * 320 + (1u << 20);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static __device__ int8_t g_noalloc_lut[kLutSize];
+static __device__ int g_noalloc_key_offset[64];
+
+struct NoAllocDevice {
+  bool ready = false;
+  Context ctx;
+  int host_ctr[C_COUNT];  // pageable host copy of the counter block
+};
+static std::mutex g_noalloc_mu;
+static NoAllocDevice g_noalloc[64];
+
+// Once per device, with that device current: the device addresses of the
+// static arrays (a host-side name of a __device__ array is not a device
+// address) and the lookup table upload.
+static int noalloc_setup(int dev) {
+  NoAllocDevice& d = g_noalloc[dev];
+  if (d.ready) return EXTREMZ_OK;
+  void* scratch = nullptr;
+  void* lut = nullptr;
+  void* keys = nullptr;
+  EZ_CHECK(cudaGetSymbolAddress(&scratch, g_noalloc_scratch));
+  EZ_CHECK(cudaGetSymbolAddress(&lut, g_noalloc_lut));
+  EZ_CHECK(cudaGetSymbolAddress(&keys, g_noalloc_key_offset));
+  const HostTables& t = host_tables();
+  EZ_CHECK(cudaMemcpyToSymbol(g_noalloc_lut, t.lut, kLutSize));
+  EZ_CHECK(cudaMemcpyToSymbol(g_noalloc_key_offset, t.key_offset, 64 * sizeof(int)));
+  d.ctx.device = dev;
+  d.ctx.has_tables = true;
+  d.ctx.tables.lut = static_cast<const int8_t*>(lut);
+  d.ctx.tables.key_offset = static_cast<const int*>(keys);
+  d.ctx.arena.base = static_cast<char*>(scratch);
+  d.ctx.arena.cap = kNoAllocScratchBytes;
+  d.ctx.arena.fixed = true;
+  d.ctx.h_ctr = d.host_ctr;
+  d.ready = true;
+  return EXTREMZ_OK;
+}
+
+static int correct_noalloc(const void* d_orig, void* d_decp, int dtype, int width, int height,
+                           int depth, const extremz_params* params, extremz_report* report,
+                           void* stream) {
+  if (!d_orig || !d_decp || !params) return EXTREMZ_BAD_ARG;
+  int rc = check_args(dtype, width, height, depth, params);
+  if (rc != EXTREMZ_OK) return rc;
+  if ((long long)width * height * depth > kNoAllocMaxVoxels) return EXTREMZ_TOO_LARGE;
+  int dev = 0;
+  EZ_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return EXTREMZ_BAD_ARG;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  rc = noalloc_setup(dev);
+  if (rc != EXTREMZ_OK) return rc;
+  if (report) std::memset(report, 0, sizeof(*report));
+  extremz_params p = *params;
+  p.flags &= ~EXTREMZ_FLAG_PROFILE;  // no timing events in this mode
+  cudaStream_t st = (cudaStream_t)stream;
+  Context& ctx = g_noalloc[dev].ctx;
+  if (dtype == EXTREMZ_F32) {
+    Corrector<float> c(ctx, (const float*)d_orig, (float*)d_decp, width, height, depth, p, st,
+                       nullptr, 0);
+    rc = c.run(report);
+  } else {
+    Corrector<double> c(ctx, (const double*)d_orig, (double*)d_decp, width, height, depth, p, st,
+                        nullptr, 0);
+    rc = c.run(report);
+  }
+  if (report) report->status = rc;
+  return rc;
+}
+
 }  // namespace extremz
 
 using namespace extremz;
@@ -892,6 +983,16 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
   return (extremz_status)rc;
 }
 
+extremz_status extremz_correct_device_noalloc(const void* d_orig, void* d_decp, int dtype,
+                                              int width, int height, int depth,
+                                              const extremz_params* params,
+                                              extremz_report* report, void* stream) {
+  return (extremz_status)correct_noalloc(d_orig, d_decp, dtype, width, height, depth, params,
+                                         report, stream);
+}
+
+long long extremz_noalloc_max_voxels(void) { return kNoAllocMaxVoxels; }
+
 int extremz_lut(int32_t* out, int n) {
   if (!out || n < kLutSize) return -1;
   const HostTables& t = host_tables();
@@ -908,6 +1009,8 @@ const char* extremz_status_string(int status) {
     case EXTREMZ_CUDA_ERR: return "CUDA error";
     case EXTREMZ_DEVICE_TIMEOUT: return "device-side iteration limit reached";
     case EXTREMZ_NO_DEVICE: return "no CUDA device";
+    case EXTREMZ_TOO_LARGE:
+      return "field larger than the static workspace of the allocation-free entry point";
     default: return "unknown status";
   }
 }

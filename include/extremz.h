@@ -33,7 +33,8 @@ typedef enum {
   EXTREMZ_OOM = 3,
   EXTREMZ_CUDA_ERR = 4,
   EXTREMZ_DEVICE_TIMEOUT = 5, /* a device-side iteration limit was hit */
-  EXTREMZ_NO_DEVICE = 6
+  EXTREMZ_NO_DEVICE = 6,
+  EXTREMZ_TOO_LARGE = 7       /* beyond EXTREMZ_NOALLOC_MAX_VOXELS (noalloc entry point) */
 } extremz_status;
 
 typedef enum { EXTREMZ_F32 = 0, EXTREMZ_F64 = 1 } extremz_dtype;
@@ -138,6 +139,35 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
                                     int dtype, int width, int height, int depth,
                                     const extremz_params* params, extremz_report* report,
                                     void* stream);
+
+/*
+ * Allocation-free variant of extremz_correct_device, for callers that cannot
+ * allocate device memory when they correct a field: work issued during CUDA
+ * graph capture, applications whose allocator owns all of the device memory,
+ * and real-time code that forbids allocation after start-up.
+ * No counterpart in the reference: it always allocates its ~60 device arrays
+ * in main() (src/ExtreM_cuda.cu:4997-5185).
+ *
+ * The whole workspace is a static device array sized for at most
+ * EXTREMZ_NOALLOC_MAX_VOXELS voxels (about 21 MB, held by every GPU that loads
+ * the library until the process exits); larger fields return
+ * EXTREMZ_TOO_LARGE without touching the device.  The call makes no
+ * cudaMalloc, cudaFree or other allocating call.  Inputs and outputs are the
+ * caller's, as for extremz_correct_device, on the current device and the given
+ * stream.  The first call on a device looks up the static arrays' device
+ * addresses and uploads the lookup table (synchronously); make that first call
+ * before any stream capture.  All calls on a device share the one workspace,
+ * so calls that overlap on the GPU race: issue them one after another.  Every
+ * call clears what it needs zeroed itself.  Profiling and tracing are off.
+ */
+#define EXTREMZ_NOALLOC_MAX_VOXELS 65536
+extremz_status extremz_correct_device_noalloc(const void* d_orig, void* d_decp, int dtype,
+                                              int width, int height, int depth,
+                                              const extremz_params* params,
+                                              extremz_report* report, void* stream);
+
+/* EXTREMZ_NOALLOC_MAX_VOXELS of the loaded library. */
+long long extremz_noalloc_max_voxels(void);
 
 /* The critical-point lookup table in the layout of the reference's
  * src/LUT.bin (24 800 int32, read by loadLUTToGPU, src/ExtreM_cuda.cu:244-260).

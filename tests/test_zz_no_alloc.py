@@ -1,0 +1,65 @@
+"""The allocation-free entry point gives the same field as the regular one.
+
+extremz_correct_device_noalloc serves callers that cannot allocate device
+memory while they correct a field (work issued during CUDA graph capture, an
+application allocator that owns the device memory, real-time code without
+allocation after start-up).  Its workspace is a static device array shared by
+all calls, so two calls in a row must both match the regular entry point: the
+second call must not see anything the first one left in the array.  This file
+is collected last so that a failure here stops a -x run only after everything
+else has run.
+"""
+
+import numpy as np
+import pytest
+
+from extrem_z_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(q=4, edit_type=1, max_outer=500, max_cloop_rounds=100000, final_join=True)
+
+
+def _regular(f, decp, eb):
+    import torch
+    from extrem_z_b200 import api
+    tf = torch.from_numpy(f).cuda()
+    tg = torch.from_numpy(decp.copy()).cuda()
+    rep, _ = api.Context(0).correct_device(tf, tg, eb, **KW)
+    torch.cuda.synchronize()
+    return tg.cpu().numpy(), rep
+
+
+def _noalloc(f, decp, eb):
+    import torch
+    from extrem_z_b200 import api
+    tf = torch.from_numpy(f).cuda()
+    tg = torch.from_numpy(decp.copy()).cuda()
+    rep = api.correct_device_noalloc(tf, tg, eb, **KW)
+    torch.cuda.synchronize()
+    return tg.cpu().numpy(), rep
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_noalloc_matches_regular_entry_point_twice(dtype):
+    from extrem_z_b200 import api
+    fld = synth.make_field(40, 32, 24, n_gauss=16, seed=31, rel=1e-3, dtype=dtype)
+    assert fld.f.size <= api.noalloc_max_voxels()
+    ref, rrep = _regular(fld.f, fld.decp, fld.eb)
+    # Bit-exact (the tolerance of every parity test here): same bytes.
+    for _ in range(2):
+        out, rep = _noalloc(fld.f, fld.decp, fld.eb)
+        assert rep.status == rrep.status == 0
+        assert rep.outer_iters == rrep.outer_iters
+        assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+
+
+def test_noalloc_rejects_fields_beyond_its_maximum():
+    import torch
+    from extrem_z_b200 import api
+    n = api.noalloc_max_voxels()
+    d = n // (64 * 64) + 1
+    f = torch.zeros((d, 64, 64), dtype=torch.float32, device="cuda")
+    with pytest.raises(api.ExtremzError) as ei:
+        api.correct_device_noalloc(f, f.clone(), 0.1, **KW)
+    assert ei.value.status == api.TOO_LARGE
