@@ -62,9 +62,10 @@ def dominant_bytes_per_launch(n: int, s: int) -> int:
     return n * (s + 8)
 
 
-# DRAM bytes per voxel per k_direction launch from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum over voxels), by value size; None until captured.
-MEASURED_TRAFFIC_PER_VOXEL = {8: None, 4: None}
+# DRAM bytes per voxel per k_direction launch from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum over voxels, 256^3 field), by
+# value size (profiles/k_direction_256cube_f64.md); None where not captured.
+MEASURED_TRAFFIC_PER_VOXEL = {8: (134.239488e6 + 96.382976e6) / 256 ** 3, 4: None}
 
 
 def measured_peaks():
@@ -140,8 +141,9 @@ def dist_setup():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        backend = "nccl" if torch.cuda.is_available() else "gloo"
-        if torch.cuda.is_available():
+        backend = os.environ.get("EXTREMZ_DIST_BACKEND") or (
+            "nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
             torch.cuda.set_device(local)
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
@@ -158,7 +160,7 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
     t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
@@ -173,8 +175,8 @@ def crop(field, edge: int):
 
 def time_oracle(field, edge: int, threads: int):
     """Oracle correction of a crop; returns (seconds, voxels, report)."""
-    os.environ["OMP_NUM_THREADS"] = str(threads)
     from oracle import ffi
+    ffi.set_threads(threads)
     f, g = crop(field, edge)
     t0 = time.perf_counter()
     _, rep, _ = ffi.correct(f, g, field.eb, q=PARAMS["q"], edit_type=PARAMS["edit_type"],

@@ -45,7 +45,8 @@ class Params(ctypes.Structure):
                 ("q", ctypes.c_int), ("edit_type", ctypes.c_int),
                 ("max_outer", ctypes.c_int), ("max_cloop_rounds", ctypes.c_int),
                 ("final_join", ctypes.c_int), ("preserve_join", ctypes.c_int),
-                ("flags", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+                ("flags", ctypes.c_int), ("device_iter_cap", ctypes.c_int),
+                ("reserved", ctypes.c_int * 4)]
 
 
 class Report(ctypes.Structure):
@@ -146,7 +147,7 @@ def _check(st: int, allow_cap: bool = True):
 def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 1,
                 max_outer: int = 1000, max_cloop_rounds: int = 100000,
                 final_join: bool = True, preserve_join: bool = False,
-                profile=False, tma: bool = True) -> Params:
+                profile=False, tma: bool = True, device_iter_cap: int = 0) -> Params:
     """profile: False, True (time every kernel class) or an iterable of class
     names from KCLASS_NAMES to time only those."""
     p = Params()
@@ -154,6 +155,7 @@ def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 
     p.bound, p.thr, p.q, p.edit_type = float(bound), float(thr), int(q), int(edit_type)
     p.max_outer, p.max_cloop_rounds = int(max_outer), int(max_cloop_rounds)
     p.final_join, p.preserve_join = int(bool(final_join)), int(bool(preserve_join))
+    p.device_iter_cap = int(device_iter_cap)
     p.flags = 0 if tma else FLAG_NO_TMA
     if profile:
         p.flags |= FLAG_PROFILE

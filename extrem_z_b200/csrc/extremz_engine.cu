@@ -250,16 +250,21 @@ class Corrector {
 
   CUtensorMap map_f_, map_g_;
   bool tma_f_ = false, tma_g_ = false;
+  // The job descriptor lives in device memory; every per-round kernel takes
+  // the descriptor array and a selection (here: the one job).
+  Job<T>* jobs_dev_ = nullptr;
+  CUtensorMap* maps_dev_ = nullptr;
+  Sel sel1_;
 
-  template <bool kDetect>
-  void launch_classify(int cls, const T* a, bool tma, const CUtensorMap& m) {
-    if (tma) launch(cls, k_classify<T, kDetect, true>, tile_grid(), 256, J, m, a);
-    else launch(cls, k_classify<T, kDetect, false>, tile_grid(), 256, J, m, a);
+  const Job<T>* jobs() const { return jobs_dev_; }
+  int ntiles() const {
+    return ((J.dim.W + TX - 1) / TX) * ((J.dim.H + TY - 1) / TY) * ((J.dim.D + TZ - 1) / TZ);
   }
-  void launch_direction(const T* a, bool tma, const CUtensorMap& m, int* ds, int* as) {
-    if (tma) launch(K_DIRECTION, k_direction<T, true>, tile_grid(), 256, J, m, a, ds, as);
-    else launch(K_DIRECTION, k_direction<T, false>, tile_grid(), 256, J, m, a, ds, as);
+  int upload_job() {
+    EZ_CHECK(cudaMemcpyAsync(jobs_dev_, &J, sizeof(J), cudaMemcpyHostToDevice, st_));
+    return EXTREMZ_OK;
   }
+  void swap_lists(int which) { launch(K_OTHER, k_swap_lists<T>, 1, 32, jobs_dev_, sel1_, which); }
 
   long long launches_ = 0;
   bool profile_ = false;
@@ -315,6 +320,8 @@ class Corrector {
     for (cudaEvent_t e : pool_) cudaEventDestroy(e);
     pool_.clear();
   }
+
+  int iter_cap() const { return p_.device_iter_cap > 0 ? p_.device_iter_cap : J.dim.N + 1; }
 
   int sm_count() {
     int dev = 0, n = 148;
@@ -414,12 +421,27 @@ class Corrector {
     J.cand = A.take<int>(N); J.cand_next = A.take<int>(N);
     J.flagged = A.take<int>(N); J.flagged1 = A.take<int>(N);
     int* bcount = A.take<int>(4ll * nb);
+    jobs_dev_ = A.take<Job<T>>(1);
+    maps_dev_ = A.take<CUtensorMap>(2);
+    if (!jobs_dev_ || !maps_dev_) return EXTREMZ_OOM;
+    EZ_CHECK(cudaMemcpyAsync(maps_dev_, &map_f_, sizeof(CUtensorMap), cudaMemcpyHostToDevice, st_));
+    EZ_CHECK(cudaMemcpyAsync(maps_dev_ + 1, &map_g_, sizeof(CUtensorMap), cudaMemcpyHostToDevice, st_));
+    J.map_f = maps_dev_;
+    J.map_g = maps_dev_ + 1;
+    J.tma_f = tma_f_;
+    J.tma_g = tma_g_;
+    std::memset(&sel1_, 0, sizeof(sel1_));
+    sel1_.n = 1;
+    sel1_.idx[0] = 0;
+    sel1_.off[0] = 0;
+    sel1_.off[1] = ntiles();
+    EZ_RUN(upload_job());
     EZ_CHECK(cudaMemsetAsync(ctr_, 0, C_COUNT * sizeof(int), st_));
 
     // Original classification and manifolds.
-    launch_classify<false>(K_SETUP, J.f, tma_f_, map_f_);
-    launch_direction(J.f, tma_f_, map_f_, J.ds, J.as);
-    launch(K_JUMP, k_jump2, grid_, 256, J.ds, J.as, N, N, ctr_ + C_ERROR);
+    launch(K_SETUP, k_classify<T, false>, ntiles(), 256, jobs(), sel1_);
+    launch(K_DIRECTION, k_direction<T, false>, ntiles(), 256, jobs(), sel1_);
+    launch(K_JUMP, k_jump2<T, false>, grid_, 256, jobs(), sel1_, iter_cap());
     EZ_RUN(launched());
     // Critical-point lists in ascending id.
     launch(K_OTHER, k_cp_count, nb, kCpBlock, J.otype, N, bcount);
@@ -443,6 +465,7 @@ class Corrector {
     J.ext_key = A.take<K>(ne);
     J.ext_id = A.take<int>(ne);
     checksum_ = A.take<unsigned long long>(8);
+    EZ_RUN(upload_job());
     launch(K_OTHER, k_cp_write, nb, kCpBlock, J.otype, N, bcount, J.sad2, J.sad1, J.maxima, J.minima);
     launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
     launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.f, J.ds, J.sad2, C_NS2, J.orow2);
@@ -508,16 +531,15 @@ class Corrector {
   int detect() {
     if (!dense_done_) {
       EZ_RUN(zero(C_MM, 4));
-      launch_classify<true>(K_DETECT, J.g, tma_g_, map_g_);
+      launch(K_DETECT, k_classify<T, true>, ntiles(), 256, jobs(), sel1_);
       dense_done_ = true;
     } else {
       ++detect_epoch_;
       EZ_RUN(zero(C_MM_NEXT));
       EZ_RUN(zero(C_CMAX, 3));
-      launch(K_DETECT, k_redetect<T>, grid_, 256, J, detect_epoch_);
-      launch(K_DETECT, k_keep<T>, grid_, 256, J, detect_epoch_);
-      std::swap(J.mm, J.mm_next);
-      EZ_CHECK(cudaMemcpyAsync(ctr_ + C_MM, ctr_ + C_MM_NEXT, 4, cudaMemcpyDeviceToDevice, st_));
+      launch(K_DETECT, k_redetect<T>, grid_, 256, jobs(), sel1_, detect_epoch_);
+      launch(K_DETECT, k_keep<T>, grid_, 256, jobs(), sel1_, detect_epoch_);
+      swap_lists(0);
     }
     EZ_RUN(zero(C_DIRTY));
     ++dirty_epoch_;
@@ -528,7 +550,7 @@ class Corrector {
   }
 
   int apply() {
-    launch(K_APPLY, k_apply<T>, grid_, 256, J, dirty_epoch_);
+    launch(K_APPLY, k_apply<T>, grid_, 256, jobs(), sel1_, dirty_epoch_);
     return launched();
   }
 
@@ -544,7 +566,7 @@ class Corrector {
       ++rounds;
       ++cloop_rounds_;
       EZ_RUN(zero(C_TOUCHED));
-      launch(K_PROPOSE, k_propose_cp<T>, grid_, 256, J);
+      launch(K_PROPOSE, k_propose_cp<T>, grid_, 256, jobs(), sel1_);
       EZ_RUN(launched());
       EZ_RUN(apply());
       EZ_RUN(detect());
@@ -560,8 +582,8 @@ class Corrector {
   int manifold_block() {
     ++manifold_rounds_;
     const int N = J.dim.N;
-    launch_direction(J.g, tma_g_, map_g_, J.dds, J.das);
-    launch(K_JUMP, k_jump2, grid_, 256, J.dds, J.das, N, N, ctr_ + C_ERROR);
+    launch(K_DIRECTION, k_direction<T, true>, ntiles(), 256, jobs(), sel1_);
+    launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs(), sel1_, iter_cap());
     const int stamp = ++ctx_.wn_stamp;
     EZ_RUN(zero(C_NFC, 2));
     EZ_RUN(resolve_side<true>(stamp));
@@ -576,25 +598,24 @@ class Corrector {
   template <bool kSplit>
   int resolve_side(int stamp) {
     EZ_RUN(zero(C_CAND));
-    launch(K_ROWS, k_saddle_pass<T, kSplit>, grid_, 256, J);
+    launch(K_ROWS, k_saddle_pass<T, kSplit>, grid_, 256, jobs(), sel1_);
     const int kRounds = 3;
     for (int r = 0; r < kRounds; ++r) {
       const unsigned long long round = ++ctx_.wn_round;
       EZ_RUN(zero(C_CAND_NEXT));
-      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, J, round, stamp);
-      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, J, round, stamp);
-      std::swap(J.cand, J.cand_next);
-      EZ_CHECK(cudaMemcpyAsync(ctr_ + C_CAND, ctr_ + C_CAND_NEXT, 4, cudaMemcpyDeviceToDevice, st_));
+      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, jobs(), sel1_, round, stamp);
+      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, jobs(), sel1_, round, stamp);
+      swap_lists(1);
     }
-    launch(K_WRONG_NBR, k_wn_sequential<T, kSplit>, 1, 1, J, stamp);
+    launch(K_WRONG_NBR, k_wn_sequential<T, kSplit>, 1, 1, jobs(), sel1_, stamp);
     return launched();
   }
 
   // r_loops (:4210-4227).
   int r_loops() {
     EZ_RUN(zero(C_TOUCHED));
-    launch(K_FIXPATH, k_fixpath<T, true>, grid_, 256, J);
-    launch(K_FIXPATH, k_fixpath<T, false>, grid_, 256, J);
+    launch(K_FIXPATH, k_fixpath<T, true>, grid_, 256, jobs(), sel1_, iter_cap());
+    launch(K_FIXPATH, k_fixpath<T, false>, grid_, 256, jobs(), sel1_, iter_cap());
     EZ_RUN(launched());
     return apply();
   }
@@ -603,8 +624,8 @@ class Corrector {
   int s_loops() {
     EZ_RUN(zero(C_WMC, 2));
     EZ_RUN(zero(C_TOUCHED));
-    launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, J);
-    launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, J, 1);
+    launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs(), sel1_);
+    launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, jobs(), sel1_, 1);
     EZ_RUN(launched());
     EZ_RUN(apply());
     // s_loops refreshes the reference's file-scope host copies (:3473-3476);
@@ -618,8 +639,8 @@ class Corrector {
   int saddle_loops() {
     EZ_RUN(zero(C_WSC));
     EZ_RUN(zero(C_TOUCHED));
-    launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, J);
-    launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, J, 1);
+    launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs(), sel1_);
+    launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs(), sel1_, 1);
     EZ_RUN(launched());
     EZ_RUN(apply());
     if (trace_) {
@@ -633,10 +654,10 @@ class Corrector {
   int s_loops_join() {
     EZ_RUN(zero(C_WMIN, 2));
     EZ_RUN(zero(C_TOUCHED));
-    launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, J);
-    launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, J, 1);
-    launch(K_OTHER, k_wim_min2_scan<T>, grid_, 256, J);
-    launch(K_OTHER, k_wim_min2_collect<T>, grid_, 256, J);
+    launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, jobs(), sel1_);
+    launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, jobs(), sel1_, 1);
+    launch(K_OTHER, k_wim_min2_scan<T>, grid_, 256, jobs(), sel1_);
+    launch(K_OTHER, k_wim_min2_collect<T>, grid_, 256, jobs(), sel1_);
     EZ_RUN(launched());
     EZ_RUN(apply());
     if (trace_) {
@@ -650,8 +671,8 @@ class Corrector {
   int saddle_loops_join() {
     EZ_RUN(zero(C_WSCJ));
     EZ_RUN(zero(C_TOUCHED));
-    launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, J);
-    launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, J, 1);
+    launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs(), sel1_);
+    launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs(), sel1_, 1);
     EZ_RUN(launched());
     EZ_RUN(apply());
     if (trace_) {
@@ -745,10 +766,10 @@ class Corrector {
       if (nfc == 0) {
         EZ_RUN(zero(C_WMC, 2));
         EZ_RUN(zero(C_WSC));
-        launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, J);
-        launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, J, 0);
-        launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, J);
-        launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, J, 0);
+        launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs(), sel1_);
+        launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, jobs(), sel1_, 0);
+        launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs(), sel1_);
+        launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs(), sel1_, 0);
         EZ_RUN(launched());
         if (trace_) {
           EZ_RUN(read_ctr());
@@ -758,10 +779,10 @@ class Corrector {
       if (nfc1 == 0 && join) {
         EZ_RUN(zero(C_WMIN, 2));
         EZ_RUN(zero(C_WSCJ));
-        launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, J);
-        launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, J, 0);
-        launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, J);
-        launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, J, 0);
+        launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, jobs(), sel1_);
+        launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, jobs(), sel1_, 0);
+        launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs(), sel1_);
+        launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs(), sel1_, 0);
         EZ_RUN(launched());
       }
       EZ_RUN(detect());  // reads the whole counter block
@@ -782,7 +803,7 @@ static int check_args(int dtype, long long W, long long H, long long D, const ex
   if (W <= 0 || H <= 0 || D <= 0) return EXTREMZ_BAD_ARG;
   if (W * H * D >= (1ll << kCatShift)) return EXTREMZ_BAD_ARG;
   if (p->q <= 0 || (p->edit_type != 0 && p->edit_type != 1)) return EXTREMZ_BAD_ARG;
-  if (p->max_outer < 0 || p->max_cloop_rounds < 0) return EXTREMZ_BAD_ARG;
+  if (p->max_outer < 0 || p->max_cloop_rounds < 0 || p->device_iter_cap < 0) return EXTREMZ_BAD_ARG;
   return EXTREMZ_OK;
 }
 
@@ -896,6 +917,7 @@ void extremz_default_params(extremz_params* p) {
   p->final_join = 1;
   p->preserve_join = 0;
   p->flags = 0;
+  p->device_iter_cap = 0;
 }
 
 extremz_status extremz_ctx_create(int device, extremz_ctx** out) {

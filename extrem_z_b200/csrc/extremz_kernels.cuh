@@ -56,6 +56,21 @@ struct Job {
 
   int* ctr;  // device counters, see Ctr
   DeviceTables tb;
+  const CUtensorMap* map_f;  // tile maps of f and g in device memory (when tma_f / tma_g)
+  const CUtensorMap* map_g;
+  int tma_f, tma_g;
+};
+
+// Jobs served by one launch.  Every per-round kernel takes the device array of
+// job descriptors and a selection: indices into that array and, for tile
+// kernels, the exclusive prefix of the selected jobs' tile counts (a block's
+// flat index picks its job by binary search).  A plain correction is a
+// selection of one job.
+constexpr int kMaxSel = 64;
+struct Sel {
+  int n;
+  int idx[kMaxSel];
+  int off[kMaxSel + 1];
 };
 
 // Indices into the device counter block.
@@ -89,14 +104,34 @@ struct alignas(128) Tile {
   T v[SZ][SY][SX];
 };
 
+// Job and tile origin of a tile kernel's block.
+template <class T>
+__device__ __forceinline__ const Job<T>& tile_job(const Job<T>* __restrict__ jobs, const Sel& sel,
+                                                  int& bx, int& by, int& bz) {
+  const int t = blockIdx.x;
+  int lo = 0, hi = sel.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sel.off[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const Job<T>& J = jobs[sel.idx[lo]];
+  const int lt = t - sel.off[lo];
+  const int ntx = (J.dim.W + TX - 1) / TX, nty = (J.dim.H + TY - 1) / TY;
+  bx = (lt % ntx) * TX;
+  by = ((lt / ntx) % nty) * TY;
+  bz = (lt / (ntx * nty)) * TZ;
+  return J;
+}
+
 // Halo tile: TMA box (one bulk tensor copy, zero fill outside the grid) when
 // the field's row stride allows it, else plain loads with every thread's loads
 // issued before its first shared store.  Outside-grid entries are never read.
-template <class T, bool kTma>
+template <class T>
 __device__ __forceinline__ bool load_tile(Tile<T>& s, uint64_t* bar, const CUtensorMap* map,
-                                          const T* __restrict__ a, const Dims& g, int bx, int by,
-                                          int bz) {
-  if (kTma) {
+                                          bool tma, const T* __restrict__ a, const Dims& g, int bx,
+                                          int by, int bz) {
+  if (tma) {
     if (threadIdx.x == 0) {
       mbar_init(bar, 1);
       mbar_expect_tx(bar, (unsigned)sizeof(Tile<T>));
@@ -195,14 +230,18 @@ __device__ __forceinline__ void count_cats(int* ctr, int cat) {
   }
 }
 
-template <class T, bool kDetect, bool kTma>
-__global__ void __launch_bounds__(256) k_classify(Job<T> J, const __grid_constant__ CUtensorMap map,
-                                                  const T* __restrict__ a) {
+// kDetect = false classifies f (setup), true classifies g (detection).
+template <class T, bool kDetect>
+__global__ void __launch_bounds__(256) k_classify(const Job<T>* __restrict__ jobs,
+                                                  const __grid_constant__ Sel sel) {
   __shared__ Tile<T> s;
   __shared__ uint64_t bar;
+  int bx, by, bz;
+  const Job<T>& J = tile_job(jobs, sel, bx, by, bz);
   const Dims g = J.dim;
-  const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
-  if (!load_tile<T, kTma>(s, &bar, &map, a, g, bx, by, bz)) {
+  const T* a = kDetect ? J.g : J.f;
+  if (!load_tile<T>(s, &bar, kDetect ? J.map_g : J.map_f, kDetect ? J.tma_g : J.tma_f, a, g, bx,
+                    by, bz)) {
     if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
     return;
   }
@@ -276,7 +315,10 @@ __device__ __forceinline__ int global_type(const Job<T>& J, int v, int& lmask) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_redetect(Job<T> J, int epoch) {
+__global__ void __launch_bounds__(256) k_redetect(const Job<T>* __restrict__ jobs,
+                                                  const __grid_constant__ Sel sel, int epoch) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[C_DIRTY];
   const long long total = (long long)n * (kNumDirs + 1);
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -306,10 +348,14 @@ __global__ void __launch_bounds__(256) k_redetect(Job<T> J, int epoch) {
     if (slot >= 0) J.mm_next[slot] = v | (cat << kCatShift);
     count_cats(J.ctr, cat);
   }
+  }
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_keep(Job<T> J, int epoch) {
+__global__ void __launch_bounds__(256) k_keep(const Job<T>* __restrict__ jobs,
+                                              const __grid_constant__ Sel sel, int epoch) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[C_MM];
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -323,6 +369,7 @@ __global__ void __launch_bounds__(256) k_keep(Job<T> J, int epoch) {
     const int slot = warp_append(J.ctr + C_MM_NEXT, cat != 0, 0xffffffffu);
     if (slot >= 0) J.mm_next[slot] = ent;
     count_cats(J.ctr, cat);
+  }
   }
 }
 
@@ -347,39 +394,87 @@ __device__ __forceinline__ int ddx(int d) { return (int)((pack_dir(0) >> (2 * d)
 __device__ __forceinline__ int ddy(int d) { return (int)((pack_dir(1) >> (2 * d)) & 3u) - 1; }
 __device__ __forceinline__ int ddz(int d) { return (int)((pack_dir(2) >> (2 * d)) & 3u) - 1; }
 
-// Follows a steepest path inside the tile from (cx, cy, cz) until it leaves
-// the tile or stops at a root; returns the global id of the first vertex
-// outside the tile, or of the root.
-__device__ __forceinline__ int follow_in_tile(const int8_t* dir, int cx, int cy, int cz, int bx,
-                                              int by, int bz, int W, int WH, int* err) {
-  int d = dir[(cz * TY + cy) * TX + cx];
-  for (int step = 0; d >= 0; ++step) {
-    const int nx = cx + ddx(d), ny = cy + ddy(d), nz = cz + ddz(d);
-    if ((unsigned)nx >= (unsigned)TX || (unsigned)ny >= (unsigned)TY || (unsigned)nz >= (unsigned)TZ)
-      return (bx + nx) + (by + ny) * W + (bz + nz) * WH;
-    cx = nx;
-    cy = ny;
-    cz = nz;
-    d = dir[(cz * TY + cy) * TX + cx];
-    if (step >= TX * TY * TZ) {  // a path cannot revisit a vertex; guard anyway
+// Steepest-ascent and steepest-descent directions of one tile voxel: the
+// maximum (minimum) of (value, id) over the voxel and its valid neighbours.
+// Ids are scanned in ascending order so that ">=" keeps the larger id on a tie;
+// the descent scans in descending order with "<=".  (Finite inputs: the scans
+// start from -inf / +inf and always meet the centre.)  kAll: every direction
+// valid, no per-direction test.
+template <class T, bool kAll>
+__device__ __forceinline__ void steepest_dirs(const Tile<T>& s, int tx, int ty, int tz, int valid,
+                                              int& hd, int& ld) {
+  const T c = s.v[tz + 1][ty + 1][tx + kXOff];
+  T hv = -T(INFINITY), lv = T(INFINITY);
+  hd = -1;
+  ld = -1;
+  T nv[kNumDirs];
+#pragma unroll
+  for (int d = 0; d < kNumDirs; ++d)
+    nv[d] = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
+#pragma unroll
+  for (int j = 0; j < kNumDirs; ++j) {
+    const int d = rank_dir(j);
+    if (j == kRankCentre && c >= hv) { hv = c; hd = -1; }
+    if ((kAll || (valid >> d & 1)) && nv[d] >= hv) { hv = nv[d]; hd = d; }
+  }
+#pragma unroll
+  for (int j = kNumDirs - 1; j >= 0; --j) {
+    const int d = rank_dir(j);
+    if ((kAll || (valid >> d & 1)) && nv[d] <= lv) { lv = nv[d]; ld = d; }
+    if (j == kRankCentre && c <= lv) { lv = c; ld = -1; }
+  }
+}
+
+// Next step of a path in tile terms: the local index of the next voxel when
+// it lies in the tile, kExit when the path leaves the tile (the global id of
+// the first outside vertex goes to *exit_gid), kRoot when the voxel is a root.
+constexpr int kExit = -1, kRoot = -2;
+__device__ __forceinline__ int next_in_tile(int d, int tx, int ty, int tz, int v, int W, int WH,
+                                            int* exit_gid) {
+  if (d < 0) return kRoot;
+  const int dx = ddx(d), dy = ddy(d), dz = ddz(d);
+  const int nx = tx + dx, ny = ty + dy, nz = tz + dz;
+  if ((unsigned)nx < (unsigned)TX && (unsigned)ny < (unsigned)TY && (unsigned)nz < (unsigned)TZ)
+    return (nz * TY + ny) * TX + nx;
+  *exit_gid = v + dx + dy * W + dz * WH;
+  return kExit;
+}
+
+// Follows next-pointers inside the tile from local voxel li to the path's
+// exit (global id of the first outside vertex) or root.
+__device__ __forceinline__ int follow(const int16_t* nxt, const int* exit_gid, int li, int bx,
+                                      int by, int bz, int W, int WH, int* err) {
+  int cur = li, t = nxt[li];
+  for (int step = 0; t >= 0; ++step) {
+    cur = t;
+    t = nxt[cur];
+    if (step > TX * TY * TZ) {  // a path never revisits a voxel; guard anyway
       atomicOr(err, kErrTile);
       break;
     }
   }
+  if (t == kExit) return exit_gid[cur];
+  const int cx = cur % TX, cy = (cur / TX) % TY, cz = cur / (TX * TY);
   return (bx + cx) + (by + cy) * W + (bz + cz) * WH;
 }
 
-template <class T, bool kTma>
-__global__ void __launch_bounds__(256) k_direction(Job<T> J, const __grid_constant__ CUtensorMap map,
-                                                   const T* __restrict__ a, int* __restrict__ ds,
-                                                   int* __restrict__ as) {
+// kDec = false: f into ds / as (setup); true: g into dds / das.
+template <class T, bool kDec>
+__global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jobs,
+                                                   const __grid_constant__ Sel sel) {
   __shared__ Tile<T> s;
   __shared__ uint64_t bar;
-  __shared__ int8_t hdir[TZ * TY * TX], ldir[TZ * TY * TX];
+  __shared__ int16_t hnext[TZ * TY * TX], lnext[TZ * TY * TX];
+  __shared__ int hexit[TZ * TY * TX], lexit[TZ * TY * TX];
+  int bx, by, bz;
+  const Job<T>& J = tile_job(jobs, sel, bx, by, bz);
   const Dims g = J.dim;
   const int WH = g.W * g.H;
-  const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
-  if (!load_tile<T, kTma>(s, &bar, &map, a, g, bx, by, bz)) {
+  const T* a = kDec ? J.g : J.f;
+  int* ds = kDec ? J.dds : J.ds;
+  int* as = kDec ? J.das : J.as;
+  if (!load_tile<T>(s, &bar, kDec ? J.map_g : J.map_f, kDec ? J.tma_g : J.tma_f, a, g, bx, by,
+                    bz)) {
     if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
     return;
   }
@@ -388,39 +483,24 @@ __global__ void __launch_bounds__(256) k_direction(Job<T> J, const __grid_consta
     const int li = (tz * TY + ty) * TX + tx;
     const int x = bx + tx, y = by + ty, z = bz + tz;
     int hd = -1, ld = -1;
-    if (x < g.W && y < g.H && z < g.D) {
-      const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
-      const T c = s.v[tz + 1][ty + 1][tx + kXOff];
-      // Steepest ascent: maximum of (value, id) over {v} and its neighbours,
-      // scanning ids in ascending order so that ">=" keeps the larger id on a
-      // tie; steepest descent scans in descending order with "<=" (finite
-      // inputs: the scans start from -inf / +inf and always meet the centre).
-      T hv = -T(INFINITY), lv = T(INFINITY);
-#pragma unroll
-      for (int j = 0; j < kNumDirs; ++j) {
-        const int d = rank_dir(j);
-        if (j == kRankCentre && c >= hv) { hv = c; hd = -1; }
-        const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
-        if ((valid >> d & 1) && nv >= hv) { hv = nv; hd = d; }
-      }
-#pragma unroll
-      for (int j = kNumDirs - 1; j >= 0; --j) {
-        const int d = rank_dir(j);
-        const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
-        if ((valid >> d & 1) && nv <= lv) { lv = nv; ld = d; }
-        if (j == kRankCentre && c <= lv) { lv = c; ld = -1; }
-      }
+    const bool in = x < g.W && y < g.H && z < g.D;
+    if (in) {
+      const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
+      if (bc == 0) steepest_dirs<T, true>(s, tx, ty, tz, (1 << kNumDirs) - 1, hd, ld);
+      else steepest_dirs<T, false>(s, tx, ty, tz, valid_mask(bc), hd, ld);
     }
-    hdir[li] = (int8_t)hd;
-    ldir[li] = (int8_t)ld;
+    const int v = x + y * g.W + z * WH;
+    hnext[li] = (int16_t)(in ? next_in_tile(hd, tx, ty, tz, v, g.W, WH, &hexit[li]) : kRoot);
+    lnext[li] = (int16_t)(in ? next_in_tile(ld, tx, ty, tz, v, g.W, WH, &lexit[li]) : kRoot);
   }
   __syncthreads();
   for (int tz = 0; tz < TZ; ++tz) {
     const int x = bx + tx, y = by + ty, z = bz + tz;
     if (!(x < g.W && y < g.H && z < g.D)) continue;
+    const int li = (tz * TY + ty) * TX + tx;
     const int v = x + y * g.W + z * WH;
-    ds[v] = follow_in_tile(hdir, tx, ty, tz, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
-    as[v] = follow_in_tile(ldir, tx, ty, tz, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
+    ds[v] = follow(hnext, hexit, li, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
+    as[v] = follow(lnext, lexit, li, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
   }
 }
 
@@ -431,14 +511,22 @@ __global__ void __launch_bounds__(256) k_direction(Job<T> J, const __grid_consta
 // Every vertex is resolved (the reference resolves descending labels only next
 // to original 2-saddles, the only places they are read).  Iterations are
 // capped; hitting the cap sets the error word instead of spinning.
-__global__ void __launch_bounds__(256) k_jump2(int* __restrict__ a, int* __restrict__ b, int N,
-                                               int cap, int* err) {
+template <class T, bool kDec>
+__global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
+                                               const __grid_constant__ Sel sel, int cap) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
+  int* a = kDec ? J.dds : J.ds;
+  int* b = kDec ? J.das : J.as;
+  int* err = J.ctr + C_ERROR;
+  const int N = J.dim.N;
+  const int cap_j = cap > 0 ? cap : N + 1;
   const int stride = gridDim.x * blockDim.x;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
     int u1 = a[v], u2 = b[v];
     bool d1 = false, d2 = false;
     int it = 0;
-    for (; it < cap && !(d1 && d2); ++it) {
+    for (; it < cap_j && !(d1 && d2); ++it) {
       if (!d1) {
         const int w = a[u1];
         if (w == u1) d1 = true;
@@ -450,9 +538,10 @@ __global__ void __launch_bounds__(256) k_jump2(int* __restrict__ a, int* __restr
         else u2 = w;
       }
     }
-    if (it == cap) atomicOr(err, kErrJump);
+    if (it == cap_j) atomicOr(err, kErrJump);
     a[v] = u1;
     b[v] = u2;
+  }
   }
 }
 
@@ -678,7 +767,9 @@ __device__ __forceinline__ void propose(const Job<T>& J, int i, T d) {
 
 // c_loop(0..2) (:2887-3055) over the mismatch list.
 template <class T>
-__global__ void __launch_bounds__(256) k_propose_cp(Job<T> J) {
+__global__ void __launch_bounds__(256) k_propose_cp(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[C_MM];
   const int stride = gridDim.x * blockDim.x;
   const Dims g = J.dim;
@@ -730,12 +821,15 @@ __global__ void __launch_bounds__(256) k_propose_cp(Job<T> J) {
       }
     }
   }
+  }
 }
 
 // applyDeltaBuffer (:3061-3111) over the vertices that received a proposal;
 // the proposal buffer is reset to the sentinel on the way (init_delta).
 template <class T>
-__global__ void __launch_bounds__(256) k_apply(Job<T> J, int dirty_epoch) {
+__global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, int dirty_epoch) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[C_TOUCHED];
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
@@ -762,6 +856,7 @@ __global__ void __launch_bounds__(256) k_apply(Job<T> J, int dirty_epoch) {
     J.g[v] = gv;
     if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0) && atomicExch(J.dstamp + v, dirty_epoch) != dirty_epoch)
       J.dirty[atomicAdd(J.ctr + C_DIRTY, 1)] = v;
+  }
   }
 }
 
@@ -846,7 +941,9 @@ __device__ __noinline__ int row_entry_k(const Job<T>& J, int s, int k) {
 }
 
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_saddle_pass(Job<T> J) {
+__global__ void __launch_bounds__(256) k_saddle_pass(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int ns = J.ctr[kSplit ? C_NS2 : C_NS1];
   const int* sad = kSplit ? J.sad2 : J.sad1;
   const uint8_t* ocnt = kSplit ? J.ocnt2 : J.ocnt1;
@@ -900,6 +997,7 @@ __global__ void __launch_bounds__(256) k_saddle_pass(Job<T> J) {
     const int slot = warp_append(J.ctr + C_CAND, has, 0xffffffffu);
     if (slot >= 0) J.cand[slot] = s;
   }
+  }
 }
 
 // Compact copy of the original rows' counts (the only field of a row most
@@ -915,7 +1013,9 @@ __global__ void k_row_counts(Job<T> J) {
 }
 
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_wn_vote(Job<T> J, unsigned long long round, int stamp) {
+__global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, unsigned long long round, int stamp) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[C_CAND];
   const int* taken = kSplit ? J.taken : J.taken1;
   const int stride = gridDim.x * blockDim.x;
@@ -927,10 +1027,13 @@ __global__ void __launch_bounds__(256) k_wn_vote(Job<T> J, unsigned long long ro
     for (int j = 0; j < k; ++j)
       if (taken[ids[j]] != stamp) atomicMax(J.claim + ids[j], vote);
   }
+  }
 }
 
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_wn_commit(Job<T> J, unsigned long long round, int stamp) {
+__global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, unsigned long long round, int stamp) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[C_CAND];
   int* taken = kSplit ? J.taken : J.taken1;
   int* flagged = kSplit ? J.flagged : J.flagged1;
@@ -952,12 +1055,15 @@ __global__ void __launch_bounds__(256) k_wn_commit(Job<T> J, unsigned long long 
       J.cand_next[atomicAdd(J.ctr + C_CAND_NEXT, 1)] = s;
     }
   }
+  }
 }
 
 // Sequential completion for whatever the bounded rounds left unresolved:
 // one thread takes the remaining saddles in ascending id.
 template <class T, bool kSplit>
-__global__ void k_wn_sequential(Job<T> J, int stamp) {
+__global__ void k_wn_sequential(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, int stamp) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   int n = J.ctr[C_CAND];
   int* taken = kSplit ? J.taken : J.taken1;
@@ -980,6 +1086,7 @@ __global__ void k_wn_sequential(Job<T> J, int stamp) {
       }
   }
   J.ctr[C_CAND] = 0;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -988,7 +1095,9 @@ __global__ void k_wn_sequential(Job<T> J, int stamp) {
 // the original choice (join).
 // ---------------------------------------------------------------------------
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_fixpath(Job<T> J) {
+__global__ void __launch_bounds__(256) k_fixpath(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, int cap) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[kSplit ? C_NFC : C_NFC1];
   const int* list = kSplit ? J.flagged : J.flagged1;
   const int stride = gridDim.x * blockDim.x;
@@ -996,8 +1105,8 @@ __global__ void __launch_bounds__(256) k_fixpath(Job<T> J) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
     int cur = list[e];
     int t = -1, fl = -1;
-    long long steps = 0;
-    for (; steps <= (long long)g.N; ++steps) {
+    int steps = 0;
+    for (; steps < cap; ++steps) {
       int ids[kNumDirs];
       const int nn = neighbours(cur, g, ids, nullptr);
       int ni = cur, nd = cur;
@@ -1017,10 +1126,14 @@ __global__ void __launch_bounds__(256) k_fixpath(Job<T> J) {
       if (ni == cur) break;
       cur = ni;
     }
-    if (steps > (long long)g.N) atomicOr(J.ctr + C_ERROR, kErrPath);
+    if (steps == cap) {
+      atomicOr(J.ctr + C_ERROR, kErrPath);
+      continue;
+    }
     if (fl == t) continue;
     const int target = kSplit ? fl : t;
     propose(J, target, step_delta(J, target));
+  }
   }
 }
 
@@ -1030,7 +1143,9 @@ __global__ void __launch_bounds__(256) k_fixpath(Job<T> J) {
 // winning per extremum, followed by the fixes (:3320-3413).
 // ---------------------------------------------------------------------------
 template <class T, bool kMax>
-__global__ void __launch_bounds__(256) k_wim_scan(Job<T> J) {
+__global__ void __launch_bounds__(256) k_wim_scan(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
   const int* orow = kMax ? J.orow2 : J.orow1;
   const int* drow = kMax ? J.drow2 : J.drow1;
@@ -1046,12 +1161,15 @@ __global__ void __launch_bounds__(256) k_wim_scan(Job<T> J) {
     const int k = cnt - 1;
     if (o[k] != d[1]) flag[J.ext[o[k]]] = 1;
   }
+  }
 }
 
 // Collect per extremum, count, propose the fix and reset the arbitration slots.
 // fix = false: detection only (the third block of the outer loop, :5932-5951).
 template <class T, bool kMax>
-__global__ void __launch_bounds__(256) k_wim_collect(Job<T> J, int fix) {
+__global__ void __launch_bounds__(256) k_wim_collect(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, int fix) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int next = J.ctr[kMax ? C_NMAX : C_NMIN];
   const int* ext_list = kMax ? J.maxima : J.minima;
   const int* drow = kMax ? J.drow2 : J.drow1;
@@ -1094,13 +1212,16 @@ __global__ void __launch_bounds__(256) k_wim_collect(Job<T> J, int fix) {
       if (b2) atomicAdd(c2, __popc(b2));
     }
   }
+  }
 }
 
 // get_wrong_index_min direction 1 (:3157-3168, fix :3393-3410) keeps the pair of
 // the lowest row per minimum and lowers the row's FALSE last entry, so it needs
 // the winning row: one more scan, arbitrating through first_sj as scratch.
 template <class T>
-__global__ void __launch_bounds__(256) k_wim_min2_scan(Job<T> J) {
+__global__ void __launch_bounds__(256) k_wim_min2_scan(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int ns = J.ctr[C_NS1];
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
@@ -1110,9 +1231,12 @@ __global__ void __launch_bounds__(256) k_wim_min2_scan(Job<T> J) {
     const int k = cnt - 1;
     if (o[k] != J.drow1[2ll * i + 1]) atomicMin(J.first_sj + J.ext[o[k]], i);
   }
+  }
 }
 template <class T>
-__global__ void __launch_bounds__(256) k_wim_min2_collect(Job<T> J) {
+__global__ void __launch_bounds__(256) k_wim_min2_collect(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int next = J.ctr[C_NMIN];
   const int stride = gridDim.x * blockDim.x;
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < next; m += stride) {
@@ -1121,6 +1245,7 @@ __global__ void __launch_bounds__(256) k_wim_min2_collect(Job<T> J) {
     J.first_sj[m] = kInf;
     const int target = J.drow1[2ll * row + 1];
     propose(J, target, step_delta(J, target));
+  }
   }
 }
 
@@ -1132,7 +1257,9 @@ __global__ void __launch_bounds__(256) k_wim_min2_collect(Job<T> J) {
 // fix_wrong_index_saddle (:3415-3463).
 // ---------------------------------------------------------------------------
 template <class T, bool kMax>
-__global__ void __launch_bounds__(256) k_wis_scan(Job<T> J) {
+__global__ void __launch_bounds__(256) k_wis_scan(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
   const int* sad = kMax ? J.sad2 : J.sad1;
   const int* rows = kMax ? J.orow2 : J.orow1;
@@ -1162,10 +1289,13 @@ __global__ void __launch_bounds__(256) k_wis_scan(Job<T> J) {
       if (wrong) atomicMin(first + m, i * kRowStride + p);
     }
   }
+  }
 }
 
 template <class T, bool kMax>
-__global__ void __launch_bounds__(256) k_wis_collect(Job<T> J, int fix) {
+__global__ void __launch_bounds__(256) k_wis_collect(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, int fix) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+  const Job<T>& J = jobs[sel.idx[jk]];
   const int next = J.ctr[kMax ? C_NMAX : C_NMIN];
   const int* sad = kMax ? J.sad2 : J.sad1;
   const int* best = kMax ? J.largest : J.smallest;
@@ -1195,11 +1325,42 @@ __global__ void __launch_bounds__(256) k_wis_collect(Job<T> J, int fix) {
     const unsigned b = __ballot_sync(0xffffffffu, hit);
     if (lane_id() == 0 && b) atomicAdd(cnt, __popc(b));
   }
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Small helpers.
 // ---------------------------------------------------------------------------
+// Swaps the current and next list of each selected job and moves the next
+// count into the current slot: which 0 = mismatch lists, 1 = wrong-neighbour
+// candidates.  (The job descriptors live in device memory, so the swap does
+// too.)
+template <class T>
+__global__ void k_swap_lists(Job<T>* jobs, const __grid_constant__ Sel sel, int which) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= sel.n) return;
+  Job<T>& J = jobs[sel.idx[k]];
+  if (which == 0) {
+    int* t = J.mm;
+    J.mm = J.mm_next;
+    J.mm_next = t;
+    J.ctr[C_MM] = J.ctr[C_MM_NEXT];
+  } else {
+    int* t = J.cand;
+    J.cand = J.cand_next;
+    J.cand_next = t;
+    J.ctr[C_CAND] = J.ctr[C_CAND_NEXT];
+  }
+}
+
+// Zeroes counter slots [slot, slot + n) of every selected job.
+template <class T>
+__global__ void k_zero_ctr(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel,
+                           int slot, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= sel.n * n) return;
+  jobs[sel.idx[k / n]].ctr[slot + k % n] = 0;
+}
 template <class K>
 __global__ void k_fill(K* p, K v, long long n) {
   const long long stride = (long long)gridDim.x * blockDim.x;

@@ -65,7 +65,11 @@ typedef struct {
   int final_join;
   int preserve_join;
   int flags;          /* EXTREMZ_FLAG_* */
-  int reserved[5];
+  int device_iter_cap; /* device-side iteration limit of pointer jumping and path
+                          walks; 0 = the field's voxel count (never reached by a
+                          valid path).  Reaching it sets report.error_bits and
+                          returns EXTREMZ_DEVICE_TIMEOUT. */
+  int reserved[4];
 } extremz_params;
 
 /* flags: time kernel launches with CUDA events, per kernel class, into

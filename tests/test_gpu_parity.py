@@ -103,3 +103,42 @@ def test_tile_load_paths_agree(tma):
     out, rep, _ = gpu_correct(fld.f, fld.decp, fld.eb, trace_cap=0, tma=tma, **KW)
     assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
     assert rep.error_bits == 0
+
+
+@pytest.mark.parametrize("seed,dtype", [(5, np.float64), (12, np.float32)])
+def test_preserve_join_tree_bit_exact(seed, dtype):
+    """preserve_join_tree = true (the join-tree passes s_loops_join /
+    saddle_loops_join inside the loop, src/ExtreM_cuda.cu:5724-5747)."""
+    from oracle import ffi
+    fld = synth.make_field(28, 22, 14, n_gauss=12, seed=seed, rel=2e-3, dtype=dtype)
+    kw = dict(KW, preserve_join=True)
+    ref, rrep, rtrace = ffi.correct(fld.f, fld.decp, fld.eb, trace_cap=200000, **kw)
+    out, rep, trace = gpu_correct(fld.f, fld.decp, fld.eb, **kw)
+    assert np.array_equal(trace, rtrace), first_divergence(trace, rtrace)
+    assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+    assert rep.status == rrep["status"]
+
+
+def test_device_iteration_limit_returns_status_and_context_survives():
+    """A device-side limit that runs out ends the call with a status, not a
+    hang or a fault, and the context stays usable."""
+    import torch
+    from extrem_z_b200 import api
+    fld = synth.make_field(32, 32, 16, n_gauss=10, seed=6, rel=1e-3)
+    ctx = api.Context(0)
+    tf = torch.from_numpy(fld.f).cuda()
+    tg = torch.from_numpy(fld.decp.copy()).cuda()
+    with pytest.raises(api.ExtremzError) as ei:
+        ctx.correct_device(tf, tg, fld.eb, device_iter_cap=1, **KW)
+    assert ei.value.status == api.DEVICE_TIMEOUT
+    tg.copy_(torch.from_numpy(fld.decp))
+    rep, _ = ctx.correct_device(tf, tg, fld.eb, **KW)
+    assert rep.status == 0 and rep.error_bits == 0
+
+
+def test_round_cap_returns_status():
+    from extrem_z_b200 import api
+    fld = synth.make_field(32, 32, 16, n_gauss=10, seed=6, rel=1e-3)
+    out, rep = api.correct(fld.f, fld.decp, fld.eb, **dict(KW, max_outer=0))
+    assert rep.status in (api.OK, api.ROUND_CAP)
+    assert np.all(out <= fld.decp)
