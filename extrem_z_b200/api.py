@@ -24,12 +24,15 @@ from . import build as _build
 _lib = None
 _lock = threading.Lock()
 
-OK, ROUND_CAP, BAD_ARG, OOM, CUDA_ERR, DEVICE_TIMEOUT, NO_DEVICE, TOO_LARGE = range(8)
+OK, ROUND_CAP, BAD_ARG, OOM, CUDA_ERR, DEVICE_TIMEOUT, NO_DEVICE, TOO_LARGE, PENDING = range(9)
 F32, F64 = 0, 1
 
 # Every entry point declared in include/extremz.h.
 EXPORTS = ("extremz_version", "extremz_default_params", "extremz_ctx_create",
            "extremz_ctx_destroy", "extremz_correct_device", "extremz_correct_host",
+           "extremz_correct_batch", "extremz_server_create", "extremz_server_destroy",
+           "extremz_server_submit", "extremz_server_poll", "extremz_server_wait",
+           "extremz_server_get_stats", "extremz_job_footprint",
            "extremz_correct_device_noalloc", "extremz_noalloc_max_voxels",
            "extremz_lut", "extremz_status_string", "extremz_last_cuda_error")
 
@@ -56,6 +59,25 @@ class Report(ctypes.Structure):
                 ("kernel_launches", ctypes.c_longlong),
                 ("prof_ms", ctypes.c_float * 10), ("prof_launches", ctypes.c_int * 10),
                 ("reserved", ctypes.c_int * 8)]
+
+class Field(ctypes.Structure):
+    _fields_ = [("orig", ctypes.c_void_p), ("decp", ctypes.c_void_p), ("dtype", ctypes.c_int),
+                ("width", ctypes.c_int), ("height", ctypes.c_int), ("depth", ctypes.c_int),
+                ("params", Params)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("max_jobs", ctypes.c_int),
+                ("reserved", ctypes.c_int * 7)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("queued", ctypes.c_longlong), ("running", ctypes.c_longlong),
+                ("bytes_in_use", ctypes.c_longlong), ("peak_bytes_in_use", ctypes.c_longlong),
+                ("ticks", ctypes.c_longlong), ("kernel_launches", ctypes.c_longlong),
+                ("peak_running", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+
 
 FLAG_PROFILE = 1
 FLAG_NO_TMA = 2
@@ -117,6 +139,24 @@ def load(build_if_missing: bool = True):
         L.extremz_correct_host.argtypes = [vp, vp, vp, i32, i32, i32, i32,
                                            ctypes.POINTER(Params), ctypes.POINTER(Report), vp]
         L.extremz_correct_host.restype = i32
+        L.extremz_correct_batch.argtypes = [vp, ctypes.POINTER(Field), i32,
+                                            ctypes.POINTER(Report), vp]
+        L.extremz_correct_batch.restype = i32
+        L.extremz_server_create.argtypes = [i32, ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+        L.extremz_server_create.restype = i32
+        L.extremz_server_destroy.argtypes = [vp]
+        L.extremz_server_submit.argtypes = [vp, ctypes.POINTER(Field), vp,
+                                            ctypes.POINTER(ctypes.c_longlong)]
+        L.extremz_server_submit.restype = i32
+        L.extremz_server_poll.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(Report),
+                                          ctypes.POINTER(ctypes.c_double)]
+        L.extremz_server_poll.restype = i32
+        L.extremz_server_wait.argtypes = [vp, ctypes.c_longlong, i32, ctypes.POINTER(Report),
+                                          ctypes.POINTER(ctypes.c_double)]
+        L.extremz_server_wait.restype = i32
+        L.extremz_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+        L.extremz_job_footprint.argtypes = [i32, i32, i32, i32]
+        L.extremz_job_footprint.restype = ctypes.c_longlong
         L.extremz_correct_device_noalloc.argtypes = [vp, vp, i32, i32, i32, i32,
                                                      ctypes.POINTER(Params),
                                                      ctypes.POINTER(Report), vp]
@@ -214,6 +254,39 @@ class Context:
             trace = trace[trace[:, 0] != 0]
         return CorrectionReport.of(r), trace
 
+    # -- batches ------------------------------------------------------------
+    def correct_batch(self, items, *, stream=None):
+        """Correct many CUDA tensors in place with shared launches.
+
+        items: sequence of (f, decp, bound) or (f, decp, bound, kwargs) where
+        kwargs are make_params() options for that field.  Fields may differ
+        in dtype, shape and parameters.  Returns (list of CorrectionReport,
+        total kernel launches of the batch).
+        """
+        import torch
+        n = len(items)
+        arr = (Field * max(n, 1))()
+        keep = []
+        for i, it in enumerate(items):
+            f, decp, bound = it[0], it[1], it[2]
+            kw = it[3] if len(it) > 3 else {}
+            assert f.is_cuda and decp.is_cuda and f.dtype == decp.dtype and f.shape == decp.shape
+            assert f.is_contiguous() and decp.is_contiguous()
+            w, h, d = _whd(tuple(f.shape))
+            arr[i].orig, arr[i].decp = f.data_ptr(), decp.data_ptr()
+            arr[i].dtype = {torch.float32: F32, torch.float64: F64}[f.dtype]
+            arr[i].width, arr[i].height, arr[i].depth = w, h, d
+            arr[i].params = make_params(bound, **kw)
+            keep.append((f, decp))
+        if stream is None:
+            dev = items[0][0].device if n else torch.device("cuda", self.device)
+            stream = torch.cuda.current_stream(dev).cuda_stream
+        reps = (Report * max(n, 1))()
+        st = load().extremz_correct_batch(self._h, arr, n, reps, stream)
+        _check(st, allow_cap=False)
+        out = [CorrectionReport.of(reps[i]) for i in range(n)]
+        return out, (int(reps[0].kernel_launches) if n else 0)
+
     # -- host arrays ----------------------------------------------------------
     def correct_host(self, f: np.ndarray, decp: np.ndarray, bound: float, *, stream=None, **kw):
         """Correct the numpy array ``decp`` in place through host buffers."""
@@ -227,6 +300,103 @@ class Context:
                                          ctypes.byref(p), ctypes.byref(r), stream)
         _check(st)
         return CorrectionReport.of(r)
+
+
+class Server:
+    """Request loop with continuous batching (extremz_server_*).
+
+    submit() queues a CUDA field pair and returns a ticket at once; the loop
+    admits requests in arrival order while their device footprint fits the
+    HBM budget, and serves all admitted requests with shared launches.
+    """
+
+    def __init__(self, device: int = 0, *, hbm_budget_bytes: int = 0, max_jobs: int = 0):
+        L = load()
+        cfg = ServerConfig()
+        cfg.hbm_budget_bytes, cfg.max_jobs = int(hbm_budget_bytes), int(max_jobs)
+        h = ctypes.c_void_p()
+        _check(L.extremz_server_create(int(device), ctypes.byref(cfg), ctypes.byref(h)),
+               allow_cap=False)
+        self._h = h
+        self.device = device
+        self._keep = {}
+
+    def close(self):
+        if self._h:
+            load().extremz_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, f, decp, bound: float, *, stream=None, **kw) -> int:
+        """Queue ``decp`` (corrected in place) against the original ``f``.
+
+        The server's work starts after what is queued on ``stream`` (default:
+        the current torch stream) at the time of the call."""
+        import torch
+        assert f.is_cuda and decp.is_cuda and f.dtype == decp.dtype and f.shape == decp.shape
+        assert f.is_contiguous() and decp.is_contiguous()
+        fd = Field()
+        fd.orig, fd.decp = f.data_ptr(), decp.data_ptr()
+        fd.dtype = {torch.float32: F32, torch.float64: F64}[f.dtype]
+        fd.width, fd.height, fd.depth = _whd(tuple(f.shape))
+        fd.params = make_params(bound, **kw)
+        if stream is None:
+            stream = torch.cuda.current_stream(f.device).cuda_stream
+        t = ctypes.c_longlong()
+        _check(load().extremz_server_submit(self._h, ctypes.byref(fd), stream, ctypes.byref(t)),
+               allow_cap=False)
+        self._keep[t.value] = (f, decp)
+        return t.value
+
+    def _take(self, st, t, r, lat):
+        if st == PENDING:
+            return None
+        self._keep.pop(t, None)
+        if st not in (OK, ROUND_CAP):
+            _check(st)
+        return CorrectionReport.of(r), lat.value
+
+    def poll(self, ticket: int):
+        """None while pending, else (CorrectionReport, latency in ms)."""
+        r, lat = Report(), ctypes.c_double()
+        st = load().extremz_server_poll(self._h, ticket, ctypes.byref(r), ctypes.byref(lat))
+        return self._take(st, ticket, r, lat)
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        r, lat = Report(), ctypes.c_double()
+        st = load().extremz_server_wait(self._h, ticket, int(timeout_ms), ctypes.byref(r),
+                                        ctypes.byref(lat))
+        return self._take(st, ticket, r, lat)
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        load().extremz_server_get_stats(self._h, ctypes.byref(s))
+        return {k: int(getattr(s, k)) for k, _ in ServerStats._fields_ if k != "reserved"}
+
+
+def job_footprint(voxels_or_shape, dtype) -> int:
+    """Device bytes a Server charges a request against its HBM budget.
+
+    voxels_or_shape: a voxel count or a (W, H, D) triple; dtype: numpy or
+    torch float32/float64."""
+    if isinstance(voxels_or_shape, (tuple, list)):
+        w, h, d = (int(x) for x in voxels_or_shape)
+    else:
+        w, h, d = int(voxels_or_shape), 1, 1
+    dt = F32 if str(dtype).endswith("float32") else F64
+    return int(load().extremz_job_footprint(dt, w, h, d))
 
 
 def _whd(shape):

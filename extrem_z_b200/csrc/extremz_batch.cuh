@@ -1,0 +1,825 @@
+// Batched, tick-driven correction engine.
+//
+// Every job (one field) runs the reference GPU driver's control flow
+// (src/ExtreM_cuda.cu main() :5508-5997) as a state machine on the host: one
+// state per phase of that flow (c_loops detection and rounds, r_loops, a
+// manifold round with the wrong-neighbour arbitration, s_loops, saddle_loops,
+// their join variants, the third block's detection, the final join pass).
+// A tick runs, in program order, every phase that any job is in: one launch
+// per kernel serves all jobs in that phase (kernels take the device array of
+// job descriptors and a selection), and a job moves on through phases whose
+// successor does not depend on a counter within the same tick.  At the end of
+// a tick the counter blocks of all jobs come back in one copy and every job
+// that stopped at a branch takes it, with the reference's rules.
+//
+// The branches read exactly the counters the reference reads at the same
+// points, so a job's sequence of kernel launches, and its result, do not
+// depend on what else is in the batch.  The plain entry points run a batch of
+// one job; the batch and serving entry points admit many.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "extremz_kernels.cuh"
+
+namespace extremz {
+
+// Trace phases (the same records as the oracle's trace).
+enum Phase : int {
+  PH_CLOOP_DETECT = 1, PH_WRONG_NBR = 2, PH_SLOOPS = 3, PH_SADDLE = 4, PH_DETECT3 = 5,
+  PH_SLOOPS_JOIN = 6, PH_SADDLE_JOIN = 7, PH_OUTER = 8, PH_CHECKSUM = 9
+};
+
+// Kernel classes for the optional per-class timing (extremz_report.prof_*).
+enum KClass : int {
+  K_SETUP = 0, K_DETECT, K_DIRECTION, K_JUMP, K_PROPOSE, K_APPLY, K_ROWS, K_WRONG_NBR,
+  K_FIXPATH, K_OTHER, K_NUM
+};
+
+// Program counter of a job, in the order phases run within a tick.
+enum Pc : int {
+  PC_SETUP_A = 0,   // classify f, f's manifolds, CP counts          -> sync
+  PC_SETUP_B,       // CP lists, rows, per-extremum saddles             -> CL_DETECT
+  PC_CL_DETECT,     // c_loops entry: detection                         -> sync
+  PC_CL_ROUND,      // c_loops round: proposals, apply, detection       -> sync
+  PC_RLOOPS,        // r_loops (fixpath)                                -> MANIFOLD
+  PC_MANIFOLD,      // manifolds, rows, wrong neighbours                -> sync
+  PC_SLOOPS,        // s_loops                                          -> sync
+  PC_SADDLE,        // saddle_loops
+  PC_SLOOPS_J,      // s_loops_join                                     -> sync
+  PC_SADDLE_J,      // saddle_loops_join (inside the loop)
+  PC_PRE_END,       // counters re-read before the loop (:5589-5599)    -> sync
+  PC_DET3,          // third block: wrong max / saddle detection
+  PC_DET3J,         // third block: join detection
+  PC_FINAL_DETECT,  // end of an outer iteration: detection             -> sync
+  PC_FINAL_JOIN,    // unconditional saddle_loops_join (:5997)          -> sync
+  PC_DONE,
+  PC_COUNT = PC_DONE
+};
+
+template <class T>
+__global__ void k_checksum(const T* __restrict__ a, int N, unsigned long long* out) {
+  unsigned long long acc = 0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
+    unsigned long long bits = 0;
+    if (sizeof(T) == 8) bits = (unsigned long long)__double_as_longlong((double)a[v]);
+    else bits = (unsigned long long)__float_as_uint((float)a[v]);
+    unsigned long long z = bits + 0x9e3779b97f4a7c15ull * (unsigned long long)(v + 1);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    acc += z ^ (z >> 31);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// Workspace bytes of one job of n voxels (every critical-point list sized n:
+// the counts are known only after the first setup phase).
+constexpr long long job_bytes_sz(long long n, long long ksz) {
+  long long b = 0;
+  auto add = [&b](long long count, long long sz) { b += (count * sz + 255) & ~255ll; };
+  const long long nb = (n + kCpBlock - 1) / kCpBlock;
+  add(n, 1); add(n, 2);                       // otype, olm
+  for (int i = 0; i < 5; ++i) add(n, 4);      // ds, as, dds, das, ext
+  add(n, ksz); add(n, 4); add(n, 4); add(n, 4);  // delta, counter, touched, mm
+  add(n, 4); add(n, 1); add(n, 4); add(n, 4); add(n, 4);  // mm_next, mstat, dirty, dstamp, rstamp
+  add(n, 8); add(n, 4); add(n, 4);            // claim, taken, taken1
+  for (int i = 0; i < 4; ++i) add(n, 4);      // cand, cand_next, flagged, flagged1
+  add(4 * nb, 4);                             // CP block counts
+  add(n, 4); add(n, 4); add(n, 4); add(n, 4); // CP lists
+  add(n * kRowStride, 4); add(n * 2, 4); add(n, 1);
+  add(n * kRowStride, 4); add(n * 2, 4); add(n, 1);
+  for (int i = 0; i < 4; ++i) add(n, 4);      // per maximum
+  for (int i = 0; i < 4; ++i) add(n, 4);      // per minimum
+  add(n, ksz); add(n, 4);                     // extreme-saddle scratch
+  add(8, 8);                                  // checksum
+  return b + 4096;
+}
+template <class T>
+constexpr long long job_bytes(long long n) {
+  return job_bytes_sz(n, sizeof(typename KeyOf<T>::K));
+}
+constexpr long long job_bytes_max(long long n) { return job_bytes_sz(n, 8); }
+
+// One job's host-side state.
+template <class T>
+struct JobHost {
+  using K = typename KeyOf<T>::K;
+  bool used = false;
+  int pc = PC_DONE;
+  int block = 0;          // 0 = before the loop, 1..3 = block of an outer iteration
+  bool waiting = false;   // stopped at a branch that needs this tick's counters
+  int outer = 0, rounds = 0, cloop_total = 0, manifold_rounds = 0;
+  int nfc = 0, nfc1 = 0;
+  int c[11] = {0};        // loop-test counters (:5603-5605)
+  bool dense_done = false;
+  int status = EXTREMZ_OK;
+  extremz_params p{};
+  Job<T> J{};
+  Arena arena;
+  bool own_arena = false;
+  int ntiles = 0, nb = 0;
+  int* bcount = nullptr;
+  unsigned long long* checksum = nullptr;
+  int32_t* trace = nullptr;
+  int trace_cap = 0, trace_len = 0;
+  std::vector<int> pending;  // trace phases to emit once the tick's counters are back
+  long long tag = 0;
+
+  void emit(int phase, int a = 0, int b = 0, int c3 = 0) {
+    if (!trace || trace_len + 4 > trace_cap) return;
+    trace[trace_len++] = phase;
+    trace[trace_len++] = a;
+    trace[trace_len++] = b;
+    trace[trace_len++] = c3;
+  }
+};
+
+template <class T>
+class BatchEngine {
+ public:
+  using K = typename KeyOf<T>::K;
+
+  explicit BatchEngine(cudaStream_t st) : st_(st) {}
+  ~BatchEngine() { release_all(); }
+
+  int init(const DeviceTables* preset_tables, Arena* fixed_storage) {
+    if (ready_) return EXTREMZ_OK;
+    int dev = 0;
+    EZ_CHECK(cudaGetDevice(&dev));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    grid_ = sms * 8;
+    if (preset_tables) tb_ = *preset_tables;
+    else if (int rc = device_tables(&tb_)) return rc;
+    const size_t desc_bytes = sizeof(Job<T>) * kMaxSel;
+    const size_t map_bytes = sizeof(CUtensorMap) * 2 * kMaxSel;
+    const size_t ctr_bytes = sizeof(int) * C_COUNT * kMaxSel;
+    if (fixed_storage) {  // borrowed: carve the engine's arrays from it
+      jobs_dev_ = fixed_storage->template take<Job<T>>(kMaxSel);
+      maps_dev_ = fixed_storage->template take<CUtensorMap>(2 * kMaxSel);
+      ctr_dev_ = fixed_storage->template take<int>(C_COUNT * kMaxSel);
+      if (!jobs_dev_ || !maps_dev_ || !ctr_dev_) return EXTREMZ_OOM;
+      borrowed_ = true;
+      ctr_host_ = static_ctr_host_;
+    } else {
+      if (cudaMalloc(&jobs_dev_, desc_bytes) != cudaSuccess ||
+          cudaMalloc(&maps_dev_, map_bytes) != cudaSuccess ||
+          cudaMalloc(&ctr_dev_, ctr_bytes) != cudaSuccess ||
+          cudaMallocHost(&ctr_host_, ctr_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return EXTREMZ_OOM;
+      }
+    }
+    slots_.assign(kMaxSel, JobHost<T>());
+    ready_ = true;
+    return EXTREMZ_OK;
+  }
+
+  void release_all() {
+    for (auto& j : slots_) free_job(j);
+    if (!borrowed_) {
+      if (jobs_dev_) cudaFree(jobs_dev_);
+      if (maps_dev_) cudaFree(maps_dev_);
+      if (ctr_dev_) cudaFree(ctr_dev_);
+      if (ctr_host_) cudaFreeHost(ctr_host_);
+    }
+    jobs_dev_ = nullptr;
+    maps_dev_ = nullptr;
+    ctr_dev_ = nullptr;
+    ctr_host_ = nullptr;
+    ready_ = false;
+  }
+
+  int free_slots() const {
+    int n = 0;
+    for (const auto& j : slots_) n += !j.used;
+    return n;
+  }
+  int active() const {
+    int n = 0;
+    for (const auto& j : slots_) n += j.used && j.pc != PC_DONE;
+    return n;
+  }
+  long long launches() const { return launches_; }
+  void set_stream(cudaStream_t st) { st_ = st; }
+  // Stream-ordered pool the job workspaces come from (nullptr: the device's
+  // default pool).
+  void set_pool(cudaMemPool_t pool) { pool_mem_ = pool; }
+  void set_profile(bool on, int mask) {
+    profile_ = on;
+    profile_mask_ = mask;
+  }
+
+  // Admits a job.  storage: borrowed workspace (nullptr = allocate).
+  int admit(const T* f, T* g, int W, int H, int D, const extremz_params& p, int32_t* trace,
+            int trace_cap, Arena* storage, long long tag, int* slot_out) {
+    int slot = -1;
+    for (int i = 0; i < kMaxSel; ++i)
+      if (!slots_[i].used) {
+        slot = i;
+        break;
+      }
+    if (slot < 0) return EXTREMZ_OOM;
+    JobHost<T>& jh = slots_[slot];
+    jh = JobHost<T>();
+    jh.used = true;
+    jh.p = p;
+    jh.tag = tag;
+    jh.trace = trace;
+    jh.trace_cap = trace_cap;
+    Job<T>& J = jh.J;
+    std::memset(&J, 0, sizeof(J));
+    J.dim = Dims{W, H, D, W * H * D};
+    J.f = f;
+    J.g = g;
+    J.bound = (T)p.bound;
+    J.thr = (T)p.thr;
+    J.sentinel = T(-4.0) * J.bound;  // init_delta (:2572)
+    J.sentinel_key = KeyOf<T>::enc(J.sentinel);
+    J.q = p.q;
+    J.edit_type = p.edit_type;
+    J.iter_cap = p.device_iter_cap > 0 ? p.device_iter_cap : J.dim.N + 1;
+    J.tb = tb_;
+    J.ctr = ctr_dev_ + (size_t)slot * C_COUNT;
+    const int N = J.dim.N;
+    const long long need = job_bytes<T>(N);
+    if (storage) {
+      jh.arena = *storage;
+      jh.arena.used = 0;
+      if ((long long)jh.arena.cap < need) {
+        jh.used = false;
+        return EXTREMZ_OOM;
+      }
+    } else {
+      void* base = nullptr;
+      const cudaError_t e = pool_mem_ ? cudaMallocFromPoolAsync(&base, (size_t)need, pool_mem_, st_)
+                                      : cudaMallocAsync(&base, (size_t)need, st_);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        jh.used = false;
+        return EXTREMZ_OOM;
+      }
+      jh.arena.base = static_cast<char*>(base);
+      jh.arena.cap = (size_t)need;
+      jh.arena.fixed = true;
+      jh.own_arena = true;
+    }
+    Arena& A = jh.arena;
+    J.otype = A.take<int8_t>(N);
+    J.olm = A.take<uint16_t>(N);
+    J.ds = A.take<int>(N);
+    J.as = A.take<int>(N);
+    J.dds = A.take<int>(N);
+    J.das = A.take<int>(N);
+    J.ext = A.take<int>(N);
+    J.delta = A.take<K>(N);
+    J.counter = A.take<int>(N);
+    J.touched = A.take<int>(N);
+    J.mm = A.take<int>(N);
+    J.mm_next = A.take<int>(N);
+    J.mstat = A.take<uint8_t>(N);
+    J.dirty = A.take<int>(N);
+    J.dstamp = A.take<int>(N);
+    J.rstamp = A.take<int>(N);
+    J.claim = A.take<unsigned long long>(N);
+    J.taken = A.take<int>(N);
+    J.taken1 = A.take<int>(N);
+    J.cand = A.take<int>(N);
+    J.cand_next = A.take<int>(N);
+    J.flagged = A.take<int>(N);
+    J.flagged1 = A.take<int>(N);
+    jh.nb = (N + kCpBlock - 1) / kCpBlock;
+    jh.bcount = A.take<int>(4ll * jh.nb);
+    jh.ntiles = ((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);
+    // Tile maps of both fields (TMA when the stride allows).
+    CUtensorMap mf, mg;
+    const bool tma_ok = (p.flags & EXTREMZ_FLAG_NO_TMA) == 0;
+    J.tma_f = tma_ok && make_tile_map(&mf, f, J.dim);
+    J.tma_g = tma_ok && make_tile_map(&mg, (const T*)g, J.dim);
+    EZ_CHECK(cudaMemcpyAsync(maps_dev_ + 2 * slot, &mf, sizeof(mf), cudaMemcpyHostToDevice, st_));
+    EZ_CHECK(cudaMemcpyAsync(maps_dev_ + 2 * slot + 1, &mg, sizeof(mg), cudaMemcpyHostToDevice, st_));
+    J.map_f = maps_dev_ + 2 * slot;
+    J.map_g = maps_dev_ + 2 * slot + 1;
+    EZ_CHECK(cudaMemsetAsync(J.ctr, 0, C_COUNT * sizeof(int), st_));
+    EZ_CHECK(cudaMemcpyAsync(jobs_dev_ + slot, &J, sizeof(J), cudaMemcpyHostToDevice, st_));
+    jh.pc = PC_SETUP_A;
+    if (slot_out) *slot_out = slot;
+    return EXTREMZ_OK;
+  }
+
+  const JobHost<T>& job(int slot) const { return slots_[slot]; }
+
+  void fill_report(int slot, extremz_report* r) const {
+    const JobHost<T>& j = slots_[slot];
+    if (!r) return;
+    r->status = j.status;
+    r->outer_iters = j.outer;
+    r->cloop_rounds = j.cloop_total;
+    r->manifold_rounds = j.manifold_rounds;
+    std::memcpy(r->counters, j.c, sizeof(j.c));
+    r->error_bits = ctr_host_ ? ctr_host_[(size_t)slot * C_COUNT + C_ERROR] : 0;
+  }
+
+  // Releases a finished job's slot and (stream-ordered) its workspace.
+  void release(int slot) { free_job(slots_[slot]); }
+
+  // One tick: every phase any job is in, in program order; then one copy of
+  // all counter blocks and the branches.  Returns a status (the jobs keep
+  // their own statuses).
+  int tick() {
+    bool any = false;
+    for (int ph = 0; ph < PC_COUNT; ++ph) {
+      std::vector<int> sel;
+      for (int i = 0; i < kMaxSel; ++i)
+        if (slots_[i].used && !slots_[i].waiting && slots_[i].pc == ph) sel.push_back(i);
+      if (sel.empty()) continue;
+      any = true;
+      EZ_RUN(run_phase(ph, sel));
+    }
+    if (!any) return EXTREMZ_OK;
+    EZ_CHECK(cudaGetLastError());
+    EZ_CHECK(cudaMemcpyAsync(ctr_host_, ctr_dev_, sizeof(int) * C_COUNT * kMaxSel,
+                             cudaMemcpyDeviceToHost, st_));
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    for (int i = 0; i < kMaxSel; ++i) {
+      JobHost<T>& j = slots_[i];
+      if (!j.used || j.pc == PC_DONE) continue;
+      flush_pending(i);
+      if (h(i, C_ERROR)) {
+        finish(i, EXTREMZ_DEVICE_TIMEOUT);
+        continue;
+      }
+      if (j.waiting) {
+        j.waiting = false;
+        EZ_RUN(decide(i));
+      }
+    }
+    return EXTREMZ_OK;
+  }
+
+  // Per-class timing of the launches since set_profile(true, ...).
+  void collect_profile(extremz_report* rep) {
+    if (recs_.empty()) return;
+    cudaStreamSynchronize(st_);
+    for (const Rec& r : recs_) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      if (rep) {
+        rep->prof_ms[r.cls] += ms;
+        rep->prof_launches[r.cls] += 1;
+      }
+      pool_.push_back(r.a);
+      pool_.push_back(r.b);
+    }
+    recs_.clear();
+  }
+  void drop_profile_events() {
+    for (const Rec& r : recs_) {
+      pool_.push_back(r.a);
+      pool_.push_back(r.b);
+    }
+    recs_.clear();
+    for (cudaEvent_t e : pool_) cudaEventDestroy(e);
+    pool_.clear();
+  }
+
+ private:
+  cudaStream_t st_;
+  cudaMemPool_t pool_mem_ = nullptr;
+  bool ready_ = false, borrowed_ = false;
+  int grid_ = 1184;
+  DeviceTables tb_{};
+  Job<T>* jobs_dev_ = nullptr;
+  CUtensorMap* maps_dev_ = nullptr;
+  int* ctr_dev_ = nullptr;
+  int* ctr_host_ = nullptr;
+  int static_ctr_host_[C_COUNT * kMaxSel];
+  std::vector<JobHost<T>> slots_;
+  long long launches_ = 0;
+  bool profile_ = false;
+  int profile_mask_ = 0;
+  struct Rec { int cls; cudaEvent_t a, b; };
+  std::vector<Rec> recs_;
+  std::vector<cudaEvent_t> pool_;
+
+  int h(int slot, int c) const { return ctr_host_[(size_t)slot * C_COUNT + c]; }
+
+  cudaEvent_t event() {
+    if (!pool_.empty()) {
+      cudaEvent_t e = pool_.back();
+      pool_.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+
+  template <class... KArgs, class... Args>
+  void launch(int cls, void (*kern)(KArgs...), dim3 grid, dim3 block, Args... args) {
+    const bool timed = profile_ && (profile_mask_ == 0 || (profile_mask_ >> cls & 1));
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (timed) {
+      a = event();
+      b = event();
+      cudaEventRecord(a, st_);
+    }
+    kern<<<grid, block, 0, st_>>>(args...);
+    ++launches_;
+    if (timed) {
+      cudaEventRecord(b, st_);
+      recs_.push_back({cls, a, b});
+    }
+  }
+
+  void free_job(JobHost<T>& j) {
+    if (j.used && j.own_arena && j.arena.base) cudaFreeAsync(j.arena.base, st_);
+    j = JobHost<T>();
+  }
+
+  Sel make_sel(const std::vector<int>& slots, bool tiles) const {
+    Sel s;
+    std::memset(&s, 0, sizeof(s));
+    s.n = (int)slots.size();
+    int off = 0;
+    for (int k = 0; k < s.n; ++k) {
+      s.idx[k] = slots[k];
+      s.off[k] = off;
+      if (tiles) off += slots_[slots[k]].ntiles;
+    }
+    s.off[s.n] = off;
+    return s;
+  }
+
+  void ctl(const Sel& s, int op) { launch(K_OTHER, k_ctl<T>, 1, 64, jobs_dev_, s, op); }
+
+  // ------------------------------------------------------------- phases --
+  int run_phase(int ph, const std::vector<int>& sel) {
+    const Sel s = make_sel(sel, false);
+    const Sel st = make_sel(sel, true);
+    const Job<T>* jobs = jobs_dev_;
+    switch (ph) {
+      case PC_SETUP_A:
+        launch(K_SETUP, k_classify<T, false>, st.off[st.n], 256, jobs, st);
+        launch(K_DIRECTION, k_direction<T, false>, st.off[st.n], 256, jobs, st);
+        launch(K_JUMP, k_jump2<T, false>, grid_, 256, jobs, s);
+        for (int i : sel) {
+          JobHost<T>& j = slots_[i];
+          launch(K_OTHER, k_cp_count, j.nb, kCpBlock, (const int8_t*)j.J.otype, j.J.dim.N, j.bcount);
+          launch(K_OTHER, k_cp_scan, 1, 1024, j.bcount, j.nb, j.J.ctr);
+          j.waiting = true;
+        }
+        return EXTREMZ_OK;
+      case PC_SETUP_B:
+        for (int i : sel) EZ_RUN(setup_b(i));
+        for (int i : sel) slots_[i].pc = PC_CL_DETECT;
+        return EXTREMZ_OK;
+      case PC_CL_DETECT:
+        detect(sel);
+        for (int i : sel) slots_[i].waiting = true;
+        return EXTREMZ_OK;
+      case PC_CL_ROUND:
+        ctl(s, OP_ZERO_TOUCHED);
+        launch(K_PROPOSE, k_propose_cp<T>, grid_, 256, jobs, s);
+        launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
+        detect(sel);
+        for (int i : sel) slots_[i].waiting = true;
+        return EXTREMZ_OK;
+      case PC_RLOOPS:
+        ctl(s, OP_ZERO_TOUCHED);
+        launch(K_FIXPATH, k_fixpath<T, true>, grid_, 256, jobs, s);
+        launch(K_FIXPATH, k_fixpath<T, false>, grid_, 256, jobs, s);
+        launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
+        for (int i : sel) slots_[i].pc = PC_MANIFOLD;
+        return EXTREMZ_OK;
+      case PC_MANIFOLD:
+        launch(K_DIRECTION, k_direction<T, true>, st.off[st.n], 256, jobs, st);
+        launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, s);
+        ctl(s, OP_WN_BEGIN);
+        wrong_neighbours<true>(s);
+        wrong_neighbours<false>(s);
+        for (int i : sel) {
+          slots_[i].manifold_rounds++;
+          slots_[i].waiting = true;
+        }
+        return EXTREMZ_OK;
+      case PC_SLOOPS:
+        ctl(s, OP_SLOOPS_BEGIN);
+        launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, jobs, s, 1);
+        launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
+        for (int i : sel) slots_[i].waiting = true;
+        return EXTREMZ_OK;
+      case PC_SADDLE:
+        ctl(s, OP_SADDLE_BEGIN);
+        launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs, s, 1);
+        launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
+        for (int i : sel) {
+          slots_[i].pending.push_back(PH_SADDLE);
+          slots_[i].pc = joinb(slots_[i]);
+        }
+        return EXTREMZ_OK;
+      case PC_SLOOPS_J:
+        ctl(s, OP_SLOOPS_JOIN_BEGIN);
+        launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, jobs, s, 1);
+        launch(K_OTHER, k_wim_min2_scan<T>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wim_min2_collect<T>, grid_, 256, jobs, s);
+        launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
+        for (int i : sel) slots_[i].waiting = true;
+        return EXTREMZ_OK;
+      case PC_SADDLE_J:
+      case PC_FINAL_JOIN:
+        ctl(s, OP_SADDLE_JOIN_BEGIN);
+        launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs, s, 1);
+        launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
+        for (int i : sel) {
+          slots_[i].pending.push_back(PH_SADDLE_JOIN);
+          if (ph == PC_SADDLE_J) slots_[i].pc = endb(slots_[i]);
+          else slots_[i].waiting = true;
+        }
+        return EXTREMZ_OK;
+      case PC_PRE_END:
+        for (int i : sel) slots_[i].waiting = true;
+        return EXTREMZ_OK;
+      case PC_DET3:
+        ctl(s, OP_DETECT3_BEGIN);
+        launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, jobs, s, 0);
+        launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs, s, 0);
+        for (int i : sel) {
+          slots_[i].pending.push_back(PH_DETECT3);
+          slots_[i].pc = join3(slots_[i]);
+        }
+        return EXTREMZ_OK;
+      case PC_DET3J:
+        ctl(s, OP_DETECT3_JOIN_BEGIN);
+        launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, jobs, s, 0);
+        launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs, s, 0);
+        for (int i : sel) slots_[i].pc = PC_FINAL_DETECT;
+        return EXTREMZ_OK;
+      case PC_FINAL_DETECT:
+        detect(sel);
+        for (int i : sel) slots_[i].waiting = true;
+        return EXTREMZ_OK;
+      default:
+        return EXTREMZ_OK;
+    }
+  }
+
+  // Mismatch detection: dense the first time a job detects, then incremental
+  // over the neighbourhoods of the vertices changed since.
+  void detect(const std::vector<int>& sel) {
+    std::vector<int> dense, incr;
+    for (int i : sel) (slots_[i].dense_done ? incr : dense).push_back(i);
+    if (!dense.empty()) {
+      const Sel s = make_sel(dense, false), st = make_sel(dense, true);
+      ctl(s, OP_DETECT_DENSE_BEGIN);
+      launch(K_DETECT, k_classify<T, true>, st.off[st.n], 256, (const Job<T>*)jobs_dev_, st);
+      ctl(s, OP_DETECT_END_DENSE);
+      for (int i : dense) slots_[i].dense_done = true;
+    }
+    if (!incr.empty()) {
+      const Sel s = make_sel(incr, false);
+      ctl(s, OP_DETECT_BEGIN);
+      launch(K_DETECT, k_redetect<T>, grid_, 256, (const Job<T>*)jobs_dev_, s);
+      launch(K_DETECT, k_keep<T>, grid_, 256, (const Job<T>*)jobs_dev_, s);
+      ctl(s, OP_DETECT_END);
+    }
+  }
+
+  // Fused row-slot / candidate pass, bounded arbitration rounds and the
+  // sequential completion, for one side.
+  template <bool kSplit>
+  void wrong_neighbours(const Sel& s) {
+    const Job<T>* jobs = jobs_dev_;
+    ctl(s, OP_WN_SIDE_BEGIN);
+    launch(K_ROWS, k_saddle_pass<T, kSplit>, grid_, 256, jobs, s);
+    for (int r = 0; r < 3; ++r) {
+      ctl(s, OP_WN_ROUND_BEGIN);
+      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, jobs, s);
+      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, jobs, s);
+      ctl(s, OP_WN_ROUND_END);
+    }
+    launch(K_WRONG_NBR, k_wn_sequential<T, kSplit>, 1, 1, jobs, s);
+  }
+
+  int setup_b(int slot) {
+    JobHost<T>& jh = slots_[slot];
+    Job<T>& J = jh.J;
+    Arena& A = jh.arena;
+    const int N = J.dim.N;
+    const int ns2 = h(slot, C_NS2), ns1 = h(slot, C_NS1), nmax = h(slot, C_NMAX),
+              nmin = h(slot, C_NMIN);
+    J.sad2 = A.take<int>(ns2);
+    J.sad1 = A.take<int>(ns1);
+    J.maxima = A.take<int>(nmax);
+    J.minima = A.take<int>(nmin);
+    J.orow2 = A.take<int>((long long)ns2 * kRowStride);
+    J.drow2 = A.take<int>((long long)ns2 * 2);
+    J.ocnt2 = A.take<uint8_t>(ns2);
+    J.orow1 = A.take<int>((long long)ns1 * kRowStride);
+    J.drow1 = A.take<int>((long long)ns1 * 2);
+    J.ocnt1 = A.take<uint8_t>(ns1);
+    J.largest = A.take<int>(nmax);
+    J.first1 = A.take<int>(nmax);
+    J.flag2 = A.take<int>(nmax);
+    J.first_s = A.take<int>(nmax);
+    J.smallest = A.take<int>(nmin);
+    J.first_min1 = A.take<int>(nmin);
+    J.flag_min2 = A.take<int>(nmin);
+    J.first_sj = A.take<int>(nmin);
+    const int ne = std::max(nmax, nmin);
+    J.ext_key = A.take<K>(ne);
+    J.ext_id = A.take<int>(ne);
+    jh.checksum = A.take<unsigned long long>(8);
+    if (!jh.checksum) return EXTREMZ_OOM;
+    launch(K_OTHER, k_cp_write, jh.nb, kCpBlock, (const int8_t*)J.otype, N, (const int*)jh.bcount,
+           J.sad2, J.sad1, J.maxima, J.minima);
+    launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
+    launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.f, (const int*)J.ds, (const int*)J.sad2,
+           (int)C_NS2, J.orow2);
+    launch(K_ROWS, k_rows<T, false>, grid_, 256, J, J.f, (const int*)J.as, (const int*)J.sad1,
+           (int)C_NS1, J.orow1);
+    launch(K_SETUP, k_row_counts<T>, grid_, 256, J);
+    // Decompressed row slots start at zero: the reference's rows are fresh
+    // cudaMalloc memory read before first written (:5338-5341, :3128-3130).
+    if (ns2) EZ_CHECK(cudaMemsetAsync(J.drow2, 0, (size_t)ns2 * 2 * 4, st_));
+    if (ns1) EZ_CHECK(cudaMemsetAsync(J.drow1, 0, (size_t)ns1 * 2 * 4, st_));
+    if (nmax) {
+      launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, K(0), (long long)nmax);
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, -1, (long long)nmax);
+      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 0);
+      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 1);
+      EZ_CHECK(cudaMemcpyAsync(J.largest, J.ext_id, nmax * 4, cudaMemcpyDeviceToDevice, st_));
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.first1, kInf, (long long)nmax);
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_s, kInf, (long long)nmax);
+      EZ_CHECK(cudaMemsetAsync(J.flag2, 0, nmax * 4, st_));
+    }
+    if (nmin) {
+      launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, ~K(0), (long long)nmin);
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, kInf, (long long)nmin);
+      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 0);
+      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 1);
+      EZ_CHECK(cudaMemcpyAsync(J.smallest, J.ext_id, nmin * 4, cudaMemcpyDeviceToDevice, st_));
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_min1, kInf, (long long)nmin);
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_sj, kInf, (long long)nmin);
+      EZ_CHECK(cudaMemsetAsync(J.flag_min2, 0, nmin * 4, st_));
+    }
+    // Proposal buffer at the sentinel, edit counters at -1 (:5082), stamps 0.
+    launch(K_OTHER, k_fill<K>, grid_, 256, J.delta, J.sentinel_key, (long long)N);
+    launch(K_OTHER, k_fill<int>, grid_, 256, J.counter, -1, (long long)N);
+    EZ_CHECK(cudaMemsetAsync(J.claim, 0, (size_t)N * 8, st_));
+    EZ_CHECK(cudaMemsetAsync(J.taken, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.taken1, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.dstamp, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.rstamp, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemcpyAsync(jobs_dev_ + slot, &J, sizeof(J), cudaMemcpyHostToDevice, st_));
+    return EXTREMZ_OK;
+  }
+
+  // ----------------------------------------------------------- branches --
+  // Immediate successors (no counter needed).
+  int after_cl(JobHost<T>& j) {
+    if (j.block == 1) return PC_RLOOPS;
+    return PC_MANIFOLD;
+  }
+  int joinb(JobHost<T>& j) {
+    if (j.nfc1 == 0 && j.p.preserve_join) return PC_SLOOPS_J;
+    return endb(j);
+  }
+  int endb(JobHost<T>& j) {
+    if (j.block == 0) return PC_PRE_END;
+    j.block += 1;  // block 1 -> 2, 2 -> 3
+    j.rounds = 0;
+    return PC_CL_DETECT;
+  }
+  int join3(JobHost<T>& j) {
+    if (j.nfc1 == 0 && j.p.preserve_join) return PC_DET3J;
+    return PC_FINAL_DETECT;
+  }
+
+  void finish(int slot, int status) {
+    JobHost<T>& j = slots_[slot];
+    j.status = status;
+    j.pc = PC_DONE;
+  }
+
+  void flush_pending(int slot) {
+    JobHost<T>& j = slots_[slot];
+    for (int ph : j.pending) {
+      if (ph == PH_SADDLE) j.emit(PH_SADDLE, h(slot, C_WSC));
+      else if (ph == PH_SADDLE_JOIN) j.emit(PH_SADDLE_JOIN, h(slot, C_WSCJ));
+      else if (ph == PH_DETECT3) j.emit(PH_DETECT3, h(slot, C_WSC), h(slot, C_WMC), h(slot, C_WMC2));
+    }
+    j.pending.clear();
+  }
+
+  void snapshot(int slot) {
+    JobHost<T>& j = slots_[slot];
+    const int v[11] = {j.nfc, j.nfc1, h(slot, C_CMAX), h(slot, C_CMIN), h(slot, C_CSAD),
+                       h(slot, C_WMC), h(slot, C_WMC2), h(slot, C_WSC), h(slot, C_WMIN),
+                       h(slot, C_WMIN2), h(slot, C_WSCJ)};
+    std::memcpy(j.c, v, sizeof(v));
+  }
+
+  int loop_test(int slot) {
+    JobHost<T>& j = slots_[slot];
+    bool any = false;
+    for (int i = 0; i < 11; ++i) any |= j.c[i] > 0;
+    if (!any) {
+      if (j.p.final_join) j.pc = PC_FINAL_JOIN;
+      else finish(slot, EXTREMZ_OK);
+      return EXTREMZ_OK;
+    }
+    if (j.outer >= j.p.max_outer) {
+      finish(slot, EXTREMZ_ROUND_CAP);
+      return EXTREMZ_OK;
+    }
+    j.outer += 1;
+    j.block = 1;
+    j.rounds = 0;
+    j.pc = PC_CL_DETECT;
+    return EXTREMZ_OK;
+  }
+
+  int checksum_emit(int slot) {
+    JobHost<T>& j = slots_[slot];
+    if (!j.trace) return EXTREMZ_OK;
+    EZ_CHECK(cudaMemsetAsync(j.checksum, 0, 8, st_));
+    launch(K_OTHER, k_checksum<T>, grid_, 256, (const T*)j.J.g, j.J.dim.N, j.checksum);
+    unsigned long long hsum = 0;
+    EZ_CHECK(cudaMemcpyAsync(&hsum, j.checksum, 8, cudaMemcpyDeviceToHost, st_));
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    j.emit(PH_CHECKSUM, (int)(hsum & 0x7fffffff), (int)((hsum >> 31) & 0x7fffffff));
+    return EXTREMZ_OK;
+  }
+
+  // Branch of a job that stopped at a counter-dependent point.
+  int decide(int slot) {
+    JobHost<T>& j = slots_[slot];
+    switch (j.pc) {
+      case PC_SETUP_A:
+        j.pc = PC_SETUP_B;
+        return EXTREMZ_OK;
+      case PC_CL_DETECT:
+      case PC_CL_ROUND:
+        j.emit(PH_CLOOP_DETECT, h(slot, C_CMAX), h(slot, C_CMIN), h(slot, C_CSAD));
+        if (h(slot, C_MM) > 0) {
+          if (j.rounds >= j.p.max_cloop_rounds) {
+            finish(slot, EXTREMZ_ROUND_CAP);
+            return EXTREMZ_OK;
+          }
+          j.rounds += 1;
+          j.cloop_total += 1;
+          j.pc = PC_CL_ROUND;
+        } else {
+          j.pc = after_cl(j);
+        }
+        return EXTREMZ_OK;
+      case PC_MANIFOLD:
+        j.nfc = h(slot, C_NFC);
+        j.nfc1 = h(slot, C_NFC1);
+        j.emit(PH_WRONG_NBR, j.nfc, j.nfc1);
+        if (j.block == 3) j.pc = j.nfc == 0 ? PC_DET3 : join3(j);
+        else j.pc = j.nfc == 0 ? PC_SLOOPS : joinb(j);
+        return EXTREMZ_OK;
+      case PC_SLOOPS:
+        // s_loops refreshes the file-scope host copies (:3473-3476).
+        j.emit(PH_SLOOPS, h(slot, C_WMC), h(slot, C_WMC2));
+        j.pc = h(slot, C_WMC) == 0 ? PC_SADDLE : joinb(j);
+        return EXTREMZ_OK;
+      case PC_SLOOPS_J:
+        j.emit(PH_SLOOPS_JOIN, h(slot, C_WMIN), h(slot, C_WMIN2));
+        j.pc = h(slot, C_WMIN) == 0 ? PC_SADDLE_J : endb(j);
+        return EXTREMZ_OK;
+      case PC_PRE_END:  // :5589-5599
+        snapshot(slot);
+        return loop_test(slot);
+      case PC_FINAL_DETECT:
+        j.emit(PH_CLOOP_DETECT, h(slot, C_CMAX), h(slot, C_CMIN), h(slot, C_CSAD));
+        snapshot(slot);
+        j.emit(PH_OUTER, j.outer);
+        EZ_RUN(checksum_emit(slot));
+        return loop_test(slot);
+      case PC_FINAL_JOIN:
+        finish(slot, EXTREMZ_OK);
+        return EXTREMZ_OK;
+      default:
+        return EXTREMZ_OK;
+    }
+  }
+};
+
+}  // namespace extremz

@@ -11,10 +11,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <new>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/extremz.h"
@@ -148,654 +153,60 @@ struct Arena {
   }
 };
 
-struct Context {
-  int device = 0;
-  bool has_tables = false;  // tables given by the owner instead of device_tables()
-  DeviceTables tables{};
-  Arena arena;
-  Arena stage;           // device copies of host fields (extremz_correct_host)
-  int* h_ctr = nullptr;  // pinned copy of the counter block
-  unsigned long long wn_round = 0;
-  int wn_stamp = 0;
-  ~Context() {
-    if (arena.base && !arena.fixed) cudaFree(arena.base);
-    if (stage.base) cudaFree(stage.base);
-    if (h_ctr) cudaFreeHost(h_ctr);
-  }
-};
-
-// Kernel classes for the optional per-class timing (extremz_report.prof_*).
-enum KClass : int {
-  K_SETUP = 0, K_DETECT, K_DIRECTION, K_JUMP, K_PROPOSE, K_APPLY, K_ROWS, K_WRONG_NBR,
-  K_FIXPATH, K_OTHER, K_NUM
-};
-
-// Phases of the trace (same records as the oracle's trace).
-enum Phase : int {
-  PH_CLOOP_DETECT = 1, PH_WRONG_NBR = 2, PH_SLOOPS = 3, PH_SADDLE = 4, PH_DETECT3 = 5,
-  PH_SLOOPS_JOIN = 6, PH_SADDLE_JOIN = 7, PH_OUTER = 8, PH_CHECKSUM = 9
-};
-
-template <class T>
-__global__ void k_checksum(const T* __restrict__ a, int N, unsigned long long* out) {
-  unsigned long long acc = 0;
-  const int stride = gridDim.x * blockDim.x;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
-    unsigned long long bits = 0;
-    if (sizeof(T) == 8) bits = (unsigned long long)__double_as_longlong((double)a[v]);
-    else bits = (unsigned long long)__float_as_uint((float)a[v]);
-    unsigned long long z = bits + 0x9e3779b97f4a7c15ull * (unsigned long long)(v + 1);
-    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-    acc += z ^ (z >> 31);
-  }
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
-}
-
-template <class T>
-class Corrector {
- public:
-  using K = typename KeyOf<T>::K;
-
-  Corrector(Context& ctx, const T* f, T* g, int W, int H, int D, const extremz_params& p,
-            cudaStream_t st, int32_t* trace, int trace_cap)
-      : ctx_(ctx), p_(p), st_(st), trace_(trace), trace_cap_(trace_cap) {
-    std::memset(&J, 0, sizeof(J));
-    J.dim = Dims{W, H, D, W * H * D};
-    J.f = f;
-    J.g = g;
-    J.bound = (T)p.bound;
-    J.thr = (T)p.thr;
-    J.sentinel = T(-4.0) * J.bound;  // init_delta (:2572)
-    J.sentinel_key = KeyOf<T>::enc(J.sentinel);
-    J.q = p.q;
-    J.edit_type = p.edit_type;
-    profile_ = (p.flags & EXTREMZ_FLAG_PROFILE) != 0;
-    const bool tma_ok = (p.flags & EXTREMZ_FLAG_NO_TMA) == 0;
-    tma_f_ = tma_ok && make_tile_map(&map_f_, f, J.dim);
-    tma_g_ = tma_ok && make_tile_map(&map_g_, (const T*)g, J.dim);
-    profile_mask_ = (p.flags >> EXTREMZ_PROFILE_CLASS_SHIFT) & ((1 << K_NUM) - 1);
-  }
-
-  int run(extremz_report* rep) {
-    int rc = setup();
-    if (rc != EXTREMZ_OK) return rc;
-    rc = main_loop();
-    if (rep) {
-      rep->status = rc;
-      rep->outer_iters = outer_;
-      rep->cloop_rounds = cloop_rounds_;
-      rep->manifold_rounds = manifold_rounds_;
-      std::memcpy(rep->counters, hc_, sizeof(hc_));
-      rep->error_bits = ctx_.h_ctr[C_ERROR];
-      rep->kernel_launches = launches_;
-    }
-    finish_profile(rep);
-    return rc;
-  }
-
- private:
-  Context& ctx_;
-  extremz_params p_;
-  cudaStream_t st_;
-  int32_t* trace_;
-  int trace_cap_, trace_len_ = 0;
-  Job<T> J;
-  int grid_ = 0;
-  int outer_ = 0, cloop_rounds_ = 0, manifold_rounds_ = 0;
-  bool capped_ = false;
-  int hc_[11] = {0};
-  int* ctr_ = nullptr;
-
-  CUtensorMap map_f_, map_g_;
-  bool tma_f_ = false, tma_g_ = false;
-  // The job descriptor lives in device memory; every per-round kernel takes
-  // the descriptor array and a selection (here: the one job).
-  Job<T>* jobs_dev_ = nullptr;
-  CUtensorMap* maps_dev_ = nullptr;
-  Sel sel1_;
-
-  const Job<T>* jobs() const { return jobs_dev_; }
-  int ntiles() const {
-    return ((J.dim.W + TX - 1) / TX) * ((J.dim.H + TY - 1) / TY) * ((J.dim.D + TZ - 1) / TZ);
-  }
-  int upload_job() {
-    EZ_CHECK(cudaMemcpyAsync(jobs_dev_, &J, sizeof(J), cudaMemcpyHostToDevice, st_));
-    return EXTREMZ_OK;
-  }
-  void swap_lists(int which) { launch(K_OTHER, k_swap_lists<T>, 1, 32, jobs_dev_, sel1_, which); }
-
-  long long launches_ = 0;
-  bool profile_ = false;
-  int profile_mask_ = 0;
-  struct Rec { int cls; cudaEvent_t a, b; };
-  std::vector<Rec> recs_;
-  std::vector<cudaEvent_t> pool_;
-
-  cudaEvent_t event() {
-    if (!pool_.empty()) {
-      cudaEvent_t e = pool_.back();
-      pool_.pop_back();
-      return e;
-    }
-    cudaEvent_t e;
-    cudaEventCreate(&e);
-    return e;
-  }
-
-  // Every kernel goes through here: counted, and bracketed by events when
-  // per-class timing is on.
-  template <class... KArgs, class... Args>
-  void launch(int cls, void (*kern)(KArgs...), dim3 grid, dim3 block, Args... args) {
-    cudaEvent_t a = nullptr, b = nullptr;
-    const bool timed = profile_ && (profile_mask_ == 0 || (profile_mask_ >> cls & 1));
-    if (timed) {
-      a = event();
-      b = event();
-      cudaEventRecord(a, st_);
-    }
-    kern<<<grid, block, 0, st_>>>(args...);
-    ++launches_;
-    if (timed) {
-      cudaEventRecord(b, st_);
-      recs_.push_back({cls, a, b});
-    }
-  }
-
-  void finish_profile(extremz_report* rep) {
-    if (!profile_) return;
-    cudaStreamSynchronize(st_);
-    for (const Rec& r : recs_) {
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, r.a, r.b);
-      if (rep) {
-        rep->prof_ms[r.cls] += ms;
-        rep->prof_launches[r.cls] += 1;
-      }
-      pool_.push_back(r.a);
-      pool_.push_back(r.b);
-    }
-    recs_.clear();
-    for (cudaEvent_t e : pool_) cudaEventDestroy(e);
-    pool_.clear();
-  }
-
-  int iter_cap() const { return p_.device_iter_cap > 0 ? p_.device_iter_cap : J.dim.N + 1; }
-
-  int sm_count() {
-    int dev = 0, n = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    return n;
-  }
-
-  void emit(int phase, int a = 0, int b = 0, int c = 0) {
-    if (!trace_ || trace_len_ + 4 > trace_cap_) return;
-    trace_[trace_len_++] = phase;
-    trace_[trace_len_++] = a;
-    trace_[trace_len_++] = b;
-    trace_[trace_len_++] = c;
-  }
-
-  int zero(int slot, int n = 1) {
-    EZ_CHECK(cudaMemsetAsync(ctr_ + slot, 0, n * sizeof(int), st_));
-    return EXTREMZ_OK;
-  }
-  int read_ctr() {
-    EZ_CHECK(cudaMemcpyAsync(ctx_.h_ctr, ctr_, C_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st_));
-    EZ_CHECK(cudaStreamSynchronize(st_));
-    if (ctx_.h_ctr[C_ERROR]) return EXTREMZ_DEVICE_TIMEOUT;
-    return EXTREMZ_OK;
-  }
-  int h(int slot) const { return ctx_.h_ctr[slot]; }
-  int launched() {
-    EZ_CHECK(cudaGetLastError());
-    return EXTREMZ_OK;
-  }
-  dim3 tile_grid() const {
-    return dim3((J.dim.W + TX - 1) / TX, (J.dim.H + TY - 1) / TY, (J.dim.D + TZ - 1) / TZ);
-  }
-
-#define EZ_RUN(expr)               \
-  do {                             \
-    int rc_ = (expr);              \
+#define EZ_RUN(expr)                   \
+  do {                                 \
+    int rc_ = (expr);                  \
     if (rc_ != EXTREMZ_OK) return rc_; \
   } while (0)
 
-  // ---------------------------------------------------------------- setup --
-  int setup() {
-    const int N = J.dim.N;
-    if (ctx_.has_tables) J.tb = ctx_.tables;
-    else EZ_RUN(device_tables(&J.tb));
-    if (!ctx_.h_ctr) EZ_CHECK(cudaMallocHost(&ctx_.h_ctr, C_COUNT * sizeof(int)));
-    grid_ = sm_count() * 8;
-    const int nb = (N + kCpBlock - 1) / kCpBlock;
-    // Phase-1 arena: per-voxel arrays and the CP block counts.  The per-CP
-    // arrays are carved after the counts are known.
-    auto bytes_for = [&](long long ns2, long long ns1, long long nmax, long long nmin) {
-      long long b = 0;
-      auto add = [&](long long count, long long sz) { b += (count * sz + 255) & ~255ll; };
-      add(C_COUNT, 4);
-      add(N, 1); add(N, 2);                    // otype, olm
-      for (int i = 0; i < 5; ++i) add(N, 4);   // ds, as, dds, das, ext
-      add(N, sizeof(K)); add(N, 4); add(N, 4); add(N, 4);  // delta, counter, touched, mm
-      add(N, 4); add(N, 1); add(N, 4); add(N, 4); add(N, 4);  // mm_next, mstat, dirty, dstamp, rstamp
-      add(N, 8); add(N, 4); add(N, 4);         // claim, taken, taken1
-      for (int i = 0; i < 4; ++i) add(N, 4);   // cand, cand_next, flagged, flagged1
-      add(4ll * nb, 4);                        // cp block counts
-      add(ns2, 4); add(ns1, 4); add(nmax, 4); add(nmin, 4);
-      add(ns2 * kRowStride, 4); add(ns2 * 2, 4); add(ns2, 1);
-      add(ns1 * kRowStride, 4); add(ns1 * 2, 4); add(ns1, 1);
-      for (int i = 0; i < 4; ++i) add(nmax, 4);  // largest, first1, flag2, first_s
-      for (int i = 0; i < 4; ++i) add(nmin, 4);  // smallest, first_min1, flag_min2, first_sj
-      long long ne = std::max(nmax, nmin);
-      add(ne, sizeof(K)); add(ne, 4);
-      add(8, 8);  // checksum
-      return b;
-    };
-    // Worst case for the CP lists is N each; reserve that up front so the
-    // arena is never re-allocated between the two phases.
-    long long worst = bytes_for(N, N, N, N);
-    int rc = ctx_.arena.reserve((size_t)worst);
-    if (rc != EXTREMZ_OK) return rc;
-    Arena& A = ctx_.arena;
-    A.used = 0;
-    ctr_ = J.ctr = A.take<int>(C_COUNT);
-    J.otype = A.take<int8_t>(N);
-    J.olm = A.take<uint16_t>(N);
-    J.ds = A.take<int>(N); J.as = A.take<int>(N);
-    J.dds = A.take<int>(N); J.das = A.take<int>(N);
-    J.ext = A.take<int>(N);
-    J.delta = A.take<K>(N);
-    J.counter = A.take<int>(N);
-    J.touched = A.take<int>(N);
-    J.mm = A.take<int>(N);
-    J.mm_next = A.take<int>(N);
-    J.mstat = A.take<uint8_t>(N);
-    J.dirty = A.take<int>(N);
-    J.dstamp = A.take<int>(N);
-    J.rstamp = A.take<int>(N);
-    J.claim = A.take<unsigned long long>(N);
-    J.taken = A.take<int>(N); J.taken1 = A.take<int>(N);
-    J.cand = A.take<int>(N); J.cand_next = A.take<int>(N);
-    J.flagged = A.take<int>(N); J.flagged1 = A.take<int>(N);
-    int* bcount = A.take<int>(4ll * nb);
-    jobs_dev_ = A.take<Job<T>>(1);
-    maps_dev_ = A.take<CUtensorMap>(2);
-    if (!jobs_dev_ || !maps_dev_) return EXTREMZ_OOM;
-    EZ_CHECK(cudaMemcpyAsync(maps_dev_, &map_f_, sizeof(CUtensorMap), cudaMemcpyHostToDevice, st_));
-    EZ_CHECK(cudaMemcpyAsync(maps_dev_ + 1, &map_g_, sizeof(CUtensorMap), cudaMemcpyHostToDevice, st_));
-    J.map_f = maps_dev_;
-    J.map_g = maps_dev_ + 1;
-    J.tma_f = tma_f_;
-    J.tma_g = tma_g_;
-    std::memset(&sel1_, 0, sizeof(sel1_));
-    sel1_.n = 1;
-    sel1_.idx[0] = 0;
-    sel1_.off[0] = 0;
-    sel1_.off[1] = ntiles();
-    EZ_RUN(upload_job());
-    EZ_CHECK(cudaMemsetAsync(ctr_, 0, C_COUNT * sizeof(int), st_));
+}  // namespace extremz
 
-    // Original classification and manifolds.
-    launch(K_SETUP, k_classify<T, false>, ntiles(), 256, jobs(), sel1_);
-    launch(K_DIRECTION, k_direction<T, false>, ntiles(), 256, jobs(), sel1_);
-    launch(K_JUMP, k_jump2<T, false>, grid_, 256, jobs(), sel1_, iter_cap());
-    EZ_RUN(launched());
-    // Critical-point lists in ascending id.
-    launch(K_OTHER, k_cp_count, nb, kCpBlock, J.otype, N, bcount);
-    launch(K_OTHER, k_cp_scan, 1, 1024, bcount, nb, ctr_);
-    EZ_RUN(launched());
-    EZ_RUN(read_ctr());
-    const int ns2 = h(C_NS2), ns1 = h(C_NS1), nmax = h(C_NMAX), nmin = h(C_NMIN);
-    J.sad2 = A.take<int>(ns2); J.sad1 = A.take<int>(ns1);
-    J.maxima = A.take<int>(nmax); J.minima = A.take<int>(nmin);
-    J.orow2 = A.take<int>((long long)ns2 * kRowStride);
-    J.drow2 = A.take<int>((long long)ns2 * 2);
-    J.ocnt2 = A.take<uint8_t>(ns2);
-    J.orow1 = A.take<int>((long long)ns1 * kRowStride);
-    J.drow1 = A.take<int>((long long)ns1 * 2);
-    J.ocnt1 = A.take<uint8_t>(ns1);
-    J.largest = A.take<int>(nmax); J.first1 = A.take<int>(nmax);
-    J.flag2 = A.take<int>(nmax); J.first_s = A.take<int>(nmax);
-    J.smallest = A.take<int>(nmin); J.first_min1 = A.take<int>(nmin);
-    J.flag_min2 = A.take<int>(nmin); J.first_sj = A.take<int>(nmin);
-    const int ne = std::max(nmax, nmin);
-    J.ext_key = A.take<K>(ne);
-    J.ext_id = A.take<int>(ne);
-    checksum_ = A.take<unsigned long long>(8);
-    EZ_RUN(upload_job());
-    launch(K_OTHER, k_cp_write, nb, kCpBlock, J.otype, N, bcount, J.sad2, J.sad1, J.maxima, J.minima);
-    launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
-    launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.f, J.ds, J.sad2, C_NS2, J.orow2);
-    launch(K_ROWS, k_rows<T, false>, grid_, 256, J, J.f, J.as, J.sad1, C_NS1, J.orow1);
-    launch(K_SETUP, k_row_counts<T>, grid_, 256, J);
-    EZ_RUN(launched());
-    // Decompressed row slots start at zero: the reference's rows are fresh
-    // cudaMalloc memory read before first written (:5338-5341, :3128-3130).
-    if (ns2) EZ_CHECK(cudaMemsetAsync(J.drow2, 0, (size_t)ns2 * 2 * 4, st_));
-    if (ns1) EZ_CHECK(cudaMemsetAsync(J.drow1, 0, (size_t)ns1 * 2 * 4, st_));
-    // Largest saddle per maximum, smallest per minimum (original field).
-    if (nmax) {
-      launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, K(0), nmax);
-      launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, -1, nmax);
-      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 0);
-      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 1);
-      EZ_CHECK(cudaMemcpyAsync(J.largest, J.ext_id, nmax * 4, cudaMemcpyDeviceToDevice, st_));
-      launch(K_OTHER, k_fill<int>, grid_, 256, J.first1, kInf, nmax);
-      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_s, kInf, nmax);
-      EZ_CHECK(cudaMemsetAsync(J.flag2, 0, nmax * 4, st_));
-    }
-    if (nmin) {
-      launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, ~K(0), nmin);
-      launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, kInf, nmin);
-      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 0);
-      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 1);
-      EZ_CHECK(cudaMemcpyAsync(J.smallest, J.ext_id, nmin * 4, cudaMemcpyDeviceToDevice, st_));
-      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_min1, kInf, nmin);
-      launch(K_OTHER, k_fill<int>, grid_, 256, J.first_sj, kInf, nmin);
-      EZ_CHECK(cudaMemsetAsync(J.flag_min2, 0, nmin * 4, st_));
-    }
-    // Proposal buffer at the sentinel, counters at -1 (:5082), stamps at 0.
-    launch(K_OTHER, k_fill<K>, grid_, 256, J.delta, J.sentinel_key, N);
-    launch(K_OTHER, k_fill<int>, grid_, 256, J.counter, -1, N);
-    EZ_CHECK(cudaMemsetAsync(J.claim, 0, (size_t)N * 8, st_));
-    EZ_CHECK(cudaMemsetAsync(J.taken, 0, (size_t)N * 4, st_));
-    EZ_CHECK(cudaMemsetAsync(J.taken1, 0, (size_t)N * 4, st_));
-    EZ_CHECK(cudaMemsetAsync(J.dstamp, 0, (size_t)N * 4, st_));
-    EZ_CHECK(cudaMemsetAsync(J.rstamp, 0, (size_t)N * 4, st_));
-    EZ_RUN(launched());
+#include "extremz_batch.cuh"
+
+namespace extremz {
+
+// A stream-ordered pool that keeps what it has grown to: workspaces of
+// successive corrections reuse the same memory without returning it to the
+// driver at every synchronisation.
+static cudaMemPool_t make_pool(int dev) {
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  uint64_t keep = ~uint64_t(0);
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  return pool;
+}
+
+struct Context {
+  int device = 0;
+  Arena stage;  // device copies of host fields (extremz_correct_host)
+  cudaMemPool_t pool = nullptr;
+  BatchEngine<float> e32{nullptr};
+  BatchEngine<double> e64{nullptr};
+  int ensure_pool() {
+    if (pool) return EXTREMZ_OK;
+    pool = make_pool(device);
+    if (!pool) return EXTREMZ_OOM;
+    e32.set_pool(pool);
+    e64.set_pool(pool);
     return EXTREMZ_OK;
   }
-
-  int dirty_epoch_ = 1, detect_epoch_ = 0;
-  bool dense_done_ = false;
-
-  unsigned long long* checksum_ = nullptr;
-
-  int checksum_emit() {
-    if (!trace_) return EXTREMZ_OK;
-    EZ_CHECK(cudaMemsetAsync(checksum_, 0, 8, st_));
-    launch(K_OTHER, k_checksum<T>, grid_, 256, J.g, J.dim.N, checksum_);
-    unsigned long long hsum = 0;
-    EZ_CHECK(cudaMemcpyAsync(&hsum, checksum_, 8, cudaMemcpyDeviceToHost, st_));
-    EZ_CHECK(cudaStreamSynchronize(st_));
-    emit(PH_CHECKSUM, (int)(hsum & 0x7fffffff), (int)((hsum >> 31) & 0x7fffffff));
-    return EXTREMZ_OK;
-  }
-
-  // ------------------------------------------------------------- c_loops --
-  // Mismatch detection: dense the first time, then incremental over the
-  // neighbourhoods of the vertices changed since the previous detection.
-  int detect() {
-    if (!dense_done_) {
-      EZ_RUN(zero(C_MM, 4));
-      launch(K_DETECT, k_classify<T, true>, ntiles(), 256, jobs(), sel1_);
-      dense_done_ = true;
-    } else {
-      ++detect_epoch_;
-      EZ_RUN(zero(C_MM_NEXT));
-      EZ_RUN(zero(C_CMAX, 3));
-      launch(K_DETECT, k_redetect<T>, grid_, 256, jobs(), sel1_, detect_epoch_);
-      launch(K_DETECT, k_keep<T>, grid_, 256, jobs(), sel1_, detect_epoch_);
-      swap_lists(0);
+  ~Context() {
+    e32.release_all();
+    e64.release_all();
+    if (pool) {
+      cudaDeviceSynchronize();
+      cudaMemPoolDestroy(pool);
     }
-    EZ_RUN(zero(C_DIRTY));
-    ++dirty_epoch_;
-    EZ_RUN(launched());
-    EZ_RUN(read_ctr());
-    emit(PH_CLOOP_DETECT, h(C_CMAX), h(C_CMIN), h(C_CSAD));
-    return EXTREMZ_OK;
+    if (stage.base) cudaFree(stage.base);
   }
-
-  int apply() {
-    launch(K_APPLY, k_apply<T>, grid_, 256, jobs(), sel1_, dirty_epoch_);
-    return launched();
-  }
-
-  // c_loops (:3913-4044).
-  int c_loops() {
-    EZ_RUN(detect());
-    int rounds = 0;
-    while (h(C_MM) > 0) {
-      if (rounds >= p_.max_cloop_rounds) {
-        capped_ = true;
-        return EXTREMZ_OK;
-      }
-      ++rounds;
-      ++cloop_rounds_;
-      EZ_RUN(zero(C_TOUCHED));
-      launch(K_PROPOSE, k_propose_cp<T>, grid_, 256, jobs(), sel1_);
-      EZ_RUN(launched());
-      EZ_RUN(apply());
-      EZ_RUN(detect());
-    }
-    return EXTREMZ_OK;
-  }
-
-  // ----------------------------------------------------------- manifolds --
-  // One manifold round: decompressed steepest roots, then per saddle side the
-  // fused row-slot / candidate pass and the wrong-neighbour arbitration
-  // (ComputeDirection + Compute*Manifold, findAscPaths / findDescPaths,
-  // get_wrong_split_neighbors / get_wrong_join_neighbors).
-  int manifold_block() {
-    ++manifold_rounds_;
-    const int N = J.dim.N;
-    launch(K_DIRECTION, k_direction<T, true>, ntiles(), 256, jobs(), sel1_);
-    launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs(), sel1_, iter_cap());
-    const int stamp = ++ctx_.wn_stamp;
-    EZ_RUN(zero(C_NFC, 2));
-    EZ_RUN(resolve_side<true>(stamp));
-    EZ_RUN(resolve_side<false>(stamp));
-    EZ_RUN(read_ctr());
-    emit(PH_WRONG_NBR, h(C_NFC), h(C_NFC1));
-    return EXTREMZ_OK;
-  }
-
-  // Bounded device rounds of vote / commit, then the sequential completion
-  // for whatever is left; no host round trip.
-  template <bool kSplit>
-  int resolve_side(int stamp) {
-    EZ_RUN(zero(C_CAND));
-    launch(K_ROWS, k_saddle_pass<T, kSplit>, grid_, 256, jobs(), sel1_);
-    const int kRounds = 3;
-    for (int r = 0; r < kRounds; ++r) {
-      const unsigned long long round = ++ctx_.wn_round;
-      EZ_RUN(zero(C_CAND_NEXT));
-      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, jobs(), sel1_, round, stamp);
-      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, jobs(), sel1_, round, stamp);
-      swap_lists(1);
-    }
-    launch(K_WRONG_NBR, k_wn_sequential<T, kSplit>, 1, 1, jobs(), sel1_, stamp);
-    return launched();
-  }
-
-  // r_loops (:4210-4227).
-  int r_loops() {
-    EZ_RUN(zero(C_TOUCHED));
-    launch(K_FIXPATH, k_fixpath<T, true>, grid_, 256, jobs(), sel1_, iter_cap());
-    launch(K_FIXPATH, k_fixpath<T, false>, grid_, 256, jobs(), sel1_, iter_cap());
-    EZ_RUN(launched());
-    return apply();
-  }
-
-  // s_loops (:3465-3487).
-  int s_loops() {
-    EZ_RUN(zero(C_WMC, 2));
-    EZ_RUN(zero(C_TOUCHED));
-    launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs(), sel1_);
-    launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, jobs(), sel1_, 1);
-    EZ_RUN(launched());
-    EZ_RUN(apply());
-    // s_loops refreshes the reference's file-scope host copies (:3473-3476);
-    // the first block branches on them right away.
-    EZ_RUN(read_ctr());
-    emit(PH_SLOOPS, h(C_WMC), h(C_WMC2));
-    return EXTREMZ_OK;
-  }
-
-  // saddle_loops (:4229-4243).
-  int saddle_loops() {
-    EZ_RUN(zero(C_WSC));
-    EZ_RUN(zero(C_TOUCHED));
-    launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs(), sel1_);
-    launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs(), sel1_, 1);
-    EZ_RUN(launched());
-    EZ_RUN(apply());
-    if (trace_) {
-      EZ_RUN(read_ctr());
-      emit(PH_SADDLE, h(C_WSC));
-    }
-    return EXTREMZ_OK;
-  }
-
-  // s_loops_join (:3489-3512).
-  int s_loops_join() {
-    EZ_RUN(zero(C_WMIN, 2));
-    EZ_RUN(zero(C_TOUCHED));
-    launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, jobs(), sel1_);
-    launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, jobs(), sel1_, 1);
-    launch(K_OTHER, k_wim_min2_scan<T>, grid_, 256, jobs(), sel1_);
-    launch(K_OTHER, k_wim_min2_collect<T>, grid_, 256, jobs(), sel1_);
-    EZ_RUN(launched());
-    EZ_RUN(apply());
-    if (trace_) {
-      EZ_RUN(read_ctr());
-      emit(PH_SLOOPS_JOIN, h(C_WMIN), h(C_WMIN2));
-    }
-    return EXTREMZ_OK;
-  }
-
-  // saddle_loops_join (:4245-4261).
-  int saddle_loops_join() {
-    EZ_RUN(zero(C_WSCJ));
-    EZ_RUN(zero(C_TOUCHED));
-    launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs(), sel1_);
-    launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs(), sel1_, 1);
-    EZ_RUN(launched());
-    EZ_RUN(apply());
-    if (trace_) {
-      EZ_RUN(read_ctr());
-      emit(PH_SADDLE_JOIN, h(C_WSCJ));
-    }
-    return EXTREMZ_OK;
-  }
-
-  // --------------------------------------------------------------- main --
-  // main() (:5508-5997).  The reference's host counters: c_loops and r_loops
-  // take them by value (main's copies unchanged); s_loops, saddle_loops and
-  // the join variants refresh the file-scope copies of wrong_max(_2),
-  // wrong_saddle, wrong_min(_2) and wrong_saddle_join (:62, :3473-3476,
-  // :4236, :3498-3501, :4252).  Each device counter changes only in the call
-  // that refreshes its host copy, so reading the counter block at the end of
-  // an iteration yields exactly those copies.
-  int main_loop() {
-    const bool join = p_.preserve_join != 0;
-    EZ_RUN(c_loops());
-    if (capped_) return EXTREMZ_ROUND_CAP;
-    EZ_RUN(manifold_block());
-    int nfc = h(C_NFC), nfc1 = h(C_NFC1);
-    if (nfc == 0) {
-      EZ_RUN(s_loops());
-      if (h(C_WMC) == 0) EZ_RUN(saddle_loops());
-    }
-    if (nfc1 == 0 && join) {
-      EZ_RUN(s_loops_join());
-      EZ_RUN(read_ctr());
-      if (h(C_WMIN) == 0) EZ_RUN(saddle_loops_join());
-    }
-    EZ_RUN(read_ctr());  // :5589-5599
-    auto snapshot = [&](int* c) {
-      const int v[11] = {nfc, nfc1, h(C_CMAX), h(C_CMIN), h(C_CSAD), h(C_WMC),
-                         h(C_WMC2), h(C_WSC), h(C_WMIN), h(C_WMIN2), h(C_WSCJ)};
-      std::memcpy(c, v, sizeof(v));
-    };
-    nfc = h(C_NFC);
-    nfc1 = h(C_NFC1);
-    int c[11];
-    snapshot(c);
-    auto any = [&] {
-      for (int i = 0; i < 11; ++i)
-        if (c[i] > 0) return true;
-      return false;
-    };
-    while (any()) {
-      if (outer_ >= p_.max_outer) {
-        capped_ = true;
-        break;
-      }
-      ++outer_;
-      // Block 1 (:5622-5747).
-      EZ_RUN(c_loops());
-      if (capped_) break;
-      EZ_RUN(r_loops());
-      EZ_RUN(manifold_block());
-      nfc = h(C_NFC);
-      nfc1 = h(C_NFC1);
-      if (nfc == 0) {
-        EZ_RUN(s_loops());
-        if (h(C_WMC) == 0) EZ_RUN(saddle_loops());
-      }
-      if (nfc1 == 0 && join) {
-        EZ_RUN(s_loops_join());
-        EZ_RUN(read_ctr());
-        if (h(C_WMIN) == 0) EZ_RUN(saddle_loops_join());
-      }
-      // Block 2 (:5749-5870).
-      EZ_RUN(c_loops());
-      if (capped_) break;
-      EZ_RUN(manifold_block());
-      nfc = h(C_NFC);
-      nfc1 = h(C_NFC1);
-      if (nfc == 0) {
-        EZ_RUN(s_loops());
-        if (h(C_WMC) == 0) EZ_RUN(saddle_loops());
-      }
-      if (nfc1 == 0 && join) {
-        EZ_RUN(s_loops_join());
-        EZ_RUN(read_ctr());
-        if (h(C_WMIN) == 0) EZ_RUN(saddle_loops_join());
-      }
-      // Block 3 (:5872-5979): detection only.
-      EZ_RUN(c_loops());
-      if (capped_) break;
-      EZ_RUN(manifold_block());
-      nfc = h(C_NFC);
-      nfc1 = h(C_NFC1);
-      if (nfc == 0) {
-        EZ_RUN(zero(C_WMC, 2));
-        EZ_RUN(zero(C_WSC));
-        launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs(), sel1_);
-        launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, jobs(), sel1_, 0);
-        launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs(), sel1_);
-        launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs(), sel1_, 0);
-        EZ_RUN(launched());
-        if (trace_) {
-          EZ_RUN(read_ctr());
-          emit(PH_DETECT3, h(C_WSC), h(C_WMC), h(C_WMC2));
-        }
-      }
-      if (nfc1 == 0 && join) {
-        EZ_RUN(zero(C_WMIN, 2));
-        EZ_RUN(zero(C_WSCJ));
-        launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, jobs(), sel1_);
-        launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, jobs(), sel1_, 0);
-        launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs(), sel1_);
-        launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs(), sel1_, 0);
-        EZ_RUN(launched());
-      }
-      EZ_RUN(detect());  // reads the whole counter block
-      snapshot(c);
-      emit(PH_OUTER, outer_);
-      EZ_RUN(checksum_emit());
-    }
-    std::memcpy(hc_, c, sizeof(c));  // counters at loop exit
-    if (!capped_ && p_.final_join) EZ_RUN(saddle_loops_join());  // unconditional (:5997)
-    EZ_RUN(read_ctr());
-    return capped_ ? EXTREMZ_ROUND_CAP : EXTREMZ_OK;
-  }
-#undef EZ_RUN
 };
 
 static int check_args(int dtype, long long W, long long H, long long D, const extremz_params* p) {
@@ -805,6 +216,43 @@ static int check_args(int dtype, long long W, long long H, long long D, const ex
   if (p->q <= 0 || (p->edit_type != 0 && p->edit_type != 1)) return EXTREMZ_BAD_ARG;
   if (p->max_outer < 0 || p->max_cloop_rounds < 0 || p->device_iter_cap < 0) return EXTREMZ_BAD_ARG;
   return EXTREMZ_OK;
+}
+
+// Runs one job to completion on an engine.
+template <class T>
+static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* tables, Arena* engine_store,
+                   Arena* job_store, const T* f, T* g, int W, int H, int D, const extremz_params& p,
+                   extremz_report* rep, int32_t* trace, int trace_cap) {
+  e.set_stream(st);
+  EZ_RUN(e.init(tables, engine_store));
+  const bool prof = (p.flags & EXTREMZ_FLAG_PROFILE) != 0;
+  e.set_profile(prof, (p.flags >> EXTREMZ_PROFILE_CLASS_SHIFT) & ((1 << K_NUM) - 1));
+  const long long l0 = e.launches();
+  int slot = -1;
+  EZ_RUN(e.admit(f, g, W, H, D, p, trace, trace_cap, job_store, 0, &slot));
+  int rc = EXTREMZ_OK;
+  while (e.job(slot).pc != PC_DONE) {
+    rc = e.tick();
+    if (rc != EXTREMZ_OK) break;
+  }
+  if (rc == EXTREMZ_OK) {
+    cudaError_t ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) {
+      last_cuda_error() = ce;
+      rc = EXTREMZ_CUDA_ERR;
+    }
+  }
+  if (rep) {
+    e.fill_report(slot, rep);
+    rep->kernel_launches = e.launches() - l0;
+    if (prof) e.collect_profile(rep);
+    if (rc != EXTREMZ_OK) rep->status = rc;
+  }
+  if (prof) e.drop_profile_events();
+  e.set_profile(false, 0);
+  if (rc == EXTREMZ_OK) rc = e.job(slot).status;
+  e.release(slot);
+  return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -820,17 +268,32 @@ static int check_args(int dtype, long long W, long long H, long long D, const ex
 // the library keeps it until the process exits.
 // ---------------------------------------------------------------------------
 constexpr long long kNoAllocMaxVoxels = EXTREMZ_NOALLOC_MAX_VOXELS;
-// Worst case of the workspace layout (every voxel a critical point of every
-// kind, 8-byte values): 297 bytes per voxel plus per-array alignment.
-constexpr size_t kNoAllocScratchBytes = (size_t)kNoAllocMaxVoxels * 320 + (1u << 20);
+// Engine arrays (descriptors, tile maps, counters) first, then one job's
+// worst-case workspace (every voxel a critical point of every kind, 8-byte
+// values: 297 bytes per voxel plus per-array alignment).
+constexpr size_t kNoAllocEngineBytes = 1u << 18;
+constexpr size_t kNoAllocScratchBytes = kNoAllocEngineBytes + (size_t)kNoAllocMaxVoxels * 320 + (1u << 20);
+// Both engines (float and double) carve their descriptor, tile-map and
+// counter arrays from the first part.
+constexpr size_t kEngineArrayBytes(size_t job) {
+  return ((job * kMaxSel + 255) & ~size_t(255)) + ((sizeof(CUtensorMap) * 2 * kMaxSel + 255) & ~size_t(255)) +
+         ((sizeof(int) * C_COUNT * kMaxSel + 255) & ~size_t(255));
+}
+static_assert(kEngineArrayBytes(sizeof(Job<float>)) + kEngineArrayBytes(sizeof(Job<double>)) <=
+                  kNoAllocEngineBytes,
+              "engine arrays exceed the static workspace");
+static_assert(job_bytes_max(kNoAllocMaxVoxels) <= (long long)(kNoAllocScratchBytes - kNoAllocEngineBytes),
+              "job workspace exceeds the static workspace");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 static __device__ int8_t g_noalloc_lut[kLutSize];
 static __device__ int g_noalloc_key_offset[64];
 
 struct NoAllocDevice {
   bool ready = false;
-  Context ctx;
-  int host_ctr[C_COUNT];  // pageable host copy of the counter block
+  DeviceTables tables{};
+  Arena engine_store, job_store;
+  BatchEngine<float> e32{nullptr};
+  BatchEngine<double> e64{nullptr};
 };
 static std::mutex g_noalloc_mu;
 static NoAllocDevice g_noalloc[64];
@@ -850,14 +313,14 @@ static int noalloc_setup(int dev) {
   const HostTables& t = host_tables();
   EZ_CHECK(cudaMemcpyToSymbol(g_noalloc_lut, t.lut, kLutSize));
   EZ_CHECK(cudaMemcpyToSymbol(g_noalloc_key_offset, t.key_offset, 64 * sizeof(int)));
-  d.ctx.device = dev;
-  d.ctx.has_tables = true;
-  d.ctx.tables.lut = static_cast<const int8_t*>(lut);
-  d.ctx.tables.key_offset = static_cast<const int*>(keys);
-  d.ctx.arena.base = static_cast<char*>(scratch);
-  d.ctx.arena.cap = kNoAllocScratchBytes;
-  d.ctx.arena.fixed = true;
-  d.ctx.h_ctr = d.host_ctr;
+  d.tables.lut = static_cast<const int8_t*>(lut);
+  d.tables.key_offset = static_cast<const int*>(keys);
+  d.engine_store.base = static_cast<char*>(scratch);
+  d.engine_store.cap = kNoAllocEngineBytes;
+  d.engine_store.fixed = true;
+  d.job_store.base = static_cast<char*>(scratch) + kNoAllocEngineBytes;
+  d.job_store.cap = kNoAllocScratchBytes - kNoAllocEngineBytes;
+  d.job_store.fixed = true;
   d.ready = true;
   return EXTREMZ_OK;
 }
@@ -878,19 +341,263 @@ static int correct_noalloc(const void* d_orig, void* d_decp, int dtype, int widt
   if (report) std::memset(report, 0, sizeof(*report));
   extremz_params p = *params;
   p.flags &= ~EXTREMZ_FLAG_PROFILE;  // no timing events in this mode
+  NoAllocDevice& d = g_noalloc[dev];
   cudaStream_t st = (cudaStream_t)stream;
-  Context& ctx = g_noalloc[dev].ctx;
-  if (dtype == EXTREMZ_F32) {
-    Corrector<float> c(ctx, (const float*)d_orig, (float*)d_decp, width, height, depth, p, st,
-                       nullptr, 0);
-    rc = c.run(report);
-  } else {
-    Corrector<double> c(ctx, (const double*)d_orig, (double*)d_decp, width, height, depth, p, st,
-                        nullptr, 0);
-    rc = c.run(report);
-  }
+  if (dtype == EXTREMZ_F32)
+    rc = run_one(d.e32, st, &d.tables, &d.engine_store, &d.job_store, (const float*)d_orig,
+                 (float*)d_decp, width, height, depth, p, report, nullptr, 0);
+  else
+    rc = run_one(d.e64, st, &d.tables, &d.engine_store, &d.job_store, (const double*)d_orig,
+                 (double*)d_decp, width, height, depth, p, report, nullptr, 0);
   if (report) report->status = rc;
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Batches: many fields, each with its own dtype, shape and parameters.  The
+// float and double jobs run on two engines; a tick of each serves all of its
+// jobs.  More than kMaxSel jobs of one dtype are admitted as slots free up.
+// ---------------------------------------------------------------------------
+template <class T>
+struct BatchDriver {
+  BatchEngine<T>* e;
+  std::vector<int> todo;   // field indices not yet admitted
+  std::vector<int> slot_of;
+  size_t next = 0;
+};
+
+static int correct_batch(Context& C, const extremz_field* fields, int n, extremz_report* reports,
+                         cudaStream_t st) {
+  for (int i = 0; i < n; ++i) {
+    EZ_RUN(check_args(fields[i].dtype, fields[i].width, fields[i].height, fields[i].depth,
+                      &fields[i].params));
+    if (!fields[i].orig || !fields[i].decp) return EXTREMZ_BAD_ARG;
+  }
+  EZ_RUN(C.ensure_pool());
+  C.e32.set_stream(st);
+  C.e64.set_stream(st);
+  EZ_RUN(C.e32.init(nullptr, nullptr));
+  EZ_RUN(C.e64.init(nullptr, nullptr));
+  std::vector<int> slot(n, -1), done(n, 0);
+  std::vector<int> which(n);  // 0 float, 1 double
+  int remaining = n;
+  size_t next = 0;
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  const long long l0 = C.e32.launches() + C.e64.launches();
+  while (remaining > 0) {
+    // Admit while slots are free.
+    while (next < order.size()) {
+      const int i = order[next];
+      const extremz_field& fd = fields[i];
+      int rc, s = -1;
+      if (fd.dtype == EXTREMZ_F32) {
+        if (C.e32.free_slots() == 0) break;
+        rc = C.e32.admit((const float*)fd.orig, (float*)fd.decp, fd.width, fd.height, fd.depth,
+                         fd.params, nullptr, 0, nullptr, i, &s);
+      } else {
+        if (C.e64.free_slots() == 0) break;
+        rc = C.e64.admit((const double*)fd.orig, (double*)fd.decp, fd.width, fd.height, fd.depth,
+                         fd.params, nullptr, 0, nullptr, i, &s);
+      }
+      if (rc == EXTREMZ_OOM && (C.e32.active() + C.e64.active()) > 0) break;  // wait for memory
+      if (rc != EXTREMZ_OK) return rc;
+      slot[i] = s;
+      which[i] = fd.dtype == EXTREMZ_F32 ? 0 : 1;
+      ++next;
+    }
+    if (C.e32.active()) EZ_RUN(C.e32.tick());
+    if (C.e64.active()) EZ_RUN(C.e64.tick());
+    for (int i = 0; i < n; ++i) {
+      if (slot[i] < 0 || done[i]) continue;
+      const bool fin = which[i] == 0 ? C.e32.job(slot[i]).pc == PC_DONE
+                                     : C.e64.job(slot[i]).pc == PC_DONE;
+      if (!fin) continue;
+      if (reports) {
+        if (which[i] == 0) C.e32.fill_report(slot[i], &reports[i]);
+        else C.e64.fill_report(slot[i], &reports[i]);
+      }
+      if (which[i] == 0) C.e32.release(slot[i]);
+      else C.e64.release(slot[i]);
+      done[i] = 1;
+      --remaining;
+    }
+  }
+  EZ_CHECK(cudaStreamSynchronize(st));
+  if (reports && n > 0) reports[0].kernel_launches = C.e32.launches() + C.e64.launches() - l0;
+  return EXTREMZ_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Serving: a request loop on its own thread and stream.  Between ticks it
+// admits queued requests in arrival order while their footprint fits the HBM
+// budget and a slot is free; every tick serves all admitted jobs.
+// ---------------------------------------------------------------------------
+using Clock = std::chrono::steady_clock;
+
+struct ServerReq {
+  long long ticket = 0;
+  extremz_field field{};
+  cudaEvent_t ready = nullptr;  // recorded on the caller's stream at submission
+  long long footprint = 0;
+  Clock::time_point t0;
+};
+
+struct ServerResult {
+  bool done = false;
+  int status = EXTREMZ_PENDING;
+  extremz_report rep{};
+  double latency_ms = 0.0;
+};
+
+struct ServerRunning {
+  long long ticket;
+  long long footprint;
+  Clock::time_point t0;
+  int dtype;
+  int slot;
+};
+
+static long long field_footprint(const extremz_field& f) {
+  const long long n = (long long)f.width * f.height * f.depth;
+  const long long vb = f.dtype == EXTREMZ_F32 ? 4 : 8;
+  return job_bytes_max(n) + 2 * n * vb;
+}
+
+}  // namespace extremz
+
+struct extremz_server_s {
+  int device = 0;
+  long long budget = 0;
+  int max_jobs = extremz::kMaxSel;
+  cudaStream_t st = nullptr;
+  cudaMemPool_t pool = nullptr;
+  extremz::BatchEngine<float> e32{nullptr};
+  extremz::BatchEngine<double> e64{nullptr};
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  bool stop = false;
+  int broken = EXTREMZ_OK;  // a CUDA error ends the loop; later requests fail with it
+  std::deque<extremz::ServerReq> queue;
+  std::unordered_map<long long, extremz::ServerResult> results;
+  std::vector<extremz::ServerRunning> running;
+  long long next_ticket = 1;
+  extremz_server_stats stats{};
+};
+
+namespace extremz {
+
+static void server_finish(extremz_server* s, const ServerRunning& r, int status,
+                          const extremz_report* rep) {
+  const double ms =
+      std::chrono::duration<double, std::milli>(Clock::now() - r.t0).count();
+  std::lock_guard<std::mutex> lk(s->mu);
+  ServerResult& res = s->results[r.ticket];
+  res.done = true;
+  res.status = status;
+  if (rep) res.rep = *rep;
+  res.rep.status = status;
+  res.latency_ms = ms;
+  s->stats.bytes_in_use -= r.footprint;
+  s->stats.completed += 1;
+  s->stats.running -= 1;
+}
+
+static void server_loop(extremz_server* s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    std::vector<ServerReq> admit_now;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      if (s->running.empty())
+        s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+      if (s->stop && s->running.empty()) break;
+      int n32 = 0, n64 = 0;
+      for (const auto& r : s->running) (r.dtype == EXTREMZ_F32 ? n32 : n64)++;
+      while (!s->stop && !s->queue.empty()) {
+        const ServerReq& r = s->queue.front();
+        int& n = r.field.dtype == EXTREMZ_F32 ? n32 : n64;
+        if (n >= s->max_jobs) break;
+        if (s->stats.bytes_in_use + r.footprint > s->budget) break;
+        s->stats.bytes_in_use += r.footprint;
+        s->stats.peak_bytes_in_use = std::max(s->stats.peak_bytes_in_use, s->stats.bytes_in_use);
+        s->stats.queued -= 1;
+        s->stats.running += 1;
+        ++n;
+        admit_now.push_back(r);
+        s->queue.pop_front();
+      }
+    }
+    for (ServerReq& r : admit_now) {
+      cudaStreamWaitEvent(s->st, r.ready, 0);
+      cudaEventDestroy(r.ready);
+      const extremz_field& f = r.field;
+      int slot = -1;
+      int rc = f.dtype == EXTREMZ_F32
+                   ? s->e32.admit((const float*)f.orig, (float*)f.decp, f.width, f.height, f.depth,
+                                  f.params, nullptr, 0, nullptr, r.ticket, &slot)
+                   : s->e64.admit((const double*)f.orig, (double*)f.decp, f.width, f.height,
+                                  f.depth, f.params, nullptr, 0, nullptr, r.ticket, &slot);
+      ServerRunning run{r.ticket, r.footprint, r.t0, f.dtype, slot};
+      if (rc != EXTREMZ_OK) {
+        server_finish(s, run, rc, nullptr);
+        continue;
+      }
+      s->running.push_back(run);
+    }
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stats.peak_running = std::max(s->stats.peak_running, (int)s->running.size());
+    }
+    int rc = EXTREMZ_OK;
+    if (s->e32.active()) rc = s->e32.tick();
+    if (rc == EXTREMZ_OK && s->e64.active()) rc = s->e64.tick();
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stats.ticks += 1;
+      s->stats.kernel_launches = s->e32.launches() + s->e64.launches();
+    }
+    std::vector<ServerRunning> still;
+    for (const ServerRunning& r : s->running) {
+      const bool f32 = r.dtype == EXTREMZ_F32;
+      const int pc = f32 ? s->e32.job(r.slot).pc : s->e64.job(r.slot).pc;
+      if (rc == EXTREMZ_OK && pc != PC_DONE) {
+        still.push_back(r);
+        continue;
+      }
+      extremz_report rep;
+      std::memset(&rep, 0, sizeof(rep));
+      int status = rc;
+      if (rc == EXTREMZ_OK) {
+        if (f32) s->e32.fill_report(r.slot, &rep);
+        else s->e64.fill_report(r.slot, &rep);
+        status = rep.status;
+      }
+      if (f32) s->e32.release(r.slot);
+      else s->e64.release(r.slot);
+      server_finish(s, r, status, &rep);
+    }
+    s->running.swap(still);
+    s->cv_done.notify_all();
+    if (rc != EXTREMZ_OK) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->broken = rc;
+      for (ServerReq& q : s->queue) {
+        cudaEventDestroy(q.ready);
+        ServerResult& res = s->results[q.ticket];
+        res.done = true;
+        res.status = rc;
+        res.rep.status = rc;
+      }
+      s->queue.clear();
+      s->stats.queued = 0;
+      s->cv_done.notify_all();
+      break;
+    }
+  }
+  cudaStreamSynchronize(s->st);
 }
 
 }  // namespace extremz
@@ -957,15 +664,17 @@ extremz_status extremz_correct_device(extremz_ctx* ctx, const void* d_orig, void
   cudaGetDevice(&prev);
   if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
   cudaStream_t st = (cudaStream_t)stream;
-  if (dtype == EXTREMZ_F32) {
-    Corrector<float> c(ctx->c, (const float*)d_orig, (float*)d_decp, width, height, depth, *params,
-                       st, trace, trace_cap);
-    rc = c.run(report);
-  } else {
-    Corrector<double> c(ctx->c, (const double*)d_orig, (double*)d_decp, width, height, depth,
-                        *params, st, trace, trace_cap);
-    rc = c.run(report);
+  rc = ctx->c.ensure_pool();
+  if (rc != EXTREMZ_OK) {
+    if (prev != ctx->c.device) cudaSetDevice(prev);
+    return (extremz_status)rc;
   }
+  if (dtype == EXTREMZ_F32)
+    rc = run_one(ctx->c.e32, st, nullptr, nullptr, nullptr, (const float*)d_orig, (float*)d_decp,
+                 width, height, depth, *params, report, trace, trace_cap);
+  else
+    rc = run_one(ctx->c.e64, st, nullptr, nullptr, nullptr, (const double*)d_orig,
+                 (double*)d_decp, width, height, depth, *params, report, trace, trace_cap);
   if (report) report->status = rc;
   if (prev != ctx->c.device) cudaSetDevice(prev);
   return (extremz_status)rc;
@@ -1005,12 +714,186 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
   return (extremz_status)rc;
 }
 
+extremz_status extremz_correct_batch(extremz_ctx* ctx, const extremz_field* fields, int n,
+                                     extremz_report* reports, void* stream) {
+  if (!ctx || (n > 0 && !fields) || n < 0) return EXTREMZ_BAD_ARG;
+  if (reports) std::memset(reports, 0, sizeof(extremz_report) * (size_t)n);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
+  int rc = correct_batch(ctx->c, fields, n, reports, (cudaStream_t)stream);
+  if (prev != ctx->c.device) cudaSetDevice(prev);
+  return (extremz_status)rc;
+}
+
 extremz_status extremz_correct_device_noalloc(const void* d_orig, void* d_decp, int dtype,
                                               int width, int height, int depth,
                                               const extremz_params* params,
                                               extremz_report* report, void* stream) {
   return (extremz_status)correct_noalloc(d_orig, d_decp, dtype, width, height, depth, params,
                                          report, stream);
+}
+
+
+extremz_status extremz_server_create(int device, const extremz_server_config* cfg,
+                                     extremz_server** out) {
+  if (!out) return EXTREMZ_BAD_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return EXTREMZ_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) return EXTREMZ_BAD_ARG;
+  const long long budget =
+      cfg && cfg->hbm_budget_bytes > 0 ? cfg->hbm_budget_bytes : 120ll * 1000 * 1000 * 1000;
+  const int max_jobs = cfg && cfg->max_jobs > 0 ? cfg->max_jobs : extremz::kMaxSel;
+  if (max_jobs > extremz::kMaxSel) return EXTREMZ_BAD_ARG;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  extremz_server* s = new (std::nothrow) extremz_server;
+  if (!s) return EXTREMZ_OOM;
+  s->device = device;
+  s->budget = budget;
+  s->max_jobs = max_jobs;
+  int rc = EXTREMZ_OK;
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) rc = EXTREMZ_CUDA_ERR;
+  if (rc == EXTREMZ_OK && !(s->pool = make_pool(device))) rc = EXTREMZ_OOM;
+  if (rc == EXTREMZ_OK) {
+    s->e32.set_stream(s->st);
+    s->e64.set_stream(s->st);
+    s->e32.set_pool(s->pool);
+    s->e64.set_pool(s->pool);
+    rc = s->e32.init(nullptr, nullptr);
+    if (rc == EXTREMZ_OK) rc = s->e64.init(nullptr, nullptr);
+  }
+  if (rc != EXTREMZ_OK) {
+    cudaGetLastError();
+    s->e32.release_all();
+    s->e64.release_all();
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+    cudaSetDevice(prev);
+    return (extremz_status)rc;
+  }
+  s->th = std::thread(server_loop, s);
+  cudaSetDevice(prev);
+  *out = s;
+  return EXTREMZ_OK;
+}
+
+void extremz_server_destroy(extremz_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    for (ServerReq& q : s->queue) cudaEventDestroy(q.ready);
+    s->queue.clear();
+  }
+  s->cv_work.notify_all();
+  if (s->th.joinable()) s->th.join();
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  s->e32.release_all();
+  s->e64.release_all();
+  cudaStreamSynchronize(s->st);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
+  cudaStreamDestroy(s->st);
+  cudaSetDevice(prev);
+  delete s;
+}
+
+extremz_status extremz_server_submit(extremz_server* s, const extremz_field* f, void* stream,
+                                     long long* ticket) {
+  if (!s || !f || !ticket || !f->orig || !f->decp) return EXTREMZ_BAD_ARG;
+  int rc = check_args(f->dtype, f->width, f->height, f->depth, &f->params);
+  if (rc != EXTREMZ_OK) return (extremz_status)rc;
+  const long long fp = field_footprint(*f);
+  if (fp > s->budget) return EXTREMZ_TOO_LARGE;
+  ServerReq r;
+  r.field = *f;
+  r.field.params.flags &= ~EXTREMZ_FLAG_PROFILE;
+  r.footprint = fp;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != s->device) cudaSetDevice(s->device);
+  if (cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventRecord(r.ready, (cudaStream_t)stream) != cudaSuccess) {
+    last_cuda_error() = cudaGetLastError();
+    if (r.ready) cudaEventDestroy(r.ready);
+    if (prev != s->device) cudaSetDevice(prev);
+    return EXTREMZ_CUDA_ERR;
+  }
+  if (prev != s->device) cudaSetDevice(prev);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->broken != EXTREMZ_OK || s->stop) {
+      cudaEventDestroy(r.ready);
+      return (extremz_status)(s->broken != EXTREMZ_OK ? s->broken : EXTREMZ_BAD_ARG);
+    }
+    r.ticket = s->next_ticket++;
+    r.t0 = Clock::now();
+    s->results[r.ticket] = ServerResult();
+    s->queue.push_back(r);
+    s->stats.submitted += 1;
+    s->stats.queued += 1;
+    *ticket = r.ticket;
+  }
+  s->cv_work.notify_one();
+  return EXTREMZ_OK;
+}
+
+static extremz_status server_take(extremz_server* s, long long ticket, extremz_report* report,
+                                  double* latency_ms) {
+  auto it = s->results.find(ticket);
+  if (it == s->results.end()) return EXTREMZ_BAD_ARG;
+  if (!it->second.done) return EXTREMZ_PENDING;
+  if (report) *report = it->second.rep;
+  if (latency_ms) *latency_ms = it->second.latency_ms;
+  const int st = it->second.status;
+  s->results.erase(it);
+  return (extremz_status)st;
+}
+
+extremz_status extremz_server_poll(extremz_server* s, long long ticket, extremz_report* report,
+                                   double* latency_ms) {
+  if (!s) return EXTREMZ_BAD_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  return server_take(s, ticket, report, latency_ms);
+}
+
+extremz_status extremz_server_wait(extremz_server* s, long long ticket, int timeout_ms,
+                                   extremz_report* report, double* latency_ms) {
+  if (!s) return EXTREMZ_BAD_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto ready = [&] {
+    auto it = s->results.find(ticket);
+    return it == s->results.end() || it->second.done;
+  };
+  if (timeout_ms < 0) s->cv_done.wait(lk, ready);
+  else s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready);
+  return server_take(s, ticket, report, latency_ms);
+}
+
+long long extremz_job_footprint(int dtype, int width, int height, int depth) {
+  if ((dtype != EXTREMZ_F32 && dtype != EXTREMZ_F64) || width <= 0 || height <= 0 || depth <= 0)
+    return -1;
+  extremz_field f;
+  std::memset(&f, 0, sizeof(f));
+  f.dtype = dtype;
+  f.width = width;
+  f.height = height;
+  f.depth = depth;
+  return field_footprint(f);
+}
+
+void extremz_server_get_stats(extremz_server* s, extremz_server_stats* out) {
+  if (!s || !out) return;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->stats;
 }
 
 long long extremz_noalloc_max_voxels(void) { return kNoAllocMaxVoxels; }
@@ -1032,7 +915,9 @@ const char* extremz_status_string(int status) {
     case EXTREMZ_DEVICE_TIMEOUT: return "device-side iteration limit reached";
     case EXTREMZ_NO_DEVICE: return "no CUDA device";
     case EXTREMZ_TOO_LARGE:
-      return "field larger than the static workspace of the allocation-free entry point";
+      return "field larger than the static workspace of the allocation-free entry point, "
+             "or than the server's HBM budget";
+    case EXTREMZ_PENDING: return "request still queued or running";
     default: return "unknown status";
   }
 }

@@ -59,6 +59,7 @@ struct Job {
   const CUtensorMap* map_f;  // tile maps of f and g in device memory (when tma_f / tma_g)
   const CUtensorMap* map_g;
   int tma_f, tma_g;
+  int iter_cap;  // device-side limit of pointer jumping and path walks
 };
 
 // Jobs served by one launch.  Every per-round kernel takes the device array of
@@ -77,7 +78,14 @@ struct Sel {
 enum Ctr : int {
   C_MM = 0, C_CMAX, C_CMIN, C_CSAD, C_TOUCHED, C_NFC, C_NFC1, C_CAND, C_CAND_NEXT,
   C_WMC, C_WMC2, C_WSC, C_WMIN, C_WMIN2, C_WSCJ, C_NS2, C_NS1, C_NMAX, C_NMIN,
-  C_ERROR, C_CHANGED, C_DIRTY, C_MM_NEXT, C_COUNT
+  C_ERROR, C_CHANGED, C_DIRTY, C_MM_NEXT,
+  // Per-job epochs and stamps, advanced by k_ctl so that one launch can serve
+  // jobs at different points of their correction.
+  C_DEPOCH,    // dirty-list epoch (k_apply)
+  C_REPOCH,    // re-evaluation epoch (k_redetect / k_keep)
+  C_WNSTAMP,   // wrong-neighbour flag stamp, one per manifold round
+  C_WNROUND,   // wrong-neighbour arbitration round (vote high word)
+  C_COUNT
 };
 // Error bits in ctr[C_ERROR].
 constexpr int kErrJump = 1, kErrPath = 2, kErrTile = 4, kErrResolve = 8;
@@ -316,10 +324,11 @@ __device__ __forceinline__ int global_type(const Job<T>& J, int v, int& lmask) {
 
 template <class T>
 __global__ void __launch_bounds__(256) k_redetect(const Job<T>* __restrict__ jobs,
-                                                  const __grid_constant__ Sel sel, int epoch) {
+                                                  const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[C_DIRTY];
+  const int epoch = J.ctr[C_REPOCH];
   const long long total = (long long)n * (kNumDirs + 1);
   const long long stride = (long long)gridDim.x * blockDim.x;
   const Dims g = J.dim;
@@ -353,10 +362,11 @@ __global__ void __launch_bounds__(256) k_redetect(const Job<T>* __restrict__ job
 
 template <class T>
 __global__ void __launch_bounds__(256) k_keep(const Job<T>* __restrict__ jobs,
-                                              const __grid_constant__ Sel sel, int epoch) {
+                                              const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
   const int n = J.ctr[C_MM];
+  const int epoch = J.ctr[C_REPOCH];
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
     const int e = base + threadIdx.x;
@@ -513,14 +523,14 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
 // capped; hitting the cap sets the error word instead of spinning.
 template <class T, bool kDec>
 __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
-                                               const __grid_constant__ Sel sel, int cap) {
+                                               const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
   int* a = kDec ? J.dds : J.ds;
   int* b = kDec ? J.das : J.as;
   int* err = J.ctr + C_ERROR;
   const int N = J.dim.N;
-  const int cap_j = cap > 0 ? cap : N + 1;
+  const int cap_j = J.iter_cap;
   const int stride = gridDim.x * blockDim.x;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
     int u1 = a[v], u2 = b[v];
@@ -827,9 +837,10 @@ __global__ void __launch_bounds__(256) k_propose_cp(const Job<T>* __restrict__ j
 // applyDeltaBuffer (:3061-3111) over the vertices that received a proposal;
 // the proposal buffer is reset to the sentinel on the way (init_delta).
 template <class T>
-__global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, int dirty_epoch) {
+__global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
+  const int dirty_epoch = J.ctr[C_DEPOCH];
   const int n = J.ctr[C_TOUCHED];
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
@@ -1013,9 +1024,11 @@ __global__ void k_row_counts(Job<T> J) {
 }
 
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, unsigned long long round, int stamp) {
+__global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
+  const unsigned long long round = (unsigned)J.ctr[C_WNROUND];
+  const int stamp = J.ctr[C_WNSTAMP];
   const int n = J.ctr[C_CAND];
   const int* taken = kSplit ? J.taken : J.taken1;
   const int stride = gridDim.x * blockDim.x;
@@ -1031,9 +1044,11 @@ __global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs
 }
 
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, unsigned long long round, int stamp) {
+__global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
+  const unsigned long long round = (unsigned)J.ctr[C_WNROUND];
+  const int stamp = J.ctr[C_WNSTAMP];
   const int n = J.ctr[C_CAND];
   int* taken = kSplit ? J.taken : J.taken1;
   int* flagged = kSplit ? J.flagged : J.flagged1;
@@ -1061,9 +1076,10 @@ __global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jo
 // Sequential completion for whatever the bounded rounds left unresolved:
 // one thread takes the remaining saddles in ascending id.
 template <class T, bool kSplit>
-__global__ void k_wn_sequential(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, int stamp) {
+__global__ void k_wn_sequential(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
+  const int stamp = J.ctr[C_WNSTAMP];
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   int n = J.ctr[C_CAND];
   int* taken = kSplit ? J.taken : J.taken1;
@@ -1095,9 +1111,10 @@ __global__ void k_wn_sequential(const Job<T>* __restrict__ jobs, const __grid_co
 // the original choice (join).
 // ---------------------------------------------------------------------------
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_fixpath(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel, int cap) {
+__global__ void __launch_bounds__(256) k_fixpath(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
+  const int cap = J.iter_cap;
   const int n = J.ctr[kSplit ? C_NFC : C_NFC1];
   const int* list = kSplit ? J.flagged : J.flagged1;
   const int stride = gridDim.x * blockDim.x;
@@ -1331,36 +1348,98 @@ __global__ void __launch_bounds__(256) k_wis_collect(const Job<T>* __restrict__ 
 // ---------------------------------------------------------------------------
 // Small helpers.
 // ---------------------------------------------------------------------------
-// Swaps the current and next list of each selected job and moves the next
-// count into the current slot: which 0 = mismatch lists, 1 = wrong-neighbour
-// candidates.  (The job descriptors live in device memory, so the swap does
-// too.)
+// Per-job control operations between kernels, one thread per selected job
+// (counter resets, epoch advances and list swaps; the job descriptors live in
+// device memory, so list swaps happen here too).
+enum CtlOp : int {
+  OP_DETECT_DENSE_BEGIN = 0,  // mismatch list and category counts to zero
+  OP_DETECT_BEGIN,            // next re-evaluation epoch, next list and counts to zero
+  OP_DETECT_END_DENSE,        // dirty list to zero, next dirty epoch
+  OP_DETECT_END,              // swap mismatch lists, then as OP_DETECT_END_DENSE
+  OP_WN_BEGIN,                // next flag stamp, flagged counts to zero
+  OP_WN_SIDE_BEGIN,           // candidate count to zero
+  OP_WN_ROUND_BEGIN,          // next arbitration round, next candidate count to zero
+  OP_WN_ROUND_END,            // swap candidate lists
+  OP_ZERO_TOUCHED,
+  OP_SLOOPS_BEGIN,            // wrong_max counters and touched to zero
+  OP_SADDLE_BEGIN,            // wrong_saddle counter and touched to zero
+  OP_SLOOPS_JOIN_BEGIN,
+  OP_SADDLE_JOIN_BEGIN,
+  OP_DETECT3_BEGIN,           // wrong_max / wrong_saddle counters to zero
+  OP_DETECT3_JOIN_BEGIN
+};
+
 template <class T>
-__global__ void k_swap_lists(Job<T>* jobs, const __grid_constant__ Sel sel, int which) {
+__global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= sel.n) return;
   Job<T>& J = jobs[sel.idx[k]];
-  if (which == 0) {
-    int* t = J.mm;
-    J.mm = J.mm_next;
-    J.mm_next = t;
-    J.ctr[C_MM] = J.ctr[C_MM_NEXT];
-  } else {
-    int* t = J.cand;
-    J.cand = J.cand_next;
-    J.cand_next = t;
-    J.ctr[C_CAND] = J.ctr[C_CAND_NEXT];
+  int* c = J.ctr;
+  switch (op) {
+    case OP_DETECT_DENSE_BEGIN:
+      c[C_MM] = c[C_CMAX] = c[C_CMIN] = c[C_CSAD] = 0;
+      break;
+    case OP_DETECT_BEGIN:
+      c[C_REPOCH] += 1;
+      c[C_MM_NEXT] = c[C_CMAX] = c[C_CMIN] = c[C_CSAD] = 0;
+      break;
+    case OP_DETECT_END: {
+      int* t = J.mm;
+      J.mm = J.mm_next;
+      J.mm_next = t;
+      c[C_MM] = c[C_MM_NEXT];
+    }  // fall through
+    case OP_DETECT_END_DENSE:
+      c[C_DIRTY] = 0;
+      c[C_DEPOCH] += 1;
+      break;
+    case OP_WN_BEGIN:
+      c[C_WNSTAMP] += 1;
+      c[C_NFC] = c[C_NFC1] = 0;
+      break;
+    case OP_WN_SIDE_BEGIN:
+      c[C_CAND] = 0;
+      break;
+    case OP_WN_ROUND_BEGIN:
+      c[C_WNROUND] += 1;
+      c[C_CAND_NEXT] = 0;
+      break;
+    case OP_WN_ROUND_END: {
+      int* t = J.cand;
+      J.cand = J.cand_next;
+      J.cand_next = t;
+      c[C_CAND] = c[C_CAND_NEXT];
+      break;
+    }
+    case OP_ZERO_TOUCHED:
+      c[C_TOUCHED] = 0;
+      break;
+    case OP_SLOOPS_BEGIN:
+      c[C_WMC] = c[C_WMC2] = c[C_TOUCHED] = 0;
+      break;
+    case OP_SADDLE_BEGIN:
+      c[C_WSC] = c[C_TOUCHED] = 0;
+      break;
+    case OP_SLOOPS_JOIN_BEGIN:
+      c[C_WMIN] = c[C_WMIN2] = c[C_TOUCHED] = 0;
+      break;
+    case OP_SADDLE_JOIN_BEGIN:
+      c[C_WSCJ] = c[C_TOUCHED] = 0;
+      break;
+    case OP_DETECT3_BEGIN:
+      c[C_WMC] = c[C_WMC2] = c[C_WSC] = 0;
+      break;
+    case OP_DETECT3_JOIN_BEGIN:
+      c[C_WMIN] = c[C_WMIN2] = c[C_WSCJ] = 0;
+      break;
+    default:
+      break;
   }
 }
 
-// Zeroes counter slots [slot, slot + n) of every selected job.
-template <class T>
-__global__ void k_zero_ctr(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel,
-                           int slot, int n) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= sel.n * n) return;
-  jobs[sel.idx[k / n]].ctr[slot + k % n] = 0;
-}
+// ---------------------------------------------------------------------------
+// Small helpers.
+// ---------------------------------------------------------------------------
 template <class K>
 __global__ void k_fill(K* p, K v, long long n) {
   const long long stride = (long long)gridDim.x * blockDim.x;

@@ -34,7 +34,9 @@ typedef enum {
   EXTREMZ_CUDA_ERR = 4,
   EXTREMZ_DEVICE_TIMEOUT = 5, /* a device-side iteration limit was hit */
   EXTREMZ_NO_DEVICE = 6,
-  EXTREMZ_TOO_LARGE = 7       /* beyond EXTREMZ_NOALLOC_MAX_VOXELS (noalloc entry point) */
+  EXTREMZ_TOO_LARGE = 7,      /* beyond EXTREMZ_NOALLOC_MAX_VOXELS (noalloc entry point),
+                                 or beyond a server's whole HBM budget */
+  EXTREMZ_PENDING = 8         /* server request still queued or running */
 } extremz_status;
 
 typedef enum { EXTREMZ_F32 = 0, EXTREMZ_F64 = 1 } extremz_dtype;
@@ -143,6 +145,87 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
                                     int dtype, int width, int height, int depth,
                                     const extremz_params* params, extremz_report* report,
                                     void* stream);
+
+/* One field of a batch: device pointers, its own dtype, shape and parameters. */
+typedef struct {
+  const void* orig;
+  void* decp;
+  int dtype;
+  int width, height, depth;
+  extremz_params params;
+} extremz_field;
+
+/*
+ * Correct n fields in place, each as extremz_correct_device would, with one
+ * launch per kernel serving every field that is at the same phase.  Fields
+ * of different dtype, shape and parameters mix freely; each field's result
+ * is bit-identical to correcting it alone.  Up to 64 fields of each dtype are
+ * in flight; the rest are admitted as earlier ones finish, and while device
+ * memory is short.  reports (optional) has n entries; reports[0].kernel_launches
+ * counts the whole batch's launches.
+ * Replaces: a loop over fields of main() of src/ExtreM_cuda.cu:5508-5997 (the
+ * reference corrects one field per process run).
+ */
+extremz_status extremz_correct_batch(extremz_ctx* ctx, const extremz_field* fields, int n,
+                                     extremz_report* reports, void* stream);
+
+/*
+ * Serving: a request loop on its own thread and CUDA stream.  Requests
+ * (device fields) arrive at any time; the loop admits them, in arrival order,
+ * while the device footprint of the admitted jobs (workspace plus both
+ * fields) stays within the HBM budget and a slot is free, and runs every
+ * admitted job together: one launch per kernel serves all jobs at the same
+ * phase (continuous batching).  A job's field, labels and edit state stay on
+ * the device from admission to completion.  Each result is bit-identical to
+ * correcting the field alone.
+ * No counterpart in the reference (one field per process run, main() of
+ * src/ExtreM_cuda.cu:4954-6078).
+ */
+typedef struct {
+  long long hbm_budget_bytes; /* admission budget; 0 = 120 GB */
+  int max_jobs;               /* jobs in flight per dtype, 1..64; 0 = 64 */
+  int reserved[7];
+} extremz_server_config;
+
+typedef struct {
+  long long submitted, completed, queued, running;
+  long long bytes_in_use, peak_bytes_in_use;
+  long long ticks, kernel_launches;
+  int peak_running;
+  int reserved[7];
+} extremz_server_stats;
+
+typedef struct extremz_server_s extremz_server;
+
+extremz_status extremz_server_create(int device, const extremz_server_config* cfg,
+                                     extremz_server** out);
+/* Finishes the jobs already admitted, fails the queued ones, then stops. */
+void extremz_server_destroy(extremz_server* srv);
+
+/*
+ * Queue one field.  Its buffers must stay valid until the request completes.
+ * stream: the caller's stream on which the field's contents were produced;
+ * the server's work on the field starts after the work queued on it so far.
+ * Returns EXTREMZ_TOO_LARGE for a field whose footprint exceeds the budget.
+ */
+extremz_status extremz_server_submit(extremz_server* srv, const extremz_field* field,
+                                     void* stream, long long* ticket);
+
+/* EXTREMZ_PENDING while queued or running; else the request's final status,
+ * its report and its latency (submission to completion, host clock), after
+ * which the ticket is forgotten. */
+extremz_status extremz_server_poll(extremz_server* srv, long long ticket, extremz_report* report,
+                                   double* latency_ms);
+
+/* As poll, waiting up to timeout_ms (< 0: without limit) for completion. */
+extremz_status extremz_server_wait(extremz_server* srv, long long ticket, int timeout_ms,
+                                   extremz_report* report, double* latency_ms);
+
+void extremz_server_get_stats(extremz_server* srv, extremz_server_stats* out);
+
+/* Device bytes a server charges a request of this shape and dtype against its
+ * budget: the worst-case workspace of the correction plus both fields. */
+long long extremz_job_footprint(int dtype, int width, int height, int depth);
 
 /*
  * Allocation-free variant of extremz_correct_device, for callers that cannot
