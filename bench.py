@@ -48,7 +48,17 @@ WORKLOADS = {
     "plain512_f64": (lambda: synth.plain_512(),
                      "512^3 float64, 4096 Gaussians + k^-5/3 noise, seed 2, eb 1e-5 rel"),
 }
+# Batched and served forms (not plain fields): their own lines.
+FORM_WORKLOADS = {
+    "mixed64": "64 fields, edges log-uniform 32-192 (25% 2-D slices), f32/f64 50/50, "
+               "eb log-uniform 1e-5..1e-2 rel, seeds 100-163",
+    "serve": "Poisson request stream, voxels log-uniform 32^3-384^3, f32/f64 50/50, eb "
+             "log-uniform 1e-5..1e-2 rel, seed 10000+id, HBM admission budget 120 GB",
+}
 DEFAULT_WORKLOAD = "plain256_f64"
+SERVE_RATES = (10, 30, 100, 300, 1000, 2000)
+# Workspace memory the server maps at start-up (within its 120 GB budget).
+SERVE_RESERVE_BYTES = 48 << 30
 PARAMS = dict(q=4, edit_type=1, thr=0.0, max_outer=1000, max_cloop_rounds=100000,
               final_join=True)
 
@@ -186,9 +196,51 @@ def time_oracle(field, edge: int, threads: int):
     return time.perf_counter() - t0, f.size, rep
 
 
+def run_reference_form(args):
+    """Reference arm of the batched / served workloads: the CPU restatement on
+    all host threads over a bounded sample of the same fields, fields/s."""
+    from oracle import ffi
+    threads = os.cpu_count() or 1
+    ffi.set_threads(threads)
+    if args.workload == "mixed64":
+        specs = synth.mixed_batch_specs(64)
+    else:
+        specs = [synth.serving_request_spec(i) for i in range(64)]
+    # Bounded sample: the smallest fields of the workload, up to 16.
+    order = sorted(range(len(specs)), key=lambda i: specs[i]["w"] * specs[i]["h"] * specs[i]["d"])
+    sample = [specs[i] for i in order[:16]]
+    fields = [synth.make_field(s["w"], s["h"], s["d"], n_gauss=s["n_gauss"], seed=s["seed"],
+                               rel=s["rel"], dtype=s["dtype"]) for s in sample]
+    total = 0.0
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for x in fields[:4] if step < args.warmup else fields:
+            ffi.correct(x.f, x.decp, x.eb, q=PARAMS["q"], edit_type=PARAMS["edit_type"],
+                        thr=PARAMS["thr"], max_outer=PARAMS["max_outer"],
+                        max_cloop_rounds=PARAMS["max_cloop_rounds"],
+                        final_join=PARAMS["final_join"])
+        if step >= args.warmup:
+            total += time.perf_counter() - t0
+    value = len(fields) * args.steps / total
+    desc = (f"the {len(fields)} smallest fields of the {args.workload} workload, each corrected "
+            f"to zero mismatch by the CPU restatement of the reference correction")
+    line = {"impl": "reference", "metric": "fields/s to zero topological mismatch", "value": value,
+            "unit": "fields/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": args.workload, "description": FORM_WORKLOADS[args.workload]},
+            "cpu_baseline": {"value": value, "unit": "fields/s", "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": "fields/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
+    if args.workload in FORM_WORKLOADS:
+        return run_reference_form(args)
     field = WORKLOADS[args.workload][0]()
     threads = os.cpu_count() or 1
     edge = args.cpu_edge
@@ -315,6 +367,24 @@ def run_ours(args, world, rank, local):
                "sample": f"leading {args.cpu_edge}^3 crop of the same field and bound, full "
                          f"correction to zero mismatch ({secs:.1f} s, status {crep['status']})"}
 
+    forms = None
+    if not args.no_forms and world == 1:
+        b = measure_batched(local, 2, 1)
+        sv = measure_served(local, (100, 2000), n_max=48, seconds=0.5)
+        forms = {"batched": {"workload": "mixed64", "fields_per_s": b["batched"]["fields_per_s"],
+                             "plain_loop_fields_per_s": b["plain_loop"]["fields_per_s"],
+                             "speedup": b["speedup"],
+                             "bit_identical_to_plain": b["bit_identical_to_plain"],
+                             "gpu_launches": b["batched"]["gpu_launches"],
+                             "plain_loop_gpu_launches": b["plain_loop"]["gpu_launches"]},
+                 "served": {"workload": "serve (48 requests per rate)",
+                            "plain_loop_fields_per_s": sv["plain_loop"]["fields_per_s"],
+                            "peak_running": sv["peak_running"],
+                            "sweep": [{k: x[k] for k in ("rate_req_s", "p50_ms", "p99_ms",
+                                                         "fields_per_s", "mean_in_system")}
+                                      for x in sv["sweep"]],
+                            "bit_identical_to_plain": sv["bit_identical_to_plain"]}}
+
     if rank == 0:
         r0 = reps[-1]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -322,7 +392,7 @@ def run_ours(args, world, rank, local):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": dtype_name(field), "data": "synthetic (seeded generator, no dataset)",
                 "config": config_of(args, field), "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "forms": forms,
                 "rounds": {"outer_iters": r0.outer_iters, "cloop_rounds": r0.cloop_rounds,
                            "manifold_rounds": r0.manifold_rounds, "status": r0.status,
                            "counters": r0.counters}}
@@ -330,12 +400,216 @@ def run_ours(args, world, rank, local):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# Batched form: the 64-field mixed batch, batched vs the plain per-field loop.
+# ---------------------------------------------------------------------------
+def mixed_fields():
+    specs = synth.mixed_batch_specs(64)
+    return specs, [synth.make_field(s["w"], s["h"], s["d"], n_gauss=s["n_gauss"], seed=s["seed"],
+                                    rel=s["rel"], dtype=s["dtype"]) for s in specs]
+
+
+def measure_batched(local, steps, warmup, fields=None):
+    """fields/s of extremz_correct_batch and of the plain loop on the same
+    fields (device-resident inputs, a fresh decompressed copy per step)."""
+    import torch
+    from extrem_z_b200 import api
+    dev = torch.device("cuda", local)
+    if fields is None:
+        _, fields = mixed_fields()
+    F = [torch.from_numpy(x.f).to(dev) for x in fields]
+    G0 = [torch.from_numpy(x.decp).to(dev) for x in fields]
+    G = [torch.empty_like(g) for g in G0]
+    ctx = api.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    vox = sum(x.f.size for x in fields)
+
+    def reset():
+        for g, g0 in zip(G, G0):
+            g.copy_(g0)
+
+    def batched():
+        reps, launches = ctx.correct_batch([(f, g, x.eb, PARAMS) for f, g, x in zip(F, G, fields)],
+                                           stream=stream.cuda_stream)
+        return reps, launches
+
+    def loop():
+        launches, reps = 0, []
+        for f, g, x in zip(F, G, fields):
+            r, _ = ctx.correct_device(f, g, x.eb, stream=stream.cuda_stream, **PARAMS)
+            launches += r.kernel_launches
+            reps.append(r)
+        return reps, launches
+
+    def timed(fn):
+        total, launches, reps = 0.0, 0, None
+        for i in range(warmup + steps):
+            reset()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            reps, ln = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i >= warmup:
+                total += e0.elapsed_time(e1)
+                launches += ln
+        return total / steps, launches // steps, reps
+
+    ms_b, l_b, reps_b = timed(batched)
+    out_b = [g.clone() for g in G]
+    ms_p, l_p, reps_p = timed(loop)
+    same = all(torch.equal(a, b) for a, b in zip(out_b, G))
+    ctx.close()
+    return {"fields": len(fields), "voxels": vox,
+            "batched": {"fields_per_s": len(fields) / (ms_b * 1e-3), "ms": ms_b,
+                        "mvox_per_s": vox / (ms_b * 1e-3) / 1e6, "gpu_launches": l_b},
+            "plain_loop": {"fields_per_s": len(fields) / (ms_p * 1e-3), "ms": ms_p,
+                           "mvox_per_s": vox / (ms_p * 1e-3) / 1e6, "gpu_launches": l_p},
+            "speedup": ms_p / ms_b, "bit_identical_to_plain": bool(same),
+            "statuses": sorted({r.status for r in reps_b}),
+            "max_outer_iters": max(r.outer_iters for r in reps_b)}
+
+
+# ---------------------------------------------------------------------------
+# Served form: Poisson arrivals into the request loop.
+# ---------------------------------------------------------------------------
+def serving_requests(n, dev):
+    reqs = []
+    for i in range(n):
+        s = synth.serving_request_spec(i)
+        f, g, eb = synth.make_field_device(s["w"], s["h"], s["d"], n_gauss=s["n_gauss"],
+                                           seed=s["seed"], rel=s["rel"], dtype=s["dtype"],
+                                           device=dev)
+        reqs.append((f, g, eb))
+    return reqs
+
+
+def measure_served(local, rates, n_max=96, seconds=3.0, reqs=None):
+    """Per rate: p50/p99 latency and served fields/s of a Poisson stream;
+    beside them the plain loop's fields/s on the same requests."""
+    import torch
+    from extrem_z_b200 import api
+    dev = torch.device("cuda", local)
+    if reqs is None:
+        reqs = serving_requests(n_max, dev)
+    n_max = len(reqs)
+    work = [torch.empty_like(g) for _, g, _ in reqs]
+    vox = [f.numel() for f, _, _ in reqs]
+    stream = torch.cuda.current_stream(dev)
+
+    # Plain loop: every request alone, one after another (warmed with the
+    # largest request, so that its workspace pool has grown).
+    ctx = api.Context(local)
+    big = max(range(n_max), key=lambda i: vox[i])
+    for i in [big] + list(range(min(3, n_max))):
+        work[i].copy_(reqs[i][1])
+        ctx.correct_device(reqs[i][0], work[i], reqs[i][2], stream=stream.cuda_stream, **PARAMS)
+    for (f, g0, eb), w in zip(reqs, work):
+        w.copy_(g0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for (f, g0, eb), w in zip(reqs, work):
+        ctx.correct_device(f, w, eb, stream=stream.cuda_stream, **PARAMS)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain_out = [w.clone() for w in work]
+    ctx.close()
+
+    sweep = []
+    identical = True
+    with api.Server(local, reserve_bytes=SERVE_RESERVE_BYTES) as srv:
+        # Warm-up burst.
+        warm = list(range(min(8, n_max)))
+        for i in warm:
+            work[i].copy_(reqs[i][1])
+        torch.cuda.synchronize()
+        for t in [srv.submit(reqs[i][0], work[i], reqs[i][2], stream=stream.cuda_stream,
+                             **PARAMS) for i in warm]:
+            srv.wait(t)
+        for rate in rates:
+            n = int(min(n_max, max(24, rate * seconds)))
+            for (f, g0, eb), w in zip(reqs[:n], work[:n]):
+                w.copy_(g0)
+            torch.cuda.synchronize()
+            gaps = np.random.default_rng(int(rate)).exponential(1.0 / rate, size=n)
+            t_start = time.perf_counter()
+            due = t_start
+            tickets = []
+            for i in range(n):
+                due += gaps[i]
+                pause = due - time.perf_counter()
+                if pause > 0:
+                    time.sleep(pause)
+                f, _, eb = reqs[i]
+                tickets.append(srv.submit(f, work[i], eb, stream=stream.cuda_stream, **PARAMS))
+            results = [srv.wait(t) for t in tickets]
+            t_end = time.perf_counter()
+            lat = np.array([r[1] for r in results])
+            identical &= all(torch.equal(work[i], plain_out[i]) for i in range(n))
+            span = t_end - t_start
+            sweep.append({"rate_req_s": rate, "requests": n,
+                          "p50_ms": float(np.percentile(lat, 50)),
+                          "p99_ms": float(np.percentile(lat, 99)),
+                          "fields_per_s": n / span,
+                          "mvox_per_s": sum(vox[:n]) / span / 1e6,
+                          # Little's law: time-averaged number of requests in the system.
+                          "mean_in_system": float(lat.sum() * 1e-3 / span),
+                          "statuses": sorted({r[0].status for r in results})})
+        st = srv.stats()
+    return {"requests_max": n_max, "voxels_total": int(sum(vox)),
+            "plain_loop": {"fields_per_s": n_max / (plain_ms * 1e-3),
+                           "mvox_per_s": sum(vox) / (plain_ms * 1e-3) / 1e6, "ms": plain_ms},
+            "sweep": sweep, "bit_identical_to_plain": bool(identical),
+            "peak_running": st["peak_running"], "peak_gb_in_use": st["peak_bytes_in_use"] / 1e9,
+            "hbm_budget_gb": 120.0,
+            "inputs": "generated on the device (torch CUDA generator seeded per request)"}
+
+
+def run_form(args, world, rank, local):
+    """Lines of the batched (mixed64) and served (serve) workloads.  Fields
+    are independent, so ranks run replicas and the value sums over ranks."""
+    import torch
+    torch.cuda.set_device(local)
+    barrier(world)
+    if args.workload == "mixed64":
+        r = measure_batched(local, args.steps, args.warmup)
+        value = max_over_ranks(-r["batched"]["fields_per_s"], world) * -world
+        line = {"metric": "fields/s to zero topological mismatch, batched form", "value": value,
+                "unit": "fields/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": r["batched"]["ms"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator)",
+                "config": {"workload": "mixed64", "description": FORM_WORKLOADS["mixed64"],
+                           "params": PARAMS, "parallelism": f"replicas x{world}"},
+                "gpu_launches": r["batched"]["gpu_launches"], "batched": r}
+    else:
+        rates = SERVE_RATES if args.rates is None else tuple(args.rates)
+        r = measure_served(local, rates)
+        top = max(r["sweep"], key=lambda x: x["fields_per_s"])
+        value = max_over_ranks(-top["fields_per_s"], world) * -world
+        line = {"metric": "fields/s served (Poisson stream), p50/p99 latency", "value": value,
+                "unit": "fields/s", "n_gpus": world, "steps": len(rates), "warmup": 0,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator)",
+                "config": {"workload": "serve", "description": FORM_WORKLOADS["serve"],
+                           "params": PARAMS, "parallelism": f"replicas x{world}"},
+                "served": r}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
+                    choices=sorted(WORKLOADS) + sorted(FORM_WORKLOADS))
+    ap.add_argument("--rates", type=float, nargs="*", default=None,
+                    help="serving arrival rates in req/s (serve workload)")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="omit the batched / served summaries from the plain line")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-edge", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -344,6 +618,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload in FORM_WORKLOADS:
+            run_form(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

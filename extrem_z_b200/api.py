@@ -67,7 +67,8 @@ class Field(ctypes.Structure):
 
 
 class ServerConfig(ctypes.Structure):
-    _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("max_jobs", ctypes.c_int),
+    _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("reserve_bytes", ctypes.c_longlong),
+                ("split_voxels", ctypes.c_longlong), ("max_jobs", ctypes.c_int),
                 ("reserved", ctypes.c_int * 7)]
 
 
@@ -310,10 +311,12 @@ class Server:
     HBM budget, and serves all admitted requests with shared launches.
     """
 
-    def __init__(self, device: int = 0, *, hbm_budget_bytes: int = 0, max_jobs: int = 0):
+    def __init__(self, device: int = 0, *, hbm_budget_bytes: int = 0, max_jobs: int = 0,
+                 reserve_bytes: int = 0, split_voxels: int = 0):
         L = load()
         cfg = ServerConfig()
         cfg.hbm_budget_bytes, cfg.max_jobs = int(hbm_budget_bytes), int(max_jobs)
+        cfg.reserve_bytes, cfg.split_voxels = int(reserve_bytes), int(split_voxels)
         h = ctypes.c_void_p()
         _check(L.extremz_server_create(int(device), ctypes.byref(cfg), ctypes.byref(h)),
                allow_cap=False)

@@ -78,27 +78,36 @@ __global__ void k_checksum(const T* __restrict__ a, int N, unsigned long long* o
   if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
 }
 
-// Workspace bytes of one job of n voxels (every critical-point list sized n:
-// the counts are known only after the first setup phase).
+// Workspace of one job of n voxels, in two parts: the per-voxel arrays, taken
+// at admission, and the per-critical-point arrays, taken once the counts are
+// known (ns2 2-saddles, ns1 1-saddles, nmax maxima, nmin minima).  ksz is the
+// size of an order-preserving key (4 or 8).
+constexpr long long arr_bytes(long long count, long long sz) { return (count * sz + 255) & ~255ll; }
+
+constexpr long long job_bytes_voxels(long long n, long long ksz) {
+  return arr_bytes(n, 1) + arr_bytes(n, 2)                          // otype, olm
+         + 5 * arr_bytes(n, 4)                                      // ds, as, dds, das, ext
+         + arr_bytes(n, ksz) + 3 * arr_bytes(n, 4)                  // delta, counter, touched, mm
+         + arr_bytes(n, 4) + arr_bytes(n, 1) + 3 * arr_bytes(n, 4)  // mm_next, mstat, dirty, stamps
+         + arr_bytes(n, 8) + 2 * arr_bytes(n, 4)                    // claim, taken, taken1
+         + 4 * arr_bytes(n, 4)                                      // cand(_next), flagged(1)
+         + arr_bytes(4 * ((n + kCpBlock - 1) / kCpBlock), 4)        // CP block counts
+         + 4096;
+}
+
+constexpr long long job_bytes_cps(long long ns2, long long ns1, long long nmax, long long nmin,
+                                  long long ksz) {
+  return arr_bytes(ns2, 4) + arr_bytes(ns1, 4) + arr_bytes(nmax, 4) + arr_bytes(nmin, 4)
+         + arr_bytes(ns2 * kRowStride, 4) + arr_bytes(ns2 * 2, 4) + arr_bytes(ns2, 1)
+         + arr_bytes(ns1 * kRowStride, 4) + arr_bytes(ns1 * 2, 4) + arr_bytes(ns1, 1)
+         + 4 * arr_bytes(nmax, 4) + 4 * arr_bytes(nmin, 4)
+         + arr_bytes(nmax > nmin ? nmax : nmin, ksz) + arr_bytes(nmax > nmin ? nmax : nmin, 4)
+         + arr_bytes(8, 8) + 4096;
+}
+
+// Worst case (every voxel a critical point of every kind).
 constexpr long long job_bytes_sz(long long n, long long ksz) {
-  long long b = 0;
-  auto add = [&b](long long count, long long sz) { b += (count * sz + 255) & ~255ll; };
-  const long long nb = (n + kCpBlock - 1) / kCpBlock;
-  add(n, 1); add(n, 2);                       // otype, olm
-  for (int i = 0; i < 5; ++i) add(n, 4);      // ds, as, dds, das, ext
-  add(n, ksz); add(n, 4); add(n, 4); add(n, 4);  // delta, counter, touched, mm
-  add(n, 4); add(n, 1); add(n, 4); add(n, 4); add(n, 4);  // mm_next, mstat, dirty, dstamp, rstamp
-  add(n, 8); add(n, 4); add(n, 4);            // claim, taken, taken1
-  for (int i = 0; i < 4; ++i) add(n, 4);      // cand, cand_next, flagged, flagged1
-  add(4 * nb, 4);                             // CP block counts
-  add(n, 4); add(n, 4); add(n, 4); add(n, 4); // CP lists
-  add(n * kRowStride, 4); add(n * 2, 4); add(n, 1);
-  add(n * kRowStride, 4); add(n * 2, 4); add(n, 1);
-  for (int i = 0; i < 4; ++i) add(n, 4);      // per maximum
-  for (int i = 0; i < 4; ++i) add(n, 4);      // per minimum
-  add(n, ksz); add(n, 4);                     // extreme-saddle scratch
-  add(8, 8);                                  // checksum
-  return b + 4096;
+  return job_bytes_voxels(n, ksz) + job_bytes_cps(n, n, n, n, ksz);
 }
 template <class T>
 constexpr long long job_bytes(long long n) {
@@ -121,8 +130,8 @@ struct JobHost {
   int status = EXTREMZ_OK;
   extremz_params p{};
   Job<T> J{};
-  Arena arena;
-  bool own_arena = false;
+  Arena arena, arena2;  // per-voxel part, per-critical-point part
+  bool own_arena = false, own_arena2 = false;
   int ntiles = 0, nb = 0;
   int* bcount = nullptr;
   unsigned long long* checksum = nullptr;
@@ -248,7 +257,8 @@ class BatchEngine {
     J.tb = tb_;
     J.ctr = ctr_dev_ + (size_t)slot * C_COUNT;
     const int N = J.dim.N;
-    const long long need = job_bytes<T>(N);
+    // Borrowed storage holds both parts; an allocation holds the first.
+    const long long need = storage ? job_bytes<T>(N) : job_bytes_voxels(N, sizeof(K));
     if (storage) {
       jh.arena = *storage;
       jh.arena.used = 0;
@@ -328,24 +338,43 @@ class BatchEngine {
 
   // Releases a finished job's slot and (stream-ordered) its workspace.
   void release(int slot) { free_job(slots_[slot]); }
+  // Releases every job (after an error that ends a batch).
+  void release_jobs() {
+    for (auto& j : slots_) free_job(j);
+  }
 
   // One tick: every phase any job is in, in program order; then one copy of
   // all counter blocks and the branches.  Returns a status (the jobs keep
   // their own statuses).
   int tick() {
-    bool any = false;
+    EZ_RUN(tick_issue());
+    return tick_complete();
+  }
+
+  // First half of a tick: the launches and the asynchronous copy of the
+  // counter blocks.  Engines on different streams issue, then complete, so
+  // their ticks overlap on the device.
+  int tick_issue() {
+    issued_ = false;
     for (int ph = 0; ph < PC_COUNT; ++ph) {
       std::vector<int> sel;
       for (int i = 0; i < kMaxSel; ++i)
         if (slots_[i].used && !slots_[i].waiting && slots_[i].pc == ph) sel.push_back(i);
       if (sel.empty()) continue;
-      any = true;
+      issued_ = true;
       EZ_RUN(run_phase(ph, sel));
     }
-    if (!any) return EXTREMZ_OK;
+    if (!issued_) return EXTREMZ_OK;
     EZ_CHECK(cudaGetLastError());
     EZ_CHECK(cudaMemcpyAsync(ctr_host_, ctr_dev_, sizeof(int) * C_COUNT * kMaxSel,
                              cudaMemcpyDeviceToHost, st_));
+    return EXTREMZ_OK;
+  }
+
+  // Second half: wait for the counters, then every job's branches.
+  int tick_complete() {
+    if (!issued_) return EXTREMZ_OK;
+    issued_ = false;
     EZ_CHECK(cudaStreamSynchronize(st_));
     for (int i = 0; i < kMaxSel; ++i) {
       JobHost<T>& j = slots_[i];
@@ -392,7 +421,7 @@ class BatchEngine {
  private:
   cudaStream_t st_;
   cudaMemPool_t pool_mem_ = nullptr;
-  bool ready_ = false, borrowed_ = false;
+  bool ready_ = false, borrowed_ = false, issued_ = false;
   int grid_ = 1184;
   DeviceTables tb_{};
   Job<T>* jobs_dev_ = nullptr;
@@ -440,7 +469,28 @@ class BatchEngine {
 
   void free_job(JobHost<T>& j) {
     if (j.used && j.own_arena && j.arena.base) cudaFreeAsync(j.arena.base, st_);
+    if (j.used && j.own_arena2 && j.arena2.base) cudaFreeAsync(j.arena2.base, st_);
     j = JobHost<T>();
+  }
+
+  // The per-critical-point part of a job's workspace: exact size from the
+  // counts, or the rest of borrowed storage.
+  int take_cp_storage(JobHost<T>& jh, int ns2, int ns1, int nmax, int nmin) {
+    if (!jh.own_arena) return EXTREMZ_OK;  // borrowed: carve from the same arena
+    const long long need = job_bytes_cps(ns2, ns1, nmax, nmin, sizeof(K));
+    void* base = nullptr;
+    const cudaError_t e = pool_mem_ ? cudaMallocFromPoolAsync(&base, (size_t)need, pool_mem_, st_)
+                                    : cudaMallocAsync(&base, (size_t)need, st_);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return EXTREMZ_OOM;
+    }
+    jh.arena2.base = static_cast<char*>(base);
+    jh.arena2.cap = (size_t)need;
+    jh.arena2.used = 0;
+    jh.arena2.fixed = true;
+    jh.own_arena2 = true;
+    return EXTREMZ_OK;
   }
 
   Sel make_sel(const std::vector<int>& slots, bool tiles) const {
@@ -477,8 +527,15 @@ class BatchEngine {
         }
         return EXTREMZ_OK;
       case PC_SETUP_B:
-        for (int i : sel) EZ_RUN(setup_b(i));
-        for (int i : sel) slots_[i].pc = PC_CL_DETECT;
+        for (int i : sel) {
+          const int rc = setup_b(i);
+          if (rc == EXTREMZ_OOM) {  // this job ends; the others go on
+            finish(i, EXTREMZ_OOM);
+            continue;
+          }
+          if (rc != EXTREMZ_OK) return rc;
+          slots_[i].pc = PC_CL_DETECT;
+        }
         return EXTREMZ_OK;
       case PC_CL_DETECT:
         detect(sel);
@@ -599,8 +656,8 @@ class BatchEngine {
     }
   }
 
-  // Fused row-slot / candidate pass, bounded arbitration rounds and the
-  // sequential completion, for one side.
+  // Fused row-slot / candidate pass, three grid-wide arbitration rounds and
+  // the per-job completion rounds, for one side.
   template <bool kSplit>
   void wrong_neighbours(const Sel& s) {
     const Job<T>* jobs = jobs_dev_;
@@ -612,16 +669,17 @@ class BatchEngine {
       launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, jobs, s);
       ctl(s, OP_WN_ROUND_END);
     }
-    launch(K_WRONG_NBR, k_wn_sequential<T, kSplit>, 1, 1, jobs, s);
+    launch(K_WRONG_NBR, k_wn_resolve<T, kSplit>, s.n, 1024, jobs, s);
   }
 
   int setup_b(int slot) {
     JobHost<T>& jh = slots_[slot];
     Job<T>& J = jh.J;
-    Arena& A = jh.arena;
     const int N = J.dim.N;
     const int ns2 = h(slot, C_NS2), ns1 = h(slot, C_NS1), nmax = h(slot, C_NMAX),
               nmin = h(slot, C_NMIN);
+    EZ_RUN(take_cp_storage(jh, ns2, ns1, nmax, nmin));
+    Arena& A = jh.own_arena2 ? jh.arena2 : jh.arena;
     J.sad2 = A.take<int>(ns2);
     J.sad1 = A.take<int>(ns1);
     J.maxima = A.take<int>(nmax);
@@ -644,7 +702,7 @@ class BatchEngine {
     J.ext_key = A.take<K>(ne);
     J.ext_id = A.take<int>(ne);
     jh.checksum = A.take<unsigned long long>(8);
-    if (!jh.checksum) return EXTREMZ_OOM;
+    if (!jh.checksum || !J.ext_id || !J.ocnt1 || !J.first_sj) return EXTREMZ_OOM;
     launch(K_OTHER, k_cp_write, jh.nb, kCpBlock, (const int8_t*)J.otype, N, (const int*)jh.bcount,
            J.sad2, J.sad1, J.maxima, J.minima);
     launch(K_OTHER, k_ext_index<T>, grid_, 256, J);

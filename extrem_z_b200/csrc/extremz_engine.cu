@@ -188,8 +188,16 @@ struct Context {
   int device = 0;
   Arena stage;  // device copies of host fields (extremz_correct_host)
   cudaMemPool_t pool = nullptr;
+  cudaStream_t aux = nullptr;  // second stream of batches (the double engine)
+  cudaEvent_t join = nullptr;
   BatchEngine<float> e32{nullptr};
   BatchEngine<double> e64{nullptr};
+  int ensure_aux() {
+    if (aux) return EXTREMZ_OK;
+    EZ_CHECK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    EZ_CHECK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    return EXTREMZ_OK;
+  }
   int ensure_pool() {
     if (pool) return EXTREMZ_OK;
     pool = make_pool(device);
@@ -206,6 +214,8 @@ struct Context {
       cudaMemPoolDestroy(pool);
     }
     if (stage.base) cudaFree(stage.base);
+    if (join) cudaEventDestroy(join);
+    if (aux) cudaStreamDestroy(aux);
   }
 };
 
@@ -366,16 +376,34 @@ struct BatchDriver {
   size_t next = 0;
 };
 
+static int correct_batch_run(Context& C, const extremz_field* fields, int n,
+                             extremz_report* reports, cudaStream_t st);
+
 static int correct_batch(Context& C, const extremz_field* fields, int n, extremz_report* reports,
                          cudaStream_t st) {
+  const int rc = correct_batch_run(C, fields, n, reports, st);
+  if (rc != EXTREMZ_OK) {  // leave no job behind in the context's engines
+    C.e32.release_jobs();
+    C.e64.release_jobs();
+  }
+  return rc;
+}
+
+static int correct_batch_run(Context& C, const extremz_field* fields, int n,
+                             extremz_report* reports, cudaStream_t st) {
   for (int i = 0; i < n; ++i) {
     EZ_RUN(check_args(fields[i].dtype, fields[i].width, fields[i].height, fields[i].depth,
                       &fields[i].params));
     if (!fields[i].orig || !fields[i].decp) return EXTREMZ_BAD_ARG;
   }
   EZ_RUN(C.ensure_pool());
+  EZ_RUN(C.ensure_aux());
+  // The double engine runs on the auxiliary stream, after what the caller
+  // queued on st; the caller's stream is synchronised with it at the end.
+  EZ_CHECK(cudaEventRecord(C.join, st));
+  EZ_CHECK(cudaStreamWaitEvent(C.aux, C.join, 0));
   C.e32.set_stream(st);
-  C.e64.set_stream(st);
+  C.e64.set_stream(C.aux);
   EZ_RUN(C.e32.init(nullptr, nullptr));
   EZ_RUN(C.e64.init(nullptr, nullptr));
   std::vector<int> slot(n, -1), done(n, 0);
@@ -385,6 +413,12 @@ static int correct_batch(Context& C, const extremz_field* fields, int n, extremz
   std::vector<int> order(n);
   for (int i = 0; i < n; ++i) order[i] = i;
   const long long l0 = C.e32.launches() + C.e64.launches();
+  // Per-class timing of the whole batch into reports[0] when the first
+  // field asks for it.
+  const bool prof = n > 0 && reports && (fields[0].params.flags & EXTREMZ_FLAG_PROFILE);
+  const int pmask = n > 0 ? (fields[0].params.flags >> EXTREMZ_PROFILE_CLASS_SHIFT) & ((1 << K_NUM) - 1) : 0;
+  C.e32.set_profile(prof, pmask);
+  C.e64.set_profile(prof, pmask);
   while (remaining > 0) {
     // Admit while slots are free.
     while (next < order.size()) {
@@ -406,8 +440,11 @@ static int correct_batch(Context& C, const extremz_field* fields, int n, extremz
       which[i] = fd.dtype == EXTREMZ_F32 ? 0 : 1;
       ++next;
     }
-    if (C.e32.active()) EZ_RUN(C.e32.tick());
-    if (C.e64.active()) EZ_RUN(C.e64.tick());
+    const bool a32 = C.e32.active() > 0, a64 = C.e64.active() > 0;
+    if (a32) EZ_RUN(C.e32.tick_issue());
+    if (a64) EZ_RUN(C.e64.tick_issue());
+    if (a32) EZ_RUN(C.e32.tick_complete());
+    if (a64) EZ_RUN(C.e64.tick_complete());
     for (int i = 0; i < n; ++i) {
       if (slot[i] < 0 || done[i]) continue;
       const bool fin = which[i] == 0 ? C.e32.job(slot[i]).pc == PC_DONE
@@ -423,16 +460,30 @@ static int correct_batch(Context& C, const extremz_field* fields, int n, extremz
       --remaining;
     }
   }
+  EZ_CHECK(cudaStreamSynchronize(C.aux));
   EZ_CHECK(cudaStreamSynchronize(st));
   if (reports && n > 0) reports[0].kernel_launches = C.e32.launches() + C.e64.launches() - l0;
+  if (prof) {
+    std::memset(reports[0].prof_ms, 0, sizeof(reports[0].prof_ms));
+    std::memset(reports[0].prof_launches, 0, sizeof(reports[0].prof_launches));
+    C.e32.collect_profile(&reports[0]);
+    C.e64.collect_profile(&reports[0]);
+    C.e32.drop_profile_events();
+    C.e64.drop_profile_events();
+    C.e32.set_profile(false, 0);
+    C.e64.set_profile(false, 0);
+  }
   return EXTREMZ_OK;
 }
 
 
 // ---------------------------------------------------------------------------
-// Serving: a request loop on its own thread and stream.  Between ticks it
-// admits queued requests in arrival order while their footprint fits the HBM
-// budget and a slot is free; every tick serves all admitted jobs.
+// Serving: request loops ("lanes"), each on its own thread with a stream per
+// dtype.  Between ticks a lane admits queued requests in arrival order while
+// their footprint fits the shared HBM budget and a slot is free; every tick
+// serves all of the lane's admitted jobs.  Requests up to split_voxels go to
+// lane 0, whose streams have the higher priority, larger ones to lane 1, so a
+// small request does not wait behind the long ticks of a large one.
 // ---------------------------------------------------------------------------
 using Clock = std::chrono::steady_clock;
 
@@ -459,30 +510,38 @@ struct ServerRunning {
   int slot;
 };
 
+struct ServerLane {
+  cudaStream_t st32 = nullptr, st64 = nullptr;
+  BatchEngine<float> e32{nullptr};
+  BatchEngine<double> e64{nullptr};
+  std::thread th;
+  std::deque<ServerReq> queue;      // guarded by the server's mutex
+  std::vector<ServerRunning> running;  // the lane thread's own
+};
+
 static long long field_footprint(const extremz_field& f) {
   const long long n = (long long)f.width * f.height * f.depth;
   const long long vb = f.dtype == EXTREMZ_F32 ? 4 : 8;
   return job_bytes_max(n) + 2 * n * vb;
 }
 
+constexpr int kServerLanes = 2;
+
 }  // namespace extremz
 
 struct extremz_server_s {
   int device = 0;
   long long budget = 0;
+  long long split = 0;
   int max_jobs = extremz::kMaxSel;
-  cudaStream_t st = nullptr;
+  int nlanes = extremz::kServerLanes;
   cudaMemPool_t pool = nullptr;
-  extremz::BatchEngine<float> e32{nullptr};
-  extremz::BatchEngine<double> e64{nullptr};
-  std::thread th;
+  extremz::ServerLane lane[extremz::kServerLanes];
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   bool stop = false;
-  int broken = EXTREMZ_OK;  // a CUDA error ends the loop; later requests fail with it
-  std::deque<extremz::ServerReq> queue;
+  int broken = EXTREMZ_OK;  // a CUDA error ends the loops; later requests fail with it
   std::unordered_map<long long, extremz::ServerResult> results;
-  std::vector<extremz::ServerRunning> running;
   long long next_ticket = 1;
   extremz_server_stats stats{};
 };
@@ -503,21 +562,38 @@ static void server_finish(extremz_server* s, const ServerRunning& r, int status,
   s->stats.bytes_in_use -= r.footprint;
   s->stats.completed += 1;
   s->stats.running -= 1;
+  s->cv_work.notify_all();  // budget released: a blocked lane may admit
 }
 
-static void server_loop(extremz_server* s) {
+// Marks every queued request of every lane failed with rc (under the lock).
+static void server_fail_queued(extremz_server* s, int rc) {
+  for (int l = 0; l < s->nlanes; ++l) {
+    for (ServerReq& q : s->lane[l].queue) {
+      cudaEventDestroy(q.ready);
+      ServerResult& res = s->results[q.ticket];
+      res.done = true;
+      res.status = rc;
+      res.rep.status = rc;
+    }
+    s->lane[l].queue.clear();
+  }
+  s->stats.queued = 0;
+}
+
+static void server_loop(extremz_server* s, int li) {
   cudaSetDevice(s->device);
+  ServerLane& L = s->lane[li];
   for (;;) {
     std::vector<ServerReq> admit_now;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      if (s->running.empty())
-        s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-      if (s->stop && s->running.empty()) break;
+      if (L.running.empty())
+        s->cv_work.wait(lk, [&] { return s->stop || s->broken || !L.queue.empty(); });
+      if ((s->stop || s->broken) && L.running.empty()) break;
       int n32 = 0, n64 = 0;
-      for (const auto& r : s->running) (r.dtype == EXTREMZ_F32 ? n32 : n64)++;
-      while (!s->stop && !s->queue.empty()) {
-        const ServerReq& r = s->queue.front();
+      for (const auto& r : L.running) (r.dtype == EXTREMZ_F32 ? n32 : n64)++;
+      while (!s->stop && !s->broken && !L.queue.empty()) {
+        const ServerReq& r = L.queue.front();
         int& n = r.field.dtype == EXTREMZ_F32 ? n32 : n64;
         if (n >= s->max_jobs) break;
         if (s->stats.bytes_in_use + r.footprint > s->budget) break;
@@ -525,44 +601,45 @@ static void server_loop(extremz_server* s) {
         s->stats.peak_bytes_in_use = std::max(s->stats.peak_bytes_in_use, s->stats.bytes_in_use);
         s->stats.queued -= 1;
         s->stats.running += 1;
+        s->stats.peak_running = std::max<int>(s->stats.peak_running, (int)s->stats.running);
         ++n;
         admit_now.push_back(r);
-        s->queue.pop_front();
+        L.queue.pop_front();
       }
     }
     for (ServerReq& r : admit_now) {
-      cudaStreamWaitEvent(s->st, r.ready, 0);
+      cudaStreamWaitEvent(r.field.dtype == EXTREMZ_F32 ? L.st32 : L.st64, r.ready, 0);
       cudaEventDestroy(r.ready);
       const extremz_field& f = r.field;
       int slot = -1;
       int rc = f.dtype == EXTREMZ_F32
-                   ? s->e32.admit((const float*)f.orig, (float*)f.decp, f.width, f.height, f.depth,
-                                  f.params, nullptr, 0, nullptr, r.ticket, &slot)
-                   : s->e64.admit((const double*)f.orig, (double*)f.decp, f.width, f.height,
-                                  f.depth, f.params, nullptr, 0, nullptr, r.ticket, &slot);
+                   ? L.e32.admit((const float*)f.orig, (float*)f.decp, f.width, f.height, f.depth,
+                                 f.params, nullptr, 0, nullptr, r.ticket, &slot)
+                   : L.e64.admit((const double*)f.orig, (double*)f.decp, f.width, f.height,
+                                 f.depth, f.params, nullptr, 0, nullptr, r.ticket, &slot);
       ServerRunning run{r.ticket, r.footprint, r.t0, f.dtype, slot};
       if (rc != EXTREMZ_OK) {
         server_finish(s, run, rc, nullptr);
         continue;
       }
-      s->running.push_back(run);
+      L.running.push_back(run);
     }
-    {
-      std::lock_guard<std::mutex> lk(s->mu);
-      s->stats.peak_running = std::max(s->stats.peak_running, (int)s->running.size());
+    if (L.running.empty()) {
+      // Blocked by the budget the other lane holds: wait for a release.
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+      continue;
     }
     int rc = EXTREMZ_OK;
-    if (s->e32.active()) rc = s->e32.tick();
-    if (rc == EXTREMZ_OK && s->e64.active()) rc = s->e64.tick();
-    {
-      std::lock_guard<std::mutex> lk(s->mu);
-      s->stats.ticks += 1;
-      s->stats.kernel_launches = s->e32.launches() + s->e64.launches();
-    }
+    const bool a32 = L.e32.active() > 0, a64 = L.e64.active() > 0;
+    if (a32) rc = L.e32.tick_issue();
+    if (rc == EXTREMZ_OK && a64) rc = L.e64.tick_issue();
+    if (rc == EXTREMZ_OK && a32) rc = L.e32.tick_complete();
+    if (rc == EXTREMZ_OK && a64) rc = L.e64.tick_complete();
     std::vector<ServerRunning> still;
-    for (const ServerRunning& r : s->running) {
+    for (const ServerRunning& r : L.running) {
       const bool f32 = r.dtype == EXTREMZ_F32;
-      const int pc = f32 ? s->e32.job(r.slot).pc : s->e64.job(r.slot).pc;
+      const int pc = f32 ? L.e32.job(r.slot).pc : L.e64.job(r.slot).pc;
       if (rc == EXTREMZ_OK && pc != PC_DONE) {
         still.push_back(r);
         continue;
@@ -571,33 +648,31 @@ static void server_loop(extremz_server* s) {
       std::memset(&rep, 0, sizeof(rep));
       int status = rc;
       if (rc == EXTREMZ_OK) {
-        if (f32) s->e32.fill_report(r.slot, &rep);
-        else s->e64.fill_report(r.slot, &rep);
+        if (f32) L.e32.fill_report(r.slot, &rep);
+        else L.e64.fill_report(r.slot, &rep);
         status = rep.status;
       }
-      if (f32) s->e32.release(r.slot);
-      else s->e64.release(r.slot);
+      if (f32) L.e32.release(r.slot);
+      else L.e64.release(r.slot);
       server_finish(s, r, status, &rep);
     }
-    s->running.swap(still);
+    L.running.swap(still);
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stats.ticks += 1;
+      if (rc != EXTREMZ_OK) {
+        s->broken = rc;
+        server_fail_queued(s, rc);
+      }
+    }
     s->cv_done.notify_all();
     if (rc != EXTREMZ_OK) {
-      std::lock_guard<std::mutex> lk(s->mu);
-      s->broken = rc;
-      for (ServerReq& q : s->queue) {
-        cudaEventDestroy(q.ready);
-        ServerResult& res = s->results[q.ticket];
-        res.done = true;
-        res.status = rc;
-        res.rep.status = rc;
-      }
-      s->queue.clear();
-      s->stats.queued = 0;
-      s->cv_done.notify_all();
+      s->cv_work.notify_all();
       break;
     }
   }
-  cudaStreamSynchronize(s->st);
+  cudaStreamSynchronize(L.st32);
+  cudaStreamSynchronize(L.st64);
 }
 
 }  // namespace extremz
@@ -749,6 +824,7 @@ extremz_status extremz_server_create(int device, const extremz_server_config* cf
       cfg && cfg->hbm_budget_bytes > 0 ? cfg->hbm_budget_bytes : 120ll * 1000 * 1000 * 1000;
   const int max_jobs = cfg && cfg->max_jobs > 0 ? cfg->max_jobs : extremz::kMaxSel;
   if (max_jobs > extremz::kMaxSel) return EXTREMZ_BAD_ARG;
+  if (cfg && (cfg->reserve_bytes < 0 || cfg->reserve_bytes > budget)) return EXTREMZ_BAD_ARG;
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(device);
@@ -757,28 +833,51 @@ extremz_status extremz_server_create(int device, const extremz_server_config* cf
   s->device = device;
   s->budget = budget;
   s->max_jobs = max_jobs;
+  s->split = cfg && cfg->split_voxels != 0 ? cfg->split_voxels : 4ll << 20;
+  s->nlanes = s->split < 0 ? 1 : kServerLanes;
   int rc = EXTREMZ_OK;
-  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) rc = EXTREMZ_CUDA_ERR;
+  int lo = 0, hi = 0;  // numerically lower = higher priority
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  for (int l = 0; l < s->nlanes && rc == EXTREMZ_OK; ++l) {
+    const int prio = l == 0 ? hi : lo;
+    if (cudaStreamCreateWithPriority(&s->lane[l].st32, cudaStreamNonBlocking, prio) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&s->lane[l].st64, cudaStreamNonBlocking, prio) != cudaSuccess)
+      rc = EXTREMZ_CUDA_ERR;
+  }
   if (rc == EXTREMZ_OK && !(s->pool = make_pool(device))) rc = EXTREMZ_OOM;
-  if (rc == EXTREMZ_OK) {
-    s->e32.set_stream(s->st);
-    s->e64.set_stream(s->st);
-    s->e32.set_pool(s->pool);
-    s->e64.set_pool(s->pool);
-    rc = s->e32.init(nullptr, nullptr);
-    if (rc == EXTREMZ_OK) rc = s->e64.init(nullptr, nullptr);
+  for (int l = 0; l < s->nlanes && rc == EXTREMZ_OK; ++l) {
+    ServerLane& L = s->lane[l];
+    L.e32.set_stream(L.st32);
+    L.e64.set_stream(L.st64);
+    L.e32.set_pool(s->pool);
+    L.e64.set_pool(s->pool);
+    rc = L.e32.init(nullptr, nullptr);
+    if (rc == EXTREMZ_OK) rc = L.e64.init(nullptr, nullptr);
+  }
+  // Grow the pool to the reservation now, so that admissions do not pay for
+  // mapping new memory.
+  if (rc == EXTREMZ_OK && cfg && cfg->reserve_bytes > 0) {
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, (size_t)cfg->reserve_bytes, s->pool, s->lane[0].st32) !=
+            cudaSuccess ||
+        cudaFreeAsync(p, s->lane[0].st32) != cudaSuccess ||
+        cudaStreamSynchronize(s->lane[0].st32) != cudaSuccess)
+      rc = EXTREMZ_OOM;
   }
   if (rc != EXTREMZ_OK) {
     cudaGetLastError();
-    s->e32.release_all();
-    s->e64.release_all();
+    for (int l = 0; l < s->nlanes; ++l) {
+      s->lane[l].e32.release_all();
+      s->lane[l].e64.release_all();
+      if (s->lane[l].st32) cudaStreamDestroy(s->lane[l].st32);
+      if (s->lane[l].st64) cudaStreamDestroy(s->lane[l].st64);
+    }
     if (s->pool) cudaMemPoolDestroy(s->pool);
-    if (s->st) cudaStreamDestroy(s->st);
     delete s;
     cudaSetDevice(prev);
     return (extremz_status)rc;
   }
-  s->th = std::thread(server_loop, s);
+  for (int l = 0; l < s->nlanes; ++l) s->lane[l].th = std::thread(server_loop, s, l);
   cudaSetDevice(prev);
   *out = s;
   return EXTREMZ_OK;
@@ -789,19 +888,29 @@ void extremz_server_destroy(extremz_server* s) {
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stop = true;
-    for (ServerReq& q : s->queue) cudaEventDestroy(q.ready);
-    s->queue.clear();
+    for (int l = 0; l < s->nlanes; ++l) {
+      for (ServerReq& q : s->lane[l].queue) cudaEventDestroy(q.ready);
+      s->lane[l].queue.clear();
+    }
   }
   s->cv_work.notify_all();
-  if (s->th.joinable()) s->th.join();
+  for (int l = 0; l < s->nlanes; ++l)
+    if (s->lane[l].th.joinable()) s->lane[l].th.join();
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(s->device);
-  s->e32.release_all();
-  s->e64.release_all();
-  cudaStreamSynchronize(s->st);
+  for (int l = 0; l < s->nlanes; ++l) {
+    ServerLane& L = s->lane[l];
+    L.e32.release_all();
+    L.e64.release_all();
+    cudaStreamSynchronize(L.st32);
+    cudaStreamSynchronize(L.st64);
+  }
   if (s->pool) cudaMemPoolDestroy(s->pool);
-  cudaStreamDestroy(s->st);
+  for (int l = 0; l < s->nlanes; ++l) {
+    cudaStreamDestroy(s->lane[l].st32);
+    cudaStreamDestroy(s->lane[l].st64);
+  }
   cudaSetDevice(prev);
   delete s;
 }
@@ -817,6 +926,8 @@ extremz_status extremz_server_submit(extremz_server* s, const extremz_field* f, 
   r.field = *f;
   r.field.params.flags &= ~EXTREMZ_FLAG_PROFILE;
   r.footprint = fp;
+  const long long voxels = (long long)f->width * f->height * f->depth;
+  const int li = (s->nlanes > 1 && voxels > s->split) ? 1 : 0;
   int prev = 0;
   cudaGetDevice(&prev);
   if (prev != s->device) cudaSetDevice(s->device);
@@ -837,12 +948,12 @@ extremz_status extremz_server_submit(extremz_server* s, const extremz_field* f, 
     r.ticket = s->next_ticket++;
     r.t0 = Clock::now();
     s->results[r.ticket] = ServerResult();
-    s->queue.push_back(r);
+    s->lane[li].queue.push_back(r);
     s->stats.submitted += 1;
     s->stats.queued += 1;
     *ticket = r.ticket;
   }
-  s->cv_work.notify_one();
+  s->cv_work.notify_all();
   return EXTREMZ_OK;
 }
 
@@ -894,6 +1005,9 @@ void extremz_server_get_stats(extremz_server* s, extremz_server_stats* out) {
   if (!s || !out) return;
   std::lock_guard<std::mutex> lk(s->mu);
   *out = s->stats;
+  out->kernel_launches = 0;
+  for (int l = 0; l < s->nlanes; ++l)
+    out->kernel_launches += s->lane[l].e32.launches() + s->lane[l].e64.launches();
 }
 
 long long extremz_noalloc_max_voxels(void) { return kNoAllocMaxVoxels; }

@@ -1073,35 +1073,74 @@ __global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jo
   }
 }
 
-// Sequential completion for whatever the bounded rounds left unresolved:
-// one thread takes the remaining saddles in ascending id.
+// Completion of the arbitration for whatever the grid-wide rounds left
+// unresolved: one block per job runs further vote / commit rounds until no
+// saddle is left.  Each round commits at least the smallest unresolved saddle
+// (its vote wins on every candidate it votes on), so at most n rounds run; the
+// device iteration limit bounds them as well.  claim and taken are read
+// through L2 (__ldcg): other threads of the block update them with atomics
+// and stores between the barriers.
 template <class T, bool kSplit>
-__global__ void k_wn_sequential(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
-  for (int jk = 0; jk < sel.n; ++jk) {
-  const Job<T>& J = jobs[sel.idx[jk]];
+__global__ void __launch_bounds__(1024) k_wn_resolve(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+  if (blockIdx.x >= sel.n) return;
+  const Job<T>& J = jobs[sel.idx[blockIdx.x]];
+  __shared__ int s_next;
   const int stamp = J.ctr[C_WNSTAMP];
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  int n = J.ctr[C_CAND];
   int* taken = kSplit ? J.taken : J.taken1;
   int* flagged = kSplit ? J.flagged : J.flagged1;
   int* nflag = J.ctr + (kSplit ? C_NFC : C_NFC1);
+  int* cur = J.cand;
+  int* nxt = J.cand_next;
+  int n = J.ctr[C_CAND];
+  unsigned long long round = (unsigned)J.ctr[C_WNROUND];
+  const int cap = J.iter_cap;
+  int it = 0;
   while (n > 0) {
-    int bi = 0;
-    for (int e = 1; e < n; ++e)
-      if (J.cand[e] < J.cand[bi]) bi = e;
-    const int s = J.cand[bi];
-    J.cand[bi] = J.cand[n - 1];
-    --n;
-    int ids[kNumDirs];
-    const int k = wn_candidates<T, kSplit>(J, s, ids);
-    for (int j = 0; j < k; ++j)
-      if (taken[ids[j]] != stamp) {
-        taken[ids[j]] = stamp;
-        flagged[(*nflag)++] = ids[j];
-        break;
+    if (it++ >= cap) {
+      if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrResolve);
+      break;
+    }
+    ++round;
+    const unsigned long long hi = round << 32;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      const int s = __ldcg(cur + e);
+      int ids[kNumDirs];
+      const int k = wn_candidates<T, kSplit>(J, s, ids);
+      const unsigned long long vote = hi | (unsigned)(~s);
+      for (int j = 0; j < k; ++j)
+        if (__ldcg(taken + ids[j]) != stamp) atomicMax(J.claim + ids[j], vote);
+    }
+    if (threadIdx.x == 0) s_next = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      const int s = __ldcg(cur + e);
+      int ids[kNumDirs];
+      const int k = wn_candidates<T, kSplit>(J, s, ids);
+      int first = -1;
+      for (int j = 0; j < k; ++j)
+        if (__ldcg(taken + ids[j]) != stamp) {
+          first = ids[j];
+          break;
+        }
+      if (first < 0) continue;  // every candidate already flagged: resolved
+      const unsigned long long vote = hi | (unsigned)(~s);
+      if (__ldcg(J.claim + first) == vote) {
+        taken[first] = stamp;
+        flagged[atomicAdd(nflag, 1)] = first;
+      } else {
+        nxt[atomicAdd(&s_next, 1)] = s;
       }
+    }
+    __syncthreads();
+    n = s_next;
+    int* t = cur;
+    cur = nxt;
+    nxt = t;
+    __syncthreads();  // every thread has read s_next before it is reset
   }
-  J.ctr[C_CAND] = 0;
+  if (threadIdx.x == 0) {
+    J.ctr[C_CAND] = 0;
+    J.ctr[C_WNROUND] = (int)round;
   }
 }
 

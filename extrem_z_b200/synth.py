@@ -166,3 +166,70 @@ def serving_request_spec(request_id: int):
     rel = float(math.exp(r.uniform(math.log(1e-5), math.log(1e-2))))
     g = max(8, int(round(512 * w * h * d / 256 ** 3)))
     return dict(w=w, h=h, d=d, n_gauss=g, seed=seed, rel=rel, dtype=dtype)
+
+
+def make_field_device(w: int, h: int, d: int, *, n_gauss: int, seed: int, rel: float,
+                      dtype=np.float64, alpha: float = 2.0, noise_rms: float = 0.05,
+                      device="cuda"):
+    """The generator of ``make_field`` evaluated on a CUDA device with torch.
+
+    Centres, widths and amplitudes come from the same numpy stream as
+    ``gaussian_field``; the white noise comes from torch's CUDA generator
+    seeded with ``seed``, so values differ from ``make_field`` while the
+    distribution is the same.  For request streams too large to generate on
+    the host in a benchmark's time.  Returns (f, decp, eb) with f and decp
+    CUDA tensors of shape (d, h, w).
+    """
+    import torch
+    rng = np.random.default_rng(seed)
+    dims = np.array([w, h, d], dtype=np.float64)
+    centres = rng.uniform(0.0, 1.0, size=(n_gauss, 3)) * dims
+    sigmas = rng.uniform(2.0, 10.0, size=(n_gauss, 3))
+    amps = rng.uniform(-1.0, 1.0, size=n_gauss)
+    dev = torch.device(device)
+    f64 = torch.float64
+    c = torch.as_tensor(centres, dtype=f64, device=dev)
+    s = torch.as_tensor(sigmas, dtype=f64, device=dev)
+    a = torch.as_tensor(amps, dtype=f64, device=dev)
+
+    def profile(n, axis):
+        t = torch.arange(n, dtype=f64, device=dev)
+        return torch.exp(-0.5 * ((t[None, :] - c[:, axis:axis + 1]) / s[:, axis:axis + 1]) ** 2)
+
+    gx, gy, gz = profile(w, 0), profile(h, 1), profile(d, 2)
+    wz = (gz * a[:, None]).T.contiguous()           # (d, G)
+    out = torch.empty((d, h, w), dtype=f64, device=dev)
+    cy = max(1, min(h, (1 << 25) // max(1, n_gauss * w)))
+    for y0 in range(0, h, cy):
+        y1 = min(h, y0 + cy)
+        kron = (gy[:, y0:y1, None] * gx[:, None, :]).reshape(n_gauss, -1)
+        out[:, y0:y1, :] = (wz @ kron).reshape(d, y1 - y0, w)
+
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(seed))
+    noise = torch.randn((d, h, w), generator=gen, dtype=f64, device=dev)
+    spec = torch.fft.rfftn(noise)
+    fz = torch.fft.fftfreq(d, device=dev, dtype=f64)[:, None, None]
+    fy = torch.fft.fftfreq(h, device=dev, dtype=f64)[None, :, None]
+    fx = torch.fft.rfftfreq(w, device=dev, dtype=f64)[None, None, :]
+    k = torch.sqrt(fx * fx + fy * fy + fz * fz)
+    amp = torch.where(k > 0, k.clamp_min(1e-300) ** (-alpha / 2.0), torch.zeros_like(k))
+    noise = torch.fft.irfftn(spec * amp, s=(d, h, w), dim=(0, 1, 2))
+    rms = float(torch.sqrt(torch.mean(noise * noise)))
+    if rms > 0:
+        noise *= noise_rms / rms
+    out += noise
+    del noise, spec
+
+    tdt = torch.float32 if np.dtype(dtype) == np.float32 else torch.float64
+    f = out.to(tdt)
+    fv = f.to(f64)
+    eb = float(rel) * (float(fv.max()) - float(fv.min()))
+    if eb <= 0.0:
+        return f, f.clone(), eb
+    q = torch.round(fv / (2.0 * eb)) * (2.0 * eb)
+    decp = q.to(tdt)
+    bad = (fv - decp.to(f64)).abs() > eb
+    if bool(bad.any()):
+        decp = torch.where(bad, torch.nextafter(decp, f), decp)
+    return f, decp, eb

@@ -170,12 +170,13 @@ extremz_status extremz_correct_batch(extremz_ctx* ctx, const extremz_field* fiel
                                      extremz_report* reports, void* stream);
 
 /*
- * Serving: a request loop on its own thread and CUDA stream.  Requests
- * (device fields) arrive at any time; the loop admits them, in arrival order,
+ * Serving: request loops on their own threads and CUDA streams.  Requests
+ * (device fields) arrive at any time; a loop admits them, in arrival order,
  * while the device footprint of the admitted jobs (workspace plus both
  * fields) stays within the HBM budget and a slot is free, and runs every
  * admitted job together: one launch per kernel serves all jobs at the same
- * phase (continuous batching).  A job's field, labels and edit state stay on
+ * phase (continuous batching).  Two loops ("lanes") split requests by size;
+ * the small-request lane's streams have the higher priority.  A job's field, labels and edit state stay on
  * the device from admission to completion.  Each result is bit-identical to
  * correcting the field alone.
  * No counterpart in the reference (one field per process run, main() of
@@ -183,7 +184,11 @@ extremz_status extremz_correct_batch(extremz_ctx* ctx, const extremz_field* fiel
  */
 typedef struct {
   long long hbm_budget_bytes; /* admission budget; 0 = 120 GB */
-  int max_jobs;               /* jobs in flight per dtype, 1..64; 0 = 64 */
+  long long reserve_bytes;    /* device memory mapped for workspaces at creation
+                                 (0 = on demand); at most the budget */
+  long long split_voxels;     /* requests above this many voxels go to the
+                                 lower-priority lane; 0 = 4 Mi, < 0 = one lane */
+  int max_jobs;               /* jobs in flight per dtype and lane, 1..64; 0 = 64 */
   int reserved[7];
 } extremz_server_config;
 
