@@ -91,6 +91,7 @@ constexpr long long job_bytes_voxels(long long n, long long ksz) {
          + arr_bytes(n, 4) + arr_bytes(n, 1) + 3 * arr_bytes(n, 4)  // mm_next, mstat, dirty, stamps
          + arr_bytes(n, 8) + 2 * arr_bytes(n, 4)                    // claim, taken, taken1
          + 4 * arr_bytes(n, 4)                                      // cand(_next), flagged(1)
+         + arr_bytes(n, 4) + arr_bytes(n, 1)                        // cand_j, mis
          + arr_bytes(4 * ((n + kCpBlock - 1) / kCpBlock), 4)        // CP block counts
          + 4096;
 }
@@ -304,6 +305,8 @@ class BatchEngine {
     J.cand_next = A.take<int>(N);
     J.flagged = A.take<int>(N);
     J.flagged1 = A.take<int>(N);
+    J.cand_j = A.take<int>(N);
+    J.mis = A.take<uint8_t>(N);
     jh.nb = (N + kCpBlock - 1) / kCpBlock;
     jh.bcount = A.take<int>(4ll * jh.nb);
     jh.ntiles = ((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);
@@ -559,8 +562,10 @@ class BatchEngine {
         launch(K_DIRECTION, k_direction<T, true>, st.off[st.n], 256, jobs, st);
         launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, s);
         ctl(s, OP_WN_BEGIN);
-        wrong_neighbours<true>(s);
-        wrong_neighbours<false>(s);
+        launch(K_ROWS, k_saddle_pass<T>, grid_, 256, jobs, s);
+        wn_rounds<true>(s);
+        ctl(s, OP_WN_JOIN_LIST);
+        wn_rounds<false>(s);
         for (int i : sel) {
           slots_[i].manifold_rounds++;
           slots_[i].waiting = true;
@@ -656,13 +661,11 @@ class BatchEngine {
     }
   }
 
-  // Fused row-slot / candidate pass, three grid-wide arbitration rounds and
-  // the per-job completion rounds, for one side.
+  // Three grid-wide arbitration rounds and the per-job completion rounds of
+  // the candidate list being resolved (one side).
   template <bool kSplit>
-  void wrong_neighbours(const Sel& s) {
+  void wn_rounds(const Sel& s) {
     const Job<T>* jobs = jobs_dev_;
-    ctl(s, OP_WN_SIDE_BEGIN);
-    launch(K_ROWS, k_saddle_pass<T, kSplit>, grid_, 256, jobs, s);
     for (int r = 0; r < 3; ++r) {
       ctl(s, OP_WN_ROUND_BEGIN);
       launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, jobs, s);

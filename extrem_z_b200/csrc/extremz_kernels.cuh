@@ -42,8 +42,10 @@ struct Job {
   unsigned long long* claim;  // wrong-neighbour arbitration, (round << 32) | ~saddle
   int* taken;         // wrong-neighbour flag stamps (== call id when flagged)
   int* taken1;
-  int* cand; int* cand_next;  // wrong-neighbour candidate saddles
+  int* cand; int* cand_next;  // wrong-neighbour candidate saddles (side being resolved)
+  int* cand_j;        // join-side candidates, produced with the split side's
   int* flagged; int* flagged1;  // flagged neighbours (split / join)
+  uint8_t* mis;       // per vertex: 1 if dds != ds, 2 if das != as
 
   int* sad2; int* sad1; int* maxima; int* minima;
   int* orow2; int* orow1;  // original rows of kRowStride ints
@@ -78,7 +80,7 @@ struct Sel {
 enum Ctr : int {
   C_MM = 0, C_CMAX, C_CMIN, C_CSAD, C_TOUCHED, C_NFC, C_NFC1, C_CAND, C_CAND_NEXT,
   C_WMC, C_WMC2, C_WSC, C_WMIN, C_WMIN2, C_WSCJ, C_NS2, C_NS1, C_NMAX, C_NMIN,
-  C_ERROR, C_CHANGED, C_DIRTY, C_MM_NEXT,
+  C_ERROR, C_CHANGED, C_DIRTY, C_MM_NEXT, C_CANDJ,
   // Per-job epochs and stamps, advanced by k_ctl so that one launch can serve
   // jobs at different points of their correction.
   C_DEPOCH,    // dirty-list epoch (k_apply)
@@ -520,7 +522,9 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
 // concurrent readers of a label being finalised see either value correctly.
 // Every vertex is resolved (the reference resolves descending labels only next
 // to original 2-saddles, the only places they are read).  Iterations are
-// capped; hitting the cap sets the error word instead of spinning.
+// capped; hitting the cap sets the error word instead of spinning.  On the
+// decompressed field it also writes each vertex's label-mismatch bits
+// (Job::mis) for the saddle pass.
 template <class T, bool kDec>
 __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
                                                const __grid_constant__ Sel sel) {
@@ -551,6 +555,8 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
     if (it == cap_j) atomicOr(err, kErrJump);
     a[v] = u1;
     b[v] = u2;
+    if constexpr (kDec)  // label-mismatch bits for the saddle pass
+      J.mis[v] = (uint8_t)((u1 != J.ds[v]) | (u2 != J.as[v]) << 1);
   }
   }
 }
@@ -900,21 +906,10 @@ __device__ __forceinline__ int wn_candidates(const Job<T>& J, int s, int* ids) {
   return k;
 }
 
-// Fused pass over the original saddles after a manifold round:
-//  * decompressed row slots.  The reference rewrites row i (findAscPaths /
-//    findDescPaths, :1832-2049) in place each round, and its only reader,
-//    get_wrong_index_max / _min (:3113-3171), reads entry 0 and entry k =
-//    (original count - 1), possibly stale when the new row is shorter.  So two
-//    persistent slots per row reproduce it: slot 0 takes the new entry 0 when
-//    the new row is non-empty, slot 1 takes the new entry k when the new row
-//    has more than k entries.  Entry 0 is the row's extreme label in the sort
-//    order and entry count-1 the opposite extreme, found in one pass; any other
-//    entry k is found by ranking the candidates (rare: the rows of both fields
-//    usually have the same length).
-//  * wrong-neighbour seeds: saddles with at least one candidate.
+// Row order of the decompressed rows: "comes first in the row" is descending
+// for ascending rows, ascending else.
 template <class T, bool kSplit>
 __device__ __forceinline__ bool row_first(T v, int m, T bv, int bm) {
-  // "comes first in the row": descending for ascending rows, ascending else.
   return kSplit ? above(v, m, bv, bm) : below(v, m, bv, bm);
 }
 
@@ -951,63 +946,112 @@ __device__ __noinline__ int row_entry_k(const Job<T>& J, int s, int k) {
   return -1;
 }
 
+// One saddle of one side: its decompressed row summary (count, first and
+// last entry in row order) into the row slots, and whether some neighbour on
+// the side has a wrong label.  The loads go out in three batches of
+// independent gathers (neighbour values; labels and mismatch bits of the
+// neighbours on the side; the labels' values), not one dependent chain per
+// neighbour.
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_saddle_pass(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
-  for (int jk = 0; jk < sel.n; ++jk) {
-  const Job<T>& J = jobs[sel.idx[jk]];
-  const int ns = J.ctr[kSplit ? C_NS2 : C_NS1];
-  const int* sad = kSplit ? J.sad2 : J.sad1;
-  const uint8_t* ocnt = kSplit ? J.ocnt2 : J.ocnt1;
-  int* slots = kSplit ? J.drow2 : J.drow1;
-  const int* lab = kSplit ? J.dds : J.das;
-  const int* olab = kSplit ? J.ds : J.as;
+__device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
   const Dims g = J.dim;
   const int WH = g.W * g.H;
-  const int stride = gridDim.x * blockDim.x;
-  for (int base = blockIdx.x * blockDim.x; base < ns; base += stride) {
-    const int i = base + threadIdx.x;
-    bool has = false;
-    int s = 0;
-    if (i < ns) {
-      s = sad[i];
-      int x, y, z;
-      coords(s, g, x, y, z);
-      const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
-      const T sv = J.g[s];
-      int cnt = 0, fm = -1, lm = -1;
-      T fv = T(0), lv = T(0);
+  int x, y, z;
+  coords(s, g, x, y, z);
+  const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
+  const T* __restrict__ gv = J.g;
+  const int* __restrict__ lab = kSplit ? J.dds : J.das;
+  const T sv = __ldg(gv + s);
+  T val[kNumDirs];
 #pragma unroll
-      for (int d = 0; d < kNumDirs; ++d) {
-        if (!(valid >> d & 1)) continue;
-        const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
-        const T rv = J.g[r];
-        if (kSplit ? above(rv, r, sv, s) : below(rv, r, sv, s)) {
-          const int m = lab[r];
-          if (m != olab[r]) has = true;
-          const T v = J.g[m];
-          if (!kSplit || tabs(T(v - sv)) >= J.thr) {
-            if (cnt == 0 || row_first<T, kSplit>(v, m, fv, fm)) { fv = v; fm = m; }
-            if (cnt == 0 || row_first<T, kSplit>(lv, lm, v, m)) { lv = v; lm = m; }
-            ++cnt;
-          }
-        }
-      }
-      const int oc = ocnt[i];
-      if (oc > 0 && cnt > 0) {
-        const int k = oc - 1;
-        slots[2ll * i] = fm;
-        if (cnt > k) {
-          int kth;
-          if (k == cnt - 1) kth = lm;
-          else if (k == 0) kth = fm;
-          else kth = row_entry_k<T, kSplit>(J, s, k);
-          slots[2ll * i + 1] = kth;
-        }
-      }
-    }
-    const int slot = warp_append(J.ctr + C_CAND, has, 0xffffffffu);
-    if (slot >= 0) J.cand[slot] = s;
+  for (int d = 0; d < kNumDirs; ++d)
+    val[d] = (valid >> d & 1) ? __ldg(gv + s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH) : T(0);
+  unsigned side = 0;
+#pragma unroll
+  for (int d = 0; d < kNumDirs; ++d) {
+    const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+    if ((valid >> d & 1) && (kSplit ? above(val[d], r, sv, s) : below(val[d], r, sv, s)))
+      side |= 1u << d;
   }
+  int ml[kNumDirs];
+  int mb = 0;
+#pragma unroll
+  for (int d = 0; d < kNumDirs; ++d) {
+    const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+    ml[d] = (side >> d & 1) ? __ldg(lab + r) : -1;
+    mb |= (side >> d & 1) ? __ldg(J.mis + r) : 0;
+  }
+#pragma unroll
+  for (int d = 0; d < kNumDirs; ++d) val[d] = ml[d] >= 0 ? __ldg(gv + ml[d]) : T(0);
+  T fv = T(0), lv = T(0);
+  int cnt = 0, fm = -1, lm = -1;
+#pragma unroll
+  for (int d = 0; d < kNumDirs; ++d) {
+    const int m = ml[d];
+    const T v = val[d];
+    if (m >= 0 && (!kSplit || tabs(T(v - sv)) >= J.thr)) {
+      if (cnt == 0 || row_first<T, kSplit>(v, m, fv, fm)) { fv = v; fm = m; }
+      if (cnt == 0 || row_first<T, kSplit>(lv, lm, v, m)) { lv = v; lm = m; }
+      ++cnt;
+    }
+  }
+  const int oc = (kSplit ? J.ocnt2 : J.ocnt1)[i];
+  if (oc > 0 && cnt > 0) {
+    int* slots = kSplit ? J.drow2 : J.drow1;
+    const int k = oc - 1;
+    slots[2ll * i] = fm;
+    if (cnt > k) {
+      int kth;
+      if (k == cnt - 1) kth = lm;
+      else if (k == 0) kth = fm;
+      else kth = row_entry_k<T, kSplit>(J, s, k);
+      slots[2ll * i + 1] = kth;
+    }
+  }
+  return (mb >> (kSplit ? 0 : 1)) & 1;
+}
+
+// Fused pass over the original saddles after a manifold round, both sides in
+// one grid (rows [0, ns2) the 2-saddles, then the 1-saddles):
+//  * decompressed row slots.  The reference rewrites row i (findAscPaths /
+//    findDescPaths, :1832-2049) in place each round, and its only reader,
+//    get_wrong_index_max / _min (:3113-3171), reads entry 0 and entry k =
+//    (original count - 1), possibly stale when the new row is shorter.  So two
+//    persistent slots per row reproduce it: slot 0 takes the new entry 0 when
+//    the new row is non-empty, slot 1 takes the new entry k when the new row
+//    has more than k entries.  Entry 0 is the row's extreme label in the sort
+//    order and entry count-1 the opposite extreme, found in one pass; any other
+//    entry k is found by ranking the candidates (rare: the rows of both fields
+//    usually have the same length).
+//  * wrong-neighbour seeds (get_wrong_split_neighbors / _join_ :2400-2513):
+//    saddles with a neighbour on the side whose label differs from the
+//    original's, 2-saddles to cand, 1-saddles to cand_j.
+template <class T>
+__global__ void __launch_bounds__(256) k_saddle_pass(const Job<T>* __restrict__ jobs,
+                                                     const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+    const Job<T>& J = jobs[sel.idx[jk]];
+    const int ns2 = J.ctr[C_NS2], ns1 = J.ctr[C_NS1];
+    const int n = ns2 + ns1;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+      const int e = base + threadIdx.x;
+      bool split = e < ns2, has = false;
+      int s = 0;
+      if (e < n) {
+        if (split) {
+          s = J.sad2[e];
+          has = saddle_row<T, true>(J, e, s);
+        } else {
+          s = J.sad1[e - ns2];
+          has = saddle_row<T, false>(J, e - ns2, s);
+        }
+      }
+      const int slot2 = warp_append(J.ctr + C_CAND, has && split, 0xffffffffu);
+      if (slot2 >= 0) J.cand[slot2] = s;
+      const int slot1 = warp_append(J.ctr + C_CANDJ, has && !split, 0xffffffffu);
+      if (slot1 >= 0) J.cand_j[slot1] = s;
+    }
   }
 }
 
@@ -1395,8 +1439,8 @@ enum CtlOp : int {
   OP_DETECT_BEGIN,            // next re-evaluation epoch, next list and counts to zero
   OP_DETECT_END_DENSE,        // dirty list to zero, next dirty epoch
   OP_DETECT_END,              // swap mismatch lists, then as OP_DETECT_END_DENSE
-  OP_WN_BEGIN,                // next flag stamp, flagged counts to zero
-  OP_WN_SIDE_BEGIN,           // candidate count to zero
+  OP_WN_BEGIN,                // next flag stamp, flagged and candidate counts to zero
+  OP_WN_JOIN_LIST,            // the join side's candidates become the list to resolve
   OP_WN_ROUND_BEGIN,          // next arbitration round, next candidate count to zero
   OP_WN_ROUND_END,            // swap candidate lists
   OP_ZERO_TOUCHED,
@@ -1435,10 +1479,15 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
     case OP_WN_BEGIN:
       c[C_WNSTAMP] += 1;
       c[C_NFC] = c[C_NFC1] = 0;
+      c[C_CAND] = c[C_CANDJ] = 0;
       break;
-    case OP_WN_SIDE_BEGIN:
-      c[C_CAND] = 0;
+    case OP_WN_JOIN_LIST: {
+      int* t = J.cand;
+      J.cand = J.cand_j;
+      J.cand_j = t;
+      c[C_CAND] = c[C_CANDJ];
       break;
+    }
     case OP_WN_ROUND_BEGIN:
       c[C_WNROUND] += 1;
       c[C_CAND_NEXT] = 0;
