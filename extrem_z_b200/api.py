@@ -58,7 +58,7 @@ class Report(ctypes.Structure):
                 ("counters", ctypes.c_int * 11), ("error_bits", ctypes.c_int),
                 ("kernel_launches", ctypes.c_longlong),
                 ("prof_ms", ctypes.c_float * 10), ("prof_launches", ctypes.c_int * 10),
-                ("reserved", ctypes.c_int * 8)]
+                ("manifold_reused", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
 
 class Field(ctypes.Structure):
     _fields_ = [("orig", ctypes.c_void_p), ("decp", ctypes.c_void_p), ("dtype", ctypes.c_int),
@@ -98,13 +98,15 @@ class CorrectionReport:
     kernel_launches: int = 0
     prof_ms: dict = None
     prof_launches: dict = None
+    manifold_reused: int = 0
 
     @staticmethod
     def of(r: Report) -> "CorrectionReport":
         return CorrectionReport(r.status, r.outer_iters, r.cloop_rounds, r.manifold_rounds,
                                 list(r.counters), r.error_bits, int(r.kernel_launches),
                                 dict(zip(KCLASS_NAMES, [float(x) for x in r.prof_ms])),
-                                dict(zip(KCLASS_NAMES, [int(x) for x in r.prof_launches])))
+                                dict(zip(KCLASS_NAMES, [int(x) for x in r.prof_launches])),
+                                int(r.manifold_reused))
 
 
 def library_path() -> str:

@@ -337,6 +337,7 @@ class BatchEngine {
     r->manifold_rounds = j.manifold_rounds;
     std::memcpy(r->counters, j.c, sizeof(j.c));
     r->error_bits = ctr_host_ ? ctr_host_[(size_t)slot * C_COUNT + C_ERROR] : 0;
+    r->manifold_reused = ctr_host_ ? ctr_host_[(size_t)slot * C_COUNT + C_MFREUSED] : 0;
   }
 
   // Releases a finished job's slot and (stream-ordered) its workspace.
@@ -559,6 +560,7 @@ class BatchEngine {
         for (int i : sel) slots_[i].pc = PC_MANIFOLD;
         return EXTREMZ_OK;
       case PC_MANIFOLD:
+        ctl(s, OP_MF_BEGIN);
         launch(K_DIRECTION, k_direction<T, true>, st.off[st.n], 256, jobs, st);
         launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, s);
         ctl(s, OP_WN_BEGIN);

@@ -80,7 +80,12 @@ struct Sel {
 enum Ctr : int {
   C_MM = 0, C_CMAX, C_CMIN, C_CSAD, C_TOUCHED, C_NFC, C_NFC1, C_CAND, C_CAND_NEXT,
   C_WMC, C_WMC2, C_WSC, C_WMIN, C_WMIN2, C_WSCJ, C_NS2, C_NS1, C_NMAX, C_NMIN,
-  C_ERROR, C_CHANGED, C_DIRTY, C_MM_NEXT, C_CANDJ,
+  C_ERROR,
+  C_CHANGED,   // some value changed since the last manifold round began
+  C_DIRTY, C_MM_NEXT, C_CANDJ,
+  C_MFSKIP,    // this manifold round repeats the last one's inputs: kernels skip it
+  C_MFDONE,    // a manifold round has run
+  C_MFREUSED,  // manifold rounds skipped so far
   // Per-job epochs and stamps, advanced by k_ctl so that one launch can serve
   // jobs at different points of their correction.
   C_DEPOCH,    // dirty-list epoch (k_apply)
@@ -480,6 +485,7 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
   __shared__ int hexit[TZ * TY * TX], lexit[TZ * TY * TX];
   int bx, by, bz;
   const Job<T>& J = tile_job(jobs, sel, bx, by, bz);
+  if (kDec && J.ctr[C_MFSKIP]) return;  // same inputs as the last manifold round
   const Dims g = J.dim;
   const int WH = g.W * g.H;
   const T* a = kDec ? J.g : J.f;
@@ -530,6 +536,7 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
                                                const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
+  if (kDec && J.ctr[C_MFSKIP]) continue;
   int* a = kDec ? J.dds : J.ds;
   int* b = kDec ? J.das : J.as;
   int* err = J.ctr + C_ERROR;
@@ -871,8 +878,11 @@ __global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, 
       else gv = fv - J.bound;
     }
     J.g[v] = gv;
-    if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0) && atomicExch(J.dstamp + v, dirty_epoch) != dirty_epoch)
-      J.dirty[atomicAdd(J.ctr + C_DIRTY, 1)] = v;
+    if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0)) {
+      J.ctr[C_CHANGED] = 1;
+      if (atomicExch(J.dstamp + v, dirty_epoch) != dirty_epoch)
+        J.dirty[atomicAdd(J.ctr + C_DIRTY, 1)] = v;
+    }
   }
   }
 }
@@ -1031,6 +1041,7 @@ __global__ void __launch_bounds__(256) k_saddle_pass(const Job<T>* __restrict__ 
                                                      const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
     const Job<T>& J = jobs[sel.idx[jk]];
+    if (J.ctr[C_MFSKIP]) continue;
     const int ns2 = J.ctr[C_NS2], ns1 = J.ctr[C_NS1];
     const int n = ns2 + ns1;
     const int stride = gridDim.x * blockDim.x;
@@ -1071,6 +1082,7 @@ template <class T, bool kSplit>
 __global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
+  if (J.ctr[C_MFSKIP]) continue;
   const unsigned long long round = (unsigned)J.ctr[C_WNROUND];
   const int stamp = J.ctr[C_WNSTAMP];
   const int n = J.ctr[C_CAND];
@@ -1091,6 +1103,7 @@ template <class T, bool kSplit>
 __global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
+  if (J.ctr[C_MFSKIP]) continue;
   const unsigned long long round = (unsigned)J.ctr[C_WNROUND];
   const int stamp = J.ctr[C_WNSTAMP];
   const int n = J.ctr[C_CAND];
@@ -1128,6 +1141,7 @@ template <class T, bool kSplit>
 __global__ void __launch_bounds__(1024) k_wn_resolve(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   if (blockIdx.x >= sel.n) return;
   const Job<T>& J = jobs[sel.idx[blockIdx.x]];
+  if (J.ctr[C_MFSKIP]) return;
   __shared__ int s_next;
   const int stamp = J.ctr[C_WNSTAMP];
   int* taken = kSplit ? J.taken : J.taken1;
@@ -1439,6 +1453,7 @@ enum CtlOp : int {
   OP_DETECT_BEGIN,            // next re-evaluation epoch, next list and counts to zero
   OP_DETECT_END_DENSE,        // dirty list to zero, next dirty epoch
   OP_DETECT_END,              // swap mismatch lists, then as OP_DETECT_END_DENSE
+  OP_MF_BEGIN,                // start of a manifold round: skip it if nothing changed
   OP_WN_BEGIN,                // next flag stamp, flagged and candidate counts to zero
   OP_WN_JOIN_LIST,            // the join side's candidates become the list to resolve
   OP_WN_ROUND_BEGIN,          // next arbitration round, next candidate count to zero
@@ -1476,12 +1491,23 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
       c[C_DIRTY] = 0;
       c[C_DEPOCH] += 1;
       break;
+    case OP_MF_BEGIN:
+      // The round's outputs (labels, row slots, flagged neighbours and their
+      // counts) are functions of the decompressed field alone, so when no
+      // value changed since the last round began they are still in place.
+      c[C_MFSKIP] = c[C_MFDONE] && !c[C_CHANGED];
+      c[C_MFREUSED] += c[C_MFSKIP];
+      c[C_CHANGED] = 0;
+      c[C_MFDONE] = 1;
+      break;
     case OP_WN_BEGIN:
+      if (c[C_MFSKIP]) break;
       c[C_WNSTAMP] += 1;
       c[C_NFC] = c[C_NFC1] = 0;
       c[C_CAND] = c[C_CANDJ] = 0;
       break;
     case OP_WN_JOIN_LIST: {
+      if (c[C_MFSKIP]) break;
       int* t = J.cand;
       J.cand = J.cand_j;
       J.cand_j = t;
@@ -1489,10 +1515,12 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
       break;
     }
     case OP_WN_ROUND_BEGIN:
+      if (c[C_MFSKIP]) break;
       c[C_WNROUND] += 1;
       c[C_CAND_NEXT] = 0;
       break;
     case OP_WN_ROUND_END: {
+      if (c[C_MFSKIP]) break;
       int* t = J.cand;
       J.cand = J.cand_next;
       J.cand_next = t;

@@ -105,7 +105,9 @@ typedef struct {
   long long kernel_launches;          /* kernels this call launched */
   float prof_ms[EXTREMZ_NUM_KCLASS];  /* with EXTREMZ_FLAG_PROFILE */
   int prof_launches[EXTREMZ_NUM_KCLASS];
-  int reserved[8];
+  int manifold_reused;  /* manifold rounds whose inputs were unchanged since the
+                           previous round, so its results were kept */
+  int reserved[7];
 } extremz_report;
 
 typedef struct extremz_ctx_s extremz_ctx;
