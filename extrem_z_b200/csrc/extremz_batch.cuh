@@ -92,6 +92,8 @@ constexpr long long job_bytes_voxels(long long n, long long ksz) {
          + arr_bytes(n, 8) + 2 * arr_bytes(n, 4)                    // claim, taken, taken1
          + 4 * arr_bytes(n, 4)                                      // cand(_next), flagged(1)
          + arr_bytes(n, 4) + arr_bytes(n, 1)                        // cand_j, mis
+         + 2 * arr_bytes(n, 4)                                      // pdd, pda
+         + arr_bytes(n, 1)                                          // tile marks (<= n tiles)
          + arr_bytes(4 * ((n + kCpBlock - 1) / kCpBlock), 4)        // CP block counts
          + 4096;
 }
@@ -307,9 +309,16 @@ class BatchEngine {
     J.flagged1 = A.take<int>(N);
     J.cand_j = A.take<int>(N);
     J.mis = A.take<uint8_t>(N);
+    J.pdd = A.take<int>(N);
+    J.pda = A.take<int>(N);
     jh.nb = (N + kCpBlock - 1) / kCpBlock;
     jh.bcount = A.take<int>(4ll * jh.nb);
     jh.ntiles = ((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);
+    J.tdirty = A.take<uint8_t>(jh.ntiles);
+    if (!J.tdirty) {
+      free_job(jh);
+      return EXTREMZ_OOM;
+    }
     // Tile maps of both fields (TMA when the stride allows).
     CUtensorMap mf, mg;
     const bool tma_ok = (p.flags & EXTREMZ_FLAG_NO_TMA) == 0;
@@ -740,6 +749,8 @@ class BatchEngine {
       launch(K_OTHER, k_fill<int>, grid_, 256, J.first_sj, kInf, (long long)nmin);
       EZ_CHECK(cudaMemsetAsync(J.flag_min2, 0, nmin * 4, st_));
     }
+    // Every tile's pointers are computed in the first manifold round.
+    EZ_CHECK(cudaMemsetAsync(J.tdirty, 1, (size_t)jh.ntiles, st_));
     // Proposal buffer at the sentinel, edit counters at -1 (:5082), stamps 0.
     launch(K_OTHER, k_fill<K>, grid_, 256, J.delta, J.sentinel_key, (long long)N);
     launch(K_OTHER, k_fill<int>, grid_, 256, J.counter, -1, (long long)N);

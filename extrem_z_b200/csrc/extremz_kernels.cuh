@@ -46,6 +46,9 @@ struct Job {
   int* cand_j;        // join-side candidates, produced with the split side's
   int* flagged; int* flagged1;  // flagged neighbours (split / join)
   uint8_t* mis;       // per vertex: 1 if dds != ds, 2 if das != as
+  int* pdd; int* pda; // decompressed steepest pointers, tile-compressed (k_direction)
+  uint8_t* tdirty;    // per tile: a value in the tile or its halo changed since
+                      // the tile's pointers were computed
 
   int* sad2; int* sad1; int* maxima; int* minima;
   int* orow2; int* orow1;  // original rows of kRowStride ints
@@ -122,7 +125,7 @@ struct alignas(128) Tile {
 // Job and tile origin of a tile kernel's block.
 template <class T>
 __device__ __forceinline__ const Job<T>& tile_job(const Job<T>* __restrict__ jobs, const Sel& sel,
-                                                  int& bx, int& by, int& bz) {
+                                                  int& bx, int& by, int& bz, int* tile = nullptr) {
   const int t = blockIdx.x;
   int lo = 0, hi = sel.n - 1;
   while (lo < hi) {
@@ -136,7 +139,20 @@ __device__ __forceinline__ const Job<T>& tile_job(const Job<T>* __restrict__ job
   bx = (lt % ntx) * TX;
   by = ((lt / ntx) % nty) * TY;
   bz = (lt / (ntx * nty)) * TZ;
+  if (tile) *tile = lt;
   return J;
+}
+
+// Marks the tiles whose halo tile contains vertex (x, y, z): those holding
+// one of its 26 neighbours or itself.
+__device__ __forceinline__ void mark_tiles(uint8_t* tdirty, const Dims& g, int x, int y, int z) {
+  const int ntx = (g.W + TX - 1) / TX, nty = (g.H + TY - 1) / TY;
+  const int x0 = max(x - 1, 0) / TX, x1 = min(x + 1, g.W - 1) / TX;
+  const int y0 = max(y - 1, 0) / TY, y1 = min(y + 1, g.H - 1) / TY;
+  const int z0 = max(z - 1, 0) / TZ, z1 = min(z + 1, g.D - 1) / TZ;
+  for (int c = z0; c <= z1; ++c)
+    for (int b = y0; b <= y1; ++b)
+      for (int a = x0; a <= x1; ++a) tdirty[(c * nty + b) * ntx + a] = 1;
 }
 
 // Halo tile: TMA box (one bulk tensor copy, zero fill outside the grid) when
@@ -397,7 +413,10 @@ __global__ void __launch_bounds__(256) k_keep(const Job<T>* __restrict__ jobs,
 // jumping (:1514-1611): each voxel's steepest-ascent (descent) pointer is
 // followed inside the tile in shared memory until it leaves the tile or stops
 // at a root, so the global jump that follows moves a tile per hop.
-// Output: ds/as = first vertex outside the tile on the path, or the root.
+// Output: ds/as (original field) or pdd/pda (decompressed field) = first
+// vertex outside the tile on the path, or the root.  On the decompressed field
+// only tiles marked dirty (a value in the tile or its halo changed) are
+// recomputed; the others keep their pointers, which depend on nothing else.
 // ---------------------------------------------------------------------------
 // Direction components packed two bits per direction (component + 1), so a
 // runtime direction index decodes with a shift and a mask.
@@ -483,14 +502,15 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
   __shared__ uint64_t bar;
   __shared__ int16_t hnext[TZ * TY * TX], lnext[TZ * TY * TX];
   __shared__ int hexit[TZ * TY * TX], lexit[TZ * TY * TX];
-  int bx, by, bz;
-  const Job<T>& J = tile_job(jobs, sel, bx, by, bz);
+  int bx, by, bz, tile;
+  const Job<T>& J = tile_job(jobs, sel, bx, by, bz, &tile);
   if (kDec && J.ctr[C_MFSKIP]) return;  // same inputs as the last manifold round
+  if (kDec && !J.tdirty[tile]) return;  // tile and halo unchanged: pointers stand
   const Dims g = J.dim;
   const int WH = g.W * g.H;
   const T* a = kDec ? J.g : J.f;
-  int* ds = kDec ? J.dds : J.ds;
-  int* as = kDec ? J.das : J.as;
+  int* ds = kDec ? J.pdd : J.ds;
+  int* as = kDec ? J.pda : J.as;
   if (!load_tile<T>(s, &bar, kDec ? J.map_g : J.map_f, kDec ? J.tma_g : J.tma_f, a, g, bx, by,
                     bz)) {
     if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
@@ -520,6 +540,7 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
     ds[v] = follow(hnext, hexit, li, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
     as[v] = follow(lnext, lexit, li, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
   }
+  if (kDec && threadIdx.x == 0) J.tdirty[tile] = 0;
 }
 
 // Global pointer jumping of both label arrays (ComputeDescendingManifold /
@@ -537,8 +558,12 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
   if (kDec && J.ctr[C_MFSKIP]) continue;
-  int* a = kDec ? J.dds : J.ds;
-  int* b = kDec ? J.das : J.as;
+  // Original field: in place on ds / as.  Decompressed field: from the
+  // tile-compressed pointers pdd / pda (kept for the next round) into dds / das.
+  const int* a = kDec ? J.pdd : J.ds;
+  const int* b = kDec ? J.pda : J.as;
+  int* ra = kDec ? J.dds : J.ds;
+  int* rb = kDec ? J.das : J.as;
   int* err = J.ctr + C_ERROR;
   const int N = J.dim.N;
   const int cap_j = J.iter_cap;
@@ -560,8 +585,8 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
       }
     }
     if (it == cap_j) atomicOr(err, kErrJump);
-    a[v] = u1;
-    b[v] = u2;
+    ra[v] = u1;
+    rb[v] = u2;
     if constexpr (kDec)  // label-mismatch bits for the saddle pass
       J.mis[v] = (uint8_t)((u1 != J.ds[v]) | (u2 != J.as[v]) << 1);
   }
@@ -880,6 +905,9 @@ __global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, 
     J.g[v] = gv;
     if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0)) {
       J.ctr[C_CHANGED] = 1;
+      int x, y, z;
+      coords(v, J.dim, x, y, z);
+      mark_tiles(J.tdirty, J.dim, x, y, z);
       if (atomicExch(J.dstamp + v, dirty_epoch) != dirty_epoch)
         J.dirty[atomicAdd(J.ctr + C_DIRTY, 1)] = v;
     }
