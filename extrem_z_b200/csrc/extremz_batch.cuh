@@ -313,6 +313,7 @@ class BatchEngine {
     J.pda = A.take<int>(N);
     jh.nb = (N + kCpBlock - 1) / kCpBlock;
     jh.bcount = A.take<int>(4ll * jh.nb);
+    J.cpoff = jh.bcount;
     jh.ntiles = ((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);
     J.tdirty = A.take<uint8_t>(jh.ntiles);
     if (!J.tdirty) {

@@ -46,6 +46,8 @@ struct Job {
   int* cand_j;        // join-side candidates, produced with the split side's
   int* flagged; int* flagged1;  // flagged neighbours (split / join)
   uint8_t* mis;       // per vertex: 1 if dds != ds, 2 if das != as
+  int* cpoff;         // per list (2-saddles, 1-saddles, maxima, minima) and
+                      // 1024-id block: offset of the block's first entry
   int* pdd; int* pda; // decompressed steepest pointers, tile-compressed (k_direction)
   uint8_t* tdirty;    // per tile: a value in the tile or its halo changed since
                       // the tile's pointers were computed
@@ -1050,7 +1052,9 @@ __device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
 }
 
 // Fused pass over the original saddles after a manifold round, both sides in
-// one grid (rows [0, ns2) the 2-saddles, then the 1-saddles):
+// one grid.  A block takes a chunk of the id space (kPassChunk blocks of 1024
+// ids) and the entries of both saddle lists in it, so that the two sides read
+// the same neighbourhoods together:
 //  * decompressed row slots.  The reference rewrites row i (findAscPaths /
 //    findDescPaths, :1832-2049) in place each round, and its only reader,
 //    get_wrong_index_max / _min (:3113-3171), reads entry 0 and entry k =
@@ -1064,32 +1068,41 @@ __device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
 //  * wrong-neighbour seeds (get_wrong_split_neighbors / _join_ :2400-2513):
 //    saddles with a neighbour on the side whose label differs from the
 //    original's, 2-saddles to cand, 1-saddles to cand_j.
+constexpr int kPassChunk = 4;
+
 template <class T>
-__global__ void __launch_bounds__(256) k_saddle_pass(const Job<T>* __restrict__ jobs,
-                                                     const __grid_constant__ Sel sel) {
+__global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict__ jobs,
+                                                        const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
     const Job<T>& J = jobs[sel.idx[jk]];
     if (J.ctr[C_MFSKIP]) continue;
     const int ns2 = J.ctr[C_NS2], ns1 = J.ctr[C_NS1];
-    const int n = ns2 + ns1;
-    const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
-      const int e = base + threadIdx.x;
-      bool split = e < ns2, has = false;
-      int s = 0;
-      if (e < n) {
-        if (split) {
-          s = J.sad2[e];
-          has = saddle_row<T, true>(J, e, s);
-        } else {
-          s = J.sad1[e - ns2];
-          has = saddle_row<T, false>(J, e - ns2, s);
+    const int nb = (J.dim.N + kCpBlock - 1) / kCpBlock;
+    const int nchunk = (nb + kPassChunk - 1) / kPassChunk;
+    for (int c = blockIdx.x; c < nchunk; c += gridDim.x) {
+      const int b0 = c * kPassChunk, b1 = min(b0 + kPassChunk, nb);
+      const int a2 = J.cpoff[b0], e2 = b1 < nb ? J.cpoff[b1] : ns2;
+      const int a1 = J.cpoff[nb + b0], e1 = b1 < nb ? J.cpoff[nb + b1] : ns1;
+      const int n2 = e2 - a2, n = n2 + (e1 - a1);
+      for (int base = 0; base < n; base += blockDim.x) {  // uniform in the block
+        const int k = base + threadIdx.x;
+        const bool split = k < n2;
+        bool has = false;
+        int s = 0;
+        if (k < n) {
+          if (split) {
+            s = J.sad2[a2 + k];
+            has = saddle_row<T, true>(J, a2 + k, s);
+          } else {
+            s = J.sad1[a1 + k - n2];
+            has = saddle_row<T, false>(J, a1 + k - n2, s);
+          }
         }
+        const int slot2 = warp_append(J.ctr + C_CAND, has && split, 0xffffffffu);
+        if (slot2 >= 0) J.cand[slot2] = s;
+        const int slot1 = warp_append(J.ctr + C_CANDJ, has && !split, 0xffffffffu);
+        if (slot1 >= 0) J.cand_j[slot1] = s;
       }
-      const int slot2 = warp_append(J.ctr + C_CAND, has && split, 0xffffffffu);
-      if (slot2 >= 0) J.cand[slot2] = s;
-      const int slot1 = warp_append(J.ctr + C_CANDJ, has && !split, 0xffffffffu);
-      if (slot1 >= 0) J.cand_j[slot1] = s;
     }
   }
 }
