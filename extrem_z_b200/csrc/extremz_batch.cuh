@@ -573,10 +573,8 @@ class BatchEngine {
         ctl(s, OP_MF_BEGIN);
         launch(K_DIRECTION, k_direction<T, true>, st.off[st.n], 256, jobs, st);
         launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, s);
-        ctl(s, OP_WN_BEGIN);
         launch(K_ROWS, k_saddle_pass<T>, grid_, 256, jobs, s);
-        wn_rounds<true>(s);
-        ctl(s, OP_WN_JOIN_LIST);
+        wn_rounds<true>(s);   // its completion brings in the join side's list
         wn_rounds<false>(s);
         for (int i : sel) {
           slots_[i].manifold_rounds++;
@@ -678,13 +676,11 @@ class BatchEngine {
   template <bool kSplit>
   void wn_rounds(const Sel& s) {
     const Job<T>* jobs = jobs_dev_;
-    for (int r = 0; r < 3; ++r) {
-      ctl(s, OP_WN_ROUND_BEGIN);
-      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, jobs, s);
-      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, jobs, s);
-      ctl(s, OP_WN_ROUND_END);
+    for (int r = 0; r < kWnGridRounds; ++r) {
+      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, jobs, s, r);
+      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, jobs, s, r);
     }
-    launch(K_WRONG_NBR, k_wn_resolve<T, kSplit>, s.n, 1024, jobs, s);
+    launch(K_WRONG_NBR, k_wn_resolve<T, kSplit>, s.n, 1024, jobs_dev_, s);
   }
 
   int setup_b(int slot) {

@@ -1120,17 +1120,21 @@ __global__ void k_row_counts(Job<T> J) {
 }
 
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+__global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel,
+                                                 int r) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
   if (J.ctr[C_MFSKIP]) continue;
-  const unsigned long long round = (unsigned)J.ctr[C_WNROUND];
+  const unsigned long long round = (unsigned)(J.ctr[C_WNROUND] + r + 1);
   const int stamp = J.ctr[C_WNSTAMP];
-  const int n = J.ctr[C_CAND];
+  const int n = J.ctr[C_CAND + (r & 1)];
+  const int* cur = (r & 1) ? J.cand_next : J.cand;
+  // The list this round's commit fills (the one read two rounds ago).
+  if (blockIdx.x == 0 && threadIdx.x == 0) J.ctr[C_CAND + ((r + 1) & 1)] = 0;
   const int* taken = kSplit ? J.taken : J.taken1;
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
-    const int s = J.cand[e];
+    const int s = cur[e];
     int ids[kNumDirs];
     const int k = wn_candidates<T, kSplit>(J, s, ids);
     const unsigned long long vote = (round << 32) | (unsigned)(~s);
@@ -1141,19 +1145,23 @@ __global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs
 }
 
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+__global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel,
+                                                   int r) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
   if (J.ctr[C_MFSKIP]) continue;
-  const unsigned long long round = (unsigned)J.ctr[C_WNROUND];
+  const unsigned long long round = (unsigned)(J.ctr[C_WNROUND] + r + 1);
   const int stamp = J.ctr[C_WNSTAMP];
-  const int n = J.ctr[C_CAND];
+  const int n = J.ctr[C_CAND + (r & 1)];
+  const int* cur = (r & 1) ? J.cand_next : J.cand;
+  int* nxt = (r & 1) ? J.cand : J.cand_next;
+  int* nnext = J.ctr + C_CAND + ((r + 1) & 1);
   int* taken = kSplit ? J.taken : J.taken1;
   int* flagged = kSplit ? J.flagged : J.flagged1;
   int* nflag = J.ctr + (kSplit ? C_NFC : C_NFC1);
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
-    const int s = J.cand[e];
+    const int s = cur[e];
     int ids[kNumDirs];
     const int k = wn_candidates<T, kSplit>(J, s, ids);
     int first = -1;
@@ -1165,11 +1173,17 @@ __global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jo
       taken[first] = stamp;
       flagged[atomicAdd(nflag, 1)] = first;
     } else {
-      J.cand_next[atomicAdd(J.ctr + C_CAND_NEXT, 1)] = s;
+      nxt[atomicAdd(nnext, 1)] = s;
     }
   }
   }
 }
+
+// Grid-wide vote / commit rounds per side before the per-job completion.
+// Round r reads the candidate list of parity r & 1 (cand / cand_next, counts
+// C_CAND / C_CAND_NEXT) and refills the other; its vote number is the job's
+// base round + r + 1.
+constexpr int kWnGridRounds = 3;
 
 // Completion of the arbitration for whatever the grid-wide rounds left
 // unresolved: one block per job runs further vote / commit rounds until no
@@ -1179,19 +1193,21 @@ __global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jo
 // through L2 (__ldcg): other threads of the block update them with atomics
 // and stores between the barriers.
 template <class T, bool kSplit>
-__global__ void __launch_bounds__(1024) k_wn_resolve(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+__global__ void __launch_bounds__(1024) k_wn_resolve(Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   if (blockIdx.x >= sel.n) return;
-  const Job<T>& J = jobs[sel.idx[blockIdx.x]];
+  Job<T>& J = jobs[sel.idx[blockIdx.x]];
   if (J.ctr[C_MFSKIP]) return;
   __shared__ int s_next;
   const int stamp = J.ctr[C_WNSTAMP];
   int* taken = kSplit ? J.taken : J.taken1;
   int* flagged = kSplit ? J.flagged : J.flagged1;
   int* nflag = J.ctr + (kSplit ? C_NFC : C_NFC1);
-  int* cur = J.cand;
-  int* nxt = J.cand_next;
-  int n = J.ctr[C_CAND];
-  unsigned long long round = (unsigned)J.ctr[C_WNROUND];
+  // The grid-wide rounds left their list in parity kWnGridRounds & 1.
+  constexpr int kPar = kWnGridRounds & 1;
+  int* cur = kPar ? J.cand_next : J.cand;
+  int* nxt = kPar ? J.cand : J.cand_next;
+  int n = J.ctr[C_CAND + kPar];
+  unsigned long long round = (unsigned)(J.ctr[C_WNROUND] + kWnGridRounds);
   const int cap = J.iter_cap;
   int it = 0;
   while (n > 0) {
@@ -1238,8 +1254,16 @@ __global__ void __launch_bounds__(1024) k_wn_resolve(const Job<T>* __restrict__ 
     __syncthreads();  // every thread has read s_next before it is reset
   }
   if (threadIdx.x == 0) {
-    J.ctr[C_CAND] = 0;
     J.ctr[C_WNROUND] = (int)round;
+    if (kSplit) {  // the join side's candidates become the list to resolve next
+      int* t = J.cand;
+      J.cand = J.cand_j;
+      J.cand_j = t;
+      J.ctr[C_CAND] = J.ctr[C_CANDJ];
+    } else {
+      J.ctr[C_CAND] = 0;
+    }
+    J.ctr[C_CAND_NEXT] = 0;
   }
 }
 
@@ -1494,11 +1518,8 @@ enum CtlOp : int {
   OP_DETECT_BEGIN,            // next re-evaluation epoch, next list and counts to zero
   OP_DETECT_END_DENSE,        // dirty list to zero, next dirty epoch
   OP_DETECT_END,              // swap mismatch lists, then as OP_DETECT_END_DENSE
-  OP_MF_BEGIN,                // start of a manifold round: skip it if nothing changed
-  OP_WN_BEGIN,                // next flag stamp, flagged and candidate counts to zero
-  OP_WN_JOIN_LIST,            // the join side's candidates become the list to resolve
-  OP_WN_ROUND_BEGIN,          // next arbitration round, next candidate count to zero
-  OP_WN_ROUND_END,            // swap candidate lists
+  OP_MF_BEGIN,                // start of a manifold round: skip it if nothing changed,
+                              // else next flag stamp, flagged / candidate counts to zero
   OP_ZERO_TOUCHED,
   OP_SLOOPS_BEGIN,            // wrong_max counters and touched to zero
   OP_SADDLE_BEGIN,            // wrong_saddle counter and touched to zero
@@ -1540,34 +1561,11 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
       c[C_MFREUSED] += c[C_MFSKIP];
       c[C_CHANGED] = 0;
       c[C_MFDONE] = 1;
-      break;
-    case OP_WN_BEGIN:
       if (c[C_MFSKIP]) break;
-      c[C_WNSTAMP] += 1;
+      c[C_WNSTAMP] += 1;  // next flag stamp; flagged and candidate counts to zero
       c[C_NFC] = c[C_NFC1] = 0;
-      c[C_CAND] = c[C_CANDJ] = 0;
+      c[C_CAND] = c[C_CANDJ] = c[C_CAND_NEXT] = 0;
       break;
-    case OP_WN_JOIN_LIST: {
-      if (c[C_MFSKIP]) break;
-      int* t = J.cand;
-      J.cand = J.cand_j;
-      J.cand_j = t;
-      c[C_CAND] = c[C_CANDJ];
-      break;
-    }
-    case OP_WN_ROUND_BEGIN:
-      if (c[C_MFSKIP]) break;
-      c[C_WNROUND] += 1;
-      c[C_CAND_NEXT] = 0;
-      break;
-    case OP_WN_ROUND_END: {
-      if (c[C_MFSKIP]) break;
-      int* t = J.cand;
-      J.cand = J.cand_next;
-      J.cand_next = t;
-      c[C_CAND] = c[C_CAND_NEXT];
-      break;
-    }
     case OP_ZERO_TOUCHED:
       c[C_TOUCHED] = 0;
       break;
