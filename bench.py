@@ -62,20 +62,24 @@ SERVE_RESERVE_BYTES = 48 << 30
 PARAMS = dict(q=4, edit_type=1, thr=0.0, max_outer=1000, max_cloop_rounds=100000,
               final_join=True)
 
-# Dominant kernel and its algorithmic bytes per voxel per launch:
-# k_direction reads the decompressed value (S bytes) and writes two int32
-# labels (8 bytes) per voxel.
-DOMINANT = "direction"
+# Dominant kernel: the saddle pass (k_saddle_pass, kernel class "rows"), one
+# launch per manifold round.  Algorithmic bytes of a launch that computes:
+# every voxel's decompressed value (S) and both labels (8) plus its label-
+# mismatch byte (1), and per original saddle (2-saddles + 1-saddles) its list
+# entry (4), original row count (1) and two row slots (8).  Launches of
+# rounds whose inputs were unchanged return at once and are not counted.
+DOMINANT = "rows"
+DOMINANT_KERNEL = "k_saddle_pass"
 
 
-def dominant_bytes_per_launch(n: int, s: int) -> int:
-    return n * (s + 8)
+def dominant_bytes_per_launch(n: int, s: int, n_saddles: int) -> int:
+    return n * (s + 9) + n_saddles * 13
 
 
-# DRAM bytes per voxel per k_direction launch from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum over voxels, 256^3 field), by
-# value size (profiles/k_direction_256cube_f64.md); None where not captured.
-MEASURED_TRAFFIC_PER_VOXEL = {8: (134.239488e6 + 96.382976e6) / 256 ** 3, 4: None}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one computing
+# k_saddle_pass launch on the 256^3 fields, from one ncu capture each, by
+# value size (profiles/k_saddle_pass_256cube_f64.md); None where not captured.
+MEASURED_TRAFFIC_256 = {8: None, 4: None}
 
 
 def measured_peaks():
@@ -325,17 +329,20 @@ def run_ours(args, world, rank, local):
     value = world * n * args.steps / (ms_max * 1e-3) / 1e6
     launches = sum(r.kernel_launches for r in reps)
 
-    # Roofline of the dominant kernel from its CUDA-event time in the timed steps.
+    # Roofline of the dominant kernel from its CUDA-event time in the timed
+    # steps, over the launches that computed (reused manifold rounds return).
     dom_ms = sum(r.prof_ms[DOMINANT] for r in reps)
-    dom_n = sum(r.prof_launches[DOMINANT] for r in reps)
+    dom_n = sum(r.manifold_rounds - r.manifold_reused for r in reps)
     peak, peak_kind = measured_peaks()
-    per_launch = dominant_bytes_per_launch(n, s)
+    n_saddles = reps[-1].cp_counts[0] + reps[-1].cp_counts[1]
+    per_launch = dominant_bytes_per_launch(n, s, n_saddles)
     achieved = per_launch * dom_n / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
-    tpv = MEASURED_TRAFFIC_PER_VOXEL.get(s)
-    roofline = {"bound": "hbm", "kernel": "k_direction", "achieved": achieved, "peak": peak,
+    traffic = MEASURED_TRAFFIC_256.get(s) if field.f.shape == (256, 256, 256) else None
+    roofline = {"bound": "hbm", "kernel": DOMINANT_KERNEL, "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": (tpv * n) if tpv else None,
+                "traffic": traffic,
                 "algorithmic_bytes_per_launch": per_launch, "launches": dom_n,
+                "launches_reused": sum(r.manifold_reused for r in reps),
                 "kernel_ms": dom_ms, "share_of_step": dom_ms / ms if ms else None}
 
     # End to end through the host-buffer entry point: H2D of both fields from
@@ -394,8 +401,9 @@ def run_ours(args, world, rank, local):
                 "config": config_of(args, field), "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "forms": forms,
                 "rounds": {"outer_iters": r0.outer_iters, "cloop_rounds": r0.cloop_rounds,
-                           "manifold_rounds": r0.manifold_rounds, "status": r0.status,
-                           "counters": r0.counters}}
+                           "manifold_rounds": r0.manifold_rounds,
+                           "manifold_reused": r0.manifold_reused, "status": r0.status,
+                           "counters": r0.counters, "cp_counts": r0.cp_counts}}
         print(json.dumps(line), flush=True)
     ctx.close()
 

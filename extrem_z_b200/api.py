@@ -58,7 +58,8 @@ class Report(ctypes.Structure):
                 ("counters", ctypes.c_int * 11), ("error_bits", ctypes.c_int),
                 ("kernel_launches", ctypes.c_longlong),
                 ("prof_ms", ctypes.c_float * 10), ("prof_launches", ctypes.c_int * 10),
-                ("manifold_reused", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+                ("manifold_reused", ctypes.c_int), ("cp_counts", ctypes.c_int * 4),
+                ("reserved", ctypes.c_int * 3)]
 
 class Field(ctypes.Structure):
     _fields_ = [("orig", ctypes.c_void_p), ("decp", ctypes.c_void_p), ("dtype", ctypes.c_int),
@@ -99,6 +100,7 @@ class CorrectionReport:
     prof_ms: dict = None
     prof_launches: dict = None
     manifold_reused: int = 0
+    cp_counts: list = None      # original 2-saddles, 1-saddles, maxima, minima
 
     @staticmethod
     def of(r: Report) -> "CorrectionReport":
@@ -106,7 +108,7 @@ class CorrectionReport:
                                 list(r.counters), r.error_bits, int(r.kernel_launches),
                                 dict(zip(KCLASS_NAMES, [float(x) for x in r.prof_ms])),
                                 dict(zip(KCLASS_NAMES, [int(x) for x in r.prof_launches])),
-                                int(r.manifold_reused))
+                                int(r.manifold_reused), list(r.cp_counts))
 
 
 def library_path() -> str:

@@ -348,6 +348,8 @@ class BatchEngine {
     std::memcpy(r->counters, j.c, sizeof(j.c));
     r->error_bits = ctr_host_ ? ctr_host_[(size_t)slot * C_COUNT + C_ERROR] : 0;
     r->manifold_reused = ctr_host_ ? ctr_host_[(size_t)slot * C_COUNT + C_MFREUSED] : 0;
+    for (int k = 0; k < 4; ++k)
+      r->cp_counts[k] = ctr_host_ ? ctr_host_[(size_t)slot * C_COUNT + C_NS2 + k] : 0;
   }
 
   // Releases a finished job's slot and (stream-ordered) its workspace.
@@ -717,9 +719,9 @@ class BatchEngine {
     launch(K_OTHER, k_cp_write, jh.nb, kCpBlock, (const int8_t*)J.otype, N, (const int*)jh.bcount,
            J.sad2, J.sad1, J.maxima, J.minima);
     launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
-    launch(K_ROWS, k_rows<T, true>, grid_, 256, J, J.f, (const int*)J.ds, (const int*)J.sad2,
+    launch(K_SETUP, k_rows<T, true>, grid_, 256, J, J.f, (const int*)J.ds, (const int*)J.sad2,
            (int)C_NS2, J.orow2);
-    launch(K_ROWS, k_rows<T, false>, grid_, 256, J, J.f, (const int*)J.as, (const int*)J.sad1,
+    launch(K_SETUP, k_rows<T, false>, grid_, 256, J, J.f, (const int*)J.as, (const int*)J.sad1,
            (int)C_NS1, J.orow1);
     launch(K_SETUP, k_row_counts<T>, grid_, 256, J);
     // Decompressed row slots start at zero: the reference's rows are fresh

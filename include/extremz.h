@@ -85,10 +85,11 @@ typedef struct {
  * W * sizeof(value) is a multiple of 16 bytes). */
 #define EXTREMZ_FLAG_NO_TMA 2
 
-/* Kernel classes of extremz_report.prof_*: 0 setup classification, 1 fused
- * classification + mismatch detection, 2 steepest directions, 3 pointer
- * jumping, 4 proposals, 5 apply, 6 saddle rows, 7 wrong-neighbour resolution,
- * 8 path walks, 9 everything else. */
+/* Kernel classes of extremz_report.prof_*: 0 setup (classification and rows of
+ * the original field), 1 fused classification + mismatch detection, 2 steepest
+ * directions, 3 pointer jumping, 4 proposals, 5 apply, 6 saddle pass
+ * (decompressed rows and wrong-neighbour seeds), 7 wrong-neighbour
+ * resolution, 8 path walks, 9 everything else. */
 #define EXTREMZ_NUM_KCLASS 10
 
 /* Outcome of one correction. counters[] are the eleven host counters of the
@@ -107,7 +108,8 @@ typedef struct {
   int prof_launches[EXTREMZ_NUM_KCLASS];
   int manifold_reused;  /* manifold rounds whose inputs were unchanged since the
                            previous round, so its results were kept */
-  int reserved[7];
+  int cp_counts[4];     /* original 2-saddles, 1-saddles, maxima, minima */
+  int reserved[3];
 } extremz_report;
 
 typedef struct extremz_ctx_s extremz_ctx;
