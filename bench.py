@@ -79,7 +79,7 @@ def dominant_bytes_per_launch(n: int, s: int, n_saddles: int) -> int:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one computing
 # k_saddle_pass launch on the 256^3 fields, from one ncu capture each, by
 # value size (profiles/k_saddle_pass_256cube_f64.md); None where not captured.
-MEASURED_TRAFFIC_256 = {8: None, 4: None}
+MEASURED_TRAFFIC_256 = {8: 345.6576e6 + 51.80928e6, 4: 258.10304e6 + 33.81376e6}
 
 
 def measured_peaks():
