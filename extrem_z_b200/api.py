@@ -59,7 +59,7 @@ class Report(ctypes.Structure):
                 ("kernel_launches", ctypes.c_longlong),
                 ("prof_ms", ctypes.c_float * 10), ("prof_launches", ctypes.c_int * 10),
                 ("manifold_reused", ctypes.c_int), ("cp_counts", ctypes.c_int * 4),
-                ("reserved", ctypes.c_int * 3)]
+                ("graph_launches", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
 
 class Field(ctypes.Structure):
     _fields_ = [("orig", ctypes.c_void_p), ("decp", ctypes.c_void_p), ("dtype", ctypes.c_int),
@@ -101,6 +101,7 @@ class CorrectionReport:
     prof_launches: dict = None
     manifold_reused: int = 0
     cp_counts: list = None      # original 2-saddles, 1-saddles, maxima, minima
+    graph_launches: int = 0     # ticks launched as one CUDA graph
 
     @staticmethod
     def of(r: Report) -> "CorrectionReport":
@@ -108,7 +109,8 @@ class CorrectionReport:
                                 list(r.counters), r.error_bits, int(r.kernel_launches),
                                 dict(zip(KCLASS_NAMES, [float(x) for x in r.prof_ms])),
                                 dict(zip(KCLASS_NAMES, [int(x) for x in r.prof_launches])),
-                                int(r.manifold_reused), list(r.cp_counts))
+                                int(r.manifold_reused), list(r.cp_counts),
+                                int(r.graph_launches))
 
 
 def library_path() -> str:

@@ -22,6 +22,9 @@
 
 #include <algorithm>
 #include <cstring>
+#include <functional>
+#include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "extremz_kernels.cuh"
@@ -194,6 +197,7 @@ class BatchEngine {
   }
 
   void release_all() {
+    drop_graphs();
     for (auto& j : slots_) free_job(j);
     if (!borrowed_) {
       if (jobs_dev_) cudaFree(jobs_dev_);
@@ -219,6 +223,12 @@ class BatchEngine {
     return n;
   }
   long long launches() const { return launches_; }
+  long long graph_replays() const { return graph_replays_; }
+  long long graph_captures() const { return graph_captures_; }
+  void set_graphs(bool on) {
+    graphs_on_ = on;
+    if (!on) drop_graphs();
+  }
   void set_stream(cudaStream_t st) { st_ = st; }
   // Stream-ordered pool the job workspaces come from (nullptr: the device's
   // default pool).
@@ -372,14 +382,31 @@ class BatchEngine {
   // their ticks overlap on the device.
   int tick_issue() {
     issued_ = false;
-    for (int ph = 0; ph < PC_COUNT; ++ph) {
+    // A tick whose launches repeat an earlier tick's exactly (kernels, launch
+    // shapes and arguments; per-job state is read from device memory) runs as
+    // one CUDA graph: recorded, captured the second time its signature is
+    // seen, replayed from then on.  Ticks that allocate (setup) or time
+    // kernels launch directly.
+    bool graph = graphs_on_ && !profile_;
+    for (const auto& j : slots_)
+      if (j.used && !j.waiting && j.pc == PC_SETUP_B) graph = false;
+    if (graph) {
+      recording_ = true;
+      sig_.clear();
+      pending_.clear();
+    }
+    int rc = EXTREMZ_OK;
+    for (int ph = 0; ph < PC_COUNT && rc == EXTREMZ_OK; ++ph) {
       std::vector<int> sel;
       for (int i = 0; i < kMaxSel; ++i)
         if (slots_[i].used && !slots_[i].waiting && slots_[i].pc == ph) sel.push_back(i);
       if (sel.empty()) continue;
       issued_ = true;
-      EZ_RUN(run_phase(ph, sel));
+      rc = run_phase(ph, sel);
     }
+    recording_ = false;
+    if (rc != EXTREMZ_OK) return rc;
+    if (graph && !pending_.empty()) EZ_RUN(run_recorded());
     if (!issued_) return EXTREMZ_OK;
     EZ_CHECK(cudaGetLastError());
     EZ_CHECK(cudaMemcpyAsync(ctr_host_, ctr_dev_, sizeof(int) * C_COUNT * kMaxSel,
@@ -436,6 +463,20 @@ class BatchEngine {
 
  private:
   cudaStream_t st_;
+  // Tick graphs (see tick_issue).
+  bool graphs_on_ = true, recording_ = false;
+  std::string sig_;
+  std::vector<std::function<void(cudaStream_t)>> pending_;
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long last = 0;
+  };
+  std::unordered_map<std::string, GraphEntry> graphs_;
+  std::unordered_map<std::string, int> seen_;
+  unsigned long long graph_clock_ = 0;
+  long long graph_replays_ = 0, graph_captures_ = 0;
+  static constexpr size_t kMaxGraphs = 256;
+  cudaStream_t cap_ = nullptr;  // capture stream
   cudaMemPool_t pool_mem_ = nullptr;
   bool ready_ = false, borrowed_ = false, issued_ = false;
   int grid_ = 1184;
@@ -466,8 +507,22 @@ class BatchEngine {
     return e;
   }
 
+  template <class A>
+  void sig_append(const A& a) {
+    sig_.append(reinterpret_cast<const char*>(&a), sizeof(A));
+  }
+
   template <class... KArgs, class... Args>
   void launch(int cls, void (*kern)(KArgs...), dim3 grid, dim3 block, Args... args) {
+    if (recording_) {  // tick graphs: record, launch later as one graph
+      sig_append(reinterpret_cast<const void*>(kern));
+      sig_append(grid);
+      sig_append(block);
+      (sig_append(args), ...);
+      pending_.push_back([=](cudaStream_t s) { kern<<<grid, block, 0, s>>>(args...); });
+      ++launches_;
+      return;
+    }
     const bool timed = profile_ && (profile_mask_ == 0 || (profile_mask_ >> cls & 1));
     cudaEvent_t a = nullptr, b = nullptr;
     if (timed) {
@@ -481,6 +536,83 @@ class BatchEngine {
       cudaEventRecord(b, st_);
       recs_.push_back({cls, a, b});
     }
+  }
+
+  void run_direct() {
+    for (auto& go : pending_) go(st_);
+    pending_.clear();
+  }
+
+  void drop_graphs() {
+    for (auto& kv : graphs_)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs_.clear();
+    seen_.clear();
+    if (cap_) cudaStreamDestroy(cap_);
+    cap_ = nullptr;
+  }
+
+  // Launches the recorded tick: replays its graph, captures it on the second
+  // sighting of its signature, or launches directly.
+  int run_recorded() {
+    ++graph_clock_;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st_, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      cudaGetLastError();  // the caller is capturing this stream: launch into it directly
+      run_direct();
+      return EXTREMZ_OK;
+    }
+    auto it = graphs_.find(sig_);
+    if (it != graphs_.end()) {
+      it->second.last = graph_clock_;
+      pending_.clear();
+      ++graph_replays_;
+      EZ_CHECK(cudaGraphLaunch(it->second.exec, st_));
+      return EXTREMZ_OK;
+    }
+    if (seen_.size() > 4 * kMaxGraphs) seen_.clear();
+    if (++seen_[sig_] < 2) {
+      run_direct();
+      return EXTREMZ_OK;
+    }
+    if (graphs_.size() >= kMaxGraphs) {  // evict the least recently used
+      auto old = graphs_.begin();
+      for (auto g = graphs_.begin(); g != graphs_.end(); ++g)
+        if (g->second.last < old->second.last) old = g;
+      cudaGraphExecDestroy(old->second.exec);
+      graphs_.erase(old);
+    }
+    // Captured on a private stream (the caller's may be the legacy stream,
+    // which cannot be captured), launched on the caller's.
+    if (!cap_ && cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      graphs_on_ = false;
+      run_direct();
+      return EXTREMZ_OK;
+    }
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      graphs_on_ = false;
+      run_direct();
+      return EXTREMZ_OK;
+    }
+    for (auto& go : pending_) go(cap_);
+    const cudaError_t ec = cudaStreamEndCapture(cap_, &g);
+    if (ec != cudaSuccess || !g || cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+      cudaGetLastError();
+      if (g) cudaGraphDestroy(g);
+      graphs_on_ = false;  // capture unavailable here: launch directly from now on
+      run_direct();
+      return EXTREMZ_OK;
+    }
+    cudaGraphDestroy(g);
+    pending_.clear();
+    graphs_[sig_] = GraphEntry{exec, graph_clock_};
+    ++graph_captures_;
+    EZ_CHECK(cudaGraphLaunch(exec, st_));
+    return EXTREMZ_OK;
   }
 
   void free_job(JobHost<T>& j) {

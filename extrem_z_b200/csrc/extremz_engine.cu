@@ -238,6 +238,7 @@ static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* table
   const bool prof = (p.flags & EXTREMZ_FLAG_PROFILE) != 0;
   e.set_profile(prof, (p.flags >> EXTREMZ_PROFILE_CLASS_SHIFT) & ((1 << K_NUM) - 1));
   const long long l0 = e.launches();
+  const long long g0 = e.graph_replays() + e.graph_captures();
   int slot = -1;
   EZ_RUN(e.admit(f, g, W, H, D, p, trace, trace_cap, job_store, 0, &slot));
   int rc = EXTREMZ_OK;
@@ -255,6 +256,7 @@ static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* table
   if (rep) {
     e.fill_report(slot, rep);
     rep->kernel_launches = e.launches() - l0;
+    rep->graph_launches = (int)(e.graph_replays() + e.graph_captures() - g0);
     if (prof) e.collect_profile(rep);
     if (rc != EXTREMZ_OK) rep->status = rc;
   }
@@ -331,6 +333,9 @@ static int noalloc_setup(int dev) {
   d.job_store.base = static_cast<char*>(scratch) + kNoAllocEngineBytes;
   d.job_store.cap = kNoAllocScratchBytes - kNoAllocEngineBytes;
   d.job_store.fixed = true;
+  // Graph instantiation may allocate: this mode launches directly.
+  d.e32.set_graphs(false);
+  d.e64.set_graphs(false);
   d.ready = true;
   return EXTREMZ_OK;
 }

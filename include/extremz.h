@@ -109,7 +109,8 @@ typedef struct {
   int manifold_reused;  /* manifold rounds whose inputs were unchanged since the
                            previous round, so its results were kept */
   int cp_counts[4];     /* original 2-saddles, 1-saddles, maxima, minima */
-  int reserved[3];
+  int graph_launches;   /* ticks launched as one CUDA graph (see extremz_correct_device) */
+  int reserved[2];
 } extremz_report;
 
 typedef struct extremz_ctx_s extremz_ctx;
@@ -130,7 +131,10 @@ void extremz_ctx_destroy(extremz_ctx* ctx);
  * width*height*depth values of dtype (x fastest).  stream is a cudaStream_t
  * (NULL = legacy default stream).  trace (host, optional) receives records of
  * four int32 (phase, counter, counter, counter) for debugging; trace_cap is its
- * length in int32.
+ * length in int32.  The launches of one step of the control flow ("tick") that
+ * repeat an earlier step's exactly run as one CUDA graph, captured the second
+ * time they occur and kept in the context (not when the caller's stream is
+ * itself being captured, nor with EXTREMZ_FLAG_PROFILE).
  * Replaces: main() of src/ExtreM_cuda.cu:5508-5997 (the correction proper, with
  * input and decompressed field already resident on the device).
  */
