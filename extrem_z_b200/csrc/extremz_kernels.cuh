@@ -115,6 +115,8 @@ __device__ __forceinline__ T tabs(T v) { return v < T(0) ? -v : v; }
 // warp ballots.
 // ---------------------------------------------------------------------------
 constexpr int TX = 32, TY = 8, TZ = 4;
+// Tile kernels run 256 threads, one per (x, y) column of the tile.
+static_assert(TX * TY == 256, "tile kernels map one thread to each (x, y) column of a tile");
 // Shared tile rows start 4 elements left of the tile origin so that the TMA
 // box origin x = bx - 4 is 16-byte aligned; the tile's x = 0 sits at kXOff.
 constexpr int SX = TX + 8, SY = TY + 2, SZ = TZ + 2, kXOff = 4;
