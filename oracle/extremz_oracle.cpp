@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -273,6 +274,14 @@ struct oracle_report {
   int manifold_rounds;
   long long edited;  // voxels whose value differs from the input decp
   int counters[11];  // final host counters (order of the loop test :5603)
+};
+struct oracle_edit_report {
+  long long index_bytes;  // bytes of the index stream
+  long long edit_bytes;   // bytes of the edit stream
+  long long edited;       // voxels whose value changed
+  long long n_edits;      // entries of the edit stream
+  double psnr_before;     // PSNR of the decompressed field against the original
+  double psnr_after;      // PSNR of the corrected field
 };
 }
 
@@ -995,7 +1004,7 @@ struct Corrector {
 
 template <class T>
 int correct_t(const T* f, T* a, int W, int H, int D, const oracle_params* p, oracle_report* rep,
-              int* trace, int trace_cap) {
+              int* trace, int trace_cap, int32_t* counter_out) {
   Corrector<T> c;
   c.g = {W, H, D, W * H * D};
   c.f = f;
@@ -1022,7 +1031,98 @@ int correct_t(const T* f, T* a, int W, int H, int D, const oracle_params* p, ora
     rep->edited = e;
     std::memcpy(rep->counters, counters, sizeof(counters));
   }
+  if (counter_out) std::memcpy(counter_out, c.counter.data(), sizeof(int) * c.g.N);
   return st;
+}
+
+// ---------------------------------------------------------------------------
+// Edit stream of a correction (cost :4557-4675 for edit_type 0,
+// floating_point_cost :4677-4797 for edit_type 1), without the files and
+// the zstd step.  A voxel is edited when the corrected value differs from the
+// decompressed one (decp_data_copy[i] != decp_data[i]).
+//  * edit_type 0: index stream = every voxel's edit counter (0 when not
+//    edited) packed three bits per voxel by encodeTo3BitBitmap (:4282-4312);
+//    edits = the snapped voxels' (counter == q) lossless edits
+//    -(decp - (input - bound)), in id order.
+//  * edit_type 1: index stream = the edited voxels' ids delta-coded
+//    (get_diff_index :4315-4323) as int32; edits = every edited voxel's
+//    -(decp - (input - bound)), in id order.
+// The reference computes the 3-bit stream but writes the first N bytes of the
+// int32 counter array instead, and writes the first n bytes of the n-entry
+// int32 delta array; the streams here are the ones its code computes, whole.
+// PSNR follows calculateMSE / calculatePSNR (:4263-4280) with the original's
+// value range.
+// ---------------------------------------------------------------------------
+template <class T>
+int encode_t(const T* f, const T* d0, const T* d1, const int32_t* counter, long long N, double bnd,
+             int q, int edit_type, uint8_t* index_out, long long index_cap, T* edits_out,
+             long long edits_cap, oracle_edit_report* r) {
+  const T bound = (T)bnd;
+  std::vector<T> edits;
+  long long edited = 0;
+  std::vector<uint8_t> index;
+  if (edit_type == 0) {
+    std::vector<int> idx((size_t)N, 0);
+    for (long long i = 0; i < N; ++i) {
+      if (d0[i] != d1[i]) {
+        idx[i] = counter[i];
+        if (idx[i] == q) edits.push_back(-(d0[i] - (f[i] - bound)));
+        ++edited;
+      }
+    }
+    // encodeTo3BitBitmap: LSB-first, bits of a value that do not fit the
+    // current byte start the next one.
+    uint8_t cur = 0;
+    int bit = 0;
+    for (int v : idx) {
+      if (v < 0 || v > 7) return -2;  // the reference returns an empty stream
+      cur |= (uint8_t)(v << bit);
+      bit += 3;
+      if (bit >= 8) {
+        index.push_back(cur);
+        bit -= 8;
+        cur = (uint8_t)(v >> (3 - bit));
+      }
+    }
+    if (bit > 0) index.push_back(cur);
+  } else {
+    std::vector<int> ids;
+    for (long long i = 0; i < N; ++i) {
+      if (d0[i] != d1[i]) {
+        ids.push_back((int)i);
+        edits.push_back(-(d0[i] - (f[i] - bound)));
+        ++edited;
+      }
+    }
+    std::vector<int> diffs;
+    if (!ids.empty()) diffs.push_back(ids[0]);
+    for (size_t k = 1; k < ids.size(); ++k) diffs.push_back(ids[k] - ids[k - 1]);
+    index.resize(diffs.size() * sizeof(int));
+    if (!diffs.empty()) std::memcpy(index.data(), diffs.data(), index.size());
+  }
+  if ((long long)index.size() > index_cap || (long long)(edits.size() * sizeof(T)) > edits_cap)
+    return -3;
+  if (!index.empty()) std::memcpy(index_out, index.data(), index.size());
+  if (!edits.empty()) std::memcpy(edits_out, edits.data(), edits.size() * sizeof(T));
+  double lo = (double)f[0], hi = (double)f[0], s0 = 0.0, s1 = 0.0;
+  for (long long i = 0; i < N; ++i) {
+    lo = std::min(lo, (double)f[i]);
+    hi = std::max(hi, (double)f[i]);
+    s0 += std::pow((double)f[i] - (double)d0[i], 2);
+    s1 += std::pow((double)f[i] - (double)d1[i], 2);
+  }
+  auto psnr = [&](double sse) {
+    const double mse = sse / (double)N;
+    if (mse == 0) return std::numeric_limits<double>::infinity();
+    return -20.0 * std::log10(std::sqrt(mse) / (hi - lo));
+  };
+  r->index_bytes = (long long)index.size();
+  r->edit_bytes = (long long)(edits.size() * sizeof(T));
+  r->edited = edited;
+  r->n_edits = (long long)edits.size();
+  r->psnr_before = psnr(s0);
+  r->psnr_after = psnr(s1);
+  return 0;
 }
 
 bool dims_ok(int W, int H, int D) {
@@ -1072,13 +1172,32 @@ int oracle_roots(const void* f, int dtype, int W, int H, int D, int32_t* ds, int
   return 0;
 }
 
-// Full correction, in place on decp.  trace (optional) receives 4-int records.
+// Full correction, in place on decp.  trace (optional) receives 4-int records;
+// counter_out (optional, N int32) the final edit counters (delta_counter).
 int oracle_correct(const void* f, void* decp, int dtype, int W, int H, int D,
-                   const oracle_params* p, oracle_report* rep, int32_t* trace, int trace_cap) {
+                   const oracle_params* p, oracle_report* rep, int32_t* trace, int trace_cap,
+                   int32_t* counter_out) {
   if (!dims_ok(W, H, D) || !p || p->q <= 0) return -1;
   if (dtype == 0)
-    return correct_t((const float*)f, (float*)decp, W, H, D, p, rep, trace, trace_cap);
-  return correct_t((const double*)f, (double*)decp, W, H, D, p, rep, trace, trace_cap);
+    return correct_t((const float*)f, (float*)decp, W, H, D, p, rep, trace, trace_cap,
+                     counter_out);
+  return correct_t((const double*)f, (double*)decp, W, H, D, p, rep, trace, trace_cap,
+                   counter_out);
+}
+
+// Edit stream of a correction (see encode_t).  Returns 0, -1 on bad
+// arguments, -2 for a counter outside 0..7 (edit_type 0), -3 when a stream
+// exceeds its buffer.
+int oracle_encode(const void* f, const void* decp0, const void* fixed, const int32_t* counter,
+                  int dtype, long long n, double bound, int q, int edit_type, uint8_t* index_out,
+                  long long index_cap, void* edits_out, long long edits_cap,
+                  oracle_edit_report* rep) {
+  if (!f || !decp0 || !fixed || n <= 0 || !rep || (edit_type == 0 && !counter)) return -1;
+  if (dtype == 0)
+    return encode_t((const float*)f, (const float*)decp0, (const float*)fixed, counter, n, bound,
+                    q, edit_type, index_out, index_cap, (float*)edits_out, edits_cap, rep);
+  return encode_t((const double*)f, (const double*)decp0, (const double*)fixed, counter, n, bound,
+                  q, edit_type, index_out, index_cap, (double*)edits_out, edits_cap, rep);
 }
 
 }  // extern "C"

@@ -34,6 +34,12 @@ class Report(ctypes.Structure):
                 ("edited", ctypes.c_longlong), ("counters", ctypes.c_int * 11)]
 
 
+class EditReport(ctypes.Structure):
+    _fields_ = [("index_bytes", ctypes.c_longlong), ("edit_bytes", ctypes.c_longlong),
+                ("edited", ctypes.c_longlong), ("n_edits", ctypes.c_longlong),
+                ("psnr_before", ctypes.c_double), ("psnr_after", ctypes.c_double)]
+
+
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the Makefile next to this file."""
     src = os.path.join(_HERE, "extremz_oracle.cpp")
@@ -56,7 +62,10 @@ def lib():
         L.oracle_classify.argtypes = [vp, i32, i32, i32, i32, vp, vp]
         L.oracle_roots.argtypes = [vp, i32, i32, i32, i32, vp, vp]
         L.oracle_correct.argtypes = [vp, vp, i32, i32, i32, i32,
-                                     ctypes.POINTER(Params), ctypes.POINTER(Report), vp, i32]
+                                     ctypes.POINTER(Params), ctypes.POINTER(Report), vp, i32, vp]
+        L.oracle_encode.argtypes = [vp, vp, vp, vp, i32, ctypes.c_longlong, ctypes.c_double,
+                                    i32, i32, vp, ctypes.c_longlong, vp, ctypes.c_longlong,
+                                    ctypes.POINTER(EditReport)]
         _lib = L
     return _lib
 
@@ -110,8 +119,12 @@ def roots(f: np.ndarray):
 
 def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, q: int = 4,
             edit_type: int = 1, max_outer: int = 500, max_cloop_rounds: int = 100000,
-            final_join: bool = True, preserve_join: bool = False, trace_cap: int = 0):
-    """Run the oracle correction; returns (corrected copy, report dict, trace)."""
+            final_join: bool = True, preserve_join: bool = False, trace_cap: int = 0,
+            counter_out: np.ndarray = None):
+    """Run the oracle correction; returns (corrected copy, report dict, trace).
+
+    counter_out (optional, int32 of the field's size) receives the final edit
+    counters (the reference's delta_counter)."""
     f = np.ascontiguousarray(f)
     out = np.ascontiguousarray(decp).copy()
     assert f.dtype == out.dtype and f.shape == out.shape
@@ -121,7 +134,8 @@ def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, 
     r = Report()
     tr = np.zeros(max(trace_cap, 1) * 4, dtype=np.int32)
     rc = lib().oracle_correct(f.ctypes.data, out.ctypes.data, _dtype_code(f), w, h, d,
-                              ctypes.byref(p), ctypes.byref(r), tr.ctypes.data, trace_cap * 4)
+                              ctypes.byref(p), ctypes.byref(r), tr.ctypes.data, trace_cap * 4,
+                              counter_out.ctypes.data if counter_out is not None else None)
     if rc < 0:
         raise ValueError("oracle rejected the arguments")
     rep = dict(status=r.status, outer_iters=r.outer_iters, cloop_rounds=r.cloop_rounds,
@@ -131,3 +145,26 @@ def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, 
     if trace_cap:
         trace = trace[trace[:, 0] != 0]
     return out, rep, trace
+
+
+def encode(f: np.ndarray, decp0: np.ndarray, fixed: np.ndarray, counter, bound: float, *,
+           q: int = 4, edit_type: int = 1):
+    """Edit stream of a correction: (index stream bytes, edits array, report dict)."""
+    f = np.ascontiguousarray(f)
+    d0 = np.ascontiguousarray(decp0)
+    d1 = np.ascontiguousarray(fixed)
+    assert f.dtype == d0.dtype == d1.dtype and f.shape == d0.shape == d1.shape
+    n = f.size
+    cnt = None if counter is None else np.ascontiguousarray(counter, dtype=np.int32)
+    index = np.zeros(max(4 * n, (3 * n + 7) // 8), dtype=np.uint8)
+    edits = np.zeros(n, dtype=f.dtype)
+    r = EditReport()
+    rc = lib().oracle_encode(f.ctypes.data, d0.ctypes.data, d1.ctypes.data,
+                             cnt.ctypes.data if cnt is not None else None, _dtype_code(f), n,
+                             float(bound), int(q), int(edit_type), index.ctypes.data, index.size,
+                             edits.ctypes.data, edits.nbytes, ctypes.byref(r))
+    if rc != 0:
+        raise ValueError(f"oracle_encode returned {rc}")
+    rep = dict(index_bytes=r.index_bytes, edit_bytes=r.edit_bytes, edited=r.edited,
+               n_edits=r.n_edits, psnr_before=r.psnr_before, psnr_after=r.psnr_after)
+    return index[:r.index_bytes].copy(), edits[:r.n_edits].copy(), rep

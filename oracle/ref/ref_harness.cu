@@ -43,7 +43,33 @@ static cudaError_t extremz_guarded_malloc(void** p, size_t n) {
 #undef main
 #undef cudaMalloc
 
+// Host-only modes that run two helpers of the reference's edit-stream
+// encoder on int32 input, for the oracle's golden vectors:
+//   ref_gpu --encode3 <in.i32> <out.u8>   encodeTo3BitBitmap (:4282-4312)
+//   ref_gpu --diff    <in.i32> <out.i32>  get_diff_index<int> (:4315-4323)
+static int helper_mode(int argc, char** argv) {
+  FILE* fi = std::fopen(argv[2], "rb");
+  if (!fi) return 6;
+  std::vector<int> in;
+  int v;
+  while (std::fread(&v, sizeof(int), 1, fi) == 1) in.push_back(v);
+  std::fclose(fi);
+  FILE* fo = std::fopen(argv[3], "wb");
+  if (!fo) return 6;
+  if (std::string(argv[1]) == "--encode3") {
+    std::vector<uint8_t> out = encodeTo3BitBitmap(in);
+    if (!out.empty()) std::fwrite(out.data(), 1, out.size(), fo);
+  } else {
+    std::vector<int> out = get_diff_index<int>(in);
+    std::fwrite(out.data(), sizeof(int), out.size(), fo);
+  }
+  std::fclose(fo);
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 4 && (std::string(argv[1]) == "--encode3" || std::string(argv[1]) == "--diff"))
+    return helper_mode(argc, argv);
   if (argc != 10) {
     std::fprintf(stderr, "usage: %s orig W H D er sim q edit_type out\n", argv[0]);
     return 2;

@@ -6,6 +6,11 @@
       python tests/golden/make_golden.py --reference /path/to/ExtreM_z
 * oracle_cases.npz -- small seeded inputs and the oracle's corrected outputs,
   reports and traces, pinning the oracle's behaviour across changes.
+* encode_cases.npz -- int32 inputs and the outputs of the reference's own
+  encodeTo3BitBitmap and get_diff_index (src/ExtreM_cuda.cu:4282-4323), run
+  through the reference harness binary oracle/_ref/ref_gpu (built from the
+  reference's source by oracle/ref/build_ref.sh; these modes use no GPU):
+      python tests/golden/make_golden.py --encode
 """
 
 import argparse
@@ -61,10 +66,38 @@ def oracle_cases():
     return out
 
 
+def encode_cases():
+    import subprocess
+    import tempfile
+    binary = os.path.join(ROOT, "oracle", "_ref", "ref_gpu")
+    rng = np.random.default_rng(2024)
+    out = {}
+    lengths = [1, 2, 3, 7, 8, 9, 16, 24, 100, 1001]
+    with tempfile.TemporaryDirectory() as tmp:
+        src, dst = os.path.join(tmp, "in.i32"), os.path.join(tmp, "out.bin")
+        for n in lengths:
+            v = rng.integers(0, 8, size=n).astype("<i4")
+            v.tofile(src)
+            subprocess.run([binary, "--encode3", src, dst], check=True)
+            out[f"pack3/{n}/in"] = v
+            out[f"pack3/{n}/out"] = np.fromfile(dst, dtype=np.uint8)
+            ids = np.sort(rng.choice(10 * n + 5, size=n, replace=False)).astype("<i4")
+            ids.tofile(src)
+            subprocess.run([binary, "--diff", src, dst], check=True)
+            out[f"diff/{n}/in"] = ids
+            out[f"diff/{n}/out"] = np.fromfile(dst, dtype="<i4")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=None, help="reference checkout (for LUT.bin)")
+    ap.add_argument("--encode", action="store_true",
+                    help="only regenerate encode_cases.npz from the reference harness binary")
     args = ap.parse_args()
+    if args.encode:
+        np.savez_compressed(os.path.join(HERE, "encode_cases.npz"), **encode_cases())
+        return
     if args.reference:
         with open(os.path.join(HERE, "lut_digest.json"), "w") as fh:
             json.dump(lut_digest(args.reference), fh, indent=1)
