@@ -30,7 +30,8 @@ F32, F64 = 0, 1
 # Every entry point declared in include/extremz.h.
 EXPORTS = ("extremz_version", "extremz_default_params", "extremz_ctx_create",
            "extremz_ctx_destroy", "extremz_correct_device", "extremz_correct_host",
-           "extremz_correct_batch", "extremz_server_create", "extremz_server_destroy",
+           "extremz_correct_batch", "extremz_correct_encode", "extremz_edit_stream_caps",
+           "extremz_zstd_size", "extremz_server_create", "extremz_server_destroy",
            "extremz_server_submit", "extremz_server_poll", "extremz_server_wait",
            "extremz_server_get_stats", "extremz_job_footprint",
            "extremz_correct_device_noalloc", "extremz_noalloc_max_voxels",
@@ -60,6 +61,15 @@ class Report(ctypes.Structure):
                 ("prof_ms", ctypes.c_float * 10), ("prof_launches", ctypes.c_int * 10),
                 ("manifold_reused", ctypes.c_int), ("cp_counts", ctypes.c_int * 4),
                 ("graph_launches", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
+
+class EditStream(ctypes.Structure):
+    _fields_ = [("index", ctypes.c_void_p), ("index_cap", ctypes.c_longlong),
+                ("edits", ctypes.c_void_p), ("edits_cap", ctypes.c_longlong),
+                ("index_bytes", ctypes.c_longlong), ("edit_bytes", ctypes.c_longlong),
+                ("edited", ctypes.c_longlong), ("n_edits", ctypes.c_longlong),
+                ("psnr_before", ctypes.c_double), ("psnr_after", ctypes.c_double),
+                ("reserved", ctypes.c_int * 4)]
+
 
 class Field(ctypes.Structure):
     _fields_ = [("orig", ctypes.c_void_p), ("decp", ctypes.c_void_p), ("dtype", ctypes.c_int),
@@ -146,6 +156,16 @@ def load(build_if_missing: bool = True):
         L.extremz_correct_host.argtypes = [vp, vp, vp, i32, i32, i32, i32,
                                            ctypes.POINTER(Params), ctypes.POINTER(Report), vp]
         L.extremz_correct_host.restype = i32
+        L.extremz_correct_encode.argtypes = [vp, vp, vp, i32, i32, i32, i32,
+                                             ctypes.POINTER(Params), ctypes.POINTER(Report), vp,
+                                             ctypes.POINTER(EditStream)]
+        L.extremz_correct_encode.restype = i32
+        L.extremz_edit_stream_caps.argtypes = [i32, i32, i32, i32, i32,
+                                               ctypes.POINTER(ctypes.c_longlong),
+                                               ctypes.POINTER(ctypes.c_longlong)]
+        L.extremz_edit_stream_caps.restype = i32
+        L.extremz_zstd_size.argtypes = [vp, ctypes.c_longlong, i32]
+        L.extremz_zstd_size.restype = ctypes.c_longlong
         L.extremz_correct_batch.argtypes = [vp, ctypes.POINTER(Field), i32,
                                             ctypes.POINTER(Report), vp]
         L.extremz_correct_batch.restype = i32
@@ -260,6 +280,46 @@ class Context:
             trace = tr.reshape(-1, 4)
             trace = trace[trace[:, 0] != 0]
         return CorrectionReport.of(r), trace
+
+    # -- edit streams -------------------------------------------------------
+    def correct_encode(self, f, decp, bound: float, *, stream=None, zstd_level: int = 3, **kw):
+        """Correct the CUDA tensor ``decp`` in place and return its edit stream.
+
+        Returns (CorrectionReport, dict) with the index stream (numpy uint8),
+        the edits (numpy, the field's dtype), the edited-voxel and entry
+        counts, PSNR before and after, and the zstd sizes of both streams
+        (-1 without libzstd).  See extremz_correct_encode.
+        """
+        import torch
+        assert f.is_cuda and decp.is_cuda and f.dtype == decp.dtype and f.shape == decp.shape
+        assert f.is_contiguous() and decp.is_contiguous()
+        dt = {torch.float32: F32, torch.float64: F64}[f.dtype]
+        w, h, d = _whd(tuple(f.shape))
+        p = make_params(bound, **kw)
+        L = load()
+        icap, ecap = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(L.extremz_edit_stream_caps(dt, w, h, d, p.edit_type, ctypes.byref(icap),
+                                          ctypes.byref(ecap)), allow_cap=False)
+        ibuf = torch.empty(max(1, icap.value), dtype=torch.uint8, device=f.device)
+        ebuf = torch.empty(max(1, ecap.value), dtype=torch.uint8, device=f.device)
+        es = EditStream()
+        es.index, es.index_cap = ibuf.data_ptr(), icap.value
+        es.edits, es.edits_cap = ebuf.data_ptr(), ecap.value
+        if stream is None:
+            stream = torch.cuda.current_stream(f.device).cuda_stream
+        r = Report()
+        st = L.extremz_correct_encode(self._h, f.data_ptr(), decp.data_ptr(), dt, w, h, d,
+                                      ctypes.byref(p), ctypes.byref(r), stream, ctypes.byref(es))
+        _check(st)
+        torch.cuda.synchronize(f.device)
+        index = ibuf[:es.index_bytes].cpu().numpy()
+        npdt = np.float32 if dt == F32 else np.float64
+        edits = ebuf[:es.edit_bytes].cpu().numpy().view(npdt)
+        out = dict(index=index, edits=edits, edited=int(es.edited), n_edits=int(es.n_edits),
+                   index_bytes=int(es.index_bytes), edit_bytes=int(es.edit_bytes),
+                   psnr_before=float(es.psnr_before), psnr_after=float(es.psnr_after),
+                   index_zstd=zstd_size(index, zstd_level), edits_zstd=zstd_size(edits, zstd_level))
+        return CorrectionReport.of(r), out
 
     # -- batches ------------------------------------------------------------
     def correct_batch(self, items, *, stream=None):
@@ -393,6 +453,12 @@ class Server:
         s = ServerStats()
         load().extremz_server_get_stats(self._h, ctypes.byref(s))
         return {k: int(getattr(s, k)) for k, _ in ServerStats._fields_ if k != "reserved"}
+
+
+def zstd_size(buf: np.ndarray, level: int = 3) -> int:
+    """zstd-compressed size of a host array (-1 when libzstd is absent)."""
+    b = np.ascontiguousarray(buf)
+    return int(load().extremz_zstd_size(b.ctypes.data, b.nbytes, int(level)))
 
 
 def job_footprint(voxels_or_shape, dtype) -> int:

@@ -13,7 +13,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libextremz.so")
 
 SOURCES = ["extremz_engine.cu"]
-HEADERS = ["extremz_common.cuh", "extremz_kernels.cuh", "extremz_batch.cuh", "extremz_lut.h"]
+HEADERS = ["extremz_common.cuh", "extremz_kernels.cuh", "extremz_batch.cuh", "extremz_encode.cuh",
+           "extremz_lut.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

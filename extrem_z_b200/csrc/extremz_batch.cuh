@@ -21,12 +21,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <functional>
 #include <string>
 #include <unordered_map>
 #include <vector>
 
+#include "extremz_encode.cuh"
 #include "extremz_kernels.cuh"
 
 namespace extremz {
@@ -86,6 +88,10 @@ __global__ void k_checksum(const T* __restrict__ a, int N, unsigned long long* o
 // known (ns2 2-saddles, ns1 1-saddles, nmax maxima, nmin minima).  ksz is the
 // size of an order-preserving key (4 or 8).
 constexpr long long arr_bytes(long long count, long long sz) { return (count * sz + 255) & ~255ll; }
+
+// Internal job flag (outside the public EXTREMZ_FLAG_* bits): keep a copy of
+// the incoming decompressed field for the edit stream.
+constexpr int kFlagKeepInput = 1 << 30;
 
 constexpr long long job_bytes_voxels(long long n, long long ksz) {
   return arr_bytes(n, 1) + arr_bytes(n, 2)                          // otype, olm
@@ -270,8 +276,11 @@ class BatchEngine {
     J.tb = tb_;
     J.ctr = ctr_dev_ + (size_t)slot * C_COUNT;
     const int N = J.dim.N;
-    // Borrowed storage holds both parts; an allocation holds the first.
-    const long long need = storage ? job_bytes<T>(N) : job_bytes_voxels(N, sizeof(K));
+    // Borrowed storage holds both parts; an allocation holds the first (and a
+    // copy of the incoming field when an edit stream will be encoded).
+    const bool keep_input = (p.flags & kFlagKeepInput) != 0;
+    const long long need = (storage ? job_bytes<T>(N) : job_bytes_voxels(N, sizeof(K))) +
+                           (keep_input ? arr_bytes(N, sizeof(T)) : 0);
     if (storage) {
       jh.arena = *storage;
       jh.arena.used = 0;
@@ -326,10 +335,13 @@ class BatchEngine {
     J.cpoff = jh.bcount;
     jh.ntiles = ((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);
     J.tdirty = A.take<uint8_t>(jh.ntiles);
-    if (!J.tdirty) {
+    J.g0 = keep_input ? A.take<T>(N) : nullptr;
+    if (!J.tdirty || (keep_input && !J.g0)) {
       free_job(jh);
       return EXTREMZ_OOM;
     }
+    if (keep_input)
+      EZ_CHECK(cudaMemcpyAsync(J.g0, g, (size_t)N * sizeof(T), cudaMemcpyDeviceToDevice, st_));
     // Tile maps of both fields (TMA when the stride allows).
     CUtensorMap mf, mg;
     const bool tma_ok = (p.flags & EXTREMZ_FLAG_NO_TMA) == 0;
@@ -360,6 +372,66 @@ class BatchEngine {
     r->manifold_reused = ctr_host_ ? ctr_host_[(size_t)slot * C_COUNT + C_MFREUSED] : 0;
     for (int k = 0; k < 4; ++k)
       r->cp_counts[k] = ctr_host_ ? ctr_host_[(size_t)slot * C_COUNT + C_NS2 + k] : 0;
+  }
+
+  // Edit stream of a finished job admitted with kFlagKeepInput, into the
+  // caller's device buffers es->index / es->edits (see extremz_encode.cuh).
+  // Synchronises the stream.  BAD_ARG when a buffer is too small (the sizes
+  // needed are filled in) or a counter does not fit three bits.
+  int encode(int slot, extremz_edit_stream* es) {
+    JobHost<T>& jh = slots_[slot];
+    const Job<T>& J = jh.J;
+    if (!J.g0 || !es) return EXTREMZ_BAD_ARG;
+    const int N = J.dim.N, nb = jh.nb, et = jh.p.edit_type, q = jh.p.q;
+    if (et == 0 && q > 7) return EXTREMZ_BAD_ARG;  // counters up to q: three bits
+    unsigned long long* acc = jh.checksum;         // 8 words of scratch
+    unsigned long long init[8] = {0, 0, KeyOf<double>::enc((double)INFINITY),
+                                  KeyOf<double>::enc(-(double)INFINITY), 0, 0, 0, 0};
+    EZ_CHECK(cudaMemcpyAsync(acc, init, sizeof(init), cudaMemcpyHostToDevice, st_));
+    int* bc = jh.bcount;  // 4 x nb ints, free once the correction is over
+    launch(K_OTHER, k_enc_count<T>, nb, kCpBlock, (const T*)J.g0, (const T*)J.g,
+           (const int*)J.counter, N, q, et, bc);
+    launch(K_OTHER, k_scan_lists, 1, 1024, bc, nb, 2, reinterpret_cast<int*>(acc + 4));
+    launch(K_OTHER, k_enc_stats<T>, grid_, 256, J.f, (const T*)J.g0, (const T*)J.g, N, acc);
+    unsigned long long h[8];
+    EZ_CHECK(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, st_));
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    int tot[2];
+    std::memcpy(tot, &h[4], sizeof(tot));
+    const long long index_bytes = et == 0 ? (3ll * N + 7) / 8 : 4ll * tot[0];
+    const long long edit_bytes = (long long)tot[1] * (long long)sizeof(T);
+    es->edited = tot[0];
+    es->n_edits = tot[1];
+    es->index_bytes = index_bytes;
+    es->edit_bytes = edit_bytes;
+    double s0, s1;
+    std::memcpy(&s0, &h[0], 8);
+    std::memcpy(&s1, &h[1], 8);
+    const double range = KeyOf<double>::dec(h[3]) - KeyOf<double>::dec(h[2]);
+    auto psnr = [&](double sse) {
+      const double mse = sse / (double)N;
+      return mse == 0 ? (double)INFINITY : -20.0 * std::log10(std::sqrt(mse) / range);
+    };
+    es->psnr_before = psnr(s0);
+    es->psnr_after = psnr(s1);
+    if (index_bytes > es->index_cap || edit_bytes > es->edits_cap ||
+        (index_bytes && !es->index) || (edit_bytes && !es->edits))
+      return EXTREMZ_BAD_ARG;
+    launch(K_OTHER, k_enc_write<T>, nb, kCpBlock, J.f, (const T*)J.g0, (const T*)J.g,
+           (const int*)J.counter, N, J.bound, q, et, (const int*)bc, J.touched,
+           static_cast<T*>(es->edits));
+    if (et == 1) {
+      launch(K_OTHER, k_enc_diff, grid_, 256, (const int*)J.touched, tot[0],
+             static_cast<int*>(es->index));
+    } else {
+      launch(K_OTHER, k_enc_pack3<T>, grid_, 256, (const T*)J.g0, (const T*)J.g,
+             (const int*)J.counter, (long long)N, static_cast<uint8_t*>(es->index), index_bytes,
+             acc + 5);
+    }
+    unsigned long long bad = 0;
+    EZ_CHECK(cudaMemcpyAsync(&bad, acc + 5, 8, cudaMemcpyDeviceToHost, st_));
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    return bad ? EXTREMZ_BAD_ARG : EXTREMZ_OK;
   }
 
   // Releases a finished job's slot and (stream-ordered) its workspace.
@@ -670,7 +742,7 @@ class BatchEngine {
         for (int i : sel) {
           JobHost<T>& j = slots_[i];
           launch(K_OTHER, k_cp_count, j.nb, kCpBlock, (const int8_t*)j.J.otype, j.J.dim.N, j.bcount);
-          launch(K_OTHER, k_cp_scan, 1, 1024, j.bcount, j.nb, j.J.ctr);
+          launch(K_OTHER, k_scan_lists, 1, 1024, j.bcount, j.nb, 4, j.J.ctr + C_NS2);
           j.waiting = true;
         }
         return EXTREMZ_OK;

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <dlfcn.h>
 #include <mutex>
 #include <new>
 #include <thread>
@@ -231,8 +232,12 @@ static int check_args(int dtype, long long W, long long H, long long D, const ex
 // Runs one job to completion on an engine.
 template <class T>
 static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* tables, Arena* engine_store,
-                   Arena* job_store, const T* f, T* g, int W, int H, int D, const extremz_params& p,
-                   extremz_report* rep, int32_t* trace, int trace_cap) {
+                   Arena* job_store, const T* f, T* g, int W, int H, int D, const extremz_params& p0,
+                   extremz_report* rep, int32_t* trace, int trace_cap,
+                   extremz_edit_stream* es = nullptr) {
+  extremz_params p = p0;
+  p.flags &= ~kFlagKeepInput;
+  if (es) p.flags |= kFlagKeepInput;
   e.set_stream(st);
   EZ_RUN(e.init(tables, engine_store));
   const bool prof = (p.flags & EXTREMZ_FLAG_PROFILE) != 0;
@@ -263,6 +268,10 @@ static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* table
   if (prof) e.drop_profile_events();
   e.set_profile(false, 0);
   if (rc == EXTREMZ_OK) rc = e.job(slot).status;
+  if (es && (rc == EXTREMZ_OK || rc == EXTREMZ_ROUND_CAP)) {
+    const int erc = e.encode(slot, es);
+    if (erc != EXTREMZ_OK) rc = erc;
+  }
   e.release(slot);
   return rc;
 }
@@ -792,6 +801,58 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
   }
   if (prev != ctx->c.device) cudaSetDevice(prev);
   return (extremz_status)rc;
+}
+
+extremz_status extremz_edit_stream_caps(int dtype, int width, int height, int depth, int edit_type,
+                                        long long* index_cap, long long* edits_cap) {
+  if ((dtype != EXTREMZ_F32 && dtype != EXTREMZ_F64) || width <= 0 || height <= 0 || depth <= 0 ||
+      (edit_type != 0 && edit_type != 1) || !index_cap || !edits_cap)
+    return EXTREMZ_BAD_ARG;
+  const long long n = (long long)width * height * depth;
+  *index_cap = edit_type == 0 ? (3 * n + 7) / 8 : 4 * n;
+  *edits_cap = n * (dtype == EXTREMZ_F32 ? 4 : 8);
+  return EXTREMZ_OK;
+}
+
+extremz_status extremz_correct_encode(extremz_ctx* ctx, const void* d_orig, void* d_decp, int dtype,
+                                      int width, int height, int depth,
+                                      const extremz_params* params, extremz_report* report,
+                                      void* stream, extremz_edit_stream* es) {
+  if (!ctx || !d_orig || !d_decp || !es) return EXTREMZ_BAD_ARG;
+  int rc = check_args(dtype, width, height, depth, params);
+  if (rc != EXTREMZ_OK) return (extremz_status)rc;
+  if (report) std::memset(report, 0, sizeof(*report));
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = ctx->c.ensure_pool();
+  if (rc == EXTREMZ_OK) {
+    if (dtype == EXTREMZ_F32)
+      rc = run_one(ctx->c.e32, st, nullptr, nullptr, nullptr, (const float*)d_orig,
+                   (float*)d_decp, width, height, depth, *params, report, nullptr, 0, es);
+    else
+      rc = run_one(ctx->c.e64, st, nullptr, nullptr, nullptr, (const double*)d_orig,
+                   (double*)d_decp, width, height, depth, *params, report, nullptr, 0, es);
+  }
+  if (report) report->status = rc;
+  if (prev != ctx->c.device) cudaSetDevice(prev);
+  return (extremz_status)rc;
+}
+
+long long extremz_zstd_size(const void* host, long long bytes, int level) {
+  typedef size_t (*bound_fn)(size_t);
+  typedef size_t (*compress_fn)(void*, size_t, const void*, size_t, int);
+  typedef unsigned (*is_error_fn)(size_t);
+  static void* h = dlopen("libzstd.so.1", RTLD_NOW | RTLD_LOCAL);
+  if (!h || !host || bytes < 0) return -1;
+  static bound_fn zbound = (bound_fn)dlsym(h, "ZSTD_compressBound");
+  static compress_fn zcompress = (compress_fn)dlsym(h, "ZSTD_compress");
+  static is_error_fn ziserr = (is_error_fn)dlsym(h, "ZSTD_isError");
+  if (!zbound || !zcompress || !ziserr) return -1;
+  std::vector<char> out(zbound((size_t)bytes));
+  const size_t n = zcompress(out.data(), out.size(), host, (size_t)bytes, level);
+  return ziserr(n) ? -1 : (long long)n;
 }
 
 extremz_status extremz_correct_batch(extremz_ctx* ctx, const extremz_field* fields, int n,

@@ -19,6 +19,7 @@ struct Job {
   Dims dim;
   const T* f;  // original field
   T* g;        // decompressed field, corrected in place
+  T* g0;       // copy of the decompressed field as it came in (edit streams only)
   T bound, thr, sentinel;
   K sentinel_key;
   int q, edit_type;
@@ -624,12 +625,13 @@ __global__ void __launch_bounds__(kCpBlock) k_cp_count(const int8_t* __restrict_
   if (threadIdx.x < 4) bcount[threadIdx.x * gridDim.x + blockIdx.x] = cnt[threadIdx.x];
 }
 
-// Single block: exclusive scan of the 4 x nb block counts in place, totals to
-// ctr[C_NS2 .. C_NMIN].
-__global__ void __launch_bounds__(1024) k_cp_scan(int* __restrict__ bcount, int nb, int* ctr) {
+// Single block: exclusive scan of nlists x nb block counts in place, list
+// totals to totals[0 .. nlists).  The CP lists use totals = ctr + C_NS2.
+__global__ void __launch_bounds__(1024) k_scan_lists(int* __restrict__ bcount, int nb, int nlists,
+                                                     int* totals) {
   __shared__ int carry;
   __shared__ int warp_sums[32];
-  for (int l = 0; l < 4; ++l) {
+  for (int l = 0; l < nlists; ++l) {
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (int base = 0; base < nb; base += 1024) {
@@ -657,7 +659,7 @@ __global__ void __launch_bounds__(1024) k_cp_scan(int* __restrict__ bcount, int 
       if (threadIdx.x == 1023) carry = excl + x;
       __syncthreads();
     }
-    if (threadIdx.x == 0) ctr[C_NS2 + l] = carry;
+    if (threadIdx.x == 0) totals[l] = carry;
     __syncthreads();
   }
 }

@@ -154,6 +154,58 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
                                     const extremz_params* params, extremz_report* report,
                                     void* stream);
 
+/*
+ * Edit stream of a correction: what the reference's cost() (edit_type 0,
+ * src/ExtreM_cuda.cu:4557-4675) and floating_point_cost() (edit_type 1,
+ * :4677-4797) compute from the decompressed and corrected fields, before
+ * their zstd step.  A voxel is edited when its corrected value differs from
+ * its decompressed value.
+ *   edit_type 0: index = every voxel's edit counter (0 when not edited),
+ *                3 bits per voxel, LSB first (encodeTo3BitBitmap :4282-4312);
+ *                edits = -(decp - (orig - bound)) of the voxels whose counter
+ *                reached q, in id order.
+ *   edit_type 1: index = the edited voxels' ids, delta-coded, int32
+ *                (get_diff_index :4315-4323); edits = -(decp - (orig - bound))
+ *                of every edited voxel, in id order.
+ * index / edits are device buffers of the caller (edits in the field's dtype);
+ * extremz_edit_stream_caps gives sizes that always suffice.
+ */
+typedef struct {
+  void* index;
+  long long index_cap;   /* bytes */
+  void* edits;
+  long long edits_cap;   /* bytes */
+  /* filled in: */
+  long long index_bytes, edit_bytes;
+  long long edited;      /* voxels whose value changed */
+  long long n_edits;     /* entries of the edit stream */
+  double psnr_before;    /* decompressed field against the original (calculatePSNR :4273) */
+  double psnr_after;     /* corrected field against the original */
+  int reserved[4];
+} extremz_edit_stream;
+
+/* Buffer sizes that hold any edit stream of a field of this shape. */
+extremz_status extremz_edit_stream_caps(int dtype, int width, int height, int depth, int edit_type,
+                                        long long* index_cap, long long* edits_cap);
+
+/*
+ * extremz_correct_device, then the edit stream of the correction into es.
+ * Returns EXTREMZ_BAD_ARG when a stream buffer is too small (es holds the
+ * sizes needed) or, for edit_type 0, when q > 7 (counters need more than
+ * three bits; the reference then writes an empty stream).
+ * Replaces: the correction and the cost() / floating_point_cost() call of
+ * main() (src/ExtreM_cuda.cu:5508-6063).
+ */
+extremz_status extremz_correct_encode(extremz_ctx* ctx, const void* d_orig, void* d_decp, int dtype,
+                                      int width, int height, int depth,
+                                      const extremz_params* params, extremz_report* report,
+                                      void* stream, extremz_edit_stream* es);
+
+/* zstd-compressed size of a host buffer at the given level (the reference
+ * compresses both streams with the zstd tool at its default level 3), from
+ * the system's libzstd.so.1 loaded at run time; -1 when it is not present. */
+long long extremz_zstd_size(const void* host, long long bytes, int level);
+
 /* One field of a batch: device pointers, its own dtype, shape and parameters. */
 typedef struct {
   const void* orig;
