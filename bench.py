@@ -374,6 +374,13 @@ def run_ours(args, world, rank, local):
                "sample": f"leading {args.cpu_edge}^3 crop of the same field and bound, full "
                          f"correction to zero mismatch ({secs:.1f} s, status {crep['status']})"}
 
+    # Edit stream of the same correction (extremz_correct_encode): the extra
+    # device time of the encoder over the plain correction, the stream sizes
+    # and their zstd sizes, beside the oracle's CPU encoder on the whole field.
+    edit_stream = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        edit_stream = measure_edit_stream(ctx, f, g, g0, field, stream, args.no_cpu_baseline)
+
     forms = None
     if not args.no_forms and world == 1:
         b = measure_batched(local, 2, 1)
@@ -400,12 +407,78 @@ def run_ours(args, world, rank, local):
                 "dtype": dtype_name(field), "data": "synthetic (seeded generator, no dataset)",
                 "config": config_of(args, field), "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "forms": forms,
+                "edit_stream": edit_stream,
                 "rounds": {"outer_iters": r0.outer_iters, "cloop_rounds": r0.cloop_rounds,
                            "manifold_rounds": r0.manifold_rounds,
                            "manifold_reused": r0.manifold_reused, "status": r0.status,
                            "counters": r0.counters, "cp_counts": r0.cp_counts}}
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def measure_edit_stream(ctx, f, g, g0, field, stream, skip_cpu):
+    """Device time of extremz_correct_encode against extremz_correct_device
+    on the same field (streams into preallocated device buffers), the stream
+    sizes and zstd sizes, and the oracle's CPU encoder on the whole field."""
+    import ctypes
+    import torch
+    from extrem_z_b200 import api
+    L = api.load()
+    dt = api.F64 if field.f.dtype == np.float64 else api.F32
+    d, h, w = field.f.shape
+    icap, ecap = ctypes.c_longlong(), ctypes.c_longlong()
+    L.extremz_edit_stream_caps(dt, w, h, d, PARAMS["edit_type"], ctypes.byref(icap),
+                               ctypes.byref(ecap))
+    ibuf = torch.empty(icap.value, dtype=torch.uint8, device=f.device)
+    ebuf = torch.empty(ecap.value, dtype=torch.uint8, device=f.device)
+    es = api.EditStream()
+    es.index, es.index_cap, es.edits, es.edits_cap = (ibuf.data_ptr(), icap.value,
+                                                      ebuf.data_ptr(), ecap.value)
+    p = api.make_params(field.eb, tuning_key=("f64" if dt == api.F64 else "f32", field.f.size),
+                        **PARAMS)
+    r = api.Report()
+
+    def timed(encode):
+        best = None
+        for _ in range(3):
+            g.copy_(g0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if encode:
+                st = L.extremz_correct_encode(ctx._h, f.data_ptr(), g.data_ptr(), dt, w, h, d,
+                                              ctypes.byref(p), ctypes.byref(r),
+                                              stream.cuda_stream, ctypes.byref(es))
+            else:
+                st = L.extremz_correct_device(ctx._h, f.data_ptr(), g.data_ptr(), dt, w, h, d,
+                                              ctypes.byref(p), ctypes.byref(r),
+                                              stream.cuda_stream, None, 0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            assert st == 0, st
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        return best
+
+    plain_ms = timed(False)
+    enc_ms = timed(True)
+    index = ibuf[:es.index_bytes].cpu().numpy()
+    edits = ebuf[:es.edit_bytes].cpu().numpy()
+    n = field.f.size
+    out = {"entry_point": "extremz_correct_encode", "edit_type": PARAMS["edit_type"],
+           "edited": int(es.edited), "edit_ratio": es.edited / n, "n_edits": int(es.n_edits),
+           "index_bytes": int(es.index_bytes), "edit_bytes": int(es.edit_bytes),
+           "index_zstd_bytes": api.zstd_size(index), "edits_zstd_bytes": api.zstd_size(edits),
+           "psnr_before": es.psnr_before, "psnr_after": es.psnr_after,
+           "correct_ms": plain_ms, "encode_extra_ms": enc_ms - plain_ms}
+    if not skip_cpu:
+        from oracle import ffi
+        fixed = g.cpu().numpy()
+        t0 = time.perf_counter()
+        ffi.encode(field.f, field.decp, fixed, None, field.eb, q=PARAMS["q"],
+                   edit_type=PARAMS["edit_type"])
+        out["cpu_encode_ms"] = 1e3 * (time.perf_counter() - t0)
+        out["cpu_encode_cores"] = 1
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -50,7 +50,8 @@ class Params(ctypes.Structure):
                 ("max_outer", ctypes.c_int), ("max_cloop_rounds", ctypes.c_int),
                 ("final_join", ctypes.c_int), ("preserve_join", ctypes.c_int),
                 ("flags", ctypes.c_int), ("device_iter_cap", ctypes.c_int),
-                ("reserved", ctypes.c_int * 4)]
+                ("tune_blocks_per_sm", ctypes.c_int), ("tune_pass_chunk", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
 
 class Report(ctypes.Structure):
@@ -214,16 +215,32 @@ def _check(st: int, allow_cap: bool = True):
 def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 1,
                 max_outer: int = 1000, max_cloop_rounds: int = 100000,
                 final_join: bool = True, preserve_join: bool = False,
-                profile=False, tma: bool = True, device_iter_cap: int = 0) -> Params:
+                profile=False, tma=None, device_iter_cap: int = 0,
+                blocks_per_sm: int = 0, pass_chunk: int = 0, tuned: bool = True,
+                tuning_key=None) -> Params:
     """profile: False, True (time every kernel class) or an iterable of class
-    names from KCLASS_NAMES to time only those."""
+    names from KCLASS_NAMES to time only those.
+
+    tma, blocks_per_sm, pass_chunk: launch-shape knobs (results do not depend
+    on them).  Those left unset come from the autotuner's table for the
+    field's dtype and size (tuning_key = (dtype name, voxels)) when ``tuned``
+    and a table exists, else the library defaults."""
     p = Params()
     load().extremz_default_params(ctypes.byref(p))
     p.bound, p.thr, p.q, p.edit_type = float(bound), float(thr), int(q), int(edit_type)
     p.max_outer, p.max_cloop_rounds = int(max_outer), int(max_cloop_rounds)
     p.final_join, p.preserve_join = int(bool(final_join)), int(bool(preserve_join))
     p.device_iter_cap = int(device_iter_cap)
-    p.flags = 0 if tma else FLAG_NO_TMA
+    if tuned and tuning_key is not None:
+        from . import autotune
+        t = autotune.lookup(*tuning_key)
+        if t:
+            if tma is None:
+                tma = t["halo"] == "tma"
+            blocks_per_sm = blocks_per_sm or t["blocks_per_sm"]
+            pass_chunk = pass_chunk or t["pass_chunk"]
+    p.tune_blocks_per_sm, p.tune_pass_chunk = int(blocks_per_sm), int(pass_chunk)
+    p.flags = 0 if (tma is None or tma) else FLAG_NO_TMA
     if profile:
         p.flags |= FLAG_PROFILE
         if profile is not True:
@@ -268,7 +285,7 @@ class Context:
         w, h, d = _whd(tuple(f.shape))
         if stream is None:
             stream = torch.cuda.current_stream(f.device).cuda_stream
-        p = make_params(bound, **kw)
+        p = make_params(bound, tuning_key=(_dtname(dt), w * h * d), **kw)
         r = Report()
         tr = np.zeros(max(trace_cap, 1) * 4, dtype=np.int32)
         st = load().extremz_correct_device(self._h, f.data_ptr(), decp.data_ptr(), dt, w, h, d,
@@ -295,7 +312,7 @@ class Context:
         assert f.is_contiguous() and decp.is_contiguous()
         dt = {torch.float32: F32, torch.float64: F64}[f.dtype]
         w, h, d = _whd(tuple(f.shape))
-        p = make_params(bound, **kw)
+        p = make_params(bound, tuning_key=(_dtname(dt), w * h * d), **kw)
         L = load()
         icap, ecap = ctypes.c_longlong(), ctypes.c_longlong()
         _check(L.extremz_edit_stream_caps(dt, w, h, d, p.edit_type, ctypes.byref(icap),
@@ -343,7 +360,8 @@ class Context:
             arr[i].orig, arr[i].decp = f.data_ptr(), decp.data_ptr()
             arr[i].dtype = {torch.float32: F32, torch.float64: F64}[f.dtype]
             arr[i].width, arr[i].height, arr[i].depth = w, h, d
-            arr[i].params = make_params(bound, **kw)
+            arr[i].params = make_params(bound, tuning_key=(_dtname(arr[i].dtype), w * h * d),
+                                        **kw)
             keep.append((f, decp))
         if stream is None:
             dev = items[0][0].device if n else torch.device("cuda", self.device)
@@ -361,7 +379,7 @@ class Context:
         assert f.flags.c_contiguous and decp.flags.c_contiguous
         dt = {np.dtype(np.float32): F32, np.dtype(np.float64): F64}[f.dtype]
         w, h, d = _whd(f.shape)
-        p = make_params(bound, **kw)
+        p = make_params(bound, tuning_key=(_dtname(dt), w * h * d), **kw)
         r = Report()
         st = load().extremz_correct_host(self._h, f.ctypes.data, decp.ctypes.data, dt, w, h, d,
                                          ctypes.byref(p), ctypes.byref(r), stream)
@@ -420,7 +438,8 @@ class Server:
         fd.orig, fd.decp = f.data_ptr(), decp.data_ptr()
         fd.dtype = {torch.float32: F32, torch.float64: F64}[f.dtype]
         fd.width, fd.height, fd.depth = _whd(tuple(f.shape))
-        fd.params = make_params(bound, **kw)
+        fd.params = make_params(bound, tuning_key=(_dtname(fd.dtype),
+                                                   fd.width * fd.height * fd.depth), **kw)
         if stream is None:
             stream = torch.cuda.current_stream(f.device).cuda_stream
         t = ctypes.c_longlong()
@@ -472,6 +491,10 @@ def job_footprint(voxels_or_shape, dtype) -> int:
         w, h, d = int(voxels_or_shape), 1, 1
     dt = F32 if str(dtype).endswith("float32") else F64
     return int(load().extremz_job_footprint(dt, w, h, d))
+
+
+def _dtname(code: int) -> str:
+    return "f32" if code == F32 else "f64"
 
 
 def _whd(shape):

@@ -150,6 +150,7 @@ struct JobHost {
   int32_t* trace = nullptr;
   int trace_cap = 0, trace_len = 0;
   std::vector<int> pending;  // trace phases to emit once the tick's counters are back
+  int blocks_per_sm = 8;      // grid-stride kernels' blocks per SM (tuning knob)
   long long tag = 0;
 
   void emit(int phase, int a = 0, int b = 0, int c3 = 0) {
@@ -175,6 +176,7 @@ class BatchEngine {
     EZ_CHECK(cudaGetDevice(&dev));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    sms_ = sms;
     grid_ = sms * 8;
     if (preset_tables) tb_ = *preset_tables;
     else if (int rc = device_tables(&tb_)) return rc;
@@ -273,6 +275,8 @@ class BatchEngine {
     J.q = p.q;
     J.edit_type = p.edit_type;
     J.iter_cap = p.device_iter_cap > 0 ? p.device_iter_cap : J.dim.N + 1;
+    J.pass_chunk = p.tune_pass_chunk > 0 ? p.tune_pass_chunk : 4;
+    jh.blocks_per_sm = p.tune_blocks_per_sm > 0 ? p.tune_blocks_per_sm : 8;
     J.tb = tb_;
     J.ctr = ctr_dev_ + (size_t)slot * C_COUNT;
     const int N = J.dim.N;
@@ -551,7 +555,8 @@ class BatchEngine {
   cudaStream_t cap_ = nullptr;  // capture stream
   cudaMemPool_t pool_mem_ = nullptr;
   bool ready_ = false, borrowed_ = false, issued_ = false;
-  int grid_ = 1184;
+  int grid_ = 1184;  // grid of the grid-stride kernels for the phase being issued
+  int sms_ = 148;
   DeviceTables tb_{};
   Job<T>* jobs_dev_ = nullptr;
   CUtensorMap* maps_dev_ = nullptr;
@@ -731,6 +736,9 @@ class BatchEngine {
 
   // ------------------------------------------------------------- phases --
   int run_phase(int ph, const std::vector<int>& sel) {
+    int bps = 1;  // jobs share launches: the largest knob of the selection
+    for (int i : sel) bps = std::max(bps, slots_[i].blocks_per_sm);
+    grid_ = sms_ * bps;
     const Sel s = make_sel(sel, false);
     const Sel st = make_sel(sel, true);
     const Job<T>* jobs = jobs_dev_;

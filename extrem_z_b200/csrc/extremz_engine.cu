@@ -226,6 +226,9 @@ static int check_args(int dtype, long long W, long long H, long long D, const ex
   if (W * H * D >= (1ll << kCatShift)) return EXTREMZ_BAD_ARG;
   if (p->q <= 0 || (p->edit_type != 0 && p->edit_type != 1)) return EXTREMZ_BAD_ARG;
   if (p->max_outer < 0 || p->max_cloop_rounds < 0 || p->device_iter_cap < 0) return EXTREMZ_BAD_ARG;
+  if (p->tune_blocks_per_sm < 0 || p->tune_blocks_per_sm > 32 || p->tune_pass_chunk < 0 ||
+      p->tune_pass_chunk > 64)
+    return EXTREMZ_BAD_ARG;
   return EXTREMZ_OK;
 }
 

@@ -68,6 +68,7 @@ struct Job {
   const CUtensorMap* map_g;
   int tma_f, tma_g;
   int iter_cap;  // device-side limit of pointer jumping and path walks
+  int pass_chunk; // 1024-id blocks per saddle-pass work item (a tuning knob)
 };
 
 // Jobs served by one launch.  Every per-round kernel takes the device array of
@@ -1056,7 +1057,7 @@ __device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
 }
 
 // Fused pass over the original saddles after a manifold round, both sides in
-// one grid.  A block takes a chunk of the id space (kPassChunk blocks of 1024
+// one grid.  A block takes a chunk of the id space (pass_chunk blocks of 1024
 // ids) and the entries of both saddle lists in it, so that the two sides read
 // the same neighbourhoods together:
 //  * decompressed row slots.  The reference rewrites row i (findAscPaths /
@@ -1072,8 +1073,6 @@ __device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
 //  * wrong-neighbour seeds (get_wrong_split_neighbors / _join_ :2400-2513):
 //    saddles with a neighbour on the side whose label differs from the
 //    original's, 2-saddles to cand, 1-saddles to cand_j.
-constexpr int kPassChunk = 4;
-
 template <class T>
 __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict__ jobs,
                                                         const __grid_constant__ Sel sel) {
@@ -1082,9 +1081,10 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
     if (J.ctr[C_MFSKIP]) continue;
     const int ns2 = J.ctr[C_NS2], ns1 = J.ctr[C_NS1];
     const int nb = (J.dim.N + kCpBlock - 1) / kCpBlock;
-    const int nchunk = (nb + kPassChunk - 1) / kPassChunk;
+    const int chunk = J.pass_chunk;
+    const int nchunk = (nb + chunk - 1) / chunk;
     for (int c = blockIdx.x; c < nchunk; c += gridDim.x) {
-      const int b0 = c * kPassChunk, b1 = min(b0 + kPassChunk, nb);
+      const int b0 = c * chunk, b1 = min(b0 + chunk, nb);
       const int a2 = J.cpoff[b0], e2 = b1 < nb ? J.cpoff[b1] : ns2;
       const int a1 = J.cpoff[nb + b0], e1 = b1 < nb ? J.cpoff[nb + b1] : ns1;
       const int n2 = e2 - a2, n = n2 + (e1 - a1);

@@ -71,7 +71,12 @@ typedef struct {
                           walks; 0 = the field's voxel count (never reached by a
                           valid path).  Reaching it sets report.error_bits and
                           returns EXTREMZ_DEVICE_TIMEOUT. */
-  int reserved[4];
+  /* Launch-shape knobs, picked per dtype and size class by the project's
+   * autotuner (extrem_z_b200/autotune.py); results do not depend on them.
+   * 0 = defaults (8 and 4). */
+  int tune_blocks_per_sm; /* blocks per SM of the grid-stride kernels, 1..32 */
+  int tune_pass_chunk;    /* 1024-id blocks per saddle-pass work item, 1..64 */
+  int reserved[2];
 } extremz_params;
 
 /* flags: time kernel launches with CUDA events, per kernel class, into
