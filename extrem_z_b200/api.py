@@ -31,7 +31,7 @@ F32, F64 = 0, 1
 EXPORTS = ("extremz_version", "extremz_default_params", "extremz_ctx_create",
            "extremz_ctx_destroy", "extremz_correct_device", "extremz_correct_host",
            "extremz_correct_batch", "extremz_correct_encode", "extremz_edit_stream_caps",
-           "extremz_zstd_size", "extremz_server_create", "extremz_server_destroy",
+           "extremz_zstd_size", "extremz_persistence_pairs", "extremz_server_create", "extremz_server_destroy",
            "extremz_server_submit", "extremz_server_poll", "extremz_server_wait",
            "extremz_server_get_stats", "extremz_job_footprint",
            "extremz_correct_device_noalloc", "extremz_noalloc_max_voxels",
@@ -165,6 +165,11 @@ def load(build_if_missing: bool = True):
                                                ctypes.POINTER(ctypes.c_longlong),
                                                ctypes.POINTER(ctypes.c_longlong)]
         L.extremz_edit_stream_caps.restype = i32
+        L.extremz_persistence_pairs.argtypes = [vp, vp, i32, i32, i32, i32, vp,
+                                                ctypes.c_longlong, vp, ctypes.c_longlong,
+                                                ctypes.POINTER(ctypes.c_longlong),
+                                                ctypes.POINTER(ctypes.c_longlong), vp]
+        L.extremz_persistence_pairs.restype = i32
         L.extremz_zstd_size.argtypes = [vp, ctypes.c_longlong, i32]
         L.extremz_zstd_size.restype = ctypes.c_longlong
         L.extremz_correct_batch.argtypes = [vp, ctypes.POINTER(Field), i32,
@@ -337,6 +342,52 @@ class Context:
                    psnr_before=float(es.psnr_before), psnr_after=float(es.psnr_after),
                    index_zstd=zstd_size(index, zstd_level), edits_zstd=zstd_size(edits, zstd_level))
         return CorrectionReport.of(r), out
+
+    # -- topology -----------------------------------------------------------
+    def persistence_pairs(self, field, *, stream=None):
+        """Merge-tree persistence pairs of a CUDA tensor field.
+
+        Returns (max_pairs, min_pairs): int32 arrays of shape (n, 2) holding
+        (partner vertex, extremum vertex), extrema by rank (maxima ascending,
+        minima descending in value then id).  See extremz_persistence_pairs.
+        """
+        import torch
+        assert field.is_cuda and field.is_contiguous()
+        dt = {torch.float32: F32, torch.float64: F64}[field.dtype]
+        w, h, d = _whd(tuple(field.shape))
+        n = w * h * d
+        mx = torch.empty(2 * n, dtype=torch.int32, device=field.device)
+        mn = torch.empty(2 * n, dtype=torch.int32, device=field.device)
+        nx, nn = ctypes.c_longlong(), ctypes.c_longlong()
+        if stream is None:
+            stream = torch.cuda.current_stream(field.device).cuda_stream
+        _check(load().extremz_persistence_pairs(self._h, field.data_ptr(), dt, w, h, d,
+                                                mx.data_ptr(), 2 * n, mn.data_ptr(), 2 * n,
+                                                ctypes.byref(nx), ctypes.byref(nn), stream),
+               allow_cap=False)
+        torch.cuda.synchronize(field.device)
+        return (mx[:2 * nx.value].view(-1, 2).cpu().numpy(),
+                mn[:2 * nn.value].view(-1, 2).cpu().numpy())
+
+    def compare_topology(self, f, g):
+        """Topology report of a corrected field g against its original f: the
+        merge-tree persistence pairs of both (split and join trees), how many
+        pairs are identical (same saddle, same extremum), and the largest
+        change of a pair's persistence (value difference)."""
+        out = {}
+        fv = f.double().flatten().cpu().numpy()
+        gv = g.double().flatten().cpu().numpy()
+        for name, pa, pb in zip(("split", "join"), self.persistence_pairs(f),
+                                self.persistence_pairs(g)):
+            sa = {(int(p), int(e)) for p, e in pa}
+            sb = {(int(p), int(e)) for p, e in pb}
+            common = sa & sb
+            dper = max((abs(abs(fv[e] - fv[p]) - abs(gv[e] - gv[p])) for p, e in common
+                        if p >= 0), default=0.0)
+            out[name] = {"pairs_original": len(sa), "pairs_corrected": len(sb),
+                         "identical": len(common), "same": sa == sb,
+                         "max_persistence_change": float(dper)}
+        return out
 
     # -- batches ------------------------------------------------------------
     def correct_batch(self, items, *, stream=None):

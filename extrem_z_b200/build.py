@@ -14,7 +14,7 @@ LIB = os.path.join(PKG, "libextremz.so")
 
 SOURCES = ["extremz_engine.cu"]
 HEADERS = ["extremz_common.cuh", "extremz_kernels.cuh", "extremz_batch.cuh", "extremz_encode.cuh",
-           "extremz_lut.h"]
+           "extremz_topo.cuh", "extremz_lut.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -30,6 +30,7 @@
 
 #include "extremz_encode.cuh"
 #include "extremz_kernels.cuh"
+#include "extremz_topo.cuh"
 
 namespace extremz {
 
@@ -92,6 +93,9 @@ constexpr long long arr_bytes(long long count, long long sz) { return (count * s
 // Internal job flag (outside the public EXTREMZ_FLAG_* bits): keep a copy of
 // the incoming decompressed field for the edit stream.
 constexpr int kFlagKeepInput = 1 << 30;
+// Internal job flag: analysis only -- classification, labels and critical-point
+// lists of the field (admitted as the original), no correction.
+constexpr int kFlagAnalysis = 1 << 29;
 
 constexpr long long job_bytes_voxels(long long n, long long ksz) {
   return arr_bytes(n, 1) + arr_bytes(n, 2)                          // otype, olm
@@ -438,6 +442,144 @@ class BatchEngine {
     return bad ? EXTREMZ_BAD_ARG : EXTREMZ_OK;
   }
 
+  // Stream-ordered scratch from the engine's pool (or the device's default).
+  void* scratch(size_t bytes) {
+    void* p = nullptr;
+    const cudaError_t e = pool_mem_ ? cudaMallocFromPoolAsync(&p, bytes, pool_mem_, st_)
+                                    : cudaMallocAsync(&p, bytes, st_);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return p;
+  }
+
+  // Merge-tree persistence pairs of a finished analysis job (see
+  // extremz_topo.cuh): split tree into max_pairs (2 ints per maximum), join
+  // tree into min_pairs (2 per minimum), device buffers of the caller.
+  // counts (host) receives the numbers of maxima and minima.  Synchronises.
+  int persistence(int slot, int* max_pairs, long long max_cap, int* min_pairs, long long min_cap,
+                  long long* counts) {
+    JobHost<T>& jh = slots_[slot];
+    const Job<T>& J = jh.J;
+    const int ne[2] = {h(slot, C_NMAX), h(slot, C_NMIN)};
+    counts[0] = ne[0];
+    counts[1] = ne[1];
+    if (2ll * ne[0] > max_cap || 2ll * ne[1] > min_cap || (ne[0] && !max_pairs) ||
+        (ne[1] && !min_pairs))
+      return EXTREMZ_BAD_ARG;
+    // Merge vertices of both trees, ascending id (the job's CP-block scratch
+    // is free once the analysis is done).
+    const int N = J.dim.N;
+    int* cand = static_cast<int*>(scratch((size_t)2 * N * sizeof(int) + 256));
+    if (!cand) return EXTREMZ_OOM;
+    int* ctot = J.ctr + C_CAND;  // two free counter slots of the finished job
+    launch(K_OTHER, k_pp_cand_count<T>, jh.nb, kCpBlock, J.f, J.dim, jh.bcount);
+    launch(K_OTHER, k_scan_lists, 1, 1024, jh.bcount, jh.nb, 2, ctot);
+    launch(K_OTHER, k_pp_cand_write<T>, jh.nb, kCpBlock, J.f, J.dim, (const int*)jh.bcount, cand,
+           cand + N);
+    int ns[2];
+    EZ_CHECK(cudaMemcpyAsync(ns, ctot, sizeof(ns), cudaMemcpyDeviceToHost, st_));
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    const int nmaxall = std::max(std::max(ns[0], ns[1]), std::max(ne[0], ne[1])) + 1;
+    // Scratch: sort keys and values (in and out), ranks, rows and counts,
+    // largest / pointer / pair per extremum, sorted list indices of both
+    // sides' extrema, and the round flag.
+    size_t cub_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (unsigned long long*)nullptr,
+                                    (unsigned long long*)nullptr, (int*)nullptr, (int*)nullptr,
+                                    nmaxall, 0, 64, st_);
+    const size_t a = ((size_t)nmaxall * 8 + 255) & ~size_t(255);
+    const size_t b = ((size_t)nmaxall * 4 + 255) & ~size_t(255);
+    const size_t rows_bytes = (((size_t)std::max(ns[0], ns[1]) + 1) * kPpRow * 4 + 255) & ~size_t(255);
+    const size_t total = 2 * a + 9 * b + rows_bytes + ((cub_bytes + 255) & ~size_t(255)) + 256;
+    char* base = static_cast<char*>(scratch(total));
+    if (!base) {
+      cudaFreeAsync(cand, st_);
+      return EXTREMZ_OOM;
+    }
+    char* q = base;
+    auto take = [&](size_t n) { char* r = q; q += n; return r; };
+    auto* kin = reinterpret_cast<unsigned long long*>(take(a));
+    auto* kout = reinterpret_cast<unsigned long long*>(take(a));
+    int* vin = reinterpret_cast<int*>(take(b));
+    int* ext_li[2] = {reinterpret_cast<int*>(take(b)), reinterpret_cast<int*>(take(b))};
+    int* sad_li = reinterpret_cast<int*>(take(b));
+    int* erank = reinterpret_cast<int*>(take(b));
+    int* largest = reinterpret_cast<int*>(take(b));
+    int* ptr = reinterpret_cast<int*>(take(b));
+    int* pair = reinterpret_cast<int*>(take(b));
+    int* cnt = reinterpret_cast<int*>(take(b));
+    int* rows = reinterpret_cast<int*>(take(rows_bytes));
+    void* cub_tmp = take((cub_bytes + 255) & ~size_t(255));
+    int* flag = reinterpret_cast<int*>(take(256));  // [0] round paired, [1] jump limit hit
+    EZ_CHECK(cudaMemsetAsync(flag, 0, 8, st_));
+    const int* elist[2] = {J.maxima, J.minima};
+    const int* slist[2] = {cand, cand + N};
+    int rc = EXTREMZ_OK;
+    auto sort = [&](const int* list, int n, bool reverse, bool complement, int* out_li) {
+      launch(K_OTHER, k_pp_keys<T>, grid_, 256, J.f, list, n, reverse, complement, kin, vin);
+      size_t tb = cub_bytes;
+      if (cub::DeviceRadixSort::SortPairs(cub_tmp, tb, kin, kout, vin, out_li, n, 0, 64, st_) !=
+          cudaSuccess)
+        rc = EXTREMZ_CUDA_ERR;
+    };
+    // Extrema ascending in each tree's order: maxima by (value, id), minima by
+    // the reverse of it.
+    if (ne[0]) sort(elist[0], ne[0], false, false, ext_li[0]);
+    if (ne[1]) sort(elist[1], ne[1], true, true, ext_li[1]);
+    int glob[2] = {-1, -1};  // global maximum, global minimum (vertex ids)
+    if (ne[0] && ne[1] && rc == EXTREMZ_OK) {
+      int li[2];
+      EZ_CHECK(cudaMemcpyAsync(&li[0], ext_li[0] + ne[0] - 1, 4, cudaMemcpyDeviceToHost, st_));
+      EZ_CHECK(cudaMemcpyAsync(&li[1], ext_li[1] + ne[1] - 1, 4, cudaMemcpyDeviceToHost, st_));
+      EZ_CHECK(cudaStreamSynchronize(st_));
+      EZ_CHECK(cudaMemcpyAsync(&glob[0], elist[0] + li[0], 4, cudaMemcpyDeviceToHost, st_));
+      EZ_CHECK(cudaMemcpyAsync(&glob[1], elist[1] + li[1], 4, cudaMemcpyDeviceToHost, st_));
+      EZ_CHECK(cudaStreamSynchronize(st_));
+    }
+    for (int side = 0; side < 2 && rc == EXTREMZ_OK; ++side) {
+      const bool kmax = side == 0;
+      const int n_e = ne[side], n_s = ns[side];
+      if (n_e == 0) continue;
+      launch(K_OTHER, k_pp_rank, grid_, 256, (const int*)ext_li[side], n_e, erank);
+      // Saddles descending in the tree's order.
+      if (n_s) sort(slist[side], n_s, kmax, kmax, sad_li);
+      if (kmax)
+        launch(K_OTHER, k_pp_rows<T, true>, grid_, 256, J.f, J.dim, slist[0], (const int*)sad_li,
+               n_s, (const int*)J.ds, (const int*)J.ext, (const int*)erank, rows, cnt);
+      else
+        launch(K_OTHER, k_pp_rows<T, false>, grid_, 256, J.f, J.dim, slist[1], (const int*)sad_li,
+               n_s, (const int*)J.as, (const int*)J.ext, (const int*)erank, rows, cnt);
+      launch(K_OTHER, k_fill<int>, grid_, 256, largest, kInf, (long long)n_e);
+      launch(K_OTHER, k_fill<int>, grid_, 256, pair, -1, (long long)n_e);
+      launch(K_OTHER, k_iota, grid_, 256, ptr, n_e);
+      for (int round = 0; round <= n_e; ++round) {  // every round but the last pairs one
+        EZ_CHECK(cudaMemsetAsync(flag, 0, 4, st_));
+        if (n_s) launch(K_OTHER, k_pp_largest, grid_, 256, (const int*)rows, (const int*)cnt, n_s,
+                        n_e - 1, largest);
+        launch(K_OTHER, k_pp_pair, grid_, 256, (const int*)rows, (const int*)cnt, n_e, n_s,
+               largest, ptr, pair, flag);
+        int changed = 0;
+        EZ_CHECK(cudaMemcpyAsync(&changed, flag, 4, cudaMemcpyDeviceToHost, st_));
+        EZ_CHECK(cudaStreamSynchronize(st_));
+        if (!changed) break;
+        launch(K_OTHER, k_pp_jump, grid_, 256, ptr, n_e, n_e + 1, flag + 1);
+        if (n_s) launch(K_OTHER, k_pp_remap, grid_, 256, rows, cnt, n_s, (const int*)ptr);
+      }
+      launch(K_OTHER, k_pp_out, grid_, 256, (const int*)pair, n_e, (const int*)ext_li[side],
+             elist[side], (const int*)sad_li, slist[side], glob[1 - side],
+             kmax ? max_pairs : min_pairs);
+    }
+    int jump_err = 0;
+    cudaMemcpyAsync(&jump_err, flag + 1, 4, cudaMemcpyDeviceToHost, st_);
+    cudaFreeAsync(base, st_);
+    cudaFreeAsync(cand, st_);
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    if (rc == EXTREMZ_OK && jump_err) rc = EXTREMZ_DEVICE_TIMEOUT;
+    return rc;
+  }
+
   // Releases a finished job's slot and (stream-ordered) its workspace.
   void release(int slot) { free_job(slots_[slot]); }
   // Releases every job (after an error that ends a batch).
@@ -762,7 +904,8 @@ class BatchEngine {
             continue;
           }
           if (rc != EXTREMZ_OK) return rc;
-          slots_[i].pc = PC_CL_DETECT;
+          if (slots_[i].p.flags & kFlagAnalysis) finish(i, EXTREMZ_OK);
+          else slots_[i].pc = PC_CL_DETECT;
         }
         return EXTREMZ_OK;
       case PC_CL_DETECT:

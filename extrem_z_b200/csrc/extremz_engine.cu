@@ -279,6 +279,27 @@ static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* table
   return rc;
 }
 
+// Persistence pairs of one field: an analysis job (classification, labels and
+// critical-point lists of the field), then the pairing rounds.
+template <class T>
+static int analyze_one(BatchEngine<T>& e, cudaStream_t st, const T* field, int W, int H, int D,
+                       int* max_pairs, long long max_cap, int* min_pairs, long long min_cap,
+                       long long* counts) {
+  e.set_stream(st);
+  EZ_RUN(e.init(nullptr, nullptr));
+  extremz_params p;
+  extremz_default_params(&p);
+  p.flags = kFlagAnalysis;
+  int slot = -1;
+  EZ_RUN(e.admit(field, const_cast<T*>(field), W, H, D, p, nullptr, 0, nullptr, 0, &slot));
+  int rc = EXTREMZ_OK;
+  while (e.job(slot).pc != PC_DONE && rc == EXTREMZ_OK) rc = e.tick();
+  if (rc == EXTREMZ_OK) rc = e.job(slot).status;
+  if (rc == EXTREMZ_OK) rc = e.persistence(slot, max_pairs, max_cap, min_pairs, min_cap, counts);
+  e.release(slot);
+  return rc;
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free correction (extremz_correct_device_noalloc).
 //
@@ -856,6 +877,36 @@ long long extremz_zstd_size(const void* host, long long bytes, int level) {
   std::vector<char> out(zbound((size_t)bytes));
   const size_t n = zcompress(out.data(), out.size(), host, (size_t)bytes, level);
   return ziserr(n) ? -1 : (long long)n;
+}
+
+extremz_status extremz_persistence_pairs(extremz_ctx* ctx, const void* d_field, int dtype,
+                                        int width, int height, int depth, int32_t* d_max_pairs,
+                                        long long max_pairs_cap, int32_t* d_min_pairs,
+                                        long long min_pairs_cap, long long* n_max,
+                                        long long* n_min, void* stream) {
+  if (!ctx || !d_field) return EXTREMZ_BAD_ARG;
+  extremz_params p;
+  extremz_default_params(&p);
+  int rc = check_args(dtype, width, height, depth, &p);
+  if (rc != EXTREMZ_OK) return (extremz_status)rc;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  long long counts[2] = {0, 0};
+  rc = ctx->c.ensure_pool();
+  if (rc == EXTREMZ_OK) {
+    if (dtype == EXTREMZ_F32)
+      rc = analyze_one(ctx->c.e32, st, (const float*)d_field, width, height, depth, d_max_pairs,
+                       max_pairs_cap, d_min_pairs, min_pairs_cap, counts);
+    else
+      rc = analyze_one(ctx->c.e64, st, (const double*)d_field, width, height, depth, d_max_pairs,
+                       max_pairs_cap, d_min_pairs, min_pairs_cap, counts);
+  }
+  if (n_max) *n_max = counts[0];
+  if (n_min) *n_min = counts[1];
+  if (prev != ctx->c.device) cudaSetDevice(prev);
+  return (extremz_status)rc;
 }
 
 extremz_status extremz_correct_batch(extremz_ctx* ctx, const extremz_field* fields, int n,

@@ -206,6 +206,28 @@ extremz_status extremz_correct_encode(extremz_ctx* ctx, const void* d_orig, void
                                       const extremz_params* params, extremz_report* report,
                                       void* stream, extremz_edit_stream* es);
 
+/*
+ * Merge-tree persistence pairs of a field (device pointer), for checking that
+ * a correction kept the topology: the split tree pairs every maximum with the
+ * vertex where its superlevel component merges into an older one, the join
+ * tree every minimum with the vertex where its sublevel component merges; the
+ * global maximum pairs with the global minimum and vice versa.  Merge vertices
+ * are found from their links (upper / lower link with two or more
+ * components), so thin grids (2-D slices) are covered too.  Pairs are (partner vertex, extremum vertex),
+ * two int32 each, one per maximum (d_max_pairs) and per minimum
+ * (d_min_pairs), extrema ordered by value then id (ascending for maxima,
+ * descending for minima).  Caps are in int32 entries; n_max / n_min receive
+ * the numbers of extrema (BAD_ARG when a buffer is too small).
+ * Replaces: constructPersistencePairs / compute_MergeT (src/ExtreM.cpp
+ * :1863-1918, :2930-2952) -- the same extremum-graph pairing, on the
+ * field's own critical points and manifold labels.
+ */
+extremz_status extremz_persistence_pairs(extremz_ctx* ctx, const void* d_field, int dtype,
+                                        int width, int height, int depth, int32_t* d_max_pairs,
+                                        long long max_pairs_cap, int32_t* d_min_pairs,
+                                        long long min_pairs_cap, long long* n_max,
+                                        long long* n_min, void* stream);
+
 /* zstd-compressed size of a host buffer at the given level (the reference
  * compresses both streams with the zstd tool at its default level 3), from
  * the system's libzstd.so.1 loaded at run time; -1 when it is not present. */

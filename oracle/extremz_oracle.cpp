@@ -1129,9 +1129,104 @@ bool dims_ok(int W, int H, int D) {
   return W > 0 && H > 0 && D > 0 && (long long)W * H * D < (1ll << 31) / 16;
 }
 
+// ---------------------------------------------------------------------------
+// Merge-tree persistence pairs by the elder rule, with a union-find over the
+// vertices in the tree's order: an independent check of the extremum-graph
+// pairing (constructPersistencePairs, src/ExtreM.cpp:1863-1918) that the
+// library runs.  Split tree: vertices by (value, id) descending; a vertex
+// without an earlier neighbour starts a component (a maximum); a vertex
+// joining several components pairs the younger components' maxima with
+// itself.  Join tree: the same in ascending order (minima, 1-saddles).
+// Output by extremum rank (maxima ascending, minima descending in value
+// then id): (partner vertex, extremum vertex); the global extremum's partner
+// is the opposite global extremum.
+// ---------------------------------------------------------------------------
+template <class T>
+void elder_pairs(const T* f, const Grid& g, bool split, std::vector<int>& out) {
+  const int N = g.N;
+  std::vector<int> order(N);
+  for (int v = 0; v < N; ++v) order[v] = v;
+  auto before = [&](int a, int b) {  // a comes first in the tree's order
+    return split ? (f[a] > f[b] || (f[a] == f[b] && a > b)) : (f[a] < f[b] || (f[a] == f[b] && a < b));
+  };
+  std::sort(order.begin(), order.end(), before);
+  std::vector<int> parent(N, -1), eldest(N, -1), pos(N);
+  for (int k = 0; k < N; ++k) pos[order[k]] = k;
+  auto find = [&](int x) {
+    while (parent[x] != x) {
+      parent[x] = parent[parent[x]];
+      x = parent[x];
+    }
+    return x;
+  };
+  std::vector<int> ext;           // extrema in processing order
+  std::vector<int> partner(N, -1);
+  for (int k = 0; k < N; ++k) {
+    const int v = order[k];
+    int ids[14];
+    const int n = g.nbrs(v, ids);
+    int roots[14], nr = 0;
+    for (int j = 0; j < n; ++j) {
+      const int u = ids[j];
+      if (pos[u] >= k) continue;
+      const int r = find(u);
+      bool dup = false;
+      for (int q = 0; q < nr; ++q) dup |= roots[q] == r;
+      if (!dup) roots[nr++] = r;
+    }
+    if (nr == 0) {
+      parent[v] = v;
+      eldest[v] = v;
+      ext.push_back(v);
+      continue;
+    }
+    int keep = roots[0];  // the component whose extremum came first survives
+    for (int q = 1; q < nr; ++q)
+      if (pos[eldest[roots[q]]] < pos[eldest[keep]]) keep = roots[q];
+    for (int q = 0; q < nr; ++q)
+      if (roots[q] != keep) {
+        partner[eldest[roots[q]]] = v;
+        parent[roots[q]] = keep;
+      }
+    parent[v] = keep;
+  }
+  // Ranks: ascending in the tree's order = reverse of the processing order.
+  out.clear();
+  const int opposite = order[N - 1];
+  for (int i = (int)ext.size() - 1; i >= 0; --i) {
+    const int e = ext[i];
+    out.push_back(i == 0 ? opposite : partner[e]);
+    out.push_back(e);
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+// Persistence pairs of a field (see elder_pairs): 2 ints per maximum into
+// max_pairs and per minimum into min_pairs; returns 0 and the counts, or -1
+// on bad arguments, -3 when a buffer (caps in ints) is too small.
+int oracle_persistence_pairs(const void* f, int dtype, int W, int H, int D, int32_t* max_pairs,
+                             long long max_cap, int32_t* min_pairs, long long min_cap,
+                             long long* n_max, long long* n_min) {
+  if (!dims_ok(W, H, D) || !f) return -1;
+  Grid g{W, H, D, W * H * D};
+  std::vector<int> mx, mn;
+  if (dtype == 0) {
+    elder_pairs((const float*)f, g, true, mx);
+    elder_pairs((const float*)f, g, false, mn);
+  } else {
+    elder_pairs((const double*)f, g, true, mx);
+    elder_pairs((const double*)f, g, false, mn);
+  }
+  *n_max = (long long)mx.size() / 2;
+  *n_min = (long long)mn.size() / 2;
+  if ((long long)mx.size() > max_cap || (long long)mn.size() > min_cap) return -3;
+  std::memcpy(max_pairs, mx.data(), mx.size() * 4);
+  std::memcpy(min_pairs, mn.data(), mn.size() * 4);
+  return 0;
+}
 
 // Threads of the dense passes (detection, manifolds, rows); results do not
 // depend on it.

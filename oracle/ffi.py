@@ -63,6 +63,10 @@ def lib():
         L.oracle_roots.argtypes = [vp, i32, i32, i32, i32, vp, vp]
         L.oracle_correct.argtypes = [vp, vp, i32, i32, i32, i32,
                                      ctypes.POINTER(Params), ctypes.POINTER(Report), vp, i32, vp]
+        L.oracle_persistence_pairs.argtypes = [vp, i32, i32, i32, i32, vp, ctypes.c_longlong,
+                                               vp, ctypes.c_longlong,
+                                               ctypes.POINTER(ctypes.c_longlong),
+                                               ctypes.POINTER(ctypes.c_longlong)]
         L.oracle_encode.argtypes = [vp, vp, vp, vp, i32, ctypes.c_longlong, ctypes.c_double,
                                     i32, i32, vp, ctypes.c_longlong, vp, ctypes.c_longlong,
                                     ctypes.POINTER(EditReport)]
@@ -168,3 +172,20 @@ def encode(f: np.ndarray, decp0: np.ndarray, fixed: np.ndarray, counter, bound: 
     rep = dict(index_bytes=r.index_bytes, edit_bytes=r.edit_bytes, edited=r.edited,
                n_edits=r.n_edits, psnr_before=r.psnr_before, psnr_after=r.psnr_after)
     return index[:r.index_bytes].copy(), edits[:r.n_edits].copy(), rep
+
+
+def persistence_pairs(f: np.ndarray):
+    """Elder-rule persistence pairs: (max pairs (n, 2), min pairs (m, 2)) of
+    (partner vertex, extremum vertex), extrema by rank."""
+    f = np.ascontiguousarray(f)
+    w, h, d = _dims(f)
+    cap = 2 * f.size
+    mx = np.zeros(cap, np.int32)
+    mn = np.zeros(cap, np.int32)
+    nx, nn = ctypes.c_longlong(), ctypes.c_longlong()
+    rc = lib().oracle_persistence_pairs(f.ctypes.data, _dtype_code(f), w, h, d, mx.ctypes.data,
+                                        cap, mn.ctypes.data, cap, ctypes.byref(nx),
+                                        ctypes.byref(nn))
+    if rc != 0:
+        raise ValueError(f"oracle_persistence_pairs returned {rc}")
+    return mx[:2 * nx.value].reshape(-1, 2), mn[:2 * nn.value].reshape(-1, 2)
