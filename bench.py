@@ -381,9 +381,16 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_forms:
         edit_stream = measure_edit_stream(ctx, f, g, g0, field, stream, args.no_cpu_baseline)
 
+    # Topology check of the corrected field: merge-tree persistence pairs of
+    # the original and the corrected field on the GPU, beside the oracle's
+    # union-find on a crop.
+    topology = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        topology = measure_topology(ctx, f, g, g0, field, stream, args)
+
     forms = None
     if not args.no_forms and world == 1:
-        b = measure_batched(local, 2, 1)
+        b = measure_batched(local, 2, 3)
         sv = measure_served(local, (100, 2000), n_max=48, seconds=0.5)
         forms = {"batched": {"workload": "mixed64", "fields_per_s": b["batched"]["fields_per_s"],
                              "plain_loop_fields_per_s": b["plain_loop"]["fields_per_s"],
@@ -407,7 +414,7 @@ def run_ours(args, world, rank, local):
                 "dtype": dtype_name(field), "data": "synthetic (seeded generator, no dataset)",
                 "config": config_of(args, field), "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "forms": forms,
-                "edit_stream": edit_stream,
+                "edit_stream": edit_stream, "topology": topology,
                 "rounds": {"outer_iters": r0.outer_iters, "cloop_rounds": r0.cloop_rounds,
                            "manifold_rounds": r0.manifold_rounds,
                            "manifold_reused": r0.manifold_reused, "status": r0.status,
@@ -478,6 +485,39 @@ def measure_edit_stream(ctx, f, g, g0, field, stream, skip_cpu):
                    edit_type=PARAMS["edit_type"])
         out["cpu_encode_ms"] = 1e3 * (time.perf_counter() - t0)
         out["cpu_encode_cores"] = 1
+    return out
+
+
+def measure_topology(ctx, f, g, g0, field, stream, args):
+    import torch
+    g.copy_(g0)
+    ctx.correct_device(f, g, field.eb, stream=stream.cuda_stream, **PARAMS)
+    torch.cuda.synchronize()
+    ctx.persistence_pairs(f)  # warm
+    best = None
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.persistence_pairs(f)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    rep = ctx.compare_topology(f, g)
+    out = {"entry_point": "extremz_persistence_pairs", "gpu_ms_per_field": 1e3 * best,
+           "note": "wall time of one call (analysis pass, sorts, pairing rounds, copy to host)",
+           "split": rep["split"], "join": rep["join"]}
+    if not args.no_cpu_baseline:
+        from oracle import ffi
+        fc, _ = crop(field, args.cpu_edge)
+        t0 = time.perf_counter()
+        ffi.persistence_pairs(fc)
+        out["cpu_union_find_ms"] = 1e3 * (time.perf_counter() - t0)
+        out["cpu_sample"] = f"leading {args.cpu_edge}^3 crop of the original field, 1 thread"
+        tc = torch.from_numpy(np.ascontiguousarray(fc)).to(f.device)
+        t0 = time.perf_counter()
+        ctx.persistence_pairs(tc)
+        torch.cuda.synchronize()
+        out["gpu_ms_same_crop"] = 1e3 * (time.perf_counter() - t0)
     return out
 
 

@@ -602,7 +602,7 @@ class BatchEngine {
     issued_ = false;
     // A tick whose launches repeat an earlier tick's exactly (kernels, launch
     // shapes and arguments; per-job state is read from device memory) runs as
-    // one CUDA graph: recorded, captured the second time its signature is
+    // one CUDA graph: recorded, captured the third time its signature is
     // seen, replayed from then on.  Ticks that allocate (setup) or time
     // kernels launch directly.
     bool graph = graphs_on_ && !profile_;
@@ -694,6 +694,10 @@ class BatchEngine {
   unsigned long long graph_clock_ = 0;
   long long graph_replays_ = 0, graph_captures_ = 0;
   static constexpr size_t kMaxGraphs = 256;
+  // A signature is captured at its third sighting: ticks of a single
+  // correction repeat many times, while a batch's changing selections often
+  // repeat once or twice, where a capture would not pay for itself.
+  static constexpr int kCaptureAt = 3;
   cudaStream_t cap_ = nullptr;  // capture stream
   cudaMemPool_t pool_mem_ = nullptr;
   bool ready_ = false, borrowed_ = false, issued_ = false;
@@ -771,7 +775,7 @@ class BatchEngine {
     cap_ = nullptr;
   }
 
-  // Launches the recorded tick: replays its graph, captures it on the second
+  // Launches the recorded tick: replays its graph, captures it on the third
   // sighting of its signature, or launches directly.
   int run_recorded() {
     ++graph_clock_;
@@ -790,7 +794,7 @@ class BatchEngine {
       return EXTREMZ_OK;
     }
     if (seen_.size() > 4 * kMaxGraphs) seen_.clear();
-    if (++seen_[sig_] < 2) {
+    if (++seen_[sig_] < kCaptureAt) {
       run_direct();
       return EXTREMZ_OK;
     }

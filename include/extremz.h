@@ -137,7 +137,7 @@ void extremz_ctx_destroy(extremz_ctx* ctx);
  * (NULL = legacy default stream).  trace (host, optional) receives records of
  * four int32 (phase, counter, counter, counter) for debugging; trace_cap is its
  * length in int32.  The launches of one step of the control flow ("tick") that
- * repeat an earlier step's exactly run as one CUDA graph, captured the second
+ * repeat an earlier step's exactly run as one CUDA graph, captured the third
  * time they occur and kept in the context (not when the caller's stream is
  * itself being captured, nor with EXTREMZ_FLAG_PROFILE).
  * Replaces: main() of src/ExtreM_cuda.cu:5508-5997 (the correction proper, with
