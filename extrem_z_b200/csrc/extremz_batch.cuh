@@ -106,6 +106,7 @@ constexpr long long job_bytes_voxels(long long n, long long ksz) {
          + 4 * arr_bytes(n, 4)                                      // cand(_next), flagged(1)
          + arr_bytes(n, 4) + arr_bytes(n, 1)                        // cand_j, mis
          + 2 * arr_bytes(n, 4)                                      // pdd, pda
+         + arr_bytes(n, 4) + arr_bytes(n, 1)                        // vstamp, dirtyv
          + arr_bytes(n, 1)                                          // tile marks (<= n tiles)
          + arr_bytes(4 * ((n + kCpBlock - 1) / kCpBlock), 4)        // CP block counts
          + 4096;
@@ -116,6 +117,7 @@ constexpr long long job_bytes_cps(long long ns2, long long ns1, long long nmax, 
   return arr_bytes(ns2, 4) + arr_bytes(ns1, 4) + arr_bytes(nmax, 4) + arr_bytes(nmin, 4)
          + arr_bytes(ns2 * kRowStride, 4) + arr_bytes(ns2 * 2, 4) + arr_bytes(ns2, 1)
          + arr_bytes(ns1 * kRowStride, 4) + arr_bytes(ns1 * 2, 4) + arr_bytes(ns1, 1)
+         + arr_bytes(ns2, 1) + arr_bytes(ns1, 1)                    // seed bits
          + 4 * arr_bytes(nmax, 4) + 4 * arr_bytes(nmin, 4)
          + arr_bytes(nmax > nmin ? nmax : nmin, ksz) + arr_bytes(nmax > nmin ? nmax : nmin, 4)
          + arr_bytes(8, 8) + 4096;
@@ -338,6 +340,8 @@ class BatchEngine {
     J.mis = A.take<uint8_t>(N);
     J.pdd = A.take<int>(N);
     J.pda = A.take<int>(N);
+    J.vstamp = A.take<int>(N);
+    J.dirtyv = A.take<uint8_t>(N);
     jh.nb = (N + kCpBlock - 1) / kCpBlock;
     jh.bcount = A.take<int>(4ll * jh.nb);
     J.cpoff = jh.bcount;
@@ -1062,6 +1066,8 @@ class BatchEngine {
     J.orow1 = A.take<int>((long long)ns1 * kRowStride);
     J.drow1 = A.take<int>((long long)ns1 * 2);
     J.ocnt1 = A.take<uint8_t>(ns1);
+    J.has2 = A.take<uint8_t>(ns2);
+    J.has1 = A.take<uint8_t>(ns1);
     J.largest = A.take<int>(nmax);
     J.first1 = A.take<int>(nmax);
     J.flag2 = A.take<int>(nmax);
@@ -1117,6 +1123,7 @@ class BatchEngine {
     EZ_CHECK(cudaMemsetAsync(J.taken1, 0, (size_t)N * 4, st_));
     EZ_CHECK(cudaMemsetAsync(J.dstamp, 0, (size_t)N * 4, st_));
     EZ_CHECK(cudaMemsetAsync(J.rstamp, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.vstamp, 0, (size_t)N * 4, st_));
     EZ_CHECK(cudaMemcpyAsync(jobs_dev_ + slot, &J, sizeof(J), cudaMemcpyHostToDevice, st_));
     return EXTREMZ_OK;
   }

@@ -47,6 +47,9 @@ struct Job {
   int* cand_j;        // join-side candidates, produced with the split side's
   int* flagged; int* flagged1;  // flagged neighbours (split / join)
   uint8_t* mis;       // per vertex: 1 if dds != ds, 2 if das != as
+  int* vstamp;        // per vertex: C_MFEPOCH when its value last changed
+  uint8_t* dirtyv;    // per vertex: an input of its saddle rows changed this round
+  uint8_t* has2; uint8_t* has1;  // per saddle row: its wrong-neighbour seed bit
   int* cpoff;         // per list (2-saddles, 1-saddles, maxima, minima) and
                       // 1024-id block: offset of the block's first entry
   int* pdd; int* pda; // decompressed steepest pointers, tile-compressed (k_direction)
@@ -93,6 +96,7 @@ enum Ctr : int {
   C_MFSKIP,    // this manifold round repeats the last one's inputs: kernels skip it
   C_MFDONE,    // a manifold round has run
   C_MFREUSED,  // manifold rounds skipped so far
+  C_MFEPOCH,   // manifold rounds computed so far (value-change stamps)
   // Per-job epochs and stamps, advanced by k_ctl so that one launch can serve
   // jobs at different points of their correction.
   C_DEPOCH,    // dirty-list epoch (k_apply)
@@ -557,7 +561,7 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
 // to original 2-saddles, the only places they are read).  Iterations are
 // capped; hitting the cap sets the error word instead of spinning.  On the
 // decompressed field it also writes each vertex's label-mismatch bits
-// (Job::mis) for the saddle pass.
+// and changed-input bytes for the saddle pass.
 template <class T, bool kDec>
 __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
                                                const __grid_constant__ Sel sel) {
@@ -570,12 +574,29 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
   const int* b = kDec ? J.pda : J.as;
   int* ra = kDec ? J.dds : J.ds;
   int* rb = kDec ? J.das : J.as;
+  const int epoch = J.ctr[C_MFEPOCH];
+  // Descriptor fields in registers: stores below could alias the descriptor.
+  const int* __restrict__ vstamp = J.vstamp;
+  const int* __restrict__ ods = J.ds;
+  const int* __restrict__ oas = J.as;
+  uint8_t* __restrict__ dirtyv = J.dirtyv;
+  uint8_t* __restrict__ mis = J.mis;
   int* err = J.ctr + C_ERROR;
   const int N = J.dim.N;
   const int cap_j = J.iter_cap;
   const int stride = gridDim.x * blockDim.x;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
     int u1 = a[v], u2 = b[v];
+    // Decompressed field: this vertex's old labels, original roots and
+    // change stamp, loaded while the chains are followed.
+    int o1 = 0, o2 = 0, r1 = 0, r2 = 0, s0 = 0;
+    if constexpr (kDec) {
+      o1 = ra[v];
+      o2 = rb[v];
+      r1 = ods[v];
+      r2 = oas[v];
+      s0 = vstamp[v];
+    }
     bool d1 = false, d2 = false;
     int it = 0;
     for (; it < cap_j && !(d1 && d2); ++it) {
@@ -591,10 +612,19 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
       }
     }
     if (it == cap_j) atomicOr(err, kErrJump);
+    if constexpr (kDec) {
+      // For the saddle pass: label-mismatch bits, and whether an input of the
+      // rows this vertex feeds changed since the previous computed round (its
+      // value, either label, or the value of either label's root).  Stamps
+      // start at 0, so the first round marks every vertex.
+      const int since = epoch - 1;
+      const int s1 = vstamp[u1], s2 = vstamp[u2];
+      dirtyv[v] = (uint8_t)((o1 != u1) | (o2 != u2) | (s0 >= since) | (s1 >= since) |
+                            (s2 >= since));
+      mis[v] = (uint8_t)((u1 != r1) | (u2 != r2) << 1);
+    }
     ra[v] = u1;
     rb[v] = u2;
-    if constexpr (kDec)  // label-mismatch bits for the saddle pass
-      J.mis[v] = (uint8_t)((u1 != J.ds[v]) | (u2 != J.as[v]) << 1);
   }
   }
 }
@@ -912,6 +942,7 @@ __global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, 
     J.g[v] = gv;
     if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0)) {
       J.ctr[C_CHANGED] = 1;
+      J.vstamp[v] = J.ctr[C_MFEPOCH];
       int x, y, z;
       coords(v, J.dim, x, y, z);
       mark_tiles(J.tdirty, J.dim, x, y, z);
@@ -1056,8 +1087,24 @@ __device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
   return (mb >> (kSplit ? 0 : 1)) & 1;
 }
 
+// Whether any input of saddle s's rows changed since the previous computed
+// round: the changed-input byte of s or of a neighbour (see k_jump2).
+template <class T>
+__device__ __forceinline__ bool saddle_inputs_changed(const Job<T>& J, int s) {
+  const Dims g = J.dim;
+  int x, y, z;
+  coords(s, g, x, y, z);
+  const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
+  int d = J.dirtyv[s];
+#pragma unroll
+  for (int k = 0; k < kNumDirs; ++k)
+    if (valid >> k & 1) d |= J.dirtyv[s + dir_x(k) + dir_y(k) * g.W + dir_z(k) * g.W * g.H];
+  return d != 0;
+}
+
 // Fused pass over the original saddles after a manifold round, both sides in
-// one grid.  A block takes a chunk of the id space (pass_chunk blocks of 1024
+// one grid.  A saddle whose inputs did not change since the previous computed
+// round keeps its row slots and reuses its stored seed bit.  A block takes a chunk of the id space (pass_chunk blocks of 1024
 // ids) and the entries of both saddle lists in it, so that the two sides read
 // the same neighbourhoods together:
 //  * decompressed row slots.  The reference rewrites row i (findAscPaths /
@@ -1094,12 +1141,14 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
         bool has = false;
         int s = 0;
         if (k < n) {
-          if (split) {
-            s = J.sad2[a2 + k];
-            has = saddle_row<T, true>(J, a2 + k, s);
-          } else {
-            s = J.sad1[a1 + k - n2];
-            has = saddle_row<T, false>(J, a1 + k - n2, s);
+          const int i = split ? a2 + k : a1 + k - n2;
+          s = split ? J.sad2[i] : J.sad1[i];
+          uint8_t* hb = split ? J.has2 : J.has1;
+          if (saddle_inputs_changed(J, s)) {
+            has = split ? saddle_row<T, true>(J, i, s) : saddle_row<T, false>(J, i, s);
+            hb[i] = (uint8_t)has;
+          } else {  // rows and seed bit as computed in an earlier round
+            has = hb[i] != 0;
           }
         }
         const int slot2 = warp_append(J.ctr + C_CAND, has && split, 0xffffffffu);
@@ -1566,6 +1615,7 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
       c[C_CHANGED] = 0;
       c[C_MFDONE] = 1;
       if (c[C_MFSKIP]) break;
+      c[C_MFEPOCH] += 1;
       c[C_WNSTAMP] += 1;  // next flag stamp; flagged and candidate counts to zero
       c[C_NFC] = c[C_NFC1] = 0;
       c[C_CAND] = c[C_CANDJ] = c[C_CAND_NEXT] = 0;
