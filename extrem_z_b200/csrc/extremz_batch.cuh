@@ -106,7 +106,7 @@ constexpr long long job_bytes_voxels(long long n, long long ksz) {
          + 4 * arr_bytes(n, 4)                                      // cand(_next), flagged(1)
          + arr_bytes(n, 4) + arr_bytes(n, 1)                        // cand_j, mis
          + 2 * arr_bytes(n, 4)                                      // pdd, pda
-         + arr_bytes(n, 4) + arr_bytes(n, 1)                        // vstamp, dirtyv
+         + arr_bytes((n + 31) / 32, 4) + arr_bytes(n, 1)            // change bitset, dirtyv
          + arr_bytes(n, 1)                                          // tile marks (<= n tiles)
          + arr_bytes(4 * ((n + kCpBlock - 1) / kCpBlock), 4)        // CP block counts
          + 4096;
@@ -340,7 +340,7 @@ class BatchEngine {
     J.mis = A.take<uint8_t>(N);
     J.pdd = A.take<int>(N);
     J.pda = A.take<int>(N);
-    J.vstamp = A.take<int>(N);
+    J.vchg = A.take<unsigned>((N + 31) / 32);
     J.dirtyv = A.take<uint8_t>(N);
     jh.nb = (N + kCpBlock - 1) / kCpBlock;
     jh.bcount = A.take<int>(4ll * jh.nb);
@@ -938,6 +938,7 @@ class BatchEngine {
         ctl(s, OP_MF_BEGIN);
         launch(K_DIRECTION, k_direction<T, true>, st.off[st.n], 256, jobs, st);
         launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_clear_changed<T>, grid_, 256, jobs, s);
         launch(K_ROWS, k_saddle_pass<T>, grid_, 256, jobs, s);
         wn_rounds<true>(s);   // its completion brings in the join side's list
         wn_rounds<false>(s);
@@ -1123,7 +1124,7 @@ class BatchEngine {
     EZ_CHECK(cudaMemsetAsync(J.taken1, 0, (size_t)N * 4, st_));
     EZ_CHECK(cudaMemsetAsync(J.dstamp, 0, (size_t)N * 4, st_));
     EZ_CHECK(cudaMemsetAsync(J.rstamp, 0, (size_t)N * 4, st_));
-    EZ_CHECK(cudaMemsetAsync(J.vstamp, 0, (size_t)N * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.vchg, 0xff, (size_t)((N + 31) / 32) * 4, st_));
     EZ_CHECK(cudaMemcpyAsync(jobs_dev_ + slot, &J, sizeof(J), cudaMemcpyHostToDevice, st_));
     return EXTREMZ_OK;
   }

@@ -47,7 +47,7 @@ struct Job {
   int* cand_j;        // join-side candidates, produced with the split side's
   int* flagged; int* flagged1;  // flagged neighbours (split / join)
   uint8_t* mis;       // per vertex: 1 if dds != ds, 2 if das != as
-  int* vstamp;        // per vertex: C_MFEPOCH when its value last changed
+  unsigned* vchg;     // bitset: vertices whose value changed since the last computed round
   uint8_t* dirtyv;    // per vertex: an input of its saddle rows changed this round
   uint8_t* has2; uint8_t* has1;  // per saddle row: its wrong-neighbour seed bit
   int* cpoff;         // per list (2-saddles, 1-saddles, maxima, minima) and
@@ -96,7 +96,6 @@ enum Ctr : int {
   C_MFSKIP,    // this manifold round repeats the last one's inputs: kernels skip it
   C_MFDONE,    // a manifold round has run
   C_MFREUSED,  // manifold rounds skipped so far
-  C_MFEPOCH,   // manifold rounds computed so far (value-change stamps)
   // Per-job epochs and stamps, advanced by k_ctl so that one launch can serve
   // jobs at different points of their correction.
   C_DEPOCH,    // dirty-list epoch (k_apply)
@@ -574,9 +573,8 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
   const int* b = kDec ? J.pda : J.as;
   int* ra = kDec ? J.dds : J.ds;
   int* rb = kDec ? J.das : J.as;
-  const int epoch = J.ctr[C_MFEPOCH];
   // Descriptor fields in registers: stores below could alias the descriptor.
-  const int* __restrict__ vstamp = J.vstamp;
+  const unsigned* __restrict__ vchg = J.vchg;
   const int* __restrict__ ods = J.ds;
   const int* __restrict__ oas = J.as;
   uint8_t* __restrict__ dirtyv = J.dirtyv;
@@ -589,13 +587,14 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
     int u1 = a[v], u2 = b[v];
     // Decompressed field: this vertex's old labels, original roots and
     // change stamp, loaded while the chains are followed.
-    int o1 = 0, o2 = 0, r1 = 0, r2 = 0, s0 = 0;
+    int o1 = 0, o2 = 0, r1 = 0, r2 = 0;
+    unsigned c0 = 0;
     if constexpr (kDec) {
       o1 = ra[v];
       o2 = rb[v];
       r1 = ods[v];
       r2 = oas[v];
-      s0 = vstamp[v];
+      c0 = vchg[v >> 5] >> (v & 31);
     }
     bool d1 = false, d2 = false;
     int it = 0;
@@ -615,12 +614,10 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
     if constexpr (kDec) {
       // For the saddle pass: label-mismatch bits, and whether an input of the
       // rows this vertex feeds changed since the previous computed round (its
-      // value, either label, or the value of either label's root).  Stamps
-      // start at 0, so the first round marks every vertex.
-      const int since = epoch - 1;
-      const int s1 = vstamp[u1], s2 = vstamp[u2];
-      dirtyv[v] = (uint8_t)((o1 != u1) | (o2 != u2) | (s0 >= since) | (s1 >= since) |
-                            (s2 >= since));
+      // value, either label, or the value of either label's root).  The
+      // change bitset starts full, so the first round marks every vertex.
+      const unsigned c1 = vchg[u1 >> 5] >> (u1 & 31), c2 = vchg[u2 >> 5] >> (u2 & 31);
+      dirtyv[v] = (uint8_t)((o1 != u1) | (o2 != u2) | ((c0 | c1 | c2) & 1u));
       mis[v] = (uint8_t)((u1 != r1) | (u2 != r2) << 1);
     }
     ra[v] = u1;
@@ -942,7 +939,7 @@ __global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, 
     J.g[v] = gv;
     if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0)) {
       J.ctr[C_CHANGED] = 1;
-      J.vstamp[v] = J.ctr[C_MFEPOCH];
+      atomicOr(J.vchg + (v >> 5), 1u << (v & 31));
       int x, y, z;
       coords(v, J.dim, x, y, z);
       mark_tiles(J.tdirty, J.dim, x, y, z);
@@ -1085,6 +1082,18 @@ __device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
     }
   }
   return (mb >> (kSplit ? 0 : 1)) & 1;
+}
+
+// Clears the value-change bitset after a computed round's jump has read it.
+template <class T>
+__global__ void k_clear_changed(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+    const Job<T>& J = jobs[sel.idx[jk]];
+    if (J.ctr[C_MFSKIP]) continue;
+    const int nw = (J.dim.N + 31) >> 5;
+    const int stride = gridDim.x * blockDim.x;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += stride) J.vchg[w] = 0u;
+  }
 }
 
 // Whether any input of saddle s's rows changed since the previous computed
@@ -1615,7 +1624,6 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
       c[C_CHANGED] = 0;
       c[C_MFDONE] = 1;
       if (c[C_MFSKIP]) break;
-      c[C_MFEPOCH] += 1;
       c[C_WNSTAMP] += 1;  // next flag stamp; flagged and candidate counts to zero
       c[C_NFC] = c[C_NFC1] = 0;
       c[C_CAND] = c[C_CANDJ] = c[C_CAND_NEXT] = 0;
