@@ -750,37 +750,56 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
                                               int ns_slot, int* __restrict__ rows) {
   const int ns = J.ctr[ns_slot];
   const int stride = gridDim.x * blockDim.x;
+  const Dims g = J.dim;
+  const int WH = g.W * g.H;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
     const int s = sad[i];
-    int ids[kNumDirs];
-    const int n = neighbours(s, J.dim, ids, nullptr);
+    int x, y, z;
+    coords(s, g, x, y, z);
+    const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
     const T sv = a[s];
+    // Neighbour values, then the side's labels, then their values: three
+    // batches of independent loads; the sort below compares cached values.
+    T val[kNumDirs];
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d)
+      val[d] = (valid >> d & 1) ? a[s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH] : T(0);
+    int lb[kNumDirs];
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d) {
+      const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+      const bool side = (valid >> d & 1) && (kAsc ? above(val[d], r, sv, s) : below(val[d], r, sv, s));
+      lb[d] = side ? lab[r] : -1;
+    }
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d) val[d] = lb[d] >= 0 ? a[lb[d]] : T(0);
     int row[kNumDirs];
+    T rv[kNumDirs];
     int cnt = 0;
-    for (int j = 0; j < n; ++j) {
-      const int r = ids[j];
-      const T rv = a[r];
-      if (kAsc) {
-        const int m = lab[r];
-        if (above(rv, r, sv, s) && tabs(T(a[m] - sv)) >= J.thr) row[cnt++] = m;
-      } else {
-        if (below(rv, r, sv, s)) row[cnt++] = lab[r];
-      }
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d) {
+      if (lb[d] < 0) continue;
+      if (kAsc && !(tabs(T(val[d] - sv)) >= J.thr)) continue;
+      row[cnt] = lb[d];
+      rv[cnt] = val[d];
+      ++cnt;
     }
     // Insertion sort: descending (insertionSort :1795-1811) for ascending
     // rows, ascending (reversed_insertionSort :1813-1829) for descending rows.
     for (int p = 1; p < cnt; ++p) {
       const int key = row[p];
-      const T kv = a[key];
+      const T kv = rv[p];
       int q = p - 1;
       while (q >= 0) {
         const int rq = row[q];
-        const bool move = kAsc ? below(a[rq], rq, kv, key) : above(a[rq], rq, kv, key);
+        const bool move = kAsc ? below(rv[q], rq, kv, key) : above(rv[q], rq, kv, key);
         if (!move) break;
         row[q + 1] = rq;
+        rv[q + 1] = rv[q];
         --q;
       }
       row[q + 1] = key;
+      rv[q + 1] = kv;
     }
     int* out = rows + (long long)i * kRowStride;
     for (int p = 0; p < cnt; ++p) out[p] = row[p];
