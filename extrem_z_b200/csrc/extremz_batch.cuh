@@ -157,6 +157,7 @@ struct JobHost {
   int trace_cap = 0, trace_len = 0;
   std::vector<int> pending;  // trace phases to emit once the tick's counters are back
   int blocks_per_sm = 8;      // grid-stride kernels' blocks per SM (tuning knob)
+  long long applied_tick = -1;  // last tick that issued edits for this job
   long long tag = 0;
 
   void emit(int phase, int a = 0, int b = 0, int c3 = 0) {
@@ -604,6 +605,7 @@ class BatchEngine {
   // their ticks overlap on the device.
   int tick_issue() {
     issued_ = false;
+    ++tick_id_;
     // A tick whose launches repeat an earlier tick's exactly (kernels, launch
     // shapes and arguments; per-job state is read from device memory) runs as
     // one CUDA graph: recorded, captured the third time its signature is
@@ -705,6 +707,7 @@ class BatchEngine {
   cudaStream_t cap_ = nullptr;  // capture stream
   cudaMemPool_t pool_mem_ = nullptr;
   bool ready_ = false, borrowed_ = false, issued_ = false;
+  long long tick_id_ = 0;
   int grid_ = 1184;  // grid of the grid-stride kernels for the phase being issued
   int sms_ = 148;
   DeviceTables tb_{};
@@ -889,6 +892,9 @@ class BatchEngine {
     int bps = 1;  // jobs share launches: the largest knob of the selection
     for (int i : sel) bps = std::max(bps, slots_[i].blocks_per_sm);
     grid_ = sms_ * bps;
+    if (ph == PC_CL_ROUND || ph == PC_RLOOPS || ph == PC_SLOOPS || ph == PC_SADDLE ||
+        ph == PC_SLOOPS_J || ph == PC_SADDLE_J || ph == PC_FINAL_JOIN)
+      for (int i : sel) slots_[i].applied_tick = tick_id_;  // phases that apply edits
     const Sel s = make_sel(sel, false);
     const Sel st = make_sel(sel, true);
     const Job<T>* jobs = jobs_dev_;
@@ -934,19 +940,36 @@ class BatchEngine {
         launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
         for (int i : sel) slots_[i].pc = PC_MANIFOLD;
         return EXTREMZ_OK;
-      case PC_MANIFOLD:
-        ctl(s, OP_MF_BEGIN);
-        launch(K_DIRECTION, k_direction<T, true>, st.off[st.n], 256, jobs, st);
-        launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, s);
-        launch(K_OTHER, k_clear_changed<T>, grid_, 256, jobs, s);
-        launch(K_ROWS, k_saddle_pass<T>, grid_, 256, jobs, s);
-        wn_rounds<true>(s);   // its completion brings in the join side's list
-        wn_rounds<false>(s);
+      case PC_MANIFOLD: {
+        // Jobs known on the host to have no value change since their last
+        // manifold round began (no edit in the counters of the last tick, none
+        // issued in this one) get only the round's bookkeeping; their kernels
+        // would return at once.  The others run the round (whose kernels
+        // check again on the device).
+        std::vector<int> quiet, busy;
+        for (int i : sel) {
+          const JobHost<T>& j = slots_[i];
+          const bool known_clean =
+              j.manifold_rounds > 0 && j.applied_tick != tick_id_ && h(i, C_CHANGED) == 0;
+          (known_clean ? quiet : busy).push_back(i);
+        }
+        if (!quiet.empty()) ctl(make_sel(quiet, false), OP_MF_BEGIN);
+        if (!busy.empty()) {
+          const Sel bs = make_sel(busy, false), bt = make_sel(busy, true);
+          ctl(bs, OP_MF_BEGIN);
+          launch(K_DIRECTION, k_direction<T, true>, bt.off[bt.n], 256, jobs, bt);
+          launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, bs);
+          launch(K_OTHER, k_clear_changed<T>, grid_, 256, jobs, bs);
+          launch(K_ROWS, k_saddle_pass<T>, grid_, 256, jobs, bs);
+          wn_rounds<true>(bs);  // its completion brings in the join side's list
+          wn_rounds<false>(bs);
+        }
         for (int i : sel) {
           slots_[i].manifold_rounds++;
           slots_[i].waiting = true;
         }
         return EXTREMZ_OK;
+      }
       case PC_SLOOPS:
         ctl(s, OP_SLOOPS_BEGIN);
         launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs, s);
