@@ -62,24 +62,26 @@ SERVE_RESERVE_BYTES = 48 << 30
 PARAMS = dict(q=4, edit_type=1, thr=0.0, max_outer=1000, max_cloop_rounds=100000,
               final_join=True)
 
-# Dominant kernel: the saddle pass (k_saddle_pass, kernel class "rows"), one
-# launch per manifold round.  Algorithmic bytes of a launch that computes:
-# every voxel's decompressed value (S) and both labels (8) plus its label-
-# mismatch byte (1), and per original saddle (2-saddles + 1-saddles) its list
-# entry (4), original row count (1) and two row slots (8).  Launches of
-# rounds whose inputs were unchanged return at once and are not counted.
-DOMINANT = "rows"
-DOMINANT_KERNEL = "k_saddle_pass"
+# Dominant kernel: the pointer jumping of the decompressed labels (k_jump2,
+# kernel class "jump"), one launch per computed manifold round, over every
+# voxel.  Algorithmic bytes per launch: read the two tile-compressed pointers,
+# the two current labels and the two original roots (24 B) and the change bit;
+# write the two labels, the label-mismatch byte and the changed-input byte
+# (10 B): 34 B per voxel.  The hops along the chains are re-reads, not counted.
+# Launches of rounds whose inputs were unchanged return at once or are not
+# issued; they are not counted.
+DOMINANT = "jump"
+DOMINANT_KERNEL = "k_jump2"
 
 
-def dominant_bytes_per_launch(n: int, s: int, n_saddles: int) -> int:
-    return n * (s + 9) + n_saddles * 13
+def dominant_bytes_per_launch(n: int, s: int) -> int:
+    return 34 * n
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one computing
-# k_saddle_pass launch on the 256^3 fields, from one ncu capture each, by
-# value size (profiles/k_saddle_pass_256cube_f64.md); None where not captured.
-MEASURED_TRAFFIC_256 = {8: 345.6576e6 + 51.80928e6, 4: 258.10304e6 + 33.81376e6}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_jump2
+# launch on the decompressed 256^3 field, from one ncu capture each, by value
+# size (profiles/k_jump2_256cube_f64.md); None where not captured.
+MEASURED_TRAFFIC_256 = {8: 518.019072e6 + 150.010368e6, 4: 518.11072e6 + 150.620928e6}
 
 
 def measured_peaks():
@@ -334,8 +336,7 @@ def run_ours(args, world, rank, local):
     dom_ms = sum(r.prof_ms[DOMINANT] for r in reps)
     dom_n = sum(r.manifold_rounds - r.manifold_reused for r in reps)
     peak, peak_kind = measured_peaks()
-    n_saddles = reps[-1].cp_counts[0] + reps[-1].cp_counts[1]
-    per_launch = dominant_bytes_per_launch(n, s, n_saddles)
+    per_launch = dominant_bytes_per_launch(n, s)
     achieved = per_launch * dom_n / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
     traffic = MEASURED_TRAFFIC_256.get(s) if field.f.shape == (256, 256, 256) else None
     roofline = {"bound": "hbm", "kernel": DOMINANT_KERNEL, "achieved": achieved, "peak": peak,

@@ -901,8 +901,8 @@ class BatchEngine {
     switch (ph) {
       case PC_SETUP_A:
         launch(K_SETUP, k_classify<T, false>, st.off[st.n], 256, jobs, st);
-        launch(K_DIRECTION, k_direction<T, false>, st.off[st.n], 256, jobs, st);
-        launch(K_JUMP, k_jump2<T, false>, grid_, 256, jobs, s);
+        launch(K_SETUP, k_direction<T, false>, st.off[st.n], 256, jobs, st);
+        launch(K_SETUP, k_jump2<T, false>, grid_, 256, jobs, s);
         for (int i : sel) {
           JobHost<T>& j = slots_[i];
           launch(K_OTHER, k_cp_count, j.nb, kCpBlock, (const int8_t*)j.J.otype, j.J.dim.N, j.bcount);

@@ -90,11 +90,11 @@ typedef struct {
  * W * sizeof(value) is a multiple of 16 bytes). */
 #define EXTREMZ_FLAG_NO_TMA 2
 
-/* Kernel classes of extremz_report.prof_*: 0 setup (classification and rows of
- * the original field), 1 fused classification + mismatch detection, 2 steepest
- * directions, 3 pointer jumping, 4 proposals, 5 apply, 6 saddle pass
- * (decompressed rows and wrong-neighbour seeds), 7 wrong-neighbour
- * resolution, 8 path walks, 9 everything else. */
+/* Kernel classes of extremz_report.prof_*: 0 setup (classification, labels and
+ * rows of the original field), 1 fused classification + mismatch detection,
+ * 2 steepest directions and 3 pointer jumping of the decompressed field,
+ * 4 proposals, 5 apply, 6 saddle pass (decompressed rows and wrong-neighbour
+ * seeds), 7 wrong-neighbour resolution, 8 path walks, 9 everything else. */
 #define EXTREMZ_NUM_KCLASS 10
 
 /* Outcome of one correction. counters[] are the eleven host counters of the
