@@ -1,0 +1,53 @@
+"""Benchmark-size corrections checked through size-independent properties.
+
+At 256^3 the oracle would take minutes, so instead of byte equality these
+tests check what every correction must satisfy: every value within the
+bound (one ulp of rounding allowed, as the reference's f - bound snap can
+round), values only lowered, zero critical-point mismatch (same vertex types
+as the original) when the loop ends without the final join pass, all eleven
+loop counters at zero, and the same result for float32 through the host
+entry point as through the device entry point.
+"""
+
+import numpy as np
+import pytest
+
+from extrem_z_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _correct(fld, **kw):
+    import torch
+    from extrem_z_b200 import api
+    f = torch.from_numpy(fld.f).cuda()
+    g = torch.from_numpy(fld.decp.copy()).cuda()
+    rep, _ = api.context(0).correct_device(f, g, fld.eb, **kw)
+    torch.cuda.synchronize()
+    return g.cpu().numpy(), rep
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_plain256_invariants(dtype):
+    from oracle import ffi
+    fld = synth.plain_256(dtype)
+    out, rep = _correct(fld, final_join=False)
+    assert rep.status == 0 and rep.error_bits == 0
+    assert rep.counters == [0] * 11
+    f64, o64, d64 = (a.astype(np.float64) for a in (fld.f, out, fld.decp))
+    slack = fld.eb + np.spacing(np.abs(fld.f)).astype(np.float64)
+    assert np.all(np.abs(f64 - o64) <= slack)
+    assert np.all(o64 <= d64)                      # edits only lower values
+    t0, m0 = ffi.classify(fld.f)
+    t1, m1 = ffi.classify(out)
+    assert np.array_equal(t0, t1)                  # zero critical-point mismatch
+    assert rep.cp_counts[2] == int((t0 == 4).sum()) and rep.cp_counts[3] == int((t0 == 0).sum())
+
+
+def test_plain256_host_equals_device():
+    from extrem_z_b200 import api
+    fld = synth.plain_256(np.float32)
+    dev, _ = _correct(fld)
+    host = fld.decp.copy()
+    api.context(0).correct_host(fld.f, host, fld.eb)
+    assert np.array_equal(dev.view(np.uint8), host.view(np.uint8))
