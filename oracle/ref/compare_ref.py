@@ -7,7 +7,7 @@ whether the reference's runs agree with one another, how many voxels the
 reference's result differs from the oracle's in, and whether the library's
 result equals the oracle's byte for byte.
 
-    python oracle/ref/compare_ref.py [--runs 3]
+    python oracle/ref/compare_ref.py [--runs 3] [--timing]
 """
 
 from __future__ import annotations
@@ -43,13 +43,47 @@ CASES = [
 ]
 
 
+def timing():
+    """The reference's own timer ("whole time", src/ExtreM_cuda.cu:5020-6000: from
+    after getdata to after the final saddle_loops_join, its allocations
+    included) beside the library's device time on the 256^3 float64 field."""
+    import re
+    import torch
+    from extrem_z_b200 import api
+    fld = synth.plain_256(np.float64)
+    _, stdout, wall = run_ref.run(fld.f, fld.decp, fld.rel, ffi.lut(), q=4, edit_type=1,
+                                  timeout=900)
+    m = re.search(r"whole time:([0-9.eE+-]+)", stdout)
+    ref_s = float(m.group(1)) if m else float("nan")
+    ctx = api.Context(0)
+    f = torch.from_numpy(fld.f).cuda()
+    g0 = torch.from_numpy(fld.decp).cuda()
+    best = None
+    for _ in range(4):
+        g = g0.clone()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.correct_device(f, g, fld.eb, q=4, edit_type=1)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    print(f"| 256^3 float64 | reference GPU {ref_s * 1e3:.1f} ms (own timer; process wall "
+          f"{wall:.2f} s) | library {best:.2f} ms | {ref_s * 1e3 / best:.0f}x |")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--runs", type=int, default=3)
+    ap.add_argument("--timing", action="store_true",
+                    help="time the reference binary and the library on the 256^3 field")
     args = ap.parse_args()
     if not run_ref.available():
         print("reference binary absent (oracle/_ref/ref_gpu)")
         return 1
+    if args.timing:
+        return timing()
     import torch
     from extrem_z_b200 import api
     lut = ffi.lut()
