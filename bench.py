@@ -355,16 +355,20 @@ def run_ours(args, world, rank, local):
     ctx.correct_host(hf, hg, field.eb, stream=stream.cuda_stream, **PARAMS)
     e2e_s = 0.0
     e2e_steps = max(1, min(args.steps, 5))
+    back = 0
     barrier(world)
     for _ in range(e2e_steps):
         np.copyto(hg, hg0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ctx.correct_host(hf, hg, field.eb, stream=stream.cuda_stream, **PARAMS)
+        hrep = ctx.correct_host(hf, hg, field.eb, stream=stream.cuda_stream, **PARAMS)
         e2e_s += time.perf_counter() - t0
+        back += hrep.host_bytes_back
     e2e_s = max_over_ranks(e2e_s, world)
+    # Device -> host: the changed voxels' ids and values (the host buffer
+    # already holds the rest), as the library reports them.
     e2e = {"value": world * n * e2e_steps / e2e_s / 1e6, "unit": UNIT,
-           "h2d_bytes_per_step": 2 * n * s, "d2h_bytes_per_step": n * s,
+           "h2d_bytes_per_step": 2 * n * s, "d2h_bytes_per_step": back // e2e_steps,
            "entry_point": "extremz_correct_host"}
 
     cpu = None

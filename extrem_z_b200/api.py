@@ -61,7 +61,7 @@ class Report(ctypes.Structure):
                 ("kernel_launches", ctypes.c_longlong),
                 ("prof_ms", ctypes.c_float * 10), ("prof_launches", ctypes.c_int * 10),
                 ("manifold_reused", ctypes.c_int), ("cp_counts", ctypes.c_int * 4),
-                ("graph_launches", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
+                ("graph_launches", ctypes.c_int), ("host_bytes_back", ctypes.c_longlong)]
 
 class EditStream(ctypes.Structure):
     _fields_ = [("index", ctypes.c_void_p), ("index_cap", ctypes.c_longlong),
@@ -113,6 +113,7 @@ class CorrectionReport:
     manifold_reused: int = 0
     cp_counts: list = None      # original 2-saddles, 1-saddles, maxima, minima
     graph_launches: int = 0     # ticks launched as one CUDA graph
+    host_bytes_back: int = 0    # correct_host: bytes copied device -> host
 
     @staticmethod
     def of(r: Report) -> "CorrectionReport":
@@ -121,7 +122,7 @@ class CorrectionReport:
                                 dict(zip(KCLASS_NAMES, [float(x) for x in r.prof_ms])),
                                 dict(zip(KCLASS_NAMES, [int(x) for x in r.prof_launches])),
                                 int(r.manifold_reused), list(r.cp_counts),
-                                int(r.graph_launches))
+                                int(r.graph_launches), int(r.host_bytes_back))
 
 
 def library_path() -> str:

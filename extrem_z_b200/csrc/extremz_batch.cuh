@@ -96,6 +96,9 @@ constexpr int kFlagKeepInput = 1 << 30;
 // Internal job flag: analysis only -- classification, labels and critical-point
 // lists of the field (admitted as the original), no correction.
 constexpr int kFlagAnalysis = 1 << 29;
+// Internal job flag: keep the bitset of voxels whose value changed (Job::edited)
+// so that only those travel back to a host buffer.
+constexpr int kFlagTrackEdits = 1 << 28;
 
 constexpr long long job_bytes_voxels(long long n, long long ksz) {
   return arr_bytes(n, 1) + arr_bytes(n, 2)                          // otype, olm
@@ -141,6 +144,7 @@ struct JobHost {
   int pc = PC_DONE;
   int block = 0;          // 0 = before the loop, 1..3 = block of an outer iteration
   bool waiting = false;   // stopped at a branch that needs this tick's counters
+  cudaEvent_t input_ready = nullptr;  // the decompressed field is still arriving until this event
   int outer = 0, rounds = 0, cloop_total = 0, manifold_rounds = 0;
   int nfc = 0, nfc1 = 0;
   int c[11] = {0};        // loop-test counters (:5603-5605)
@@ -245,6 +249,7 @@ class BatchEngine {
     if (!on) drop_graphs();
   }
   void set_stream(cudaStream_t st) { st_ = st; }
+  cudaStream_t stream() const { return st_; }
   // Stream-ordered pool the job workspaces come from (nullptr: the device's
   // default pool).
   void set_pool(cudaMemPool_t pool) { pool_mem_ = pool; }
@@ -290,8 +295,10 @@ class BatchEngine {
     // Borrowed storage holds both parts; an allocation holds the first (and a
     // copy of the incoming field when an edit stream will be encoded).
     const bool keep_input = (p.flags & kFlagKeepInput) != 0;
+    const bool track_edits = (p.flags & kFlagTrackEdits) != 0;
     const long long need = (storage ? job_bytes<T>(N) : job_bytes_voxels(N, sizeof(K))) +
-                           (keep_input ? arr_bytes(N, sizeof(T)) : 0);
+                           (keep_input ? arr_bytes(N, sizeof(T)) : 0) +
+                           (track_edits ? arr_bytes((N + 31) / 32, 4) : 0);
     if (storage) {
       jh.arena = *storage;
       jh.arena.used = 0;
@@ -349,10 +356,13 @@ class BatchEngine {
     jh.ntiles = ((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);
     J.tdirty = A.take<uint8_t>(jh.ntiles);
     J.g0 = keep_input ? A.take<T>(N) : nullptr;
-    if (!J.tdirty || (keep_input && !J.g0)) {
+    J.edited = track_edits ? A.take<unsigned>((N + 31) / 32) : nullptr;
+    if (!J.tdirty || (keep_input && !J.g0) || (track_edits && !J.edited)) {
       free_job(jh);
       return EXTREMZ_OOM;
     }
+    if (track_edits)
+      EZ_CHECK(cudaMemsetAsync(J.edited, 0, (size_t)((N + 31) / 32) * 4, st_));
     if (keep_input)
       EZ_CHECK(cudaMemcpyAsync(J.g0, g, (size_t)N * sizeof(T), cudaMemcpyDeviceToDevice, st_));
     // Tile maps of both fields (TMA when the stride allows).
@@ -446,6 +456,28 @@ class BatchEngine {
     EZ_CHECK(cudaStreamSynchronize(st_));
     return bad ? EXTREMZ_BAD_ARG : EXTREMZ_OK;
   }
+
+  // Voxels of a finished job admitted with kFlagTrackEdits whose value
+  // changed: ids (ascending) into the job's `touched` array and their
+  // corrected values into its proposal buffer, both free once the correction
+  // is over.  Returns the count; edited_ids / edited_vals give the arrays.
+  int edited_list(int slot, int* count) {
+    JobHost<T>& jh = slots_[slot];
+    const Job<T>& J = jh.J;
+    static_assert(sizeof(K) == sizeof(T), "values are written over the proposal keys");
+    if (!J.edited) return EXTREMZ_BAD_ARG;
+    const int N = J.dim.N, nb = jh.nb;
+    int* tot = reinterpret_cast<int*>(jh.checksum);
+    launch(K_OTHER, k_edit_count, nb, 32, (const unsigned*)J.edited, N, jh.bcount);
+    launch(K_OTHER, k_scan_lists, 1, 1024, jh.bcount, nb, 1, tot);
+    launch(K_OTHER, k_edit_write<T>, nb, 32, (const unsigned*)J.edited, (const T*)J.g, N,
+           (const int*)jh.bcount, J.touched, reinterpret_cast<T*>(J.delta));
+    EZ_CHECK(cudaMemcpyAsync(count, tot, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    EZ_CHECK(cudaStreamSynchronize(st_));
+    return EXTREMZ_OK;
+  }
+  const int* edited_ids(int slot) const { return slots_[slot].J.touched; }
+  const T* edited_vals(int slot) const { return reinterpret_cast<const T*>(slots_[slot].J.delta); }
 
   // Stream-ordered scratch from the engine's pool (or the device's default).
   void* scratch(size_t bytes) {
@@ -586,7 +618,14 @@ class BatchEngine {
   }
 
   // Releases a finished job's slot and (stream-ordered) its workspace.
-  void release(int slot) { free_job(slots_[slot]); }
+  void release(int slot) {
+    slots_[slot].input_ready = nullptr;
+    free_job(slots_[slot]);
+  }
+  // The job's decompressed field is still being copied in until `ev` (on
+  // another stream): setup, which reads only the original field, runs
+  // meanwhile, and the first tick that reads the decompressed field waits.
+  void set_input_event(int slot, cudaEvent_t ev) { slots_[slot].input_ready = ev; }
   // Releases every job (after an error that ends a batch).
   void release_jobs() {
     for (auto& j : slots_) free_job(j);
@@ -619,6 +658,11 @@ class BatchEngine {
       sig_.clear();
       pending_.clear();
     }
+    for (auto& j : slots_)
+      if (j.used && !j.waiting && j.input_ready && j.pc >= PC_CL_DETECT) {
+        EZ_CHECK(cudaStreamWaitEvent(st_, j.input_ready, 0));
+        j.input_ready = nullptr;
+      }
     int rc = EXTREMZ_OK;
     for (int ph = 0; ph < PC_COUNT && rc == EXTREMZ_OK; ++ph) {
       std::vector<int> sel;

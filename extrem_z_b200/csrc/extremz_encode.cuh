@@ -151,4 +151,40 @@ __global__ void __launch_bounds__(256) k_enc_stats(const T* __restrict__ f, cons
   }
 }
 
+// List of the voxels whose value changed during a correction, for the
+// host-buffer entry point: the caller's buffer already holds the decompressed
+// field, so only these voxels travel back.  `bits` is the bitset k_apply
+// keeps (Job::edited); one warp per 32 words (1024 voxels), one count per
+// block, then (after k_scan_lists) ids and corrected values in id order.
+__global__ void __launch_bounds__(32) k_edit_count(const unsigned* __restrict__ bits, int N,
+                                                   int* __restrict__ bcount) {
+  const int w = blockIdx.x * 32 + threadIdx.x;
+  int c = w < (N + 31) / 32 ? __popc(bits[w]) : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (threadIdx.x == 0) bcount[blockIdx.x] = c;
+}
+
+template <class T>
+__global__ void __launch_bounds__(32) k_edit_write(const unsigned* __restrict__ bits,
+                                                   const T* __restrict__ g, int N,
+                                                   const int* __restrict__ boff,
+                                                   int* __restrict__ ids, T* __restrict__ vals) {
+  const int w = blockIdx.x * 32 + threadIdx.x;
+  unsigned m = w < (N + 31) / 32 ? bits[w] : 0u;
+  const int c = __popc(m);
+  int incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane_id() >= (unsigned)o) incl += y;
+  }
+  int pos = boff[blockIdx.x] + incl - c;
+  while (m) {
+    const int v = w * 32 + __ffs(m) - 1;
+    m &= m - 1;
+    ids[pos] = v;
+    vals[pos] = g[v];
+    ++pos;
+  }
+}
+
 }  // namespace extremz

@@ -188,15 +188,30 @@ static cudaMemPool_t make_pool(int dev) {
 struct Context {
   int device = 0;
   Arena stage;  // device copies of host fields (extremz_correct_host)
+  char* hstage = nullptr;  // pinned host staging of edited-voxel lists
+  size_t hstage_cap = 0;
+  int ensure_hstage(size_t bytes) {
+    if (bytes <= hstage_cap) return EXTREMZ_OK;
+    if (hstage) cudaFreeHost(hstage);
+    hstage = nullptr;
+    hstage_cap = 0;
+    EZ_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&hstage), bytes, cudaHostAllocDefault));
+    hstage_cap = bytes;
+    return EXTREMZ_OK;
+  }
   cudaMemPool_t pool = nullptr;
-  cudaStream_t aux = nullptr;  // second stream of batches (the double engine)
+  cudaStream_t aux = nullptr;  // second stream of batches (the double engine) and
+                               // of the decompressed field's copy in (host entry)
   cudaEvent_t join = nullptr;
+  cudaEvent_t orig_in = nullptr, decp_in = nullptr;  // host entry: copies in have ended
   BatchEngine<float> e32{nullptr};
   BatchEngine<double> e64{nullptr};
   int ensure_aux() {
     if (aux) return EXTREMZ_OK;
     EZ_CHECK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
     EZ_CHECK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    EZ_CHECK(cudaEventCreateWithFlags(&orig_in, cudaEventDisableTiming));
+    EZ_CHECK(cudaEventCreateWithFlags(&decp_in, cudaEventDisableTiming));
     return EXTREMZ_OK;
   }
   int ensure_pool() {
@@ -215,7 +230,10 @@ struct Context {
       cudaMemPoolDestroy(pool);
     }
     if (stage.base) cudaFree(stage.base);
+    if (hstage) cudaFreeHost(hstage);
     if (join) cudaEventDestroy(join);
+    if (orig_in) cudaEventDestroy(orig_in);
+    if (decp_in) cudaEventDestroy(decp_in);
     if (aux) cudaStreamDestroy(aux);
   }
 };
@@ -232,15 +250,80 @@ static int check_args(int dtype, long long W, long long H, long long D, const ex
   return EXTREMZ_OK;
 }
 
+// Copy-back of a corrected field into the caller's host buffer, which still
+// holds the decompressed field: only the voxels whose value changed travel
+// (ids and values, then a scatter on the host) unless they are so many that
+// the whole field is cheaper.
+template <class T>
+struct HostWriteBack {
+  Context* c;
+  T* h_decp;
+  cudaEvent_t input_ready = nullptr;  // the decompressed field's copy in has ended
+  long long moved = 0;                // bytes copied device -> host
+};
+
+// out[ids[k]] = vals[k]: scattered stores into a large host buffer, bound by
+// the latency of their cache misses, so large lists are split over threads
+// and each thread prefetches ahead.
+template <class T>
+static void scatter_host(T* out, const int* ids, const T* vals, int n) {
+  auto part = [=](int lo, int hi) {
+    for (int k = lo; k < hi; ++k) {
+      if (k + 16 < hi) __builtin_prefetch(out + ids[k + 16], 1, 0);
+      out[ids[k]] = vals[k];
+    }
+  };
+  const unsigned hc = std::thread::hardware_concurrency();
+  const int nt = n < (1 << 15) ? 1 : (int)std::min(8u, std::max(1u, hc));
+  if (nt == 1) {
+    part(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t)
+    th.emplace_back(part, (int)((long long)n * t / nt), (int)((long long)n * (t + 1) / nt));
+  part(0, (int)((long long)n / nt));
+  for (auto& x : th) x.join();
+}
+
+template <class T>
+static int write_back(BatchEngine<T>& e, int slot, const T* d_decp, long long N,
+                      HostWriteBack<T>& wb) {
+  cudaStream_t st = e.stream();
+  int n = 0;
+  EZ_RUN(e.edited_list(slot, &n));
+  // A list entry costs (4 + sizeof(T)) bytes on the bus plus a scattered
+  // store on the host; past 1/16 of the voxels the plain copy is faster.
+  if ((long long)n * 16 > N) {
+    EZ_CHECK(cudaMemcpyAsync(wb.h_decp, d_decp, (size_t)N * sizeof(T), cudaMemcpyDeviceToHost, st));
+    EZ_CHECK(cudaStreamSynchronize(st));
+    wb.moved = N * (long long)sizeof(T) + 4;
+    return EXTREMZ_OK;
+  }
+  const size_t id_bytes = ((size_t)n * 4 + 255) & ~size_t(255);
+  EZ_RUN(wb.c->ensure_hstage(id_bytes + (size_t)n * sizeof(T) + 256));
+  int* hid = reinterpret_cast<int*>(wb.c->hstage);
+  T* hv = reinterpret_cast<T*>(wb.c->hstage + id_bytes);
+  if (n) {
+    EZ_CHECK(cudaMemcpyAsync(hid, e.edited_ids(slot), (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    EZ_CHECK(cudaMemcpyAsync(hv, e.edited_vals(slot), (size_t)n * sizeof(T), cudaMemcpyDeviceToHost, st));
+    EZ_CHECK(cudaStreamSynchronize(st));
+  }
+  scatter_host(wb.h_decp, hid, hv, n);
+  wb.moved = (long long)n * (4 + (long long)sizeof(T)) + 4;
+  return EXTREMZ_OK;
+}
+
 // Runs one job to completion on an engine.
 template <class T>
 static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* tables, Arena* engine_store,
                    Arena* job_store, const T* f, T* g, int W, int H, int D, const extremz_params& p0,
                    extremz_report* rep, int32_t* trace, int trace_cap,
-                   extremz_edit_stream* es = nullptr) {
+                   extremz_edit_stream* es = nullptr, HostWriteBack<T>* wb = nullptr) {
   extremz_params p = p0;
-  p.flags &= ~kFlagKeepInput;
+  p.flags &= ~(kFlagKeepInput | kFlagTrackEdits);
   if (es) p.flags |= kFlagKeepInput;
+  if (wb) p.flags |= kFlagTrackEdits;
   e.set_stream(st);
   EZ_RUN(e.init(tables, engine_store));
   const bool prof = (p.flags & EXTREMZ_FLAG_PROFILE) != 0;
@@ -249,6 +332,7 @@ static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* table
   const long long g0 = e.graph_replays() + e.graph_captures();
   int slot = -1;
   EZ_RUN(e.admit(f, g, W, H, D, p, trace, trace_cap, job_store, 0, &slot));
+  if (wb && wb->input_ready) e.set_input_event(slot, wb->input_ready);
   int rc = EXTREMZ_OK;
   while (e.job(slot).pc != PC_DONE) {
     rc = e.tick();
@@ -274,6 +358,10 @@ static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* table
   if (es && (rc == EXTREMZ_OK || rc == EXTREMZ_ROUND_CAP)) {
     const int erc = e.encode(slot, es);
     if (erc != EXTREMZ_OK) rc = erc;
+  }
+  if (wb && (rc == EXTREMZ_OK || rc == EXTREMZ_ROUND_CAP)) {
+    const int wrc = write_back(e, slot, g, (long long)W * H * D, *wb);
+    if (wrc != EXTREMZ_OK) rc = wrc;
   }
   e.release(slot);
   return rc;
@@ -799,12 +887,16 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
   if (!ctx || !h_orig || !h_decp) return EXTREMZ_BAD_ARG;
   int rc = check_args(dtype, width, height, depth, params);
   if (rc != EXTREMZ_OK) return (extremz_status)rc;
+  if (report) std::memset(report, 0, sizeof(*report));
   int prev = 0;
   cudaGetDevice(&prev);
   if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
-  const size_t bytes = (size_t)width * height * depth * (dtype == EXTREMZ_F32 ? 4 : 8);
+  const long long N = (long long)width * height * depth;
+  const size_t bytes = (size_t)N * (dtype == EXTREMZ_F32 ? 4 : 8);
   cudaStream_t st = (cudaStream_t)stream;
   rc = ctx->c.stage.reserve(2 * bytes + 512);
+  if (rc == EXTREMZ_OK) rc = ctx->c.ensure_pool();
+  if (rc == EXTREMZ_OK) rc = ctx->c.ensure_aux();
   if (rc != EXTREMZ_OK) {
     if (prev != ctx->c.device) cudaSetDevice(prev);
     return (extremz_status)rc;
@@ -812,16 +904,37 @@ extremz_status extremz_correct_host(extremz_ctx* ctx, const void* h_orig, void* 
   ctx->c.stage.used = 0;
   char* df = ctx->c.stage.take<char>(bytes);
   char* dg = ctx->c.stage.take<char>(bytes);
+  // The original field first, on the caller's stream; then the decompressed
+  // field on the second stream, behind it on the bus, while the setup (which
+  // reads only the original) runs.
+  cudaStream_t aux = ctx->c.aux;
   if (cudaMemcpyAsync(df, h_orig, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemcpyAsync(dg, h_decp, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      cudaEventRecord(ctx->c.orig_in, st) != cudaSuccess ||
+      cudaStreamWaitEvent(aux, ctx->c.orig_in, 0) != cudaSuccess ||
+      cudaMemcpyAsync(dg, h_decp, bytes, cudaMemcpyHostToDevice, aux) != cudaSuccess ||
+      cudaEventRecord(ctx->c.decp_in, aux) != cudaSuccess)
     rc = EXTREMZ_CUDA_ERR;
-  if (rc == EXTREMZ_OK)
-    rc = extremz_correct_device(ctx, df, dg, dtype, width, height, depth, params, report, stream,
-                                nullptr, 0);
-  if (rc == EXTREMZ_OK || rc == EXTREMZ_ROUND_CAP) {
-    if (cudaMemcpyAsync(h_decp, dg, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      rc = EXTREMZ_CUDA_ERR;
+  long long moved = 0;
+  if (rc == EXTREMZ_OK) {
+    // The corrected voxels come back into h_decp inside run_one.
+    if (dtype == EXTREMZ_F32) {
+      HostWriteBack<float> wb{&ctx->c, static_cast<float*>(h_decp), ctx->c.decp_in};
+      rc = run_one(ctx->c.e32, st, nullptr, nullptr, nullptr, (const float*)df, (float*)dg, width,
+                   height, depth, *params, report, nullptr, 0, nullptr, &wb);
+      moved = wb.moved;
+    } else {
+      HostWriteBack<double> wb{&ctx->c, static_cast<double*>(h_decp), ctx->c.decp_in};
+      rc = run_one(ctx->c.e64, st, nullptr, nullptr, nullptr, (const double*)df, (double*)dg, width,
+                   height, depth, *params, report, nullptr, 0, nullptr, &wb);
+      moved = wb.moved;
+    }
+  }
+  // Whatever happened, the copy in has ended before h_decp is written or
+  // handed back.
+  if (cudaEventSynchronize(ctx->c.decp_in) != cudaSuccess && rc == EXTREMZ_OK) rc = EXTREMZ_CUDA_ERR;
+  if (report) {
+    report->status = rc;
+    report->host_bytes_back = moved;
   }
   if (prev != ctx->c.device) cudaSetDevice(prev);
   return (extremz_status)rc;

@@ -48,6 +48,7 @@ struct Job {
   int* flagged; int* flagged1;  // flagged neighbours (split / join)
   uint8_t* mis;       // per vertex: 1 if dds != ds, 2 if das != as
   unsigned* vchg;     // bitset: vertices whose value changed since the last computed round
+  unsigned* edited;   // bitset: vertices whose value changed in this correction (or null)
   uint8_t* dirtyv;    // per vertex: an input of its saddle rows changed this round
   uint8_t* has2; uint8_t* has1;  // per saddle row: its wrong-neighbour seed bit
   int* cpoff;         // per list (2-saddles, 1-saddles, maxima, minima) and
@@ -959,6 +960,7 @@ __global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, 
     if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0)) {
       J.ctr[C_CHANGED] = 1;
       atomicOr(J.vchg + (v >> 5), 1u << (v & 31));
+      if (J.edited) atomicOr(J.edited + (v >> 5), 1u << (v & 31));
       int x, y, z;
       coords(v, J.dim, x, y, z);
       mark_tiles(J.tdirty, J.dim, x, y, z);

@@ -115,7 +115,7 @@ typedef struct {
                            previous round, so its results were kept */
   int cp_counts[4];     /* original 2-saddles, 1-saddles, maxima, minima */
   int graph_launches;   /* ticks launched as one CUDA graph (see extremz_correct_device) */
-  int reserved[2];
+  long long host_bytes_back;  /* extremz_correct_host: bytes copied device -> host */
 } extremz_report;
 
 typedef struct extremz_ctx_s extremz_ctx;
@@ -149,8 +149,12 @@ extremz_status extremz_correct_device(extremz_ctx* ctx, const void* d_orig, void
                                       void* stream, int32_t* trace, int trace_cap);
 
 /*
- * Same with host buffers: copies both fields to the device, corrects, copies
- * the corrected field back into h_decp.
+ * Same with host buffers: copies both fields to the device, corrects, and
+ * writes the corrected field back into h_decp.  h_decp still holds the
+ * decompressed field at that point, so only the voxels whose value changed
+ * travel back (their ids and values, stored into h_decp on the host) unless
+ * more than 1/16 of the voxels changed, when the whole field is copied;
+ * report->host_bytes_back gives the bytes copied.
  * Replaces: the correction sequence of main.cpp:65-446 (host arrays in,
  * corrected decp_data out, saved by saveArrayToBin at main.cpp:507).
  */
