@@ -648,15 +648,18 @@ class BatchEngine {
     // A tick whose launches repeat an earlier tick's exactly (kernels, launch
     // shapes and arguments; per-job state is read from device memory) runs as
     // one CUDA graph: recorded, captured the third time its signature is
-    // seen, replayed from then on.  Ticks that allocate (setup) or time
-    // kernels launch directly.
-    bool graph = graphs_on_ && !profile_;
+    // seen, replayed from then on.  Ticks that allocate (setup) launch
+    // directly.  Timed launches (EXTREMZ_FLAG_PROFILE) keep their events
+    // inside the graph, so profiling does not change how a tick launches.
+    bool graph = graphs_on_;
     for (const auto& j : slots_)
       if (j.used && !j.waiting && j.pc == PC_SETUP_B) graph = false;
     if (graph) {
       recording_ = true;
       sig_.clear();
       pending_.clear();
+      pending_timed_.clear();
+      sig_append(profile_ ? profile_mask_ | (1 << 30) : 0);
     }
     for (auto& j : slots_)
       if (j.used && !j.waiting && j.input_ready && j.pc >= PC_CL_DETECT) {
@@ -687,6 +690,7 @@ class BatchEngine {
     if (!issued_) return EXTREMZ_OK;
     issued_ = false;
     EZ_CHECK(cudaStreamSynchronize(st_));
+    fold_timings();
     for (int i = 0; i < kMaxSel; ++i) {
       JobHost<T>& j = slots_[i];
       if (!j.used || j.pc == PC_DONE) continue;
@@ -705,39 +709,43 @@ class BatchEngine {
 
   // Per-class timing of the launches since set_profile(true, ...).
   void collect_profile(extremz_report* rep) {
-    if (recs_.empty()) return;
-    cudaStreamSynchronize(st_);
-    for (const Rec& r : recs_) {
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, r.a, r.b);
-      if (rep) {
-        rep->prof_ms[r.cls] += ms;
-        rep->prof_launches[r.cls] += 1;
-      }
-      pool_.push_back(r.a);
-      pool_.push_back(r.b);
+    if (!recs_.empty()) {
+      cudaStreamSynchronize(st_);
+      fold_timings();
     }
-    recs_.clear();
+    if (rep)
+      for (int c = 0; c < K_NUM; ++c) {
+        rep->prof_ms[c] += prof_ms_[c];
+        rep->prof_launches[c] += prof_n_[c];
+      }
+    reset_timings();
   }
   void drop_profile_events() {
-    for (const Rec& r : recs_) {
-      pool_.push_back(r.a);
-      pool_.push_back(r.b);
-    }
+    for (const Rec& r : recs_)
+      if (r.owned) {
+        pool_.push_back(r.a);
+        pool_.push_back(r.b);
+      }
     recs_.clear();
+    reset_timings();
     for (cudaEvent_t e : pool_) cudaEventDestroy(e);
     pool_.clear();
   }
 
  private:
   cudaStream_t st_;
+  struct Rec { int cls; cudaEvent_t a, b; bool owned; };
   // Tick graphs (see tick_issue).
-  bool graphs_on_ = true, recording_ = false;
+  bool graphs_on_ = true, recording_ = false, capturing_ = false;
   std::string sig_;
   std::vector<std::function<void(cudaStream_t)>> pending_;
+  // Timed launches of the tick being recorded: class, and the event pair the
+  // launch records around itself (filled in just before the launches run).
+  std::vector<Rec> pending_timed_;
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
     unsigned long long last = 0;
+    std::vector<Rec> timed;  // events recorded by the graph's timed launches
   };
   std::unordered_map<std::string, GraphEntry> graphs_;
   std::unordered_map<std::string, int> seen_;
@@ -764,8 +772,34 @@ class BatchEngine {
   long long launches_ = 0;
   bool profile_ = false;
   int profile_mask_ = 0;
-  struct Rec { int cls; cudaEvent_t a, b; };
+  // A timed launch: events around it.  Events of a launch inside a captured
+  // tick graph belong to the graph (recorded again at every replay, read after
+  // the tick's synchronisation); the others return to the pool.
   std::vector<Rec> recs_;
+  float prof_ms_[K_NUM] = {};
+  int prof_n_[K_NUM] = {};
+  void fold_timings() {
+    for (const Rec& r : recs_) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) {
+        cudaGetLastError();
+        ms = 0.f;
+      }
+      prof_ms_[r.cls] += ms;
+      prof_n_[r.cls] += 1;
+      if (r.owned) {
+        pool_.push_back(r.a);
+        pool_.push_back(r.b);
+      }
+    }
+    recs_.clear();
+  }
+  void reset_timings() {
+    for (int c = 0; c < K_NUM; ++c) {
+      prof_ms_[c] = 0.f;
+      prof_n_[c] = 0;
+    }
+  }
   std::vector<cudaEvent_t> pool_;
 
   int h(int slot, int c) const { return ctr_host_[(size_t)slot * C_COUNT + c]; }
@@ -788,16 +822,29 @@ class BatchEngine {
 
   template <class... KArgs, class... Args>
   void launch(int cls, void (*kern)(KArgs...), dim3 grid, dim3 block, Args... args) {
+    const bool timed = profile_ && (profile_mask_ == 0 || (profile_mask_ >> cls & 1));
     if (recording_) {  // tick graphs: record, launch later as one graph
       sig_append(reinterpret_cast<const void*>(kern));
       sig_append(grid);
       sig_append(block);
       (sig_append(args), ...);
-      pending_.push_back([=](cudaStream_t s) { kern<<<grid, block, 0, s>>>(args...); });
+      if (timed) {
+        const size_t k = pending_timed_.size();
+        pending_timed_.push_back({cls, nullptr, nullptr, false});
+        pending_.push_back([=](cudaStream_t s) {
+          // In a capture the events become event-record nodes of the graph.
+          const Rec& r = pending_timed_[k];
+          const unsigned fl = capturing_ ? cudaEventRecordExternal : cudaEventRecordDefault;
+          if (r.a) cudaEventRecordWithFlags(r.a, s, fl);
+          kern<<<grid, block, 0, s>>>(args...);
+          if (r.b) cudaEventRecordWithFlags(r.b, s, fl);
+        });
+      } else {
+        pending_.push_back([=](cudaStream_t s) { kern<<<grid, block, 0, s>>>(args...); });
+      }
       ++launches_;
       return;
     }
-    const bool timed = profile_ && (profile_mask_ == 0 || (profile_mask_ >> cls & 1));
     cudaEvent_t a = nullptr, b = nullptr;
     if (timed) {
       a = event();
@@ -808,18 +855,42 @@ class BatchEngine {
     ++launches_;
     if (timed) {
       cudaEventRecord(b, st_);
-      recs_.push_back({cls, a, b});
+      recs_.push_back({cls, a, b, true});
     }
   }
 
-  void run_direct() {
+  // Event pairs for the recorded tick's timed launches, from the pool.
+  void arm_timed() {
+    for (Rec& r : pending_timed_) {
+      r.a = event();
+      r.b = event();
+      r.owned = true;
+    }
+  }
+
+  void run_direct(bool timing = true) {
+    if (timing) arm_timed();
     for (auto& go : pending_) go(st_);
     pending_.clear();
+    for (const Rec& r : pending_timed_)
+      if (r.a) recs_.push_back(r);
+    pending_timed_.clear();
+  }
+
+  // (cudaEventDestroy of an event still pending releases it once it completes.)
+  static void release_graph_events(GraphEntry& e) {
+    for (const Rec& r : e.timed) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    e.timed.clear();
   }
 
   void drop_graphs() {
-    for (auto& kv : graphs_)
+    for (auto& kv : graphs_) {
       if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+      release_graph_events(kv.second);
+    }
     graphs_.clear();
     seen_.clear();
     if (cap_) cudaStreamDestroy(cap_);
@@ -833,15 +904,20 @@ class BatchEngine {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st_, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
       cudaGetLastError();  // the caller is capturing this stream: launch into it directly
-      run_direct();
+      run_direct(false);   // (untimed: the events would not have run when read)
       return EXTREMZ_OK;
     }
     auto it = graphs_.find(sig_);
     if (it != graphs_.end()) {
       it->second.last = graph_clock_;
       pending_.clear();
+      pending_timed_.clear();
       ++graph_replays_;
       EZ_CHECK(cudaGraphLaunch(it->second.exec, st_));
+      for (Rec r : it->second.timed) {
+        r.owned = false;
+        recs_.push_back(r);
+      }
       return EXTREMZ_OK;
     }
     if (seen_.size() > 4 * kMaxGraphs) seen_.clear();
@@ -854,6 +930,7 @@ class BatchEngine {
       for (auto g = graphs_.begin(); g != graphs_.end(); ++g)
         if (g->second.last < old->second.last) old = g;
       cudaGraphExecDestroy(old->second.exec);
+      release_graph_events(old->second);
       graphs_.erase(old);
     }
     // Captured on a private stream (the caller's may be the legacy stream,
@@ -872,20 +949,34 @@ class BatchEngine {
       run_direct();
       return EXTREMZ_OK;
     }
+    arm_timed();
+    capturing_ = true;
     for (auto& go : pending_) go(cap_);
+    capturing_ = false;
     const cudaError_t ec = cudaStreamEndCapture(cap_, &g);
     if (ec != cudaSuccess || !g || cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
       cudaGetLastError();
       if (g) cudaGraphDestroy(g);
       graphs_on_ = false;  // capture unavailable here: launch directly from now on
+      for (const Rec& r : pending_timed_) {
+        pool_.push_back(r.a);
+        pool_.push_back(r.b);
+      }
       run_direct();
       return EXTREMZ_OK;
     }
     cudaGraphDestroy(g);
     pending_.clear();
-    graphs_[sig_] = GraphEntry{exec, graph_clock_};
+    GraphEntry ge{exec, graph_clock_};
+    ge.timed = pending_timed_;
+    pending_timed_.clear();
     ++graph_captures_;
     EZ_CHECK(cudaGraphLaunch(exec, st_));
+    for (Rec r : ge.timed) {
+      r.owned = false;
+      recs_.push_back(r);
+    }
+    graphs_[sig_] = std::move(ge);
     return EXTREMZ_OK;
   }
 

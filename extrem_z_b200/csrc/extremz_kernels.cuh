@@ -583,8 +583,7 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
   int* err = J.ctr + C_ERROR;
   const int N = J.dim.N;
   const int cap_j = J.iter_cap;
-  const int stride = gridDim.x * blockDim.x;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) {
+  auto jump_one = [&](int v) {
     int u1 = a[v], u2 = b[v];
     // Decompressed field: this vertex's old labels, original roots and
     // change stamp, loaded while the chains are followed.
@@ -623,7 +622,25 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
     }
     ra[v] = u1;
     rb[v] = u2;
+  };
+  if constexpr (kDec) {
+    // Tile order: a block takes whole 32x8x4 tiles, whose vertices share most
+    // chain targets (the tile's exits and roots), so the hops hit L1.
+    const Dims g = J.dim;
+    const int ntx = (g.W + TX - 1) / TX, nty = (g.H + TY - 1) / TY, ntz = (g.D + TZ - 1) / TZ;
+    const int ntiles = ntx * nty * ntz;
+    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+    const int WH = g.W * g.H;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const int x = (t % ntx) * TX + tx, y = ((t / ntx) % nty) * TY + ty;
+      const int z0 = (t / (ntx * nty)) * TZ;
+      if (x >= g.W || y >= g.H) continue;
+      for (int tz = 0; tz < TZ && z0 + tz < g.D; ++tz) jump_one(x + y * g.W + (z0 + tz) * WH);
+    }
+    continue;
   }
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) jump_one(v);
   }
 }
 

@@ -139,7 +139,8 @@ void extremz_ctx_destroy(extremz_ctx* ctx);
  * length in int32.  The launches of one step of the control flow ("tick") that
  * repeat an earlier step's exactly run as one CUDA graph, captured the third
  * time they occur and kept in the context (not when the caller's stream is
- * itself being captured, nor with EXTREMZ_FLAG_PROFILE).
+ * itself being captured).  With EXTREMZ_FLAG_PROFILE the timed launches' events
+ * are part of the graphs, so profiling does not change how ticks launch.
  * Replaces: main() of src/ExtreM_cuda.cu:5508-5997 (the correction proper, with
  * input and decompressed field already resident on the device).
  */
