@@ -369,7 +369,10 @@ def run_ours(args, world, rank, local):
     # already holds the rest), as the library reports them.
     e2e = {"value": world * n * e2e_steps / e2e_s / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": 2 * n * s, "d2h_bytes_per_step": back // e2e_steps,
-           "entry_point": "extremz_correct_host"}
+           "entry_point": "extremz_correct_host",
+           # the host buffer against the device-resident correction (outside the timing)
+           "bit_identical_to_device": bool(np.array_equal(
+               hg.view(np.uint8), g.cpu().numpy().view(np.uint8)))}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -661,11 +661,6 @@ class BatchEngine {
       pending_timed_.clear();
       sig_append(profile_ ? profile_mask_ | (1 << 30) : 0);
     }
-    for (auto& j : slots_)
-      if (j.used && !j.waiting && j.input_ready && j.pc >= PC_CL_DETECT) {
-        EZ_CHECK(cudaStreamWaitEvent(st_, j.input_ready, 0));
-        j.input_ready = nullptr;
-      }
     int rc = EXTREMZ_OK;
     for (int ph = 0; ph < PC_COUNT && rc == EXTREMZ_OK; ++ph) {
       std::vector<int> sel;
@@ -673,6 +668,14 @@ class BatchEngine {
         if (slots_[i].used && !slots_[i].waiting && slots_[i].pc == ph) sel.push_back(i);
       if (sel.empty()) continue;
       issued_ = true;
+      // A job can reach its first phase that reads the decompressed field in
+      // the same tick as its setup, so the wait goes right before that phase.
+      if (ph >= PC_CL_DETECT)
+        for (int i : sel)
+          if (slots_[i].input_ready) {
+            EZ_CHECK(cudaStreamWaitEvent(st_, slots_[i].input_ready, 0));
+            slots_[i].input_ready = nullptr;
+          }
       rc = run_phase(ph, sel);
     }
     recording_ = false;
