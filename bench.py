@@ -81,7 +81,7 @@ def dominant_bytes_per_launch(n: int, s: int) -> int:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_jump2
 # launch on the decompressed 256^3 field, from one ncu capture each, by value
 # size (profiles/k_jump2_256cube_f64.md); None where not captured.
-MEASURED_TRAFFIC_256 = {8: 518.019072e6 + 150.010368e6, 4: 518.11072e6 + 150.620928e6}
+MEASURED_TRAFFIC_256 = {8: 455.880448e6 + 143.172096e6}
 
 
 def measured_peaks():
