@@ -1203,9 +1203,12 @@ class BatchEngine {
   template <bool kSplit>
   void wn_rounds(const Sel& s) {
     const Job<T>* jobs = jobs_dev_;
+    // Candidate lists are short next to the field (a few per cent of the
+    // saddles at most), so two blocks per SM cover them.
+    const int grid = std::min(grid_, 2 * sms_);
     for (int r = 0; r < kWnGridRounds; ++r) {
-      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid_, 256, jobs, s, r);
-      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid_, 256, jobs, s, r);
+      launch(K_WRONG_NBR, k_wn_vote<T, kSplit>, grid, 256, jobs, s, r);
+      launch(K_WRONG_NBR, k_wn_commit<T, kSplit>, grid, 256, jobs, s, r);
     }
     launch(K_WRONG_NBR, k_wn_resolve<T, kSplit>, s.n, 1024, jobs_dev_, s);
   }

@@ -103,6 +103,7 @@ enum Ctr : int {
   C_REPOCH,    // re-evaluation epoch (k_redetect / k_keep)
   C_WNSTAMP,   // wrong-neighbour flag stamp, one per manifold round
   C_WNROUND,   // wrong-neighbour arbitration round (vote high word)
+  C_WNSMALL,   // this side's candidate list is small: the block completion does it all
   C_COUNT
 };
 // Error bits in ctr[C_ERROR].
@@ -1057,6 +1058,9 @@ __global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, 
 // commits, and a larger one never takes what a smaller one could still take,
 // so the result equals the sequential greedy.
 // ---------------------------------------------------------------------------
+// Candidate lists this short are resolved by one block (k_wn_resolve) alone.
+constexpr int kWnBlockMax = 4096;
+
 template <class T, bool kSplit>
 __device__ __forceinline__ int wn_candidates(const Job<T>& J, int s, int* ids) {
   const int n = neighbours(s, J.dim, ids, nullptr);
@@ -1280,6 +1284,16 @@ __global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
   if (J.ctr[C_MFSKIP]) continue;
+  if (r == 0) {
+    // A short list (every round after the first few of a correction) goes to
+    // the block completion whole: the grid rounds would be launches with
+    // nothing to do.
+    const bool small = J.ctr[C_CAND] <= kWnBlockMax;
+    if (blockIdx.x == 0 && threadIdx.x == 0) J.ctr[C_WNSMALL] = small;
+    if (small) continue;
+  } else if (J.ctr[C_WNSMALL]) {
+    continue;
+  }
   const unsigned long long round = (unsigned)(J.ctr[C_WNROUND] + r + 1);
   const int stamp = J.ctr[C_WNSTAMP];
   const int n = J.ctr[C_CAND + (r & 1)];
@@ -1304,7 +1318,7 @@ __global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jo
                                                    int r) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
-  if (J.ctr[C_MFSKIP]) continue;
+  if (J.ctr[C_MFSKIP] || J.ctr[C_WNSMALL]) continue;
   const unsigned long long round = (unsigned)(J.ctr[C_WNROUND] + r + 1);
   const int stamp = J.ctr[C_WNSTAMP];
   const int n = J.ctr[C_CAND + (r & 1)];
@@ -1337,7 +1351,7 @@ __global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jo
 // Grid-wide vote / commit rounds per side before the per-job completion.
 // Round r reads the candidate list of parity r & 1 (cand / cand_next, counts
 // C_CAND / C_CAND_NEXT) and refills the other; its vote number is the job's
-// base round + r + 1.
+// base round + r + 1.  Lists of at most kWnBlockMax saddles skip them.
 constexpr int kWnGridRounds = 3;
 
 // Completion of the arbitration for whatever the grid-wide rounds left
@@ -1357,11 +1371,12 @@ __global__ void __launch_bounds__(1024) k_wn_resolve(Job<T>* __restrict__ jobs, 
   int* taken = kSplit ? J.taken : J.taken1;
   int* flagged = kSplit ? J.flagged : J.flagged1;
   int* nflag = J.ctr + (kSplit ? C_NFC : C_NFC1);
-  // The grid-wide rounds left their list in parity kWnGridRounds & 1.
-  constexpr int kPar = kWnGridRounds & 1;
-  int* cur = kPar ? J.cand_next : J.cand;
-  int* nxt = kPar ? J.cand : J.cand_next;
-  int n = J.ctr[C_CAND + kPar];
+  // The grid-wide rounds left their list in parity kWnGridRounds & 1; a short
+  // list skipped them and is still in parity 0.
+  const int par = J.ctr[C_WNSMALL] ? 0 : (kWnGridRounds & 1);
+  int* cur = par ? J.cand_next : J.cand;
+  int* nxt = par ? J.cand : J.cand_next;
+  int n = J.ctr[C_CAND + par];
   unsigned long long round = (unsigned)(J.ctr[C_WNROUND] + kWnGridRounds);
   const int cap = J.iter_cap;
   int it = 0;
