@@ -625,22 +625,14 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
     rb[v] = u2;
   };
   if constexpr (kDec) {
-    // Tile order: a block takes whole 32x8x4 tiles, whose vertices share most
-    // chain targets (the tile's exits and roots), so the hops hit L1.
-    const Dims g = J.dim;
-    const int ntx = (g.W + TX - 1) / TX, nty = (g.H + TY - 1) / TY, ntz = (g.D + TZ - 1) / TZ;
-    const int ntiles = ntx * nty * ntz;
-    const int WH = g.W * g.H;
-    if ((g.W & 3) == 0) {
-      // Four consecutive vertices per thread (8 threads per tile row): one
-      // 16-byte load per array and one 4-byte store per byte array, a quarter
-      // of the memory requests of the vertex-per-thread loop.
-      const int qx = (threadIdx.x & 7) * 4, qy = (threadIdx.x >> 3) & 7, qz = threadIdx.x >> 6;
-      for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int x = (t % ntx) * TX + qx, y = ((t / ntx) % nty) * TY + qy;
-        const int z = (t / (ntx * nty)) * TZ + qz;
-        if (x >= g.W || y >= g.H || z >= g.D) continue;
-        const int v0 = x + y * g.W + z * WH;  // a multiple of 4: W is
+    if ((N & 3) == 0) {
+      // Four consecutive vertices per thread: one 16-byte load per array and
+      // one 4-byte store per byte array, a quarter of the memory requests of
+      // the vertex-per-thread loop, with eight chains interleaved.
+      const int nq = N >> 2;
+      const int qstride = gridDim.x * blockDim.x;
+      for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += qstride) {
+        const int v0 = q << 2;
         const int4 A = *reinterpret_cast<const int4*>(a + v0);
         const int4 B = *reinterpret_cast<const int4*>(b + v0);
         const int4 O1 = *reinterpret_cast<const int4*>(ra + v0);
@@ -651,24 +643,26 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
         int u1[4] = {A.x, A.y, A.z, A.w}, u2[4] = {B.x, B.y, B.z, B.w};
         const int o1[4] = {O1.x, O1.y, O1.z, O1.w}, o2[4] = {O2.x, O2.y, O2.z, O2.w};
         const int r1[4] = {R1.x, R1.y, R1.z, R1.w}, r2[4] = {R2.x, R2.y, R2.z, R2.w};
-        unsigned done = 0;  // bit 2k: chain 1 of vertex k resolved; bit 2k+1: chain 2
+        // One hop of every unfinished chain per iteration: the eight loads
+        // depend only on their own chain, so they are all in flight at once.
+        bool more = true;
         int it = 0;
-        for (; it < cap_j && done != 0xffu; ++it) {
+        for (; it < cap_j && more; ++it) {
+          int w1[4], w2[4];
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
-            if (!((done >> (2 * k)) & 1u)) {
-              const int w = a[u1[k]];
-              if (w == u1[k]) done |= 1u << (2 * k);
-              else u1[k] = w;
-            }
-            if (!((done >> (2 * k + 1)) & 1u)) {
-              const int w = b[u2[k]];
-              if (w == u2[k]) done |= 2u << (2 * k);
-              else u2[k] = w;
-            }
+            w1[k] = a[u1[k]];
+            w2[k] = b[u2[k]];
+          }
+          more = false;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            more |= (w1[k] != u1[k]) | (w2[k] != u2[k]);
+            u1[k] = w1[k];
+            u2[k] = w2[k];
           }
         }
-        if (it == cap_j) atomicOr(err, kErrJump);
+        if (it == cap_j && more) atomicOr(err, kErrJump);
         unsigned dv = 0, mv = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -686,14 +680,6 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
       }
       continue;
     }
-    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      const int x = (t % ntx) * TX + tx, y = ((t / ntx) % nty) * TY + ty;
-      const int z0 = (t / (ntx * nty)) * TZ;
-      if (x >= g.W || y >= g.H) continue;
-      for (int tz = 0; tz < TZ && z0 + tz < g.D; ++tz) jump_one(x + y * g.W + (z0 + tz) * WH);
-    }
-    continue;
   }
   const int stride = gridDim.x * blockDim.x;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < N; v += stride) jump_one(v);
@@ -1621,21 +1607,33 @@ __global__ void __launch_bounds__(256) k_wis_scan(const Job<T>* __restrict__ job
     if (cnt == 0) continue;
     const int s = sad[i];
     const T gs = J.g[s];
-    const int4* row4 = reinterpret_cast<const int4*>(rows + (long long)i * kRowStride);
-    int row[kRowStride];
+    // Rows hold 2-3 entries typically: the first four entries go through
+    // their three dependent gathers (extremum index, its true largest /
+    // smallest saddle, that saddle's value) stage by stage, so the four
+    // chains overlap; longer rows finish entry by entry.
+    const int* row = rows + (long long)i * kRowStride;
+    const int4 r4 = *reinterpret_cast<const int4*>(row);
+    const int r0[4] = {r4.x, r4.y, r4.z, r4.w};
+    int m[4], tb[4];
+    T gt[4];
 #pragma unroll
-    for (int q = 0; q < kRowStride / 4; ++q) {
-      const int4 t = row4[q];
-      row[4 * q] = t.x; row[4 * q + 1] = t.y; row[4 * q + 2] = t.z; row[4 * q + 3] = t.w;
-    }
+    for (int p = 0; p < 4; ++p) m[p] = p < cnt ? J.ext[r0[p]] : 0;
 #pragma unroll
-    for (int p = 0; p < kNumDirs; ++p) {
+    for (int p = 0; p < 4; ++p) tb[p] = p < cnt ? best[m[p]] : 0;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) gt[p] = p < cnt ? J.g[tb[p]] : T(0);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
       if (p >= cnt) break;
-      const int m = J.ext[row[p]];
-      const int tb = best[m];
-      const T gt = J.g[tb];
-      const bool wrong = kMax ? above(gs, s, gt, tb) : below(gs, s, gt, tb);
-      if (wrong) atomicMin(first + m, i * kRowStride + p);
+      const bool wrong = kMax ? above(gs, s, gt[p], tb[p]) : below(gs, s, gt[p], tb[p]);
+      if (wrong) atomicMin(first + m[p], i * kRowStride + p);
+    }
+    for (int p = 4; p < cnt; ++p) {
+      const int mp = J.ext[row[p]];
+      const int tp = best[mp];
+      const T gp = J.g[tp];
+      const bool wrong = kMax ? above(gs, s, gp, tp) : below(gs, s, gp, tp);
+      if (wrong) atomicMin(first + mp, i * kRowStride + p);
     }
   }
   }
