@@ -104,6 +104,7 @@ enum Ctr : int {
   C_WNSTAMP,   // wrong-neighbour flag stamp, one per manifold round
   C_WNROUND,   // wrong-neighbour arbitration round (vote high word)
   C_WNSMALL,   // this side's candidate list is small: the block completion does it all
+  C_MFFIRST,   // the manifold round being computed is the job's first: every input is new
   C_COUNT
 };
 // Error bits in ctr[C_ERROR].
@@ -1222,6 +1223,9 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
     const int nb = (J.dim.N + kCpBlock - 1) / kCpBlock;
     const int chunk = J.pass_chunk;
     const int nchunk = (nb + chunk - 1) / chunk;
+    // In the first round every changed-input byte is set (the change bitset
+    // starts full), so the check is skipped.
+    const bool all_new = J.ctr[C_MFFIRST] != 0;
     for (int c = blockIdx.x; c < nchunk; c += gridDim.x) {
       const int b0 = c * chunk, b1 = min(b0 + chunk, nb);
       const int a2 = J.cpoff[b0], e2 = b1 < nb ? J.cpoff[b1] : ns2;
@@ -1236,7 +1240,7 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
           const int i = split ? a2 + k : a1 + k - n2;
           s = split ? J.sad2[i] : J.sad1[i];
           uint8_t* hb = split ? J.has2 : J.has1;
-          if (saddle_inputs_changed(J, s)) {
+          if (all_new || saddle_inputs_changed(J, s)) {
             has = split ? saddle_row<T, true>(J, i, s) : saddle_row<T, false>(J, i, s);
             hb[i] = (uint8_t)has;
           } else {  // rows and seed bit as computed in an earlier round
@@ -1727,6 +1731,7 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
       // value changed since the last round began they are still in place.
       c[C_MFSKIP] = c[C_MFDONE] && !c[C_CHANGED];
       c[C_MFREUSED] += c[C_MFSKIP];
+      c[C_MFFIRST] = !c[C_MFDONE];
       c[C_CHANGED] = 0;
       c[C_MFDONE] = 1;
       if (c[C_MFSKIP]) break;
