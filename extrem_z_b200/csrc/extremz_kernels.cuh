@@ -1238,13 +1238,14 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
         int s = 0;
         if (k < n) {
           const int i = split ? a2 + k : a1 + k - n2;
-          s = split ? J.sad2[i] : J.sad1[i];
           uint8_t* hb = split ? J.has2 : J.has1;
+          s = split ? J.sad2[i] : J.sad1[i];
+          const uint8_t kept = hb[i];  // loaded with the id: no round trip of its own
           if (all_new || saddle_inputs_changed(J, s)) {
             has = split ? saddle_row<T, true>(J, i, s) : saddle_row<T, false>(J, i, s);
             hb[i] = (uint8_t)has;
           } else {  // rows and seed bit as computed in an earlier round
-            has = hb[i] != 0;
+            has = kept != 0;
           }
         }
         const int slot2 = warp_append(J.ctr + C_CAND, has && split, 0xffffffffu);
