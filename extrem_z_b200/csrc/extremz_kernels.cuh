@@ -834,36 +834,31 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
     }
 #pragma unroll
     for (int d = 0; d < kNumDirs; ++d) val[d] = lb[d] >= 0 ? a[lb[d]] : T(0);
-    int row[kNumDirs];
-    T rv[kNumDirs];
-    int cnt = 0;
+    unsigned keep = 0;
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d)
+      if (lb[d] >= 0 && (!kAsc || tabs(T(val[d] - sv)) >= J.thr)) keep |= 1u << d;
+    const int cnt = __popc(keep);
+    // The order of insertionSort (:1795-1811, descending) for ascending rows
+    // and of reversed_insertionSort (:1813-1829, ascending) for descending
+    // rows, by rank: each entry's position is the number of entries before it,
+    // equal entries (the same label) in direction order as the stable
+    // insertion sort leaves them.  All indices are static, so the entries stay
+    // in registers.
+    int* out = rows + (long long)i * kRowStride;
 #pragma unroll
     for (int d = 0; d < kNumDirs; ++d) {
-      if (lb[d] < 0) continue;
-      if (kAsc && !(tabs(T(val[d] - sv)) >= J.thr)) continue;
-      row[cnt] = lb[d];
-      rv[cnt] = val[d];
-      ++cnt;
-    }
-    // Insertion sort: descending (insertionSort :1795-1811) for ascending
-    // rows, ascending (reversed_insertionSort :1813-1829) for descending rows.
-    for (int p = 1; p < cnt; ++p) {
-      const int key = row[p];
-      const T kv = rv[p];
-      int q = p - 1;
-      while (q >= 0) {
-        const int rq = row[q];
-        const bool move = kAsc ? below(rv[q], rq, kv, key) : above(rv[q], rq, kv, key);
-        if (!move) break;
-        row[q + 1] = rq;
-        rv[q + 1] = rv[q];
-        --q;
+      if (!(keep >> d & 1u)) continue;
+      int rank = 0;
+#pragma unroll
+      for (int e = 0; e < kNumDirs; ++e) {
+        if (!(keep >> e & 1u) || e == d) continue;
+        const bool before = kAsc ? above(val[e], lb[e], val[d], lb[d])
+                                 : below(val[e], lb[e], val[d], lb[d]);
+        rank += before || (lb[e] == lb[d] && e < d);
       }
-      row[q + 1] = key;
-      rv[q + 1] = kv;
+      out[rank] = lb[d];
     }
-    int* out = rows + (long long)i * kRowStride;
-    for (int p = 0; p < cnt; ++p) out[p] = row[p];
     out[14] = cnt;
   }
 }
