@@ -930,21 +930,36 @@ __global__ void __launch_bounds__(256) k_propose_cp(const Job<T>* __restrict__ j
   const int n = J.ctr[C_MM];
   const int stride = gridDim.x * blockDim.x;
   const Dims g = J.dim;
+  const int WH = g.W * g.H;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
     const int ent = J.mm[e];
     const int v = ent & ((1 << kCatShift) - 1);
     const int cat = (unsigned)ent >> kCatShift;
-    int ids[kNumDirs], dirs[kNumDirs];
-    const int nn = neighbours(v, g, ids, dirs);
+    int x, y, z;
+    coords(v, g, x, y, z);
+    // Neighbours in direction order (the reference's scan order), visited
+    // through static indices so that the values stay in registers and their
+    // loads go out together.
+    const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
     const int ot = J.otype[v];
     const T gv = J.g[v];
+    const bool need_g = (cat & kCatSaddle) || ((cat & kCatMax) && ot == 4);
+    T gn[kNumDirs];
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d)
+      gn[d] = (need_g && (valid >> d & 1)) ? J.g[v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH] : T(0);
     if (cat & kCatMin) {  // c_loop(1) (:2965-3039)
       if (ot != 0) {
+        T fn[kNumDirs];
+#pragma unroll
+        for (int d = 0; d < kNumDirs; ++d)
+          fn[d] = (valid >> d & 1) ? J.f[v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH] : T(0);
         int S = v;
         T sval = J.f[v];
-        for (int j = 0; j < nn; ++j) {
-          const T nv = J.f[ids[j]];
-          if (below(nv, ids[j], sval, S)) { S = ids[j]; sval = nv; }
+#pragma unroll
+        for (int d = 0; d < kNumDirs; ++d) {
+          const int r = v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+          if ((valid >> d & 1) && below(fn[d], r, sval, S)) { S = r; sval = fn[d]; }
         }
         const T gs = J.g[S];
         const T d = J.edit_type == 1 ? ((sval - J.bound) + gs) / T(2) - gs : -J.bound / T(J.q);
@@ -955,13 +970,17 @@ __global__ void __launch_bounds__(256) k_propose_cp(const Job<T>* __restrict__ j
     }
     if (cat & kCatSaddle) {  // c_loop(2) -> fix_saddle_local (:2804-2884)
       int dm = 0;
-      for (int j = 0; j < nn; ++j) {
-        const T nv = J.g[ids[j]];
-        if (nv < gv || (nv == gv && ids[j] < v)) dm |= 1 << dirs[j];
+#pragma unroll
+      for (int d = 0; d < kNumDirs; ++d) {
+        const int r = v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+        if ((valid >> d & 1) && (gn[d] < gv || (gn[d] == gv && r < v))) dm |= 1 << d;
       }
       const int om = J.olm[v];
-      for (int j = 0; j < nn; ++j)
-        if ((om >> dirs[j] & 1) && !(dm >> dirs[j] & 1)) propose(J, ids[j], step_delta(J, ids[j]));
+#pragma unroll
+      for (int d = 0; d < kNumDirs; ++d) {
+        const int r = v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+        if ((valid >> d & 1) && (om >> d & 1) && !(dm >> d & 1)) propose(J, r, step_delta(J, r));
+      }
       if (dm & ~om) propose(J, v, step_delta(J, v));
     }
     if (cat & kCatMax) {  // c_loop(0) (:2890-2963)
@@ -970,9 +989,10 @@ __global__ void __launch_bounds__(256) k_propose_cp(const Job<T>* __restrict__ j
       } else {
         int L = v;
         T lval = gv;
-        for (int j = 0; j < nn; ++j) {
-          const T nv = J.g[ids[j]];
-          if (above(nv, ids[j], lval, L)) { L = ids[j]; lval = nv; }
+#pragma unroll
+        for (int d = 0; d < kNumDirs; ++d) {
+          const int r = v + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+          if ((valid >> d & 1) && above(gn[d], r, lval, L)) { L = r; lval = gn[d]; }
         }
         if (L != v) propose(J, L, step_delta(J, L));
       }
