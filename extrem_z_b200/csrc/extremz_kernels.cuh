@@ -283,18 +283,28 @@ __global__ void __launch_bounds__(256) k_classify(const Job<T>* __restrict__ job
   const Job<T>& J = tile_job(jobs, sel, bx, by, bz);
   const Dims g = J.dim;
   const T* a = kDetect ? J.g : J.f;
-  if (!load_tile<T>(s, &bar, kDetect ? J.map_g : J.map_f, kDetect ? J.tma_g : J.tma_f, a, g, bx,
-                    by, bz)) {
+  // The block decides together: its threads meet at barriers further on.
+  if (!__syncthreads_and(load_tile<T>(s, &bar, kDetect ? J.map_g : J.map_f,
+                                      kDetect ? J.tma_g : J.tma_f, a, g, bx, by, bz))) {
     if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
     return;
   }
+  // Detection: the tile's mismatching vertices are gathered in shared memory
+  // and appended with one global atomic per block (per warp, the appends of a
+  // dense pass all queue on the same counter).
+  __shared__ int s_list[kDetect ? TZ * TY * TX : 1];
+  __shared__ int s_n, s_base, s_cat[3];
+  if (kDetect && threadIdx.x == 0) {
+    s_n = 0;
+    s_cat[0] = s_cat[1] = s_cat[2] = 0;
+  }
+  if (kDetect) __syncthreads();
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   for (int tz = 0; tz < TZ; ++tz) {
     const int x = bx + tx, y = by + ty, z = bz + tz;
     const bool in = x < g.W && y < g.H && z < g.D;
-    int cat = 0, v = 0;
     if (in) {
-      v = x + y * g.W + z * g.W * g.H;
+      const int v = x + y * g.W + z * g.W * g.H;
       const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
       const int valid = valid_mask(bc);
       int lm, um;
@@ -304,15 +314,27 @@ __global__ void __launch_bounds__(256) k_classify(const Job<T>* __restrict__ job
         J.otype[v] = (int8_t)t;
         J.olm[v] = (uint16_t)lm;
       } else {
-        cat = mismatch_cats(t, J.otype[v], lm, J.olm[v]);
+        const int cat = mismatch_cats(t, J.otype[v], lm, J.olm[v]);
         J.mstat[v] = (uint8_t)cat;
+        if (cat) {
+          s_list[atomicAdd(&s_n, 1)] = v | (cat << kCatShift);
+          if (cat & kCatMax) atomicAdd(&s_cat[0], 1);
+          if (cat & kCatMin) atomicAdd(&s_cat[1], 1);
+          if (cat & kCatSaddle) atomicAdd(&s_cat[2], 1);
+        }
       }
     }
-    if (kDetect) {
-      const int slot = warp_append(J.ctr + C_MM, cat != 0, 0xffffffffu);
-      if (slot >= 0) J.mm[slot] = v | (cat << kCatShift);
-      count_cats(J.ctr, cat);
+  }
+  if (kDetect) {
+    __syncthreads();
+    if (threadIdx.x == 0 && s_n) {
+      s_base = atomicAdd(J.ctr + C_MM, s_n);
+      if (s_cat[0]) atomicAdd(J.ctr + C_CMAX, s_cat[0]);
+      if (s_cat[1]) atomicAdd(J.ctr + C_CMIN, s_cat[1]);
+      if (s_cat[2]) atomicAdd(J.ctr + C_CSAD, s_cat[2]);
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < s_n; k += blockDim.x) J.mm[s_base + k] = s_list[k];
   }
 }
 
@@ -523,8 +545,9 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
   const T* a = kDec ? J.g : J.f;
   int* ds = kDec ? J.pdd : J.ds;
   int* as = kDec ? J.pda : J.as;
-  if (!load_tile<T>(s, &bar, kDec ? J.map_g : J.map_f, kDec ? J.tma_g : J.tma_f, a, g, bx, by,
-                    bz)) {
+  // The block decides together: its threads meet at a barrier further on.
+  if (!__syncthreads_and(load_tile<T>(s, &bar, kDec ? J.map_g : J.map_f, kDec ? J.tma_g : J.tma_f,
+                                      a, g, bx, by, bz))) {
     if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
     return;
   }
