@@ -31,7 +31,8 @@ F32, F64 = 0, 1
 EXPORTS = ("extremz_version", "extremz_default_params", "extremz_ctx_create",
            "extremz_ctx_destroy", "extremz_correct_device", "extremz_correct_host",
            "extremz_correct_batch", "extremz_correct_encode", "extremz_edit_stream_caps",
-           "extremz_zstd_size", "extremz_persistence_pairs", "extremz_server_create", "extremz_server_destroy",
+           "extremz_zstd_size", "extremz_persistence_pairs", "extremz_persistence_tree",
+           "extremz_server_create", "extremz_server_destroy",
            "extremz_server_submit", "extremz_server_poll", "extremz_server_wait",
            "extremz_server_get_stats", "extremz_job_footprint",
            "extremz_correct_device_noalloc", "extremz_noalloc_max_voxels",
@@ -171,6 +172,11 @@ def load(build_if_missing: bool = True):
                                                 ctypes.POINTER(ctypes.c_longlong),
                                                 ctypes.POINTER(ctypes.c_longlong), vp]
         L.extremz_persistence_pairs.restype = i32
+        L.extremz_persistence_tree.argtypes = [vp, vp, i32, i32, i32, i32, vp,
+                                               ctypes.c_longlong, vp, ctypes.c_longlong, vp, vp,
+                                               ctypes.POINTER(ctypes.c_longlong),
+                                               ctypes.POINTER(ctypes.c_longlong), vp]
+        L.extremz_persistence_tree.restype = i32
         L.extremz_zstd_size.argtypes = [vp, ctypes.c_longlong, i32]
         L.extremz_zstd_size.restype = ctypes.c_longlong
         L.extremz_correct_batch.argtypes = [vp, ctypes.POINTER(Field), i32,
@@ -370,6 +376,38 @@ class Context:
         return (mx[:2 * nx.value].view(-1, 2).cpu().numpy(),
                 mn[:2 * nn.value].view(-1, 2).cpu().numpy())
 
+    def persistence_tree(self, field, *, stream=None):
+        """Persistence pairs plus each extremum's merge target.
+
+        Returns (max_pairs, min_pairs, max_parent, min_parent): the pairs of
+        persistence_pairs() and, per extremum in the same order, the vertex of
+        the extremum it merges into at its partner (the largest maximum /
+        smallest minimum of its saddle's row, before constructMergeTree's
+        compression; the global extremum holds itself).  See
+        extremz_persistence_tree and merge_tree_branches().
+        """
+        import torch
+        assert field.is_cuda and field.is_contiguous()
+        dt = {torch.float32: F32, torch.float64: F64}[field.dtype]
+        w, h, d = _whd(tuple(field.shape))
+        n = w * h * d
+        mx = torch.empty(2 * n, dtype=torch.int32, device=field.device)
+        mn = torch.empty(2 * n, dtype=torch.int32, device=field.device)
+        px = torch.empty(n, dtype=torch.int32, device=field.device)
+        pn = torch.empty(n, dtype=torch.int32, device=field.device)
+        nx, nn = ctypes.c_longlong(), ctypes.c_longlong()
+        if stream is None:
+            stream = torch.cuda.current_stream(field.device).cuda_stream
+        _check(load().extremz_persistence_tree(self._h, field.data_ptr(), dt, w, h, d,
+                                               mx.data_ptr(), 2 * n, mn.data_ptr(), 2 * n,
+                                               px.data_ptr(), pn.data_ptr(), ctypes.byref(nx),
+                                               ctypes.byref(nn), stream),
+               allow_cap=False)
+        torch.cuda.synchronize(field.device)
+        return (mx[:2 * nx.value].view(-1, 2).cpu().numpy(),
+                mn[:2 * nn.value].view(-1, 2).cpu().numpy(),
+                px[:nx.value].cpu().numpy(), pn[:nn.value].cpu().numpy())
+
     def compare_topology(self, f, g):
         """Topology report of a corrected field g against its original f: the
         merge-tree persistence pairs of both (split and join trees), how many
@@ -388,6 +426,12 @@ class Context:
             out[name] = {"pairs_original": len(sa), "pairs_corrected": len(sb),
                          "identical": len(common), "same": sa == sb,
                          "max_persistence_change": float(dper)}
+        # Branch decompositions of the split tree, compared branch by branch
+        # as the CPU driver does (main.cpp:478-504).
+        tf, tg = self.persistence_tree(f), self.persistence_tree(g)
+        bf = merge_tree_branches(fv, tf[0], tf[2], split=True)
+        bg = merge_tree_branches(gv, tg[0], tg[2], split=True)
+        out["split"]["branches"] = compare_branches(bf, bg)
         return out
 
     # -- batches ------------------------------------------------------------
@@ -437,6 +481,94 @@ class Context:
                                          ctypes.byref(p), ctypes.byref(r), stream)
         _check(st)
         return CorrectionReport.of(r)
+
+
+def _tree_rank(values: np.ndarray, verts: np.ndarray, split: bool) -> np.ndarray:
+    """Rank of vertices in a tree's order: by (value, id) ascending for the
+    split tree, descending for the join tree; a vertex listed twice gets the
+    same rank."""
+    verts = np.asarray(verts, np.int64)
+    u = np.unique(verts)
+    r = np.lexsort((u, np.asarray(values, np.float64)[u]))   # ascending (value, id)
+    rank_u = np.empty(len(u), np.int64)
+    rank_u[r] = np.arange(len(u))
+    if not split:
+        rank_u = len(u) - 1 - rank_u
+    return rank_u[np.searchsorted(u, verts)]
+
+
+def _compress_parents(values, pairs, par, split: bool) -> np.ndarray:
+    """constructMergeTree's loop (:1869-1885) on parent ranks: a parent whose
+    own partner comes before the extremum's partner in the descending order
+    (it died first) is replaced by its parent, until nothing moves."""
+    pairs = np.asarray(pairs, np.int64)
+    n = len(pairs)
+    par = np.array(par, np.int64)
+    root = n - 1
+    par[root] = root
+    # Partner position in the descending order (smaller = earlier).
+    srank = np.full(n, np.iinfo(np.int64).max)
+    srank[:root] = -_tree_rank(values, pairs[:root, 0], split)
+    while True:
+        nxt = par[par]
+        move = (nxt != par) & (srank[par] < srank)
+        if not move.any():
+            return par
+        par = np.where(move, nxt, par)
+
+
+def merge_tree_branches(values, pairs, parent, *, split: bool = True):
+    """Branch decomposition of a merge tree (constructMergeTree,
+    src/ExtreM.cpp:1863-1918) from persistence_tree() output.
+
+    values: the field, flat.  pairs: (n, 2) (partner, extremum) by extremum
+    rank, the global extremum last.  parent: per extremum, the extremum it
+    merges into at its partner.  Each parent is first compressed to the
+    first extremum along the parent chain that is still alive at the
+    extremum's partner (whose own partner comes later in the tree order),
+    as constructMergeTree's loop does.  Returns one int64 array of vertex
+    ids per extremum: the extremum, the partners of the branches that join
+    it, and its own partner (the opposite global extremum for the global
+    one), in descending tree order -- the vertices of a reference Branch.
+    The reference orders vertices by getSortedPositions, a sort by value
+    alone whose order among equal values is unspecified; here ties go by id.
+    """
+    pairs = np.asarray(pairs, np.int64)
+    n = len(pairs)
+    if n == 0:
+        return []
+    ext, sad = pairs[:, 1], pairs[:, 0]
+    idx = np.argsort(ext)
+    par = _compress_parents(values, pairs, idx[np.searchsorted(ext[idx], np.asarray(parent, np.int64))],
+                            split)
+    # Vertices of every branch with their tree-order keys.
+    allv = np.concatenate([ext, sad])
+    key = _tree_rank(values, allv, split)
+    kext, ksad = key[:n], key[n:]
+    members = [[(int(kext[b]), int(ext[b]))] for b in range(n)]
+    for b in range(n):
+        p = int(par[b])
+        if p != b:
+            members[b].append((int(ksad[b]), int(sad[b])))
+            members[p].append((int(ksad[b]), int(sad[b])))
+        else:
+            members[b].append((-1, int(sad[b])))
+    return [np.array([v for _, v in sorted(m, reverse=True)], np.int64) for m in members]
+
+
+def compare_branches(a, b):
+    """Branch-by-branch comparison of two decompositions (main.cpp:478-504):
+    how many branches hold the same vertex sequence, and the first few that
+    do not, with the first position where they differ."""
+    same, diffs = 0, []
+    for i, (x, y) in enumerate(zip(a, b)):
+        if len(x) == len(y) and np.array_equal(x, y):
+            same += 1
+        elif len(diffs) < 8:
+            k = next((p for p in range(min(len(x), len(y))) if x[p] != y[p]), min(len(x), len(y)))
+            diffs.append({"branch": i, "position": int(k)})
+    return {"branches_original": len(a), "branches_corrected": len(b), "identical": same,
+            "same": same == len(a) == len(b), "first_differences": diffs}
 
 
 class Server:

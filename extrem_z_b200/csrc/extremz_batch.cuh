@@ -496,7 +496,7 @@ class BatchEngine {
   // tree into min_pairs (2 per minimum), device buffers of the caller.
   // counts (host) receives the numbers of maxima and minima.  Synchronises.
   int persistence(int slot, int* max_pairs, long long max_cap, int* min_pairs, long long min_cap,
-                  long long* counts) {
+                  long long* counts, int* max_parent = nullptr, int* min_parent = nullptr) {
     JobHost<T>& jh = slots_[slot];
     const Job<T>& J = jh.J;
     const int ne[2] = {h(slot, C_NMAX), h(slot, C_NMIN)};
@@ -529,7 +529,7 @@ class BatchEngine {
     const size_t a = ((size_t)nmaxall * 8 + 255) & ~size_t(255);
     const size_t b = ((size_t)nmaxall * 4 + 255) & ~size_t(255);
     const size_t rows_bytes = (((size_t)std::max(ns[0], ns[1]) + 1) * kPpRow * 4 + 255) & ~size_t(255);
-    const size_t total = 2 * a + 9 * b + rows_bytes + ((cub_bytes + 255) & ~size_t(255)) + 256;
+    const size_t total = 2 * a + 10 * b + rows_bytes + ((cub_bytes + 255) & ~size_t(255)) + 256;
     char* base = static_cast<char*>(scratch(total));
     if (!base) {
       cudaFreeAsync(cand, st_);
@@ -546,6 +546,7 @@ class BatchEngine {
     int* largest = reinterpret_cast<int*>(take(b));
     int* ptr = reinterpret_cast<int*>(take(b));
     int* pair = reinterpret_cast<int*>(take(b));
+    int* lmax = reinterpret_cast<int*>(take(b));
     int* cnt = reinterpret_cast<int*>(take(b));
     int* rows = reinterpret_cast<int*>(take(rows_bytes));
     void* cub_tmp = take((cub_bytes + 255) & ~size_t(255));
@@ -596,7 +597,7 @@ class BatchEngine {
         if (n_s) launch(K_OTHER, k_pp_largest, grid_, 256, (const int*)rows, (const int*)cnt, n_s,
                         n_e - 1, largest);
         launch(K_OTHER, k_pp_pair, grid_, 256, (const int*)rows, (const int*)cnt, n_e, n_s,
-               largest, ptr, pair, flag);
+               largest, ptr, pair, lmax, flag);
         int changed = 0;
         EZ_CHECK(cudaMemcpyAsync(&changed, flag, 4, cudaMemcpyDeviceToHost, st_));
         EZ_CHECK(cudaStreamSynchronize(st_));
@@ -606,7 +607,7 @@ class BatchEngine {
       }
       launch(K_OTHER, k_pp_out, grid_, 256, (const int*)pair, n_e, (const int*)ext_li[side],
              elist[side], (const int*)sad_li, slist[side], glob[1 - side],
-             kmax ? max_pairs : min_pairs);
+             kmax ? max_pairs : min_pairs, (const int*)lmax, kmax ? max_parent : min_parent);
     }
     int jump_err = 0;
     cudaMemcpyAsync(&jump_err, flag + 1, 4, cudaMemcpyDeviceToHost, st_);

@@ -372,7 +372,7 @@ static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* table
 template <class T>
 static int analyze_one(BatchEngine<T>& e, cudaStream_t st, const T* field, int W, int H, int D,
                        int* max_pairs, long long max_cap, int* min_pairs, long long min_cap,
-                       long long* counts) {
+                       long long* counts, int* max_parent = nullptr, int* min_parent = nullptr) {
   e.set_stream(st);
   EZ_RUN(e.init(nullptr, nullptr));
   extremz_params p;
@@ -383,7 +383,9 @@ static int analyze_one(BatchEngine<T>& e, cudaStream_t st, const T* field, int W
   int rc = EXTREMZ_OK;
   while (e.job(slot).pc != PC_DONE && rc == EXTREMZ_OK) rc = e.tick();
   if (rc == EXTREMZ_OK) rc = e.job(slot).status;
-  if (rc == EXTREMZ_OK) rc = e.persistence(slot, max_pairs, max_cap, min_pairs, min_cap, counts);
+  if (rc == EXTREMZ_OK)
+    rc = e.persistence(slot, max_pairs, max_cap, min_pairs, min_cap, counts, max_parent,
+                       min_parent);
   e.release(slot);
   return rc;
 }
@@ -992,11 +994,12 @@ long long extremz_zstd_size(const void* host, long long bytes, int level) {
   return ziserr(n) ? -1 : (long long)n;
 }
 
-extremz_status extremz_persistence_pairs(extremz_ctx* ctx, const void* d_field, int dtype,
-                                        int width, int height, int depth, int32_t* d_max_pairs,
-                                        long long max_pairs_cap, int32_t* d_min_pairs,
-                                        long long min_pairs_cap, long long* n_max,
-                                        long long* n_min, void* stream) {
+extremz_status extremz_persistence_tree(extremz_ctx* ctx, const void* d_field, int dtype, int width,
+                                       int height, int depth, int32_t* d_max_pairs,
+                                       long long max_pairs_cap, int32_t* d_min_pairs,
+                                       long long min_pairs_cap, int32_t* d_max_parent,
+                                       int32_t* d_min_parent, long long* n_max, long long* n_min,
+                                       void* stream) {
   if (!ctx || !d_field) return EXTREMZ_BAD_ARG;
   extremz_params p;
   extremz_default_params(&p);
@@ -1011,15 +1014,27 @@ extremz_status extremz_persistence_pairs(extremz_ctx* ctx, const void* d_field, 
   if (rc == EXTREMZ_OK) {
     if (dtype == EXTREMZ_F32)
       rc = analyze_one(ctx->c.e32, st, (const float*)d_field, width, height, depth, d_max_pairs,
-                       max_pairs_cap, d_min_pairs, min_pairs_cap, counts);
+                       max_pairs_cap, d_min_pairs, min_pairs_cap, counts, d_max_parent,
+                       d_min_parent);
     else
       rc = analyze_one(ctx->c.e64, st, (const double*)d_field, width, height, depth, d_max_pairs,
-                       max_pairs_cap, d_min_pairs, min_pairs_cap, counts);
+                       max_pairs_cap, d_min_pairs, min_pairs_cap, counts, d_max_parent,
+                       d_min_parent);
   }
   if (n_max) *n_max = counts[0];
   if (n_min) *n_min = counts[1];
   if (prev != ctx->c.device) cudaSetDevice(prev);
   return (extremz_status)rc;
+}
+
+extremz_status extremz_persistence_pairs(extremz_ctx* ctx, const void* d_field, int dtype,
+                                        int width, int height, int depth, int32_t* d_max_pairs,
+                                        long long max_pairs_cap, int32_t* d_min_pairs,
+                                        long long min_pairs_cap, long long* n_max,
+                                        long long* n_min, void* stream) {
+  return extremz_persistence_tree(ctx, d_field, dtype, width, height, depth, d_max_pairs,
+                                  max_pairs_cap, d_min_pairs, min_pairs_cap, nullptr, nullptr,
+                                  n_max, n_min, stream);
 }
 
 extremz_status extremz_correct_batch(extremz_ctx* ctx, const extremz_field* fields, int n,

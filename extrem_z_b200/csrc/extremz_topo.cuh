@@ -207,10 +207,13 @@ __global__ void k_pp_largest(const int* __restrict__ rows, const int* __restrict
     }
 }
 
-// Pairing of the round; resets largest for the next round.
+// Pairing of the round; resets largest for the next round.  lmax keeps the
+// extremum each paired one merges into (its saddle row's largest entry, the
+// second element of the reference's maximaTriplets, :2187), which ptr then
+// loses to compression.
 __global__ void k_pp_pair(const int* __restrict__ rows, const int* __restrict__ cnt, int ne, int ns,
                           int* __restrict__ largest, int* __restrict__ ptr, int* __restrict__ pair,
-                          int* changed) {
+                          int* __restrict__ lmax, int* changed) {
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += stride) {
     const int i = largest[e];
@@ -218,7 +221,9 @@ __global__ void k_pp_pair(const int* __restrict__ rows, const int* __restrict__ 
     if (i >= ns || pair[e] >= 0) continue;
     if (rows[(long long)i * kPpRow] == e) {
       pair[e] = i;
-      ptr[e] = rows[(long long)i * kPpRow + cnt[i] - 1];
+      const int l = rows[(long long)i * kPpRow + cnt[i] - 1];
+      ptr[e] = l;
+      lmax[e] = l;
       *changed = 1;
     }
   }
@@ -273,14 +278,19 @@ __global__ void k_iota(int* __restrict__ p, int n) {
 
 // Output pairs (partner vertex, extremum vertex) by extremum rank; the global
 // extremum's partner is the opposite global extremum, an unpaired one -1.
+// parent (optional): the vertex of the extremum each one merges into (lmax),
+// the global extremum its own, an unpaired one -1.
 __global__ void k_pp_out(const int* __restrict__ pair, int ne, const int* __restrict__ ext_li,
                          const int* __restrict__ elist, const int* __restrict__ sad_li,
-                         const int* __restrict__ slist, int opposite, int* __restrict__ out) {
+                         const int* __restrict__ slist, int opposite, int* __restrict__ out,
+                         const int* __restrict__ lmax, int* __restrict__ parent) {
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += stride) {
     const int i = pair[e];
     out[2 * e] = e == ne - 1 ? opposite : (i >= 0 ? slist[sad_li[i]] : -1);
     out[2 * e + 1] = elist[ext_li[e]];
+    if (parent)
+      parent[e] = e == ne - 1 ? elist[ext_li[e]] : (i >= 0 ? elist[ext_li[lmax[e]]] : -1);
   }
 }
 

@@ -223,8 +223,8 @@ extremz_status extremz_correct_encode(extremz_ctx* ctx, const void* d_orig, void
  * (d_min_pairs), extrema ordered by value then id (ascending for maxima,
  * descending for minima).  Caps are in int32 entries; n_max / n_min receive
  * the numbers of extrema (BAD_ARG when a buffer is too small).
- * Replaces: constructPersistencePairs / compute_MergeT (src/ExtreM.cpp
- * :1863-1918, :2930-2952) -- the same extremum-graph pairing, on the
+ * Replaces: constructPersistencePairs (src/ExtreM.cpp :2132-2249), called by
+ * compute_MergeT (:2930-2952) -- the same extremum-graph pairing, on the
  * field's own critical points and manifold labels.
  */
 extremz_status extremz_persistence_pairs(extremz_ctx* ctx, const void* d_field, int dtype,
@@ -232,6 +232,24 @@ extremz_status extremz_persistence_pairs(extremz_ctx* ctx, const void* d_field, 
                                         long long max_pairs_cap, int32_t* d_min_pairs,
                                         long long min_pairs_cap, long long* n_max,
                                         long long* n_min, void* stream);
+
+/*
+ * The same pairs, plus per extremum the vertex of the extremum it merges into
+ * at its partner vertex (d_max_parent / d_min_parent, one int32 per extremum
+ * in the same order, each buffer at least half the pair buffer's cap; either
+ * may be NULL): the largest maximum (smallest minimum) of its saddle's row
+ * when it pairs, the second element of the reference's maximaTriplets
+ * (constructPersistencePairs :2183-2187).  The global extremum holds itself.
+ * The branch decomposition of constructMergeTree (:1863-1918) follows from
+ * these by compressing each parent to the first one still alive at the
+ * extremum's partner (extrem_z_b200.api.merge_tree_branches).
+ */
+extremz_status extremz_persistence_tree(extremz_ctx* ctx, const void* d_field, int dtype, int width,
+                                       int height, int depth, int32_t* d_max_pairs,
+                                       long long max_pairs_cap, int32_t* d_min_pairs,
+                                       long long min_pairs_cap, int32_t* d_max_parent,
+                                       int32_t* d_min_parent, long long* n_max, long long* n_min,
+                                       void* stream);
 
 /* zstd-compressed size of a host buffer at the given level (the reference
  * compresses both streams with the zstd tool at its default level 3), from

@@ -1142,7 +1142,8 @@ bool dims_ok(int W, int H, int D) {
 // is the opposite global extremum.
 // ---------------------------------------------------------------------------
 template <class T>
-void elder_pairs(const T* f, const Grid& g, bool split, std::vector<int>& out) {
+void elder_pairs(const T* f, const Grid& g, bool split, std::vector<int>& out,
+                 std::vector<int>* parents = nullptr) {
   const int N = g.N;
   std::vector<int> order(N);
   for (int v = 0; v < N; ++v) order[v] = v;
@@ -1161,6 +1162,7 @@ void elder_pairs(const T* f, const Grid& g, bool split, std::vector<int>& out) {
   };
   std::vector<int> ext;           // extrema in processing order
   std::vector<int> partner(N, -1);
+  std::vector<int> merged_into(N, -1);  // the eldest of the surviving component
   for (int k = 0; k < N; ++k) {
     const int v = order[k];
     int ids[14];
@@ -1186,17 +1188,23 @@ void elder_pairs(const T* f, const Grid& g, bool split, std::vector<int>& out) {
     for (int q = 0; q < nr; ++q)
       if (roots[q] != keep) {
         partner[eldest[roots[q]]] = v;
+        merged_into[eldest[roots[q]]] = eldest[keep];
         parent[roots[q]] = keep;
       }
     parent[v] = keep;
   }
   // Ranks: ascending in the tree's order = reverse of the processing order.
   out.clear();
+  if (parents) parents->clear();
   const int opposite = order[N - 1];
   for (int i = (int)ext.size() - 1; i >= 0; --i) {
     const int e = ext[i];
     out.push_back(i == 0 ? opposite : partner[e]);
     out.push_back(e);
+    // The branch an extremum joins: the elder rule's survivor at its merge
+    // vertex, which is alive there by construction (constructMergeTree's
+    // compressed parent, src/ExtreM.cpp:1863-1918); the global extremum its own.
+    if (parents) parents->push_back(i == 0 ? e : merged_into[e]);
   }
 }
 
@@ -1225,6 +1233,33 @@ int oracle_persistence_pairs(const void* f, int dtype, int W, int H, int D, int3
   if ((long long)mx.size() > max_cap || (long long)mn.size() > min_cap) return -3;
   std::memcpy(max_pairs, mx.data(), mx.size() * 4);
   std::memcpy(min_pairs, mn.data(), mn.size() * 4);
+  return 0;
+}
+
+// The same pairs plus, per extremum, the extremum whose branch it joins at
+// its partner vertex (one int per extremum into max_parent / min_parent,
+// caps in ints as for the pairs).
+int oracle_persistence_tree(const void* f, int dtype, int W, int H, int D, int32_t* max_pairs,
+                            long long max_cap, int32_t* min_pairs, long long min_cap,
+                            int32_t* max_parent, int32_t* min_parent, long long* n_max,
+                            long long* n_min) {
+  if (!dims_ok(W, H, D) || !f) return -1;
+  Grid g{W, H, D, W * H * D};
+  std::vector<int> mx, mn, px, pn;
+  if (dtype == 0) {
+    elder_pairs((const float*)f, g, true, mx, &px);
+    elder_pairs((const float*)f, g, false, mn, &pn);
+  } else {
+    elder_pairs((const double*)f, g, true, mx, &px);
+    elder_pairs((const double*)f, g, false, mn, &pn);
+  }
+  *n_max = (long long)px.size();
+  *n_min = (long long)pn.size();
+  if ((long long)mx.size() > max_cap || (long long)mn.size() > min_cap) return -3;
+  std::memcpy(max_pairs, mx.data(), mx.size() * 4);
+  std::memcpy(min_pairs, mn.data(), mn.size() * 4);
+  std::memcpy(max_parent, px.data(), px.size() * 4);
+  std::memcpy(min_parent, pn.data(), pn.size() * 4);
   return 0;
 }
 

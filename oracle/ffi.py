@@ -67,6 +67,10 @@ def lib():
                                                vp, ctypes.c_longlong,
                                                ctypes.POINTER(ctypes.c_longlong),
                                                ctypes.POINTER(ctypes.c_longlong)]
+        L.oracle_persistence_tree.argtypes = [vp, i32, i32, i32, i32, vp, ctypes.c_longlong,
+                                              vp, ctypes.c_longlong, vp, vp,
+                                              ctypes.POINTER(ctypes.c_longlong),
+                                              ctypes.POINTER(ctypes.c_longlong)]
         L.oracle_encode.argtypes = [vp, vp, vp, vp, i32, ctypes.c_longlong, ctypes.c_double,
                                     i32, i32, vp, ctypes.c_longlong, vp, ctypes.c_longlong,
                                     ctypes.POINTER(EditReport)]
@@ -189,3 +193,22 @@ def persistence_pairs(f: np.ndarray):
     if rc != 0:
         raise ValueError(f"oracle_persistence_pairs returned {rc}")
     return mx[:2 * nx.value].reshape(-1, 2), mn[:2 * nn.value].reshape(-1, 2)
+
+
+def persistence_tree(f: np.ndarray):
+    """Elder-rule pairs and branch parents: (max pairs (n, 2), min pairs (m, 2),
+    max parents (n,), min parents (m,)); a parent is the extremum whose branch
+    the extremum joins at its partner vertex (the global extremum its own)."""
+    f = np.ascontiguousarray(f)
+    w, h, d = _dims(f)
+    cap = 2 * f.size
+    mx, mn = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+    px, pn = np.zeros(f.size, np.int32), np.zeros(f.size, np.int32)
+    nx, nn = ctypes.c_longlong(), ctypes.c_longlong()
+    rc = lib().oracle_persistence_tree(f.ctypes.data, _dtype_code(f), w, h, d, mx.ctypes.data,
+                                       cap, mn.ctypes.data, cap, px.ctypes.data, pn.ctypes.data,
+                                       ctypes.byref(nx), ctypes.byref(nn))
+    if rc != 0:
+        raise ValueError(f"oracle_persistence_tree returned {rc}")
+    return (mx[:2 * nx.value].reshape(-1, 2), mn[:2 * nn.value].reshape(-1, 2),
+            px[:nx.value].copy(), pn[:nn.value].copy())

@@ -59,3 +59,37 @@ def test_correction_report():
     t, _ = ffi.classify(g.cpu().numpy())
     assert rep["join"]["pairs_corrected"] == int((t == 0).sum())
     assert rep["split"]["pairs_corrected"] == int((t == 4).sum())
+
+
+@pytest.mark.parametrize("name", [c[0] for c in CASES])
+def test_merge_targets_match_rounds(name):
+    # Each extremum's merge target (constructPersistencePairs' largestMax)
+    # against the numpy restatement of the same rounds, exactly; and the
+    # branches built from them.
+    import torch
+    from extrem_z_b200 import api
+    from oracle import merge_tree
+    fld = dict(CASES)[name]()
+    fv = fld.f.astype(np.float64).ravel()
+    mx, mn, px, pn = api.context(0).persistence_tree(torch.from_numpy(fld.f).cuda())
+    for pairs, par, split in ((mx, px, True), (mn, pn, False)):
+        rpairs, rpar = merge_tree.persistence_tree(fld.f, split)
+        assert np.array_equal(pairs, rpairs), name
+        assert np.array_equal(par, rpar), name
+        b = api.merge_tree_branches(fv, pairs, par, split=split)
+        rb = api.merge_tree_branches(fv, rpairs, rpar, split=split)
+        assert all(np.array_equal(x, y) for x, y in zip(b, rb)), name
+
+
+def test_branch_report_of_a_correction():
+    import torch
+    from extrem_z_b200 import api
+    fld = synth.plain_64(np.float64)
+    f = torch.from_numpy(fld.f).cuda()
+    g = torch.from_numpy(fld.decp.copy()).cuda()
+    ctx = api.context(0)
+    ctx.correct_device(f, g, fld.eb, final_join=False)
+    rep = ctx.compare_topology(f, g)["split"]["branches"]
+    assert rep["branches_original"] == rep["branches_corrected"] > 0
+    assert 0 <= rep["identical"] <= rep["branches_original"]
+    assert rep["same"] == (rep["identical"] == rep["branches_original"])
