@@ -280,9 +280,14 @@ static void scatter_host(T* out, const int* ids, const T* vals, int n) {
     return;
   }
   std::vector<std::thread> th;
-  for (int t = 1; t < nt; ++t)
-    th.emplace_back(part, (int)((long long)n * t / nt), (int)((long long)n * (t + 1) / nt));
+  int done = 1;  // parts [0, done) are handed out; a thread that cannot start leaves its part here
+  try {
+    for (int t = 1; t < nt; ++t, ++done)
+      th.emplace_back(part, (int)((long long)n * t / nt), (int)((long long)n * (t + 1) / nt));
+  } catch (...) {
+  }
   part(0, (int)((long long)n / nt));
+  if (done < nt) part((int)((long long)n * done / nt), n);
   for (auto& x : th) x.join();
 }
 
