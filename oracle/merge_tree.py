@@ -89,12 +89,12 @@ def _rows_sorted_unique(e: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     return r, cnt
 
 
-def persistence_tree(f: np.ndarray, split: bool = True):
-    """(pairs (n, 2), merge targets (n,)) of one tree, extrema by rank.
-
-    pairs[k] = (partner vertex, extremum vertex); targets[k] = the vertex of
-    the extremum it merges into (the global extremum: itself; unpaired: -1).
-    """
+def extremum_graph(f: np.ndarray, split: bool = True) -> dict:
+    """The extremum graph of one tree: rank (every vertex's position in the
+    tree's order), ext (extrema, ascending), sad (merge vertices,
+    descending), rows / cnt (per merge vertex, distinct extremum ranks
+    ascending, -1 padded; single-entry rows emptied) and opposite (the
+    vertex first in the tree's order)."""
     global _TABLE
     if _TABLE is None:
         _TABLE = _link_components_table()
@@ -133,6 +133,20 @@ def persistence_tree(f: np.ndarray, split: bool = True):
         on = (u >= 0) & ((side[sad] >> d) & 1).astype(bool)
         e[:, d] = np.where(on, erank[lab[np.where(on, u, 0)]], -1)
     rows, cnt = _rows_sorted_unique(e)
+    opposite = int(np.argmax(rank == 0))            # first in the tree's order
+    return {"rank": rank, "ext": ext, "sad": sad, "rows": rows, "cnt": cnt,
+            "opposite": opposite}
+
+
+def persistence_tree(f: np.ndarray, split: bool = True):
+    """(pairs (n, 2), merge targets (n,)) of one tree, extrema by rank.
+
+    pairs[k] = (partner vertex, extremum vertex); targets[k] = the vertex of
+    the extremum it merges into (the global extremum: itself; unpaired: -1).
+    """
+    gr = extremum_graph(f, split)
+    ext, sad, rows, cnt = gr["ext"], gr["sad"], gr["rows"], gr["cnt"]
+    ne, ns = len(ext), len(sad)
     glob = ne - 1
     ptr = np.arange(ne)
     pair = np.full(ne, -1, np.int64)
@@ -160,7 +174,7 @@ def persistence_tree(f: np.ndarray, split: bool = True):
             ptr = nxt
         e = np.where(rows >= 0, ptr[np.where(rows >= 0, rows, 0)], -1)
         rows, cnt = _rows_sorted_unique(e)
-    opposite = int(np.argmax(rank == 0))            # first in the tree's order
+    opposite = gr["opposite"]
     out = np.empty((ne, 2), np.int64)
     out[:, 1] = ext
     out[:, 0] = np.where(pair >= 0, sad[np.maximum(pair, 0)], -1)
