@@ -118,7 +118,11 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
-            time.sleep(0.3)
+            # nvidia-smi's start-up (driver library load and init) must not
+            # overlap the timed region: wait for its first sample.
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10.0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
@@ -746,7 +750,7 @@ def run_form(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
                     choices=sorted(WORKLOADS) + sorted(FORM_WORKLOADS))
