@@ -684,7 +684,11 @@ class BatchEngine {
     if (graph && !pending_.empty()) EZ_RUN(run_recorded());
     if (!issued_) return EXTREMZ_OK;
     EZ_CHECK(cudaGetLastError());
-    EZ_CHECK(cudaMemcpyAsync(ctr_host_, ctr_dev_, sizeof(int) * C_COUNT * kMaxSel,
+    // The counter blocks up to the last slot in use (the host reads no other).
+    int hi = 0;
+    for (int i = 0; i < kMaxSel; ++i)
+      if (slots_[i].used) hi = i + 1;
+    EZ_CHECK(cudaMemcpyAsync(ctr_host_, ctr_dev_, sizeof(int) * C_COUNT * (size_t)hi,
                              cudaMemcpyDeviceToHost, st_));
     return EXTREMZ_OK;
   }
@@ -822,6 +826,13 @@ class BatchEngine {
   template <class A>
   void sig_append(const A& a) {
     sig_.append(reinterpret_cast<const char*>(&a), sizeof(A));
+  }
+  // A job selection by its used part (kernels read no entry past n): the
+  // signature of a one-job tick stays a few hundred bytes to hash.
+  void sig_append(const Sel& s) {
+    sig_.append(reinterpret_cast<const char*>(&s.n), sizeof(int));
+    sig_.append(reinterpret_cast<const char*>(s.idx), sizeof(int) * (size_t)s.n);
+    sig_.append(reinterpret_cast<const char*>(s.off), sizeof(int) * (size_t)(s.n + 1));
   }
 
   template <class... KArgs, class... Args>
