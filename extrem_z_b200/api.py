@@ -557,18 +557,28 @@ def merge_tree_branches(values, pairs, parent, *, split: bool = True):
 
 
 def compare_branches(a, b):
-    """Branch-by-branch comparison of two decompositions (main.cpp:478-504):
-    how many branches hold the same vertex sequence, and the first few that
-    do not, with the first position where they differ."""
-    same, diffs = 0, []
+    """Comparison of two branch decompositions.
+
+    by rank: branch i against branch i, as the CPU driver prints it
+    (main.cpp:478-504) -- a correction that reorders two maxima by value
+    shifts every branch between them; by extremum: each branch against the
+    branch of the same extremum vertex, the count that shows whether the
+    merge tree kept its shape.  first_differences lists a few branches (by
+    rank) that differ, with the first position where they do.
+    """
+    same_rank, diffs = 0, []
     for i, (x, y) in enumerate(zip(a, b)):
         if len(x) == len(y) and np.array_equal(x, y):
-            same += 1
+            same_rank += 1
         elif len(diffs) < 8:
             k = next((p for p in range(min(len(x), len(y))) if x[p] != y[p]), min(len(x), len(y)))
             diffs.append({"branch": i, "position": int(k)})
-    return {"branches_original": len(a), "branches_corrected": len(b), "identical": same,
-            "same": same == len(a) == len(b), "first_differences": diffs}
+    by_ext = {int(y[0]): y for y in b if len(y)}
+    same_ext = sum(1 for x in a if len(x) and int(x[0]) in by_ext
+                   and np.array_equal(x, by_ext[int(x[0])]))
+    return {"branches_original": len(a), "branches_corrected": len(b),
+            "identical_by_rank": same_rank, "identical_by_extremum": same_ext,
+            "same": same_rank == len(a) == len(b), "first_differences": diffs}
 
 
 class Server:

@@ -91,5 +91,5 @@ def test_branch_report_of_a_correction():
     ctx.correct_device(f, g, fld.eb, final_join=False)
     rep = ctx.compare_topology(f, g)["split"]["branches"]
     assert rep["branches_original"] == rep["branches_corrected"] > 0
-    assert 0 <= rep["identical"] <= rep["branches_original"]
-    assert rep["same"] == (rep["identical"] == rep["branches_original"])
+    assert 0 <= rep["identical_by_rank"] <= rep["identical_by_extremum"] <= rep["branches_original"]
+    assert rep["same"] == (rep["identical_by_rank"] == rep["branches_original"])

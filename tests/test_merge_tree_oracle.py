@@ -75,3 +75,13 @@ def test_rounds_on_line_field():
     f = np.array([1.0, 0.0, 3.0, -1.0, 2.0]).reshape(1, 1, 5)
     pairs, tgt = merge_tree.persistence_tree(f, True)
     assert pairs.tolist() == [[1, 0], [3, 4], [3, 2]] and tgt.tolist() == [2, 2, 2]
+
+
+def test_branch_comparison_by_rank_and_by_extremum():
+    a = [np.array([5, 3, 1]), np.array([7, 2]), np.array([9, 3, 3])]
+    b = [np.array([7, 2]), np.array([5, 3, 1]), np.array([9, 3, 3])]   # two maxima swapped in rank
+    rep = api.compare_branches(a, b)
+    assert rep["identical_by_rank"] == 1 and rep["identical_by_extremum"] == 3
+    assert not rep["same"]
+    assert [d["branch"] for d in rep["first_differences"]] == [0, 1]
+    assert api.compare_branches(a, a)["same"]
