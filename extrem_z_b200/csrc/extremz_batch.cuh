@@ -110,6 +110,7 @@ constexpr long long job_bytes_voxels(long long n, long long ksz) {
          + arr_bytes(n, 4) + arr_bytes(n, 1)                        // cand_j, mis
          + 2 * arr_bytes(n, 4)                                      // pdd, pda
          + arr_bytes((n + 31) / 32, 4) + arr_bytes(n, 1)            // change bitset, dirtyv
+         + arr_bytes(2 * ((n + kCpBlock - 1) / kCpBlock), 1)        // dirtyv per 1024-id block, x2
          + arr_bytes(n, 1)                                          // tile marks (<= n tiles)
          + arr_bytes(4 * ((n + kCpBlock - 1) / kCpBlock), 4)        // CP block counts
          + 4096;
@@ -351,6 +352,7 @@ class BatchEngine {
     J.vchg = A.take<unsigned>((N + 31) / 32);
     J.dirtyv = A.take<uint8_t>(N);
     jh.nb = (N + kCpBlock - 1) / kCpBlock;
+    J.bdirty = A.take<uint8_t>(2ll * jh.nb);
     jh.bcount = A.take<int>(4ll * jh.nb);
     J.cpoff = jh.bcount;
     jh.ntiles = ((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);

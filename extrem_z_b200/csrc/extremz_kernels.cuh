@@ -50,6 +50,7 @@ struct Job {
   unsigned* vchg;     // bitset: vertices whose value changed since the last computed round
   unsigned* edited;   // bitset: vertices whose value changed in this correction (or null)
   uint8_t* dirtyv;    // per vertex: an input of its saddle rows changed this round
+  uint8_t* bdirty;    // 2 x per 1024-id block: some dirtyv byte in it is set (when N % 4 == 0)
   uint8_t* has2; uint8_t* has1;  // per saddle row: its wrong-neighbour seed bit
   int* cpoff;         // per list (2-saddles, 1-saddles, maxima, minima) and
                       // 1024-id block: offset of the block's first entry
@@ -109,6 +110,8 @@ enum Ctr : int {
 };
 // Error bits in ctr[C_ERROR].
 constexpr int kErrJump = 1, kErrPath = 2, kErrTile = 4, kErrResolve = 8;
+// Ids per changed-input flag of the jump (the CP-list block size, kCpBlock).
+constexpr int kCpBlockJ = 1024;
 
 template <class T>
 __device__ __forceinline__ T tabs(T v) { return v < T(0) ? -v : v; }
@@ -588,7 +591,7 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
 // decompressed field it also writes each vertex's label-mismatch bits
 // and changed-input bytes for the saddle pass.
 template <class T, bool kDec>
-__global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
+__global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ jobs,
                                                const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
@@ -655,52 +658,66 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
       // the vertex-per-thread loop, with eight chains interleaved.
       const int nq = N >> 2;
       const int qstride = gridDim.x * blockDim.x;
+      // Changed-input flags per 1024-id block, in two buffers by round
+      // parity: this round's are set by the threads whose vertices have a
+      // changed-input byte; the other buffer, next round's, is cleared
+      // meanwhile by the thread that takes the block's first vertices.  (The
+      // buffers' address is read where it is used: kept in registers for
+      // the whole loop it costs spills.)
+      const int nbk = (N + kCpBlockJ - 1) / kCpBlockJ;
       for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += qstride) {
-        const int v0 = q << 2;
-        const int4 A = *reinterpret_cast<const int4*>(a + v0);
-        const int4 B = *reinterpret_cast<const int4*>(b + v0);
-        const int4 O1 = *reinterpret_cast<const int4*>(ra + v0);
-        const int4 O2 = *reinterpret_cast<const int4*>(rb + v0);
-        const int4 R1 = *reinterpret_cast<const int4*>(ods + v0);
-        const int4 R2 = *reinterpret_cast<const int4*>(oas + v0);
-        const unsigned cw = vchg[v0 >> 5] >> (v0 & 31);
-        int u1[4] = {A.x, A.y, A.z, A.w}, u2[4] = {B.x, B.y, B.z, B.w};
-        const int o1[4] = {O1.x, O1.y, O1.z, O1.w}, o2[4] = {O2.x, O2.y, O2.z, O2.w};
-        const int r1[4] = {R1.x, R1.y, R1.z, R1.w}, r2[4] = {R2.x, R2.y, R2.z, R2.w};
-        // One hop of every unfinished chain per iteration: the eight loads
-        // depend only on their own chain, so they are all in flight at once.
-        bool more = true;
-        int it = 0;
-        for (; it < cap_j && more; ++it) {
-          int w1[4], w2[4];
+        {
+          const int v0 = q << 2;
+          const int4 A = *reinterpret_cast<const int4*>(a + v0);
+          const int4 B = *reinterpret_cast<const int4*>(b + v0);
+          const int4 O1 = *reinterpret_cast<const int4*>(ra + v0);
+          const int4 O2 = *reinterpret_cast<const int4*>(rb + v0);
+          const int4 R1 = *reinterpret_cast<const int4*>(ods + v0);
+          const int4 R2 = *reinterpret_cast<const int4*>(oas + v0);
+          const unsigned cw = vchg[v0 >> 5] >> (v0 & 31);
+          int u1[4] = {A.x, A.y, A.z, A.w}, u2[4] = {B.x, B.y, B.z, B.w};
+          const int o1[4] = {O1.x, O1.y, O1.z, O1.w}, o2[4] = {O2.x, O2.y, O2.z, O2.w};
+          const int r1[4] = {R1.x, R1.y, R1.z, R1.w}, r2[4] = {R2.x, R2.y, R2.z, R2.w};
+          // One hop of every unfinished chain per iteration: the eight loads
+          // depend only on their own chain, so they are all in flight at once.
+          bool more = true;
+          int it = 0;
+          for (; it < cap_j && more; ++it) {
+            int w1[4], w2[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              w1[k] = a[u1[k]];
+              w2[k] = b[u2[k]];
+            }
+            more = false;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              more |= (w1[k] != u1[k]) | (w2[k] != u2[k]);
+              u1[k] = w1[k];
+              u2[k] = w2[k];
+            }
+          }
+          if (it == cap_j && more) atomicOr(err, kErrJump);
+          unsigned dv = 0, mv = 0;
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
-            w1[k] = a[u1[k]];
-            w2[k] = b[u2[k]];
+            const unsigned c1 = vchg[u1[k] >> 5] >> (u1[k] & 31);
+            const unsigned c2 = vchg[u2[k] >> 5] >> (u2[k] & 31);
+            const unsigned d = (o1[k] != u1[k]) | (o2[k] != u2[k]) | ((cw >> k | c1 | c2) & 1u);
+            const unsigned m = (u1[k] != r1[k]) | (u2[k] != r2[k]) << 1;
+            dv |= d << (8 * k);
+            mv |= m << (8 * k);
           }
-          more = false;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            more |= (w1[k] != u1[k]) | (w2[k] != u2[k]);
-            u1[k] = w1[k];
-            u2[k] = w2[k];
+          *reinterpret_cast<unsigned*>(dirtyv + v0) = dv;
+          *reinterpret_cast<unsigned*>(mis + v0) = mv;
+          *reinterpret_cast<int4*>(ra + v0) = make_int4(u1[0], u1[1], u1[2], u1[3]);
+          *reinterpret_cast<int4*>(rb + v0) = make_int4(u2[0], u2[1], u2[2], u2[3]);
+          if (dv || (v0 & (kCpBlockJ - 1)) == 0) {
+            const int par = J.ctr[C_WNSTAMP] & 1;
+            if (dv) J.bdirty[(size_t)par * nbk + (v0 >> 10)] = 1;
+            if ((v0 & (kCpBlockJ - 1)) == 0) J.bdirty[(size_t)(par ^ 1) * nbk + (v0 >> 10)] = 0;
           }
         }
-        if (it == cap_j && more) atomicOr(err, kErrJump);
-        unsigned dv = 0, mv = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const unsigned c1 = vchg[u1[k] >> 5] >> (u1[k] & 31);
-          const unsigned c2 = vchg[u2[k] >> 5] >> (u2[k] & 31);
-          const unsigned d = (o1[k] != u1[k]) | (o2[k] != u2[k]) | ((cw >> k | c1 | c2) & 1u);
-          const unsigned m = (u1[k] != r1[k]) | (u2[k] != r2[k]) << 1;
-          dv |= d << (8 * k);
-          mv |= m << (8 * k);
-        }
-        *reinterpret_cast<unsigned*>(dirtyv + v0) = dv;
-        *reinterpret_cast<unsigned*>(mis + v0) = mv;
-        *reinterpret_cast<int4*>(ra + v0) = make_int4(u1[0], u1[1], u1[2], u1[3]);
-        *reinterpret_cast<int4*>(rb + v0) = make_int4(u2[0], u2[1], u2[2], u2[3]);
       }
       continue;
     }
@@ -716,6 +733,7 @@ __global__ void __launch_bounds__(256) k_jump2(const Job<T>* __restrict__ jobs,
 // block counts, pass 3 writes.
 // ---------------------------------------------------------------------------
 constexpr int kCpBlock = 1024;
+static_assert(kCpBlockJ == kCpBlock, "the jump's flags cover the CP-list blocks");
 
 __device__ __forceinline__ int cp_bits(int t) {
   return ((t == 2 || t == 3) ? 1 : 0) | ((t == 1 || t == 3) ? 2 : 0) | (t == 4 ? 4 : 0) |
@@ -1264,11 +1282,46 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
     // In the first round every changed-input byte is set (the change bitset
     // starts full), so the check is skipped.
     const bool all_new = J.ctr[C_MFFIRST] != 0;
+    // Later rounds first ask the jump's per-block flags (written when N is a
+    // multiple of 4) whether any changed-input byte is set where the chunk's
+    // saddles could see one: the 3 x 3 row windows of the planes and rows
+    // next to the chunk, one id wider on each side.
+    const bool by_block = !all_new && (J.dim.N & 3) == 0;
+    const long long W = J.dim.W, WH = W * J.dim.H, N = J.dim.N;
     for (int c = blockIdx.x; c < nchunk; c += gridDim.x) {
       const int b0 = c * chunk, b1 = min(b0 + chunk, nb);
       const int a2 = J.cpoff[b0], e2 = b1 < nb ? J.cpoff[b1] : ns2;
       const int a1 = J.cpoff[nb + b0], e1 = b1 < nb ? J.cpoff[nb + b1] : ns1;
       const int n2 = e2 - a2, n = n2 + (e1 - a1);
+      if (by_block) {
+        int seen = 0;
+        if (threadIdx.x < 9) {
+          const int t = (int)threadIdx.x;  // signed: the offsets below go negative
+          const long long off = (long long)(t / 3 - 1) * WH + (long long)(t % 3 - 1) * W;
+          const long long lo = max(0ll, (long long)b0 * kCpBlock + off - 1);
+          const long long hi = min(N - 1, (long long)b1 * kCpBlock - 1 + off + 1);
+          const uint8_t* bcur = J.bdirty + (size_t)(J.ctr[C_WNSTAMP] & 1) * nb;
+          for (long long b = lo >> 10; b <= (hi >> 10) && lo <= hi; ++b) seen |= bcur[b];
+        }
+        if (!__syncthreads_or(seen)) {  // no saddle here has a changed input
+          for (int base = 0; base < n; base += blockDim.x) {
+            const int k = base + threadIdx.x;
+            const bool split = k < n2;
+            bool has = false;
+            int s = 0;
+            if (k < n) {
+              const int i = split ? a2 + k : a1 + k - n2;
+              s = split ? J.sad2[i] : J.sad1[i];
+              has = (split ? J.has2 : J.has1)[i] != 0;
+            }
+            const int slot2 = warp_append(J.ctr + C_CAND, has && split, 0xffffffffu);
+            if (slot2 >= 0) J.cand[slot2] = s;
+            const int slot1 = warp_append(J.ctr + C_CANDJ, has && !split, 0xffffffffu);
+            if (slot1 >= 0) J.cand_j[slot1] = s;
+          }
+          continue;
+        }
+      }
       for (int base = 0; base < n; base += blockDim.x) {  // uniform in the block
         const int k = base + threadIdx.x;
         const bool split = k < n2;
