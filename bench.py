@@ -85,7 +85,7 @@ def dominant_bytes_per_launch(n: int, s: int) -> int:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_jump2
 # launch on the decompressed 256^3 field, from one ncu capture each, by value
 # size (profiles/k_jump2_256cube_f64.md); None where not captured.
-MEASURED_TRAFFIC_256 = {8: 453.571328e6 + 142.624768e6}
+MEASURED_TRAFFIC_256 = {8: 453.590272e6 + 145.40672e6}
 
 
 def measured_peaks():
