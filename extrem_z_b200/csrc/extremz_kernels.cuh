@@ -699,19 +699,27 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
           }
           if (it == cap_j && more) atomicOr(err, kErrJump);
           unsigned dv = 0, mv = 0;
+          bool n1 = false, n2 = false;
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
             const unsigned c1 = vchg[u1[k] >> 5] >> (u1[k] & 31);
             const unsigned c2 = vchg[u2[k] >> 5] >> (u2[k] & 31);
+            n1 |= o1[k] != u1[k];
+            n2 |= o2[k] != u2[k];
             const unsigned d = (o1[k] != u1[k]) | (o2[k] != u2[k]) | ((cw >> k | c1 | c2) & 1u);
             const unsigned m = (u1[k] != r1[k]) | (u2[k] != r2[k]) << 1;
             dv |= d << (8 * k);
             mv |= m << (8 * k);
           }
           *reinterpret_cast<unsigned*>(dirtyv + v0) = dv;
-          *reinterpret_cast<unsigned*>(mis + v0) = mv;
-          *reinterpret_cast<int4*>(ra + v0) = make_int4(u1[0], u1[1], u1[2], u1[3]);
-          *reinterpret_cast<int4*>(rb + v0) = make_int4(u2[0], u2[1], u2[2], u2[3]);
+          // Stores that would rewrite the stored value are skipped.  The
+          // mismatch bits follow the labels alone (the original roots are
+          // fixed), so with dv == 0 (no label and no change bit) last round's
+          // bits stand; the first round of a job, whose change bitset is
+          // full, writes every group.
+          if (dv) *reinterpret_cast<unsigned*>(mis + v0) = mv;
+          if (n1) *reinterpret_cast<int4*>(ra + v0) = make_int4(u1[0], u1[1], u1[2], u1[3]);
+          if (n2) *reinterpret_cast<int4*>(rb + v0) = make_int4(u2[0], u2[1], u2[2], u2[3]);
           if (dv || (v0 & (kCpBlockJ - 1)) == 0) {
             const int par = J.ctr[C_WNSTAMP] & 1;
             if (dv) J.bdirty[(size_t)par * nbk + (v0 >> 10)] = 1;
