@@ -94,6 +94,23 @@ def test_repeated_calls_on_one_context_are_identical():
     assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
 
 
+def test_fields_in_turn_on_one_context_bit_exact():
+    """A field corrected after another of the same shape, whose labels,
+    mismatch bits and changed-input bytes are still in the workspace: the
+    jump skips the stores of label groups equal to the stored ones, so each
+    job's first manifold round must still write every group's mismatch bits
+    (N a multiple of 4: the four-vertices-per-thread path)."""
+    from oracle import ffi
+    a = synth.make_field(24, 20, 16, n_gauss=10, seed=21, rel=2e-3)
+    b = synth.make_field(24, 20, 16, n_gauss=14, seed=22, rel=2e-3)
+    assert a.f.size % 4 == 0
+    for fld in (a, b, a, a):
+        ref, rrep, _ = ffi.correct(fld.f, fld.decp, fld.eb, **KW)
+        out, rep, _ = gpu_correct(fld.f, fld.decp, fld.eb, trace_cap=0, **KW)
+        assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+        assert rep.status == rrep["status"] == 0
+
+
 @pytest.mark.parametrize("tma", [True, False])
 def test_tile_load_paths_agree(tma):
     """TMA halo tiles and plain-load tiles give the same bytes (64^3 f32)."""
