@@ -722,9 +722,9 @@ def noalloc_max_voxels() -> int:
 def correct_device_noalloc(f, decp, bound: float, *, stream=None, **kw) -> CorrectionReport:
     """Allocation-free correction of the CUDA tensor ``decp`` in place.
 
-    For callers that cannot allocate device memory while correcting (work
-    issued during CUDA graph capture, applications whose allocator owns the
-    device memory, real-time code that forbids allocation after start-up):
+    For callers that cannot allocate device memory while correcting
+    (applications whose allocator owns the device memory, real-time code that
+    forbids allocation after start-up):
     the workspace is a static device array of the library, for fields of at
     most noalloc_max_voxels() voxels.  Calls share that array, so they must not
     overlap on the GPU.  The first call on a device does a synchronous set-up;

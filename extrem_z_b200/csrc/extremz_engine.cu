@@ -399,9 +399,9 @@ static int analyze_one(BatchEngine<T>& e, cudaStream_t st, const T* field, int W
 // Allocation-free correction (extremz_correct_device_noalloc).
 //
 // Some callers cannot allocate device memory at the time they correct a
-// field: code that runs while a CUDA graph is being captured, allocators
-// that own all of the device's memory, or real-time paths that forbid
-// allocation after start-up.  For them the whole workspace of one correction
+// field: applications whose allocator owns all of the device's memory, or
+// real-time paths that forbid allocation after start-up because an
+// allocation can block.  For them the whole workspace of one correction
 // lives in a fixed-size static device array, and the lookup table in static
 // device arrays, so a call allocates nothing.  The array is sized for the
 // worst case of EXTREMZ_NOALLOC_MAX_VOXELS voxels and every GPU that loads

@@ -344,9 +344,10 @@ long long extremz_job_footprint(int dtype, int width, int height, int depth);
 
 /*
  * Allocation-free variant of extremz_correct_device, for callers that cannot
- * allocate device memory when they correct a field: work issued during CUDA
- * graph capture, applications whose allocator owns all of the device memory,
- * and real-time code that forbids allocation after start-up.
+ * allocate device memory when they correct a field: applications whose
+ * allocator owns all of the device memory, so that a cudaMalloc of the
+ * library's own would fail or break its accounting, and real-time code that
+ * forbids allocation after start-up because an allocation can block.
  * No counterpart in the reference: it always allocates its ~60 device arrays
  * in main() (src/ExtreM_cuda.cu:4997-5185).
  *

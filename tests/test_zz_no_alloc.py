@@ -1,9 +1,8 @@
 """The allocation-free entry point gives the same field as the regular one.
 
 extremz_correct_device_noalloc serves callers that cannot allocate device
-memory while they correct a field (work issued during CUDA graph capture, an
-application allocator that owns the device memory, real-time code without
-allocation after start-up).  Its workspace is a static device array shared by
+memory while they correct a field (an application whose allocator owns the
+device memory, real-time code that allows no allocation after start-up).  Its workspace is a static device array shared by
 all calls, so two calls in a row must both match the regular entry point: the
 second call must not see anything the first one left in the array.  This file
 is collected last so that a failure here stops a -x run only after everything
