@@ -325,7 +325,7 @@ def run_ours(args, world, rank, local):
         raise RuntimeError(f"correction did not converge: {rep}")
 
     # Timed region: device time of exactly K steps, max over ranks.
-    sampler = ClockSampler(local) if rank == 0 or True else None
+    sampler = ClockSampler(local)  # every rank samples its own GPU; rank 0 reports
     sampler.start()
     barrier(world)
     torch.cuda.synchronize()
