@@ -1,6 +1,6 @@
-"""Host-side arithmetic of bench.py, on CPU: the dominant kernel's algorithmic
-bytes and the parsing of the clock samples that decide whether a run was
-throttled."""
+"""Host-side parts of bench.py, on CPU: the dominant kernel's algorithmic
+bytes, the parsing of the clock samples that decide whether a run was
+throttled, and the reference arm's JSON line."""
 
 import os
 import sys
@@ -57,3 +57,24 @@ def test_clock_sampler_flags_thermal_slowdown(monkeypatch):
 def test_clock_sampler_without_nvidia_smi_says_unsampled():
     s = bench.ClockSampler(0)
     assert s.stop()["reasons"] == ["unsampled"]
+
+
+def test_reference_arm_prints_one_contract_line():
+    """`bench.py --impl reference` (the CPU restatement on the host cores, on a
+    small crop here) prints one JSON line with the contract's keys."""
+    import json
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "0", "--cpu-edge", "16"],
+                         cwd=root, capture_output=True, text=True, timeout=600, check=True)
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
+    for key in ("metric", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "scaling",
+                "vs_baseline", "dtype", "data", "config"):
+        assert key in d
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
