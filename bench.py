@@ -2,7 +2,9 @@
 
 One step = one full correction (setup, c_loops, the outer loop to zero
 mismatch counters, final join-saddle pass) of a fresh copy of the synthetic
-decompressed field, inputs resident in HBM.
+decompressed field, inputs resident in HBM.  The default workload is the
+512^3 float64 field (4096 Gaussians, k^-5/3 noise, seed 2, eb 1e-5 relative);
+the 256^3 fields in float64 and float32 are measured beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
                     [--impl ours|reference]
@@ -13,7 +15,8 @@ replicas and the value is all ranks' voxels over the max-over-ranks time.
 
 --impl reference times the reference algorithm's CPU implementation on the
 host cores (the CPU restatement of the reference's GPU correction, built
-with OpenMP) on a bounded crop of the same workload, rank 0 only.
+with OpenMP) on a bounded crop of the same workload, rank 0 only; its
+config names the crop's shape.
 """
 
 from __future__ import annotations
@@ -37,7 +40,7 @@ from extrem_z_b200 import synth  # noqa: E402
 METRIC = "Mvox/s to zero topological mismatch"
 UNIT = "Mvox/s"
 
-# name -> (constructor, description); the headline is the 256^3 float64 field.
+# name -> (constructor, description); the headline is the 512^3 float64 field.
 WORKLOADS = {
     "plain256_f64": (lambda: synth.plain_256(np.float64),
                      "256^3 float64, 512 Gaussians + k^-2 noise, seed 1, eb 1e-4 rel"),
@@ -55,41 +58,54 @@ FORM_WORKLOADS = {
     "serve": "Poisson request stream, voxels log-uniform 32^3-384^3, f32/f64 50/50, eb "
              "log-uniform 1e-5..1e-2 rel, seed 10000+id, HBM admission budget 120 GB",
 }
-DEFAULT_WORKLOAD = "plain256_f64"
+DEFAULT_WORKLOAD = "plain512_f64"
+# Measured beside the headline (fewer steps): the 256^3 field in both dtypes.
+SECONDARY = ("plain256_f64", "plain256_f32")
+# Edge of the cubic crop the CPU legs correct (a full 512^3 correction takes
+# the OpenMP oracle minutes per step).
+CPU_EDGE = 128
 SERVE_RATES = (10, 30, 100, 300, 1000, 2000)
 # Workspace memory the server maps at start-up (within its 120 GB budget).
 SERVE_RESERVE_BYTES = 48 << 30
 PARAMS = dict(q=4, edit_type=1, thr=0.0, max_outer=1000, max_cloop_rounds=100000,
               final_join=True)
 
-# Dominant kernel: the pointer jumping of the decompressed labels (k_jump2,
-# kernel class "jump"), one launch per computed manifold round, over every
-# voxel.  Algorithmic bytes per voxel: read the two tile-compressed pointers,
-# the two current labels and the two original roots (24 B) and the change bit,
-# and write the changed-input byte (1 B); the first computed round of a
-# correction also writes the two labels and the label-mismatch byte (9 B), which
-# later rounds write only for the groups of four voxels whose labels changed (a
-# few; not counted, so the figure is a lower bound).  The hops along the chains
-# are re-reads, not counted.  Launches of rounds whose inputs were unchanged
-# return at once or are not issued; they are not counted.
-DOMINANT = "jump"
+# Dominant work: the manifold round of the decompressed field, one launch of
+# the steepest directions (k_direction, kernel class "direction") and one of
+# the pointer jumping (k_jump2, class "jump") per computed round.  Its
+# algorithmic bytes are N*(S + 8) per round: read every decompressed value
+# (S bytes) and write its two int32 labels.  Everything else the kernels move
+# (tile-compressed pointers, original roots, change marks, chain hops) is the
+# design's own traffic, not counted.  Rounds whose inputs were unchanged since
+# the previous round are not launched or return at once; they are not counted.
+DOMINANT = ("direction", "jump")
+DOMINANT_KERNEL = "manifold round (k_direction + k_jump2)"
 # The next kernel by device time (the saddle pass after each manifold round),
-# timed beside the dominant one so that the line shows which leads.
+# timed beside the dominant ones in a few extra steps.
 RUNNER_UP = "rows"
 RUNNER_UP_KERNEL = "k_saddle_pass"
-DOMINANT_KERNEL = "k_jump2"
 
 
-def dominant_bytes(n: int, launches: int, corrections: int) -> int:
-    """Algorithmic bytes of `launches` computed jumps over `corrections`
-    corrections of an n-voxel field (one full first round each)."""
+def round_bytes(n: int, s: int) -> int:
+    """Algorithmic bytes of one manifold round of an n-voxel field of s-byte
+    values: the value read and the two label writes per voxel."""
+    return n * (s + 8)
+
+
+def jump_design_bytes(n: int, launches: int, corrections: int) -> int:
+    """Bytes k_jump2 itself must move in `launches` computed rounds over
+    `corrections` corrections: per voxel the two tile-compressed pointers, the
+    two current labels and the two original roots (24 B) plus the change bit,
+    and the changed-input byte (1 B); a correction's first computed round also
+    writes both labels and the mismatch byte (9 B)."""
     return 34 * n * corrections + 25 * n * (launches - corrections)
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_jump2
-# launch on the decompressed 256^3 field, from one ncu capture each, by value
-# size (profiles/k_jump2_256cube_f64.md); None where not captured.
-MEASURED_TRAFFIC_256 = {8: 453.590272e6 + 145.40672e6}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one manifold
+# round (k_direction + k_jump2 of a later round, where k_direction recomputes
+# only changed tiles), by workload, from one ncu capture each; None where not
+# captured.  Filled from the profiles/ summaries.
+MEASURED_TRAFFIC = {}
 
 
 def measured_peaks():
@@ -261,7 +277,7 @@ def run_reference(args, world, rank):
         return run_reference_form(args)
     field = WORKLOADS[args.workload][0]()
     threads = os.cpu_count() or 1
-    edge = args.cpu_edge
+    edge = min(args.cpu_edge, *field.f.shape)
     for _ in range(args.warmup):
         time_oracle(field, edge, threads)
     total_s, vox = 0.0, 0
@@ -272,11 +288,15 @@ def run_reference(args, world, rank):
     value = vox / total_s / 1e6
     sample = (f"leading {edge}^3 crop of the {args.workload} field (same bound), full "
               f"correction to zero mismatch, CPU restatement of the reference correction")
+    # The config names what was timed: the crop, not the whole field (the
+    # rate to zero mismatch depends on the field's size and round count).
+    cfg = config_of(args, field, shape_whd=list(crop(field, edge)[0].shape[::-1]))
+    cfg["sample_of"] = {"workload": args.workload, "shape_whd": list(field.shape_whd)}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": dtype_name(field),
-            "data": "synthetic", "config": config_of(args, field),
+            "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -288,13 +308,106 @@ def dtype_name(field):
     return "f64" if field.f.dtype == np.float64 else "f32"
 
 
-def config_of(args, field):
+def config_of(args, field, shape_whd=None):
     d, h, w = field.f.shape
     return {"workload": args.workload, "description": WORKLOADS[args.workload][1],
-            "shape_whd": [w, h, d], "eb_abs": field.eb, "params": PARAMS,
+            "shape_whd": shape_whd or [w, h, d], "eb_abs": field.eb, "params": PARAMS,
             "l2": "inputs larger than L2 (two fields of N*S bytes > 126 MB)" if
             2 * field.f.nbytes > 126e6 else "inputs smaller than L2",
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single"}
+
+
+def correct_steps(ctx, f, g, g0, field, stream, steps, profile=False, **over):
+    """`steps` corrections of fresh copies of the decompressed field; reports."""
+    params = dict(PARAMS, **over)
+    reps = []
+    for _ in range(steps):
+        g.copy_(g0)
+        rep, _ = ctx.correct_device(f, g, field.eb, stream=stream.cuda_stream,
+                                    profile=profile or False, **params)
+        reps.append(rep)
+    return reps
+
+
+def timed_steps(ctx, f, g, g0, field, stream, steps, profile=False, **over):
+    """Device time (ms, CUDA events on the launching stream) of `steps`
+    corrections, and their reports."""
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    reps = correct_steps(ctx, f, g, g0, field, stream, steps, profile, **over)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), reps
+
+
+def manifold_roofline(reps, n, s, step_ms, peak, peak_kind, traffic=None):
+    """Roofline of the decompressed manifold rounds of `reps` (corrections
+    run with the "direction" and "jump" classes timed)."""
+    dir_ms = sum(r.prof_ms["direction"] for r in reps)
+    jump_ms = sum(r.prof_ms["jump"] for r in reps)
+    rounds = sum(r.manifold_rounds - r.manifold_reused for r in reps)
+    ms = dir_ms + jump_ms
+    alg = round_bytes(n, s) * rounds
+    achieved = alg / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+    jb = jump_design_bytes(n, rounds, len(reps))
+    jump_gbs = jb / (jump_ms * 1e-3) / 1e9 if jump_ms > 0 else 0.0
+    return {"bound": "hbm", "kernel": DOMINANT_KERNEL, "achieved": achieved, "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic,
+            "traffic_note": "ncu DRAM bytes of one later manifold round (k_direction + "
+                            "k_jump2), scaled to this field by its voxel count" if traffic else None,
+            "algorithmic_bytes_per_launch": round_bytes(n, s),
+            "algorithmic_bytes_note": "N*(S+8) per manifold round: the value read and two "
+                                      "int32 label writes per voxel",
+            "launches": rounds, "launches_reused": sum(r.manifold_reused for r in reps),
+            "kernel_ms": ms, "direction_ms": dir_ms, "jump_ms": jump_ms,
+            "share_of_step": ms / step_ms if step_ms else None,
+            "jump_design_bytes": {"kernel": "k_jump2", "bytes": jb, "achieved_gbs": jump_gbs,
+                                  "frac": jump_gbs / peak,
+                                  "note": "the bytes k_jump2 itself moves (pointers, labels, "
+                                          "original roots, change marks), a lower bound"}}
+
+
+def census_of(ctx, f, g):
+    """Mismatch census of the corrected field g against f (GPU, untimed)."""
+    import torch
+    c = ctx.mismatch_census(f, g)
+    torch.cuda.synchronize()
+    c["critical_point_mismatches"] = c["false_max"] + c["false_min"] + c["false_saddle"]
+    c["label_mismatches"] = c["wrong_split_nbrs"] + c["wrong_join_nbrs"]
+    c["split_tree_zero"] = all(c[k] == 0 for k in ("wrong_split_nbrs", "false_max", "false_min",
+                                                   "false_saddle", "wrong_max", "wrong_max_2",
+                                                   "wrong_saddle"))
+    return c
+
+
+def measure_secondary(ctx, local, name, steps, peak, peak_kind):
+    """One 256^3 line beside the headline: Mvox/s to zero mismatch, rounds,
+    manifold-round roofline and the census of the corrected field."""
+    import torch
+    dev = torch.device("cuda", local)
+    field = WORKLOADS[name][0]()
+    n, s = field.f.size, field.f.itemsize
+    f = torch.from_numpy(field.f).to(dev)
+    g0 = torch.from_numpy(field.decp).to(dev)
+    g = torch.empty_like(g0)
+    stream = torch.cuda.current_stream(dev)
+    correct_steps(ctx, f, g, g0, field, stream, 2)
+    ms, reps = timed_steps(ctx, f, g, g0, field, stream, steps, profile=list(DOMINANT))
+    r0 = reps[-1]
+    out = {"workload": name, "description": WORKLOADS[name][1], "steps": steps,
+           "value": n * steps / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms / steps,
+           "rounds": {"outer_iters": r0.outer_iters, "cloop_rounds": r0.cloop_rounds,
+                      "manifold_rounds": r0.manifold_rounds,
+                      "manifold_reused": r0.manifold_reused, "status": r0.status},
+           "roofline": manifold_roofline(reps, n, s, ms, peak, peak_kind,
+                                         MEASURED_TRAFFIC.get(name)),
+           "census": census_of(ctx, f, g)}
+    del f, g, g0
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -312,28 +425,21 @@ def run_ours(args, world, rank, local):
     ctx = api.Context(local)
     stream = torch.cuda.current_stream(dev)
 
-    def step(profile=False):
-        g.copy_(g0)
-        rep, _ = ctx.correct_device(f, g, field.eb, stream=stream.cuda_stream,
-                                    profile=profile or False, **PARAMS)
-        return rep
-
-    for _ in range(args.warmup):
-        rep = step()
+    reps = correct_steps(ctx, f, g, g0, field, stream, args.warmup)
     torch.cuda.synchronize()
-    if rep.status != 0:
-        raise RuntimeError(f"correction did not converge: {rep}")
+    if reps and reps[-1].status != 0:
+        raise RuntimeError(f"correction did not converge: {reps[-1]}")
 
-    # Timed region: device time of exactly K steps, max over ranks.
+    # Timed region: device time of exactly K steps, max over ranks.  The
+    # manifold-round kernels record CUDA events around themselves (inside the
+    # tick graphs) for the roofline.
     sampler = ClockSampler(local)  # every rank samples its own GPU; rank 0 reports
     sampler.start()
     barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    reps = []
-    for _ in range(args.steps):
-        reps.append(step(profile=[DOMINANT]))
+    reps = correct_steps(ctx, f, g, g0, field, stream, args.steps, profile=list(DOMINANT))
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
@@ -342,33 +448,30 @@ def run_ours(args, world, rank, local):
     ms_max = max_over_ranks(ms, world)
     value = world * n * args.steps / (ms_max * 1e-3) / 1e6
     launches = sum(r.kernel_launches for r in reps)
+    # What the corrected field (final join pass on, as in the reference's
+    # main()) still differs in: the loop test's counters evaluated once more.
+    census = census_of(ctx, f, g)
 
-    # The next kernel by device time, timed beside the dominant one in a few
-    # steps after the timed region (each timed launch adds two event nodes to
-    # its tick's graph, so the timed steps carry only the dominant kernel's).
-    ru_reps = [step(profile=[DOMINANT, RUNNER_UP]) for _ in range(2)]
-    torch.cuda.synchronize()
-    runner_up = {"kernel": RUNNER_UP_KERNEL, "steps": len(ru_reps),
-                 "kernel_ms": sum(r.prof_ms[RUNNER_UP] for r in ru_reps),
-                 "dominant_kernel_ms": sum(r.prof_ms[DOMINANT] for r in ru_reps),
-                 "launches": sum(r.prof_launches[RUNNER_UP] for r in ru_reps)}
-
-    # Roofline of the dominant kernel from its CUDA-event time in the timed
-    # steps, over the launches that computed (reused manifold rounds return).
-    dom_ms = sum(r.prof_ms[DOMINANT] for r in reps)
-    dom_n = sum(r.manifold_rounds - r.manifold_reused for r in reps)
     peak, peak_kind = measured_peaks()
-    dom_bytes = dominant_bytes(n, dom_n, len(reps))
-    per_launch = dom_bytes / dom_n if dom_n else 0.0
-    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
-    traffic = MEASURED_TRAFFIC_256.get(s) if field.f.shape == (256, 256, 256) else None
-    roofline = {"bound": "hbm", "kernel": DOMINANT_KERNEL, "achieved": achieved, "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "traffic_launch": "first computed round (writes every group)",
-                "algorithmic_bytes_per_launch": per_launch, "launches": dom_n,
-                "launches_reused": sum(r.manifold_reused for r in reps),
-                "kernel_ms": dom_ms, "share_of_step": dom_ms / ms if ms else None,
-                "runner_up": runner_up}
+    roofline = manifold_roofline(reps, n, s, ms, peak, peak_kind,
+                                 MEASURED_TRAFFIC.get(args.workload))
+    # The next kernel by device time, timed beside the dominant ones in a few
+    # steps after the timed region.
+    ru_reps = correct_steps(ctx, f, g, g0, field, stream, 2, profile=list(DOMINANT) + [RUNNER_UP])
+    torch.cuda.synchronize()
+    roofline["runner_up"] = {
+        "kernel": RUNNER_UP_KERNEL, "steps": len(ru_reps),
+        "kernel_ms": sum(r.prof_ms[RUNNER_UP] for r in ru_reps),
+        "dominant_kernel_ms": sum(r.prof_ms[k] for r in ru_reps for k in DOMINANT),
+        "launches": sum(r.prof_launches[RUNNER_UP] for r in ru_reps)}
+
+    # The same correction without the final join-saddle pass: the loop ends
+    # at zero counters, so the field keeps zero split-tree mismatch.
+    fj_steps = max(1, min(args.steps, 5))
+    fj_ms, fj_reps = timed_steps(ctx, f, g, g0, field, stream, fj_steps, final_join=False)
+    final_join_off = {"steps": fj_steps, "value": n * fj_steps / (fj_ms * 1e-3) / 1e6,
+                      "unit": UNIT, "ms_per_step": fj_ms / fj_steps,
+                      "status": fj_reps[-1].status, "census": census_of(ctx, f, g)}
 
     # End to end through the host-buffer entry point: H2D of both fields from
     # pinned memory, correction, D2H of the corrected field, every step.
@@ -391,20 +494,41 @@ def run_ours(args, world, rank, local):
     e2e_s = max_over_ranks(e2e_s, world)
     # Device -> host: the changed voxels' ids and values (the host buffer
     # already holds the rest), as the library reports them.
+    g.copy_(g0)
+    ctx.correct_device(f, g, field.eb, stream=stream.cuda_stream, **PARAMS)
     e2e = {"value": world * n * e2e_steps / e2e_s / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": 2 * n * s, "d2h_bytes_per_step": back // e2e_steps,
            "entry_point": "extremz_correct_host",
            # the host buffer against the device-resident correction (outside the timing)
            "bit_identical_to_device": bool(np.array_equal(
                hg.view(np.uint8), g.cpu().numpy().view(np.uint8)))}
+    del hf, hg
 
+    # The CPU restatement of the reference correction on all host cores, on a
+    # crop of the same field (a full 512^3 correction takes it minutes), and
+    # this library on the same crop, so that the two rates compare like with
+    # like.
     cpu = None
+    same_crop = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = 1
-        secs, vox, crep = time_oracle(field, args.cpu_edge, threads)
+        threads = os.cpu_count() or 1
+        edge = min(args.cpu_edge, *field.f.shape)
+        secs, vox, crep = time_oracle(field, edge, threads)
         cpu = {"value": vox / secs / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"leading {args.cpu_edge}^3 crop of the same field and bound, full "
-                         f"correction to zero mismatch ({secs:.1f} s, status {crep['status']})"}
+               "sample": f"leading {edge}^3 crop of the same field and bound, full "
+                         f"correction to zero mismatch by the OpenMP CPU restatement of the "
+                         f"reference correction ({secs:.2f} s, status {crep['status']})"}
+        cf, cg = crop(field, edge)
+        tf = torch.from_numpy(cf).to(dev)
+        tg0 = torch.from_numpy(cg).to(dev)
+        tg = torch.empty_like(tg0)
+        crop_field = synth.Field(f=cf, decp=cg, eb=field.eb, seed=field.seed, rel=field.rel)
+        correct_steps(ctx, tf, tg, tg0, crop_field, stream, 2)
+        cms, _ = timed_steps(ctx, tf, tg, tg0, crop_field, stream, 5)
+        same_crop = {"shape_whd": [edge] * 3, "value": vox * 5 / (cms * 1e-3) / 1e6, "unit": UNIT,
+                     "cpu_value": cpu["value"], "ratio": vox * 5 / (cms * 1e-3) / 1e6 / cpu["value"],
+                     "note": "this library, device-resident, on the crop the CPU leg corrects"}
+        del tf, tg, tg0
 
     # Edit stream of the same correction (extremz_correct_encode): the extra
     # device time of the encoder over the plain correction, the stream sizes
@@ -420,37 +544,51 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_forms:
         topology = measure_topology(ctx, f, g, g0, field, stream, args)
 
+    r0 = reps[-1]
+    rounds = {"outer_iters": r0.outer_iters, "cloop_rounds": r0.cloop_rounds,
+              "manifold_rounds": r0.manifold_rounds, "manifold_reused": r0.manifold_reused,
+              "status": r0.status, "counters": r0.counters, "cp_counts": r0.cp_counts}
+    del f, g, g0
+    torch.cuda.empty_cache()
+
+    secondary = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        secondary = [measure_secondary(ctx, local, name, 5, peak, peak_kind)
+                     for name in SECONDARY if name != args.workload]
+
     forms = None
     if not args.no_forms and world == 1:
         b = measure_batched(local, 2, 3)
-        sv = measure_served(local, (100, 2000), n_max=48, seconds=0.5)
+        sv = measure_served(local, SERVE_RATES)
         forms = {"batched": {"workload": "mixed64", "fields_per_s": b["batched"]["fields_per_s"],
                              "plain_loop_fields_per_s": b["plain_loop"]["fields_per_s"],
                              "speedup": b["speedup"],
                              "bit_identical_to_plain": b["bit_identical_to_plain"],
                              "gpu_launches": b["batched"]["gpu_launches"],
                              "plain_loop_gpu_launches": b["plain_loop"]["gpu_launches"]},
-                 "served": {"workload": "serve (48 requests per rate)",
+                 "served": {"workload": f"serve ({sv['requests_max']} requests at most per rate)",
                             "plain_loop_fields_per_s": sv["plain_loop"]["fields_per_s"],
                             "peak_running": sv["peak_running"],
-                            "sweep": [{k: x[k] for k in ("rate_req_s", "p50_ms", "p99_ms",
-                                                         "fields_per_s", "mean_in_system")}
+                            "sweep": [{k: x[k] for k in ("rate_req_s", "requests", "p50_ms",
+                                                         "p99_ms", "fields_per_s",
+                                                         "mean_in_system")}
                                       for x in sv["sweep"]],
                             "bit_identical_to_plain": sv["bit_identical_to_plain"]}}
 
     if rank == 0:
-        r0 = reps[-1]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": dtype_name(field), "data": "synthetic (seeded generator, no dataset)",
                 "config": config_of(args, field), "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "forms": forms,
-                "edit_stream": edit_stream, "topology": topology,
-                "rounds": {"outer_iters": r0.outer_iters, "cloop_rounds": r0.cloop_rounds,
-                           "manifold_rounds": r0.manifold_rounds,
-                           "manifold_reused": r0.manifold_reused, "status": r0.status,
-                           "counters": r0.counters, "cp_counts": r0.cp_counts}}
+                "roofline": roofline, "cpu_baseline": cpu, "gpu_same_crop": same_crop,
+                "clocks": clocks,
+                "headline": "final join-saddle pass on, as the reference's main() runs it "
+                            "unconditionally (src/ExtreM_cuda.cu:5997); the output is the "
+                            "reference's control flow, bit-exact with the oracle",
+                "census": census, "final_join_off": final_join_off,
+                "secondary": secondary, "forms": forms,
+                "edit_stream": edit_stream, "topology": topology, "rounds": rounds}
         print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -764,8 +902,10 @@ def main():
     ap.add_argument("--no-forms", action="store_true",
                     help="omit the batched / served summaries from the plain line")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-edge", type=int, default=96)
+    ap.add_argument("--cpu-edge", type=int, default=CPU_EDGE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="omit the 256^3 lines measured beside the headline")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

@@ -29,7 +29,8 @@ F32, F64 = 0, 1
 
 # Every entry point declared in include/extremz.h.
 EXPORTS = ("extremz_version", "extremz_default_params", "extremz_ctx_create",
-           "extremz_ctx_destroy", "extremz_correct_device", "extremz_correct_host",
+           "extremz_ctx_destroy", "extremz_correct_device", "extremz_mismatch_census",
+           "extremz_correct_host",
            "extremz_correct_batch", "extremz_correct_encode", "extremz_edit_stream_caps",
            "extremz_zstd_size", "extremz_persistence_pairs", "extremz_persistence_tree",
            "extremz_server_create", "extremz_server_destroy",
@@ -156,6 +157,9 @@ def load(build_if_missing: bool = True):
                                              ctypes.POINTER(Params), ctypes.POINTER(Report),
                                              vp, vp, i32]
         L.extremz_correct_device.restype = i32
+        L.extremz_mismatch_census.argtypes = [vp, vp, vp, i32, i32, i32, i32, ctypes.c_double,
+                                              vp, vp]
+        L.extremz_mismatch_census.restype = i32
         L.extremz_correct_host.argtypes = [vp, vp, vp, i32, i32, i32, i32,
                                            ctypes.POINTER(Params), ctypes.POINTER(Report), vp]
         L.extremz_correct_host.restype = i32
@@ -309,6 +313,26 @@ class Context:
             trace = tr.reshape(-1, 4)
             trace = trace[trace[:, 0] != 0]
         return CorrectionReport.of(r), trace
+
+    def mismatch_census(self, f, g, *, thr: float = 0.0, stream=None):
+        """The eleven loop-test counters of field ``g`` against the original
+        ``f`` (CUDA tensors), evaluated once with no edit; a dict by name
+        (``COUNTER_NAMES``) plus the list under ``"counters"``."""
+        import torch
+        assert f.is_cuda and g.is_cuda and f.dtype == g.dtype and f.shape == g.shape
+        assert f.is_contiguous() and g.is_contiguous()
+        dt = {torch.float32: F32, torch.float64: F64}[f.dtype]
+        w, h, d = _whd(tuple(f.shape))
+        if stream is None:
+            stream = torch.cuda.current_stream(f.device).cuda_stream
+        out = np.zeros(11, dtype=np.int32)
+        st = load().extremz_mismatch_census(self._h, f.data_ptr(), g.data_ptr(), dt, w, h, d,
+                                            float(thr), out.ctypes.data, stream)
+        _check(st, allow_cap=False)
+        c = [int(x) for x in out]
+        res = dict(zip(COUNTER_NAMES, c))
+        res["counters"] = c
+        return res
 
     # -- edit streams -------------------------------------------------------
     def correct_encode(self, f, decp, bound: float, *, stream=None, zstd_level: int = 3, **kw):
@@ -685,6 +709,12 @@ def job_footprint(voxels_or_shape, dtype) -> int:
         w, h, d = int(voxels_or_shape), 1, 1
     dt = F32 if str(dtype).endswith("float32") else F64
     return int(load().extremz_job_footprint(dt, w, h, d))
+
+
+# Names of the eleven loop-test counters (extremz_report.counters order).
+COUNTER_NAMES = ("wrong_split_nbrs", "wrong_join_nbrs", "false_max", "false_min", "false_saddle",
+                 "wrong_max", "wrong_max_2", "wrong_saddle", "wrong_min", "wrong_min_2",
+                 "wrong_saddle_join")
 
 
 def _dtname(code: int) -> str:

@@ -99,6 +99,12 @@ constexpr int kFlagAnalysis = 1 << 29;
 // Internal job flag: keep the bitset of voxels whose value changed (Job::edited)
 // so that only those travel back to a host buffer.
 constexpr int kFlagTrackEdits = 1 << 28;
+// Internal job flag: mismatch census -- the loop test's eleven counters
+// evaluated once on the decompressed field (detection, one manifold round
+// with the wrong-neighbour arbitration, and the wrong-extremum / wrong-saddle
+// detection of both trees), no edit.
+constexpr int kFlagCensus = 1 << 27;
+constexpr int kInternalFlags = kFlagKeepInput | kFlagAnalysis | kFlagTrackEdits | kFlagCensus;
 
 constexpr long long job_bytes_voxels(long long n, long long ksz) {
   return arr_bytes(n, 1) + arr_bytes(n, 2)                          // otype, olm
@@ -1171,7 +1177,7 @@ class BatchEngine {
         launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs, s, 0);
         for (int i : sel) {
           slots_[i].pending.push_back(PH_DETECT3);
-          slots_[i].pc = join3(slots_[i]);
+          slots_[i].pc = (slots_[i].p.flags & kFlagCensus) ? PC_DET3J : join3(slots_[i]);
         }
         return EXTREMZ_OK;
       case PC_DET3J:
@@ -1394,6 +1400,11 @@ class BatchEngine {
       case PC_CL_DETECT:
       case PC_CL_ROUND:
         j.emit(PH_CLOOP_DETECT, h(slot, C_CMAX), h(slot, C_CMIN), h(slot, C_CSAD));
+        if (j.p.flags & kFlagCensus) {  // no edit: on to the third block's checks
+          j.block = 3;
+          j.pc = PC_MANIFOLD;
+          return EXTREMZ_OK;
+        }
         if (h(slot, C_MM) > 0) {
           if (j.rounds >= j.p.max_cloop_rounds) {
             finish(slot, EXTREMZ_ROUND_CAP);
@@ -1410,7 +1421,8 @@ class BatchEngine {
         j.nfc = h(slot, C_NFC);
         j.nfc1 = h(slot, C_NFC1);
         j.emit(PH_WRONG_NBR, j.nfc, j.nfc1);
-        if (j.block == 3) j.pc = j.nfc == 0 ? PC_DET3 : join3(j);
+        if (j.p.flags & kFlagCensus) j.pc = PC_DET3;
+        else if (j.block == 3) j.pc = j.nfc == 0 ? PC_DET3 : join3(j);
         else j.pc = j.nfc == 0 ? PC_SLOOPS : joinb(j);
         return EXTREMZ_OK;
       case PC_SLOOPS:
@@ -1428,6 +1440,10 @@ class BatchEngine {
       case PC_FINAL_DETECT:
         j.emit(PH_CLOOP_DETECT, h(slot, C_CMAX), h(slot, C_CMIN), h(slot, C_CSAD));
         snapshot(slot);
+        if (j.p.flags & kFlagCensus) {
+          finish(slot, EXTREMZ_OK);
+          return EXTREMZ_OK;
+        }
         j.emit(PH_OUTER, j.outer);
         EZ_RUN(checksum_emit(slot));
         return loop_test(slot);

@@ -324,11 +324,13 @@ template <class T>
 static int run_one(BatchEngine<T>& e, cudaStream_t st, const DeviceTables* tables, Arena* engine_store,
                    Arena* job_store, const T* f, T* g, int W, int H, int D, const extremz_params& p0,
                    extremz_report* rep, int32_t* trace, int trace_cap,
-                   extremz_edit_stream* es = nullptr, HostWriteBack<T>* wb = nullptr) {
+                   extremz_edit_stream* es = nullptr, HostWriteBack<T>* wb = nullptr,
+                   bool census = false) {
   extremz_params p = p0;
-  p.flags &= ~(kFlagKeepInput | kFlagTrackEdits);
+  p.flags &= ~kInternalFlags;
   if (es) p.flags |= kFlagKeepInput;
   if (wb) p.flags |= kFlagTrackEdits;
+  if (census) p.flags |= kFlagCensus;
   e.set_stream(st);
   EZ_RUN(e.init(tables, engine_store));
   const bool prof = (p.flags & EXTREMZ_FLAG_PROFILE) != 0;
@@ -492,6 +494,10 @@ static int correct_noalloc(const void* d_orig, void* d_decp, int dtype, int widt
   else
     rc = run_one(d.e64, st, &d.tables, &d.engine_store, &d.job_store, (const double*)d_orig,
                  (double*)d_decp, width, height, depth, p, report, nullptr, 0);
+  // run_one can leave early on an error with kernels still writing the shared
+  // workspace; wait for them before the lock is released, so that the next
+  // call (perhaps on another stream) does not race with them.
+  if (cudaStreamSynchronize(st) != cudaSuccess) cudaGetLastError();
   if (report) report->status = rc;
   return rc;
 }
@@ -884,6 +890,38 @@ extremz_status extremz_correct_device(extremz_ctx* ctx, const void* d_orig, void
     rc = run_one(ctx->c.e64, st, nullptr, nullptr, nullptr, (const double*)d_orig,
                  (double*)d_decp, width, height, depth, *params, report, trace, trace_cap);
   if (report) report->status = rc;
+  if (prev != ctx->c.device) cudaSetDevice(prev);
+  return (extremz_status)rc;
+}
+
+extremz_status extremz_mismatch_census(extremz_ctx* ctx, const void* d_orig, const void* d_field,
+                                      int dtype, int width, int height, int depth, double thr,
+                                      int32_t* counters, void* stream) {
+  if (!ctx || !d_orig || !d_field || !counters) return EXTREMZ_BAD_ARG;
+  extremz_params p;
+  extremz_default_params(&p);
+  p.thr = thr;
+  int rc = check_args(dtype, width, height, depth, &p);
+  if (rc != EXTREMZ_OK) return (extremz_status)rc;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  extremz_report rep;
+  std::memset(&rep, 0, sizeof(rep));
+  rc = ctx->c.ensure_pool();
+  // The census job reads the field and writes only its own workspace.
+  if (rc == EXTREMZ_OK) {
+    if (dtype == EXTREMZ_F32)
+      rc = run_one<float>(ctx->c.e32, st, nullptr, nullptr, nullptr, (const float*)d_orig,
+                   const_cast<float*>((const float*)d_field), width, height, depth, p, &rep,
+                   nullptr, 0, nullptr, nullptr, true);
+    else
+      rc = run_one<double>(ctx->c.e64, st, nullptr, nullptr, nullptr, (const double*)d_orig,
+                   const_cast<double*>((const double*)d_field), width, height, depth, p, &rep,
+                   nullptr, 0, nullptr, nullptr, true);
+  }
+  std::memcpy(counters, rep.counters, sizeof(rep.counters));
   if (prev != ctx->c.device) cudaSetDevice(prev);
   return (extremz_status)rc;
 }

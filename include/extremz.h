@@ -150,6 +150,25 @@ extremz_status extremz_correct_device(extremz_ctx* ctx, const void* d_orig, void
                                       void* stream, int32_t* trace, int trace_cap);
 
 /*
+ * Mismatch census of a (corrected) field d_field against the original d_orig,
+ * both on the device: the eleven loop-test counters, in the order of
+ * extremz_report.counters, evaluated once with no edit (d_field is only read).
+ * The counters are: wrong split / join neighbours (manifold-label mismatches),
+ * false maxima / minima / saddles (critical-point mismatches), wrong maxima,
+ * wrong maxima (second), wrong saddles, wrong minima, wrong minima (second),
+ * wrong join saddles.  The reference's loop evaluates the wrong-extremum and
+ * wrong-saddle counters only when the wrong-neighbour counts are zero, and the
+ * join ones only with preserve_join_tree; the census evaluates all of them.
+ * Synchronises the stream.
+ * Replaces: the loop test's counters (src/ExtreM_cuda.cu:5589-5605) read on
+ * the final field, which the reference never does after its unconditional
+ * saddle_loops_join (:5997).
+ */
+extremz_status extremz_mismatch_census(extremz_ctx* ctx, const void* d_orig, const void* d_field,
+                                      int dtype, int width, int height, int depth, double thr,
+                                      int32_t* counters, void* stream);
+
+/*
  * Same with host buffers: copies both fields to the device, corrects, and
  * writes the corrected field back into h_decp.  h_decp still holds the
  * decompressed field at that point, so only the voxels whose value changed
@@ -359,9 +378,12 @@ long long extremz_job_footprint(int dtype, int width, int height, int depth);
  * caller's, as for extremz_correct_device, on the current device and the given
  * stream.  The first call on a device looks up the static arrays' device
  * addresses and uploads the lookup table (synchronously); make that first call
- * before any stream capture.  All calls on a device share the one workspace,
- * so calls that overlap on the GPU race: issue them one after another.  Every
- * call clears what it needs zeroed itself.  Profiling and tracing are off.
+ * before any stream capture.  Every call synchronises the stream: it reads the
+ * loop counters back between rounds and waits for its kernels before it
+ * returns, errors included.  All calls on a device share the one
+ * workspace, so calls that overlap on the GPU race: issue them one after
+ * another.  Every call clears what it needs zeroed itself.  Profiling and
+ * tracing are off.
  */
 #define EXTREMZ_NOALLOC_MAX_VOXELS 65536
 extremz_status extremz_correct_device_noalloc(const void* d_orig, void* d_decp, int dtype,

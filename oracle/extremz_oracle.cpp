@@ -34,6 +34,7 @@
 #include <cstdint>
 #include <cstring>
 #include <limits>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -890,6 +891,25 @@ struct Corrector {
     wrong_neighbors();
   }
 
+  // Mismatch census of the current decompressed field: the eleven loop-test
+  // counters (order of the loop test :5603-5605) evaluated once, with no
+  // edit.  The third block of the outer loop (:5872-5979) evaluates the
+  // wrong-extremum and wrong-saddle counters only when the wrong-neighbour
+  // counts are zero, and the join ones only with preserve_join_tree; the
+  // census evaluates all of them.
+  void census(int* out) {
+    setup();
+    detect();
+    manifold_block();
+    wrong_index_max();
+    wrong_index_saddles();
+    wrong_index_min();
+    wrong_index_saddles_join();
+    const int c[11] = {d_nfc, d_nfc1, d_cfmax, d_cfmin, d_cfsad, d_wmc,
+                       d_wmc2, d_wsc, d_wmin, d_wmin2, d_wscj};
+    std::memcpy(out, c, sizeof(c));
+  }
+
   // main() (:5508-5997), preserve_join_tree as configured.
   int run(int max_outer, bool final_join, bool preserve_join, int* outer_out, int* counters) {
     setup();
@@ -1126,7 +1146,8 @@ int encode_t(const T* f, const T* d0, const T* d1, const int32_t* counter, long 
 }
 
 bool dims_ok(int W, int H, int D) {
-  return W > 0 && H > 0 && D > 0 && (long long)W * H * D < (1ll << 31) / 16;
+  // Saddle rows hold 15 ints per saddle, indexed with int offsets.
+  return W > 0 && H > 0 && D > 0 && (long long)W * H * D * 15 < (1ll << 31);
 }
 
 // ---------------------------------------------------------------------------
@@ -1313,6 +1334,33 @@ int oracle_correct(const void* f, void* decp, int dtype, int W, int H, int D,
                      counter_out);
   return correct_t((const double*)f, (double*)decp, W, H, D, p, rep, trace, trace_cap,
                    counter_out);
+}
+
+// Mismatch census of `decp` against the original `f` (Corrector::census):
+// out receives the eleven loop-test counters.
+int oracle_census(const void* f, const void* decp, int dtype, int W, int H, int D, double thr,
+                  int32_t* out) {
+  if (!dims_ok(W, H, D) || !out) return -1;
+  auto run = [&](auto* tag) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    const T* ff = static_cast<const T*>(f);
+    std::vector<T> a(static_cast<const T*>(decp), static_cast<const T*>(decp) + (size_t)W * H * D);
+    Corrector<T> c;
+    c.g = {W, H, D, W * H * D};
+    c.f = ff;
+    c.a = a.data();
+    c.bound = T(0);
+    c.thr = (T)thr;
+    c.q = 1;
+    c.edit_type = 1;
+    c.sentinel = T(0);
+    c.trace = nullptr;
+    c.trace_cap = 0;
+    c.census(out);
+  };
+  if (dtype == 0) run((float*)nullptr);
+  else run((double*)nullptr);
+  return 0;
 }
 
 // Edit stream of a correction (see encode_t).  Returns 0, -1 on bad

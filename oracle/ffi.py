@@ -71,6 +71,7 @@ def lib():
                                               vp, ctypes.c_longlong, vp, vp,
                                               ctypes.POINTER(ctypes.c_longlong),
                                               ctypes.POINTER(ctypes.c_longlong)]
+        L.oracle_census.argtypes = [vp, vp, i32, i32, i32, i32, ctypes.c_double, vp]
         L.oracle_encode.argtypes = [vp, vp, vp, vp, i32, ctypes.c_longlong, ctypes.c_double,
                                     i32, i32, vp, ctypes.c_longlong, vp, ctypes.c_longlong,
                                     ctypes.POINTER(EditReport)]
@@ -153,6 +154,26 @@ def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, 
     if trace_cap:
         trace = trace[trace[:, 0] != 0]
     return out, rep, trace
+
+
+COUNTER_NAMES = ("wrong_split_nbrs", "wrong_join_nbrs", "false_max", "false_min", "false_saddle",
+                 "wrong_max", "wrong_max_2", "wrong_saddle", "wrong_min", "wrong_min_2",
+                 "wrong_saddle_join")
+
+
+def census(f: np.ndarray, decp: np.ndarray, *, thr: float = 0.0):
+    """Mismatch census of decp against f: the eleven loop-test counters
+    (order of ``Report.counters``) evaluated once, no edit."""
+    f = np.ascontiguousarray(f)
+    g = np.ascontiguousarray(decp)
+    assert f.dtype == g.dtype and f.shape == g.shape
+    w, h, d = _dims(f)
+    out = np.zeros(11, dtype=np.int32)
+    rc = lib().oracle_census(f.ctypes.data, g.ctypes.data, _dtype_code(f), w, h, d, float(thr),
+                             out.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"oracle_census returned {rc}")
+    return [int(x) for x in out]
 
 
 def encode(f: np.ndarray, decp0: np.ndarray, fixed: np.ndarray, counter, bound: float, *,

@@ -2,11 +2,11 @@
 # Builds the reference GPU correction from the reference checkout's own
 # source (src/ExtreM_cuda.cu, unmodified) into oracle/_ref/ref_gpu, with the
 # stub headers next to this script.  Test infrastructure only; needs the
-# reference checkout (default /root/reference) -- the GPU box uses the built
+# reference checkout given as the first argument -- the GPU box uses the built
 # binary, which travels with the repository.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:?usage: build_ref.sh <reference checkout>}"
 OUT="$HERE/../_ref"
 mkdir -p "$OUT"
 test -f "$REF/src/ExtreM_cuda.cu"

@@ -1,6 +1,6 @@
 #!/bin/bash
 # Builds the reference's CPU correction (src/ExtreM.cpp + main.cpp of the
-# reference checkout, default /root/reference) into oracle/_ref/ref_cpu, the
+# reference checkout given as the first argument) into oracle/_ref/ref_cpu, the
 # same program with zero-filled allocations into oracle/_ref/ref_cpu_zero,
 # and its merge-tree functions behind a file interface into
 # oracle/_ref/ref_mergetree.
@@ -8,7 +8,7 @@
 # path on 2-D fields (census_cpu.py).
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:?usage: build_ref_cpu.sh <reference checkout>}"
 OUT="$HERE/../_ref"
 mkdir -p "$OUT"
 test -f "$REF/src/ExtreM.cpp"

@@ -10,14 +10,20 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 import bench  # noqa: E402
 
 
-def test_dominant_bytes_first_round_full_later_rounds_lower_bound():
+def test_manifold_round_bytes_are_value_read_plus_two_label_writes():
+    n = 512 ** 3
+    assert bench.round_bytes(n, 8) == 16 * n
+    assert bench.round_bytes(n, 4) == 12 * n
+
+
+def test_jump_design_bytes_first_round_full_later_rounds_lower_bound():
     n = 256 ** 3
     # One correction: the first computed round reads 24 B and writes 10 B per
     # voxel; later rounds read 24 B and write the changed-input byte.
-    assert bench.dominant_bytes(n, 1, 1) == 34 * n
-    assert bench.dominant_bytes(n, 13, 1) == 34 * n + 12 * 25 * n
+    assert bench.jump_design_bytes(n, 1, 1) == 34 * n
+    assert bench.jump_design_bytes(n, 13, 1) == 34 * n + 12 * 25 * n
     # Thirty corrections of twelve computed rounds each.
-    assert bench.dominant_bytes(n, 360, 30) == 30 * 34 * n + 330 * 25 * n
+    assert bench.jump_design_bytes(n, 360, 30) == 30 * 34 * n + 330 * 25 * n
 
 
 class _Proc:
@@ -66,7 +72,8 @@ def test_reference_arm_prints_one_contract_line():
     import subprocess
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
-                          "--steps", "1", "--warmup", "0", "--cpu-edge", "16"],
+                          "--workload", "plain256_f64", "--steps", "1", "--warmup", "0",
+                          "--cpu-edge", "16"],
                          cwd=root, capture_output=True, text=True, timeout=600, check=True)
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
@@ -76,5 +83,8 @@ def test_reference_arm_prints_one_contract_line():
                 "vs_baseline", "dtype", "data", "config"):
         assert key in d
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    # The config names the crop that was timed, and the field it was cut from.
+    assert d["config"]["shape_whd"] == [16, 16, 16]
+    assert d["config"]["sample_of"] == {"workload": "plain256_f64", "shape_whd": [256, 256, 256]}
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}

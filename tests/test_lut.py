@@ -10,7 +10,9 @@ import pytest
 from oracle import ffi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_LUT = "/root/reference/src/LUT.bin"
+# The reference checkout, when one is named (e.g. EXTREMZ_REFERENCE_DIR=<checkout>).
+_REF_DIR = os.environ.get("EXTREMZ_REFERENCE_DIR", "")
+REFERENCE_LUT = os.path.join(_REF_DIR, "src", "LUT.bin") if _REF_DIR else ""
 
 
 def _digest():
@@ -32,7 +34,7 @@ def test_library_lut_matches_oracle():
     assert np.array_equal(api.lut(), ffi.lut())
 
 
-@pytest.mark.skipif(not os.path.exists(REFERENCE_LUT), reason="reference checkout not mounted")
+@pytest.mark.skipif(not os.path.exists(REFERENCE_LUT), reason="EXTREMZ_REFERENCE_DIR names no reference checkout")
 def test_oracle_lut_matches_reference_file_entrywise():
     ref = np.fromfile(REFERENCE_LUT, dtype="<i4")
     assert np.array_equal(ffi.lut(), ref)

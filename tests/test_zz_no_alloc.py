@@ -53,6 +53,25 @@ def test_noalloc_matches_regular_entry_point_twice(dtype):
         assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
 
 
+def test_noalloc_second_call_unaffected_by_a_different_first_call():
+    """A first call on another field (other shape, seed and dtype, near the
+    maximum size, with many more critical points) leaves its state in the
+    shared workspace; the next call must still match the regular entry point
+    byte for byte, so nothing it reads may be left over."""
+    from extrem_z_b200 import api
+    n_max = api.noalloc_max_voxels()
+    big = synth.make_field(48, 40, 32, n_gauss=40, seed=77, rel=3e-4, dtype=np.float64)
+    small = synth.make_field(36, 28, 20, n_gauss=12, seed=78, rel=2e-3, dtype=np.float32)
+    assert big.f.size <= n_max and big.f.size > 0.9 * n_max
+    ref_big, _ = _regular(big.f, big.decp, big.eb)
+    ref_small, rrep = _regular(small.f, small.decp, small.eb)
+    for fld, ref in ((big, ref_big), (small, ref_small), (big, ref_big), (small, ref_small)):
+        out, rep = _noalloc(fld.f, fld.decp, fld.eb)
+        assert rep.status == 0
+        assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+    assert rep.outer_iters == rrep.outer_iters
+
+
 def test_noalloc_rejects_fields_beyond_its_maximum():
     import torch
     from extrem_z_b200 import api
