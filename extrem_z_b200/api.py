@@ -32,7 +32,8 @@ EXPORTS = ("extremz_version", "extremz_default_params", "extremz_ctx_create",
            "extremz_ctx_destroy", "extremz_correct_device", "extremz_mismatch_census",
            "extremz_correct_host",
            "extremz_correct_batch", "extremz_correct_encode", "extremz_edit_stream_caps",
-           "extremz_zstd_size", "extremz_persistence_pairs", "extremz_persistence_tree",
+           "extremz_zstd_size", "extremz_classify", "extremz_persistence_pairs",
+           "extremz_persistence_tree",
            "extremz_server_create", "extremz_server_destroy",
            "extremz_server_submit", "extremz_server_poll", "extremz_server_wait",
            "extremz_server_get_stats", "extremz_job_footprint",
@@ -160,6 +161,8 @@ def load(build_if_missing: bool = True):
         L.extremz_mismatch_census.argtypes = [vp, vp, vp, i32, i32, i32, i32, ctypes.c_double,
                                               vp, vp]
         L.extremz_mismatch_census.restype = i32
+        L.extremz_classify.argtypes = [vp, vp, i32, i32, i32, i32, vp, vp, vp, vp]
+        L.extremz_classify.restype = i32
         L.extremz_correct_host.argtypes = [vp, vp, vp, i32, i32, i32, i32,
                                            ctypes.POINTER(Params), ctypes.POINTER(Report), vp]
         L.extremz_correct_host.restype = i32
@@ -333,6 +336,23 @@ class Context:
         res = dict(zip(COUNTER_NAMES, c))
         res["counters"] = c
         return res
+
+    def classify(self, field, *, stream=None):
+        """Vertex types (int8) and steepest-ascent / steepest-descent roots
+        (int32) of the CUDA tensor ``field``: three CUDA tensors of its shape."""
+        import torch
+        assert field.is_cuda and field.is_contiguous()
+        dt = {torch.float32: F32, torch.float64: F64}[field.dtype]
+        w, h, d = _whd(tuple(field.shape))
+        if stream is None:
+            stream = torch.cuda.current_stream(field.device).cuda_stream
+        t = torch.empty(field.shape, dtype=torch.int8, device=field.device)
+        ds = torch.empty(field.shape, dtype=torch.int32, device=field.device)
+        as_ = torch.empty(field.shape, dtype=torch.int32, device=field.device)
+        st = load().extremz_classify(self._h, field.data_ptr(), dt, w, h, d, t.data_ptr(),
+                                     ds.data_ptr(), as_.data_ptr(), stream)
+        _check(st, allow_cap=False)
+        return t, ds, as_
 
     # -- edit streams -------------------------------------------------------
     def correct_encode(self, f, decp, bound: float, *, stream=None, zstd_level: int = 3, **kw):

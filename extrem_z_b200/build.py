@@ -1,4 +1,6 @@
-"""Build the CUDA library in-tree: extrem_z_b200/libextremz.so (sm_100a)."""
+"""Build the libraries in-tree: extrem_z_b200/libextremz.so (the CUDA library,
+sm_100a) and extrem_z_b200/libExtreMz.so (the reference host API
+include/api/ExtreM.h over it, compat/extrem_api.cpp)."""
 
 from __future__ import annotations
 
@@ -11,6 +13,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libextremz.so")
+COMPAT_LIB = os.path.join(PKG, "libExtreMz.so")
+COMPAT_SOURCES = [os.path.join(PKG, "compat", "extrem_api.cpp"),
+                  os.path.join(PKG, "compat", "extrem_api.h")]
 
 SOURCES = ["extremz_engine.cu"]
 HEADERS = ["extremz_common.cuh", "extremz_kernels.cuh", "extremz_batch.cuh", "extremz_encode.cuh",
@@ -44,6 +49,7 @@ def _stale() -> bool:
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     if not force and not _stale():
+        build_compat()
         return LIB
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"),
@@ -52,7 +58,26 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_compat(force=True, verbose=verbose)
     return LIB
+
+
+def build_compat(force: bool = False, verbose: bool = False) -> str:
+    """libExtreMz.so: the reference's host API over libextremz.so (found next
+    to it at run time)."""
+    if not force and os.path.exists(COMPAT_LIB) and all(
+            os.path.getmtime(p) <= os.path.getmtime(COMPAT_LIB) for p in COMPAT_SOURCES + [LIB]):
+        return COMPAT_LIB
+    tmp = COMPAT_LIB + ".tmp"
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O2",
+           "-Xcompiler", "-fPIC", "-shared",
+           "-I", os.path.join(ROOT, "include"), COMPAT_SOURCES[0], "-o", tmp,
+           "-L", PKG, "-lextremz", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, COMPAT_LIB)
+    return COMPAT_LIB
 
 
 if __name__ == "__main__":

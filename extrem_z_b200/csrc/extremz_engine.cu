@@ -397,6 +397,38 @@ static int analyze_one(BatchEngine<T>& e, cudaStream_t st, const T* field, int W
   return rc;
 }
 
+// Vertex types and steepest-ascent / steepest-descent roots of one field: an
+// analysis job, whose arrays are copied out before its workspace goes back.
+template <class T>
+static int classify_one(BatchEngine<T>& e, cudaStream_t st, const T* field, int W, int H, int D,
+                        int8_t* d_type, int32_t* d_ds, int32_t* d_as) {
+  e.set_stream(st);
+  EZ_RUN(e.init(nullptr, nullptr));
+  extremz_params p;
+  extremz_default_params(&p);
+  p.flags = kFlagAnalysis;
+  int slot = -1;
+  EZ_RUN(e.admit(field, const_cast<T*>(field), W, H, D, p, nullptr, 0, nullptr, 0, &slot));
+  int rc = EXTREMZ_OK;
+  while (e.job(slot).pc != PC_DONE && rc == EXTREMZ_OK) rc = e.tick();
+  if (rc == EXTREMZ_OK) rc = e.job(slot).status;
+  const Job<T>& J = e.job(slot).J;
+  const size_t n = (size_t)W * H * D;
+  if (rc == EXTREMZ_OK && d_type &&
+      cudaMemcpyAsync(d_type, J.otype, n, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    rc = EXTREMZ_CUDA_ERR;
+  if (rc == EXTREMZ_OK && d_ds &&
+      cudaMemcpyAsync(d_ds, J.ds, n * 4, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    rc = EXTREMZ_CUDA_ERR;
+  if (rc == EXTREMZ_OK && d_as &&
+      cudaMemcpyAsync(d_as, J.as, n * 4, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    rc = EXTREMZ_CUDA_ERR;
+  if (rc == EXTREMZ_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = EXTREMZ_CUDA_ERR;
+  if (rc == EXTREMZ_CUDA_ERR) last_cuda_error() = cudaGetLastError();
+  e.release(slot);
+  return rc;
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free correction (extremz_correct_device_noalloc).
 //
@@ -1066,6 +1098,31 @@ extremz_status extremz_persistence_tree(extremz_ctx* ctx, const void* d_field, i
   }
   if (n_max) *n_max = counts[0];
   if (n_min) *n_min = counts[1];
+  if (prev != ctx->c.device) cudaSetDevice(prev);
+  return (extremz_status)rc;
+}
+
+extremz_status extremz_classify(extremz_ctx* ctx, const void* d_field, int dtype, int width,
+                                int height, int depth, int8_t* d_type, int32_t* d_ds,
+                                int32_t* d_as, void* stream) {
+  if (!ctx || !d_field) return EXTREMZ_BAD_ARG;
+  extremz_params p;
+  extremz_default_params(&p);
+  int rc = check_args(dtype, width, height, depth, &p);
+  if (rc != EXTREMZ_OK) return (extremz_status)rc;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != ctx->c.device) cudaSetDevice(ctx->c.device);
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = ctx->c.ensure_pool();
+  if (rc == EXTREMZ_OK) {
+    if (dtype == EXTREMZ_F32)
+      rc = classify_one(ctx->c.e32, st, (const float*)d_field, width, height, depth, d_type, d_ds,
+                        d_as);
+    else
+      rc = classify_one(ctx->c.e64, st, (const double*)d_field, width, height, depth, d_type,
+                        d_ds, d_as);
+  }
   if (prev != ctx->c.device) cudaSetDevice(prev);
   return (extremz_status)rc;
 }

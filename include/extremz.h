@@ -231,6 +231,23 @@ extremz_status extremz_correct_encode(extremz_ctx* ctx, const void* d_orig, void
                                       void* stream, extremz_edit_stream* es);
 
 /*
+ * Per-vertex critical-point type (int8: 0 minimum, 1 1-saddle, 2 2-saddle,
+ * 3 both, 4 maximum, 5 regular, -1 no table entry) and the roots of the
+ * steepest-ascent (d_ds, the maximum a vertex ascends to) and steepest-descent
+ * (d_as, the minimum) paths of every vertex, into caller device buffers of
+ * width*height*depth entries (any of the three may be NULL).  Ties are broken
+ * by vertex id.  Synchronises the stream.
+ * Replaces: classifyVertex_CUDA (src/ExtreM_cuda.cu:3720-3911) and
+ * ComputeDirection + ComputeDescendingManifold / ComputeAscendingManifold
+ * (:1464-1611), which the host API exposes as classifyAllVertices and
+ * ComputeDescendingManifold / ComputeAscendingManifold
+ * (include/api/ExtreM.h:52-54).
+ */
+extremz_status extremz_classify(extremz_ctx* ctx, const void* d_field, int dtype, int width,
+                                int height, int depth, int8_t* d_type, int32_t* d_ds,
+                                int32_t* d_as, void* stream);
+
+/*
  * Merge-tree persistence pairs of a field (device pointer), for checking that
  * a correction kept the topology: the split tree pairs every maximum with the
  * vertex where its superlevel component merges into an older one, the join

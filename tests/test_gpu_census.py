@@ -53,6 +53,22 @@ def test_census_matches_oracle(name, make):
             assert want[:8] == [0] * 8
 
 
+@pytest.mark.parametrize("name,make", CASES[1:3], ids=[c[0] for c in CASES[1:3]])
+def test_classify_and_roots_match_oracle(name, make):
+    """extremz_classify: vertex types and steepest-path roots, exact."""
+    import torch
+    from extrem_z_b200 import api
+    from oracle import ffi
+    fld = make()
+    for a in (fld.f, fld.decp):
+        t, ds, as_ = api.context(0).classify(torch.from_numpy(np.ascontiguousarray(a)).cuda())
+        t0, _ = ffi.classify(a)
+        r_ds, r_as = ffi.roots(a)
+        assert np.array_equal(t.cpu().numpy().reshape(-1), t0)
+        assert np.array_equal(ds.cpu().numpy().reshape(-1), r_ds)
+        assert np.array_equal(as_.cpu().numpy().reshape(-1), r_as)
+
+
 def test_census_of_original_is_zero():
     fld = synth.make_field(30, 26, 18, n_gauss=10, seed=43, rel=1e-3)
     assert _census_gpu(fld.f, fld.f) == [0] * 11
