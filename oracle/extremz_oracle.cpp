@@ -267,6 +267,9 @@ struct oracle_params {
   int max_cloop_rounds;  // cap on rounds of one c_loops call
   int final_join;        // run the final saddle_loops_join (:5997)
   int preserve_join;     // preserve_join_tree (:4969, false in the reference)
+  int wn_lag;            // wrong-neighbour flagging: < 0 canonical (ascending
+                         // saddle id, sequential); k >= 0 the lockstep model of
+                         // the reference's concurrent launch (see wrong_neighbors)
 };
 struct oracle_report {
   int status;        // 0 ok, 1 round cap hit
@@ -307,6 +310,7 @@ struct Corrector {
   T* a;  // decompressed field, corrected in place
   T bound, thr;
   int q, edit_type;
+  int wn_lag = -1;
   T sentinel;
 
   std::vector<int8_t> otype;
@@ -562,6 +566,37 @@ struct Corrector {
     dec_rows();
   }
 
+  // The same flagging under a lockstep model of the reference's launch, in
+  // which every saddle thread examines its j-th neighbour at step j and a
+  // flag set at step i is seen by reads from step i + lag + 1 on.  A saddle
+  // whose candidate was flagged within the last `lag` steps flags it again
+  // (a duplicate list entry) and stops, where the sequential rule would go on
+  // to its next candidate: the check-then-set race of :2426-2431 / :2483-2488.
+  void wrong_neighbors_lockstep(const std::vector<int>& sads, bool split,
+                                std::vector<uint8_t>& flag, std::vector<int>& list, int lag) {
+    std::vector<int> set_at(g.N, -1);  // step at which this launch flagged a vertex
+    std::vector<uint8_t> done(sads.size(), 0);
+    for (int j = 0; j < 14; ++j) {
+      for (size_t i = 0; i < sads.size(); ++i) {
+        if (done[i]) continue;
+        const int s = sads[i];
+        int x = s % g.W, y = (s / g.W) % g.H, z = s / (g.W * g.H);
+        int nx = x + kDir[j][0], ny = y + kDir[j][1], nz = z + kDir[j][2];
+        if (nx < 0 || nx >= g.W || ny < 0 || ny >= g.H || nz < 0 || nz >= g.D) continue;
+        const int r = nx + (ny + nz * g.H) * g.W;
+        const bool cand = split ? (above(a, r, s) && dDS[r] != DS[r])
+                                : (below(a, r, s) && dAS[r] != AS[r]);
+        if (!cand) continue;
+        const bool seen = flag[r] && set_at[r] + lag + 1 <= j;
+        if (seen) continue;
+        if (!flag[r]) set_at[r] = j;
+        flag[r] = 1;
+        list.push_back(r);
+        done[i] = 1;
+      }
+    }
+  }
+
   // get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513), with
   // saddles visited in ascending id.
   void wrong_neighbors() {
@@ -569,6 +604,14 @@ struct Corrector {
     for (int v : wn_as_list) wn_as[v] = 0;
     wn_ds_list.clear();
     wn_as_list.clear();
+    if (wn_lag >= 0) {
+      wrong_neighbors_lockstep(sad2, true, wn_ds, wn_ds_list, wn_lag);
+      wrong_neighbors_lockstep(sad1, false, wn_as, wn_as_list, wn_lag);
+      d_nfc = (int)wn_ds_list.size();
+      d_nfc1 = (int)wn_as_list.size();
+      emit(PH_WRONG_NBR, d_nfc, d_nfc1);
+      return;
+    }
     int nb[14];
     for (int s : sad2) {
       int n = g.nbrs(s, nb);
@@ -1035,6 +1078,7 @@ int correct_t(const T* f, T* a, int W, int H, int D, const oracle_params* p, ora
   c.edit_type = p->edit_type;
   c.sentinel = T(-4.0) * c.bound;  // init_delta (:2572)
   c.max_cloop_rounds = p->max_cloop_rounds;
+  c.wn_lag = p->wn_lag;
   c.trace = trace;
   c.trace_cap = trace_cap;
   std::vector<T> a0(a, a + c.g.N);

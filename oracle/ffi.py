@@ -25,7 +25,8 @@ class Params(ctypes.Structure):
     _fields_ = [("bound", ctypes.c_double), ("thr", ctypes.c_double),
                 ("q", ctypes.c_int), ("edit_type", ctypes.c_int),
                 ("max_outer", ctypes.c_int), ("max_cloop_rounds", ctypes.c_int),
-                ("final_join", ctypes.c_int), ("preserve_join", ctypes.c_int)]
+                ("final_join", ctypes.c_int), ("preserve_join", ctypes.c_int),
+                ("wn_lag", ctypes.c_int)]
 
 
 class Report(ctypes.Structure):
@@ -129,7 +130,7 @@ def roots(f: np.ndarray):
 def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, q: int = 4,
             edit_type: int = 1, max_outer: int = 500, max_cloop_rounds: int = 100000,
             final_join: bool = True, preserve_join: bool = False, trace_cap: int = 0,
-            counter_out: np.ndarray = None):
+            counter_out: np.ndarray = None, wn_lag: int = -1):
     """Run the oracle correction; returns (corrected copy, report dict, trace).
 
     counter_out (optional, int32 of the field's size) receives the final edit
@@ -139,7 +140,7 @@ def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, 
     assert f.dtype == out.dtype and f.shape == out.shape
     w, h, d = _dims(f)
     p = Params(bound, thr, q, edit_type, max_outer, max_cloop_rounds,
-               int(final_join), int(preserve_join))
+               int(final_join), int(preserve_join), int(wn_lag))
     r = Report()
     tr = np.zeros(max(trace_cap, 1) * 4, dtype=np.int32)
     rc = lib().oracle_correct(f.ctypes.data, out.ctypes.data, _dtype_code(f), w, h, d,
