@@ -438,10 +438,14 @@ def run_ours(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # An NVTX range names the timed steps for a profiler's kernel filter
+    # (ncu --nvtx --nvtx-include "timed/").
+    torch.cuda.nvtx.range_push("timed")
     ev0.record(stream)
     reps = correct_steps(ctx, f, g, g0, field, stream, args.steps, profile=list(DOMINANT))
     ev1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     barrier(world)
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
@@ -568,9 +572,11 @@ def run_ours(args, world, rank, local):
                              "plain_loop_gpu_launches": b["plain_loop"]["gpu_launches"]},
                  "served": {"workload": f"serve ({sv['requests_max']} requests at most per rate)",
                             "plain_loop_fields_per_s": sv["plain_loop"]["fields_per_s"],
+                            "alone_ms": sv["alone_ms"],
                             "peak_running": sv["peak_running"],
                             "sweep": [{k: x[k] for k in ("rate_req_s", "requests", "p50_ms",
-                                                         "p99_ms", "fields_per_s",
+                                                         "p99_ms", "slowdown_p50",
+                                                         "slowdown_p99", "fields_per_s",
                                                          "mean_in_system")}
                                       for x in sv["sweep"]],
                             "bit_identical_to_plain": sv["bit_identical_to_plain"]}}
@@ -798,13 +804,17 @@ def measure_served(local, rates, n_max=96, seconds=3.0, reqs=None):
     for (f, g0, eb), w in zip(reqs, work):
         w.copy_(g0)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for (f, g0, eb), w in zip(reqs, work):
+    # Each request alone, timed on its own: the service time that a served
+    # request's latency is compared with (its slowdown).
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in reqs]
+    for (f, g0, eb), w, (a, b) in zip(reqs, work, evs):
+        a.record(stream)
         ctx.correct_device(f, w, eb, stream=stream.cuda_stream, **PARAMS)
-    e1.record(stream)
+        b.record(stream)
     torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1)
+    alone_ms = np.array([a.elapsed_time(b) for a, b in evs])
+    plain_ms = evs[0][0].elapsed_time(evs[-1][1])
     plain_out = [w.clone() for w in work]
     ctx.close()
 
@@ -840,9 +850,16 @@ def measure_served(local, rates, n_max=96, seconds=3.0, reqs=None):
             lat = np.array([r[1] for r in results])
             identical &= all(torch.equal(work[i], plain_out[i]) for i in range(n))
             span = t_end - t_start
+            # Slowdown: latency over the request's own service time alone.  At
+            # light load the latency spread is the spread of request sizes
+            # (32^3 to 384^3 voxels); the slowdown shows what waiting and
+            # sharing the device add.
+            slow = lat / np.maximum(alone_ms[:n], 1e-3)
             sweep.append({"rate_req_s": rate, "requests": n,
                           "p50_ms": float(np.percentile(lat, 50)),
                           "p99_ms": float(np.percentile(lat, 99)),
+                          "slowdown_p50": float(np.percentile(slow, 50)),
+                          "slowdown_p99": float(np.percentile(slow, 99)),
                           "fields_per_s": n / span,
                           "mvox_per_s": sum(vox[:n]) / span / 1e6,
                           # Little's law: time-averaged number of requests in the system.
@@ -850,6 +867,9 @@ def measure_served(local, rates, n_max=96, seconds=3.0, reqs=None):
                           "statuses": sorted({r[0].status for r in results})})
         st = srv.stats()
     return {"requests_max": n_max, "voxels_total": int(sum(vox)),
+            "alone_ms": {"p50": float(np.percentile(alone_ms, 50)),
+                         "p99": float(np.percentile(alone_ms, 99)),
+                         "max": float(alone_ms.max())},
             "plain_loop": {"fields_per_s": n_max / (plain_ms * 1e-3),
                            "mvox_per_s": sum(vox) / (plain_ms * 1e-3) / 1e6, "ms": plain_ms},
             "sweep": sweep, "bit_identical_to_plain": bool(identical),

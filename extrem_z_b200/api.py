@@ -97,6 +97,7 @@ class ServerStats(ctypes.Structure):
 
 FLAG_PROFILE = 1
 FLAG_NO_TMA = 2
+FLAG_WN_LOCKSTEP = 4
 PROFILE_CLASS_SHIFT = 8
 KCLASS_NAMES = ("setup_classify", "classify_detect", "direction", "jump", "propose", "apply",
                 "rows", "wrong_nbr", "fixpath", "other")
@@ -236,9 +237,12 @@ def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 
                 final_join: bool = True, preserve_join: bool = False,
                 profile=False, tma=None, device_iter_cap: int = 0,
                 blocks_per_sm: int = 0, pass_chunk: int = 0, tuned: bool = True,
-                tuning_key=None) -> Params:
+                tuning_key=None, wn_lockstep: bool = False) -> Params:
     """profile: False, True (time every kernel class) or an iterable of class
     names from KCLASS_NAMES to time only those.
+
+    wn_lockstep: resolve the wrong-neighbour race of the reference in lockstep
+    order (EXTREMZ_FLAG_WN_LOCKSTEP) instead of the canonical ascending order.
 
     tma, blocks_per_sm, pass_chunk: launch-shape knobs (results do not depend
     on them).  Those left unset come from the autotuner's table for the
@@ -260,6 +264,8 @@ def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 
             pass_chunk = pass_chunk or t["pass_chunk"]
     p.tune_blocks_per_sm, p.tune_pass_chunk = int(blocks_per_sm), int(pass_chunk)
     p.flags = 0 if (tma is None or tma) else FLAG_NO_TMA
+    if wn_lockstep:
+        p.flags |= FLAG_WN_LOCKSTEP
     if profile:
         p.flags |= FLAG_PROFILE
         if profile is not True:

@@ -295,6 +295,7 @@ class BatchEngine {
     J.edit_type = p.edit_type;
     J.iter_cap = p.device_iter_cap > 0 ? p.device_iter_cap : J.dim.N + 1;
     J.pass_chunk = p.tune_pass_chunk > 0 ? p.tune_pass_chunk : 4;
+    J.wn_lockstep = (p.flags & EXTREMZ_FLAG_WN_LOCKSTEP) != 0;
     jh.blocks_per_sm = p.tune_blocks_per_sm > 0 ? p.tune_blocks_per_sm : 8;
     J.tb = tb_;
     J.ctr = ctr_dev_ + (size_t)slot * C_COUNT;
@@ -1119,8 +1120,19 @@ class BatchEngine {
           launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, bs);
           launch(K_OTHER, k_clear_changed<T>, grid_, 256, jobs, bs);
           launch(K_ROWS, k_saddle_pass<T>, grid_, 256, jobs, bs);
-          wn_rounds<true>(bs);  // its completion brings in the join side's list
-          wn_rounds<false>(bs);
+          bool vote = false, lockstep = false;
+          for (int i : busy) (slots_[i].J.wn_lockstep ? lockstep : vote) = true;
+          if (vote) {
+            wn_rounds<true>(bs);  // its completion brings in the join side's list
+            wn_rounds<false>(bs);
+          }
+          if (lockstep) {
+            const int grid = std::min(grid_, 2 * sms_);
+            for (int d = 0; d < kNumDirs; ++d)
+              launch(K_WRONG_NBR, k_wn_step<T, true>, grid, 256, jobs, bs, d);
+            for (int d = 0; d < kNumDirs; ++d)
+              launch(K_WRONG_NBR, k_wn_step<T, false>, grid, 256, jobs, bs, d);
+          }
         }
         for (int i : sel) {
           slots_[i].manifold_rounds++;

@@ -74,6 +74,7 @@ struct Job {
   int tma_f, tma_g;
   int iter_cap;  // device-side limit of pointer jumping and path walks
   int pass_chunk; // 1024-id blocks per saddle-pass work item (a tuning knob)
+  int wn_lockstep; // wrong neighbours by the lockstep resolution (k_wn_step)
 };
 
 // Jobs served by one launch.  Every per-round kernel takes the device array of
@@ -1373,7 +1374,7 @@ __global__ void __launch_bounds__(256) k_wn_vote(const Job<T>* __restrict__ jobs
                                                  int r) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
-  if (J.ctr[C_MFSKIP]) continue;
+  if (J.ctr[C_MFSKIP] || J.wn_lockstep) continue;
   if (r == 0) {
     // A short list (every round after the first few of a correction) goes to
     // the block completion whole: the grid rounds would be launches with
@@ -1408,7 +1409,7 @@ __global__ void __launch_bounds__(256) k_wn_commit(const Job<T>* __restrict__ jo
                                                    int r) {
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
-  if (J.ctr[C_MFSKIP] || J.ctr[C_WNSMALL]) continue;
+  if (J.ctr[C_MFSKIP] || J.ctr[C_WNSMALL] || J.wn_lockstep) continue;
   const unsigned long long round = (unsigned)(J.ctr[C_WNROUND] + r + 1);
   const int stamp = J.ctr[C_WNSTAMP];
   const int n = J.ctr[C_CAND + (r & 1)];
@@ -1455,7 +1456,7 @@ template <class T, bool kSplit>
 __global__ void __launch_bounds__(1024) k_wn_resolve(Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   if (blockIdx.x >= sel.n) return;
   Job<T>& J = jobs[sel.idx[blockIdx.x]];
-  if (J.ctr[C_MFSKIP]) return;
+  if (J.ctr[C_MFSKIP] || J.wn_lockstep) return;
   __shared__ int s_next;
   const int stamp = J.ctr[C_WNSTAMP];
   int* taken = kSplit ? J.taken : J.taken1;
@@ -1524,6 +1525,51 @@ __global__ void __launch_bounds__(1024) k_wn_resolve(Job<T>* __restrict__ jobs, 
       J.ctr[C_CAND] = 0;
     }
     J.ctr[C_CAND_NEXT] = 0;
+  }
+}
+
+// Lockstep resolution of the wrong-neighbour flags (jobs with wn_lockstep).
+// Launch d flags, for every saddle of the side's candidate list that no
+// earlier launch resolved, its direction-d neighbour when that neighbour is a
+// candidate (on the side, label differs from the original's) and no earlier
+// launch flagged it.  Two saddles never share their direction-d neighbour, so
+// a launch has no conflict, and the launches in direction order make each see
+// every earlier one.  This is how the reference's concurrent launch resolves
+// its check-then-set when its threads advance through their neighbour loops
+// in step (get_wrong_split_neighbors / _join_, src/ExtreM_cuda.cu:2400-2513):
+// a shared candidate goes to the saddle that meets it at the earlier
+// neighbour index.  A saddle's resolution is marked in claim[] (unused by this
+// mode), per side and per round stamp.
+template <class T, bool kSplit>
+__global__ void __launch_bounds__(256) k_wn_step(const Job<T>* __restrict__ jobs,
+                                                 const __grid_constant__ Sel sel, int d) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+    const Job<T>& J = jobs[sel.idx[jk]];
+    if (J.ctr[C_MFSKIP] || !J.wn_lockstep) continue;
+    const int stamp = J.ctr[C_WNSTAMP];
+    const unsigned long long done =
+        (1ull << 63) | (kSplit ? 0ull : (1ull << 62)) | (unsigned)stamp;
+    const int n = J.ctr[kSplit ? C_CAND : C_CANDJ];
+    const int* list = kSplit ? J.cand : J.cand_j;
+    int* taken = kSplit ? J.taken : J.taken1;
+    int* flagged = kSplit ? J.flagged : J.flagged1;
+    int* nflag = J.ctr + (kSplit ? C_NFC : C_NFC1);
+    const Dims g = J.dim;
+    const int stride = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+      const int s = list[e];
+      int x, y, z;
+      coords(s, g, x, y, z);
+      if (!dir_valid(d, boundary_code(x, y, z, g.W, g.H, g.D))) continue;
+      if (J.claim[s] == done) continue;
+      const int r = s + ddx(d) + ddy(d) * g.W + ddz(d) * g.W * g.H;
+      const T sv = J.g[s], rv = J.g[r];
+      if (!(kSplit ? above(rv, r, sv, s) : below(rv, r, sv, s))) continue;
+      if ((kSplit ? J.dds[r] == J.ds[r] : J.das[r] == J.as[r]) || taken[r] == stamp) continue;
+      taken[r] = stamp;
+      flagged[atomicAdd(nflag, 1)] = r;
+      J.claim[s] = done;
+    }
   }
 }
 

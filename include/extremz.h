@@ -89,6 +89,15 @@ typedef struct {
  * (TMA is used whenever the field's base is 16-byte aligned and its row stride
  * W * sizeof(value) is a multiple of 16 bytes). */
 #define EXTREMZ_FLAG_NO_TMA 2
+/* flags: resolve the wrong-neighbour flags (get_wrong_split_neighbors /
+ * get_wrong_join_neighbors, src/ExtreM_cuda.cu:2400-2513) in lockstep order --
+ * a neighbour two saddles share goes to the saddle that meets it at the
+ * earlier neighbour index, as the reference's concurrent launch does when its
+ * threads advance in step -- instead of the default canonical order
+ * (saddles in ascending id, sequentially).  The reference's check-then-set is
+ * a race, so its runs can differ; its runs on the 256^3 benchmark field give
+ * the lockstep result, its runs on the 512^3 field the result of both. */
+#define EXTREMZ_FLAG_WN_LOCKSTEP 4
 
 /* Kernel classes of extremz_report.prof_*: 0 setup (classification, labels and
  * rows of the original field), 1 fused classification + mismatch detection,

@@ -98,3 +98,30 @@ def test_mixed_batch_matches_oracle_digests(final_join):
         d = e[f"final_join_{final_join}"]
         census = ctx.mismatch_census(f, g)["counters"]
         check(d, sha(g.cpu().numpy()), rep, census)
+
+
+with open(os.path.join(HERE, "golden", "ref_gpu_cases.json")) as _fh:
+    REF_RUNS = json.load(_fh)
+
+
+@pytest.mark.parametrize("name,lockstep", [("plain256_f64", True), ("plain512_f64", False),
+                                           ("plain512_f64", True)])
+def test_benchmark_fields_equal_the_reference_gpu_output(name, lockstep):
+    """The reference's own GPU correction of the 256^3 and 512^3 float64
+    benchmark fields (its runs agree with one another): the library's output
+    is byte-identical to it, with the wrong-neighbour race resolved in
+    lockstep order at 256^3 (the resolution the reference's runs took) and in
+    either order at 512^3."""
+    import torch
+    from extrem_z_b200 import api
+    fld = field(name)
+    runs = REF_RUNS[name]["run_sha256"]
+    assert REF_RUNS[name]["runs_agree"]
+    f = torch.from_numpy(fld.f).cuda()
+    g = torch.from_numpy(fld.decp).cuda()
+    rep, _ = api.context(0).correct_device(f, g, fld.eb, q=4, edit_type=1, max_outer=1000,
+                                           final_join=True, wn_lockstep=lockstep)
+    assert rep.status == 0
+    assert sha(g.cpu().numpy()) == runs[0]
+    del f, g
+    torch.cuda.empty_cache()

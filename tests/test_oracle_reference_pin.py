@@ -64,6 +64,18 @@ def test_reference_runs_agree_and_equal_canonical_oracle(name):
     assert oracle_sha(name) == REF[name]["run_sha256"][0]
 
 
+@pytest.mark.skipif("lockstep_final_join_1" not in DIGESTS.get("plain256_f64", {}),
+                    reason="no lockstep digest of the 256^3 field")
+def test_256_field_reference_equals_lockstep_oracle():
+    """256^3 float64 (512 Gaussians, seed 1, eb 1e-4 rel): the reference's runs
+    agree with one another and equal the oracle's lockstep resolution of the
+    wrong-neighbour race (its canonical resolution differs)."""
+    runs = REF["plain256_f64"]["run_sha256"]
+    assert REF["plain256_f64"]["runs_agree"]
+    assert DIGESTS["plain256_f64"]["lockstep_final_join_1"]["fixed_sha256"] == runs[0]
+    assert DIGESTS["plain256_f64"]["final_join_1"]["fixed_sha256"] != runs[0]
+
+
 def test_headline_field_reference_equals_oracle():
     """512^3 float64 (4096 Gaussians, k^-5/3 noise, eb 1e-5 rel): the
     reference's corrected field equals the oracle's digest of the same field."""
@@ -99,7 +111,7 @@ def table() -> str:
         runs = entry["run_sha256"]
         if name in DIGESTS:
             canon = DIGESTS[name]["final_join_1"]["fixed_sha256"]
-            lock = None
+            lock = DIGESTS[name].get("lockstep_final_join_1", {}).get("fixed_sha256")
         else:
             canon, lock = oracle_sha(name), oracle_sha(name, lockstep=True)
         def hits(h):
