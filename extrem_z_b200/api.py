@@ -97,7 +97,7 @@ class ServerStats(ctypes.Structure):
 
 FLAG_PROFILE = 1
 FLAG_NO_TMA = 2
-FLAG_WN_LOCKSTEP = 4
+FLAG_WN_ASCENDING = 4
 PROFILE_CLASS_SHIFT = 8
 KCLASS_NAMES = ("setup_classify", "classify_detect", "direction", "jump", "propose", "apply",
                 "rows", "wrong_nbr", "fixpath", "other")
@@ -237,12 +237,13 @@ def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 
                 final_join: bool = True, preserve_join: bool = False,
                 profile=False, tma=None, device_iter_cap: int = 0,
                 blocks_per_sm: int = 0, pass_chunk: int = 0, tuned: bool = True,
-                tuning_key=None, wn_lockstep: bool = False) -> Params:
+                tuning_key=None, wn_order: str = "lockstep") -> Params:
     """profile: False, True (time every kernel class) or an iterable of class
     names from KCLASS_NAMES to time only those.
 
-    wn_lockstep: resolve the wrong-neighbour race of the reference in lockstep
-    order (EXTREMZ_FLAG_WN_LOCKSTEP) instead of the canonical ascending order.
+    wn_order: how the reference's wrong-neighbour race is resolved:
+    "lockstep" (default, the reference's own outcome) or "ascending" (saddles
+    in ascending id, EXTREMZ_FLAG_WN_ASCENDING).
 
     tma, blocks_per_sm, pass_chunk: launch-shape knobs (results do not depend
     on them).  Those left unset come from the autotuner's table for the
@@ -264,8 +265,10 @@ def make_params(bound: float, *, thr: float = 0.0, q: int = 4, edit_type: int = 
             pass_chunk = pass_chunk or t["pass_chunk"]
     p.tune_blocks_per_sm, p.tune_pass_chunk = int(blocks_per_sm), int(pass_chunk)
     p.flags = 0 if (tma is None or tma) else FLAG_NO_TMA
-    if wn_lockstep:
-        p.flags |= FLAG_WN_LOCKSTEP
+    if wn_order not in ("lockstep", "ascending"):
+        raise ValueError(f"wn_order must be 'lockstep' or 'ascending', not {wn_order!r}")
+    if wn_order == "ascending":
+        p.flags |= FLAG_WN_ASCENDING
     if profile:
         p.flags |= FLAG_PROFILE
         if profile is not True:

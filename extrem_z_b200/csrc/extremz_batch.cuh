@@ -127,6 +127,7 @@ constexpr long long job_bytes_cps(long long ns2, long long ns1, long long nmax, 
   return arr_bytes(ns2, 4) + arr_bytes(ns1, 4) + arr_bytes(nmax, 4) + arr_bytes(nmin, 4)
          + arr_bytes(ns2 * kRowStride, 4) + arr_bytes(ns2 * 2, 4) + arr_bytes(ns2, 1)
          + arr_bytes(ns1 * kRowStride, 4) + arr_bytes(ns1 * 2, 4) + arr_bytes(ns1, 1)
+         + 2 * arr_bytes(ns2, 16) + 2 * arr_bytes(ns1, 16)  // compact rows (orm, oend)
          + arr_bytes(ns2, 1) + arr_bytes(ns1, 1)                    // seed bits
          + 4 * arr_bytes(nmax, 4) + 4 * arr_bytes(nmin, 4)
          + arr_bytes(nmax > nmin ? nmax : nmin, ksz) + arr_bytes(nmax > nmin ? nmax : nmin, 4)
@@ -295,7 +296,7 @@ class BatchEngine {
     J.edit_type = p.edit_type;
     J.iter_cap = p.device_iter_cap > 0 ? p.device_iter_cap : J.dim.N + 1;
     J.pass_chunk = p.tune_pass_chunk > 0 ? p.tune_pass_chunk : 4;
-    J.wn_lockstep = (p.flags & EXTREMZ_FLAG_WN_LOCKSTEP) != 0;
+    J.wn_lockstep = (p.flags & EXTREMZ_FLAG_WN_ASCENDING) == 0;
     jh.blocks_per_sm = p.tune_blocks_per_sm > 0 ? p.tune_blocks_per_sm : 8;
     J.tb = tb_;
     J.ctr = ctr_dev_ + (size_t)slot * C_COUNT;
@@ -1116,8 +1117,28 @@ class BatchEngine {
         if (!busy.empty()) {
           const Sel bs = make_sel(busy, false), bt = make_sel(busy, true);
           ctl(bs, OP_MF_BEGIN);
-          launch(K_DIRECTION, k_direction<T, true>, bt.off[bt.n], 256, jobs, bt);
-          launch(K_JUMP, k_jump2<T, true>, grid_, 256, jobs, bs);
+          // Steepest pointers: every tile in a job's first round, one block
+          // per tile; in later rounds the tiles that changed, listed first,
+          // then taken by a fixed grid (a launch of one block per tile of
+          // the field costs more than the few changed tiles).
+          std::vector<int> fresh, later;
+          for (int i : busy) (slots_[i].manifold_rounds == 0 ? fresh : later).push_back(i);
+          if (!fresh.empty()) {
+            const Sel ft = make_sel(fresh, true);
+            launch(K_DIRECTION, k_direction<T, true>, ft.off[ft.n], 256, jobs, ft);
+          }
+          if (!later.empty()) {
+            const Sel ls = make_sel(later, false), lt = make_sel(later, true);
+            const int ntiles = lt.off[lt.n];
+            launch(K_DIRECTION, k_tile_list<T>,
+                   std::max(1, std::min((ntiles + 255) / 256, 2 * sms_)), 256, jobs, ls);
+            launch(K_DIRECTION, k_direction_list<T>, std::max(1, std::min(ntiles, 3 * sms_)),
+                   256, jobs, ls);
+          }
+          if (!fresh.empty())
+            launch(K_JUMP, k_jump2<T, true, false>, grid_, 256, jobs, make_sel(fresh, false));
+          if (!later.empty())
+            launch(K_JUMP, k_jump2<T, true, true>, grid_, 256, jobs, make_sel(later, false));
           launch(K_OTHER, k_clear_changed<T>, grid_, 256, jobs, bs);
           launch(K_ROWS, k_saddle_pass<T>, grid_, 256, jobs, bs);
           bool vote = false, lockstep = false;
@@ -1149,6 +1170,7 @@ class BatchEngine {
         return EXTREMZ_OK;
       case PC_SADDLE:
         ctl(s, OP_SADDLE_BEGIN);
+        launch(K_OTHER, k_wis_table<T, true>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs, s, 1);
         launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
@@ -1169,6 +1191,7 @@ class BatchEngine {
       case PC_SADDLE_J:
       case PC_FINAL_JOIN:
         ctl(s, OP_SADDLE_JOIN_BEGIN);
+        launch(K_OTHER, k_wis_table<T, false>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs, s, 1);
         launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
@@ -1185,6 +1208,7 @@ class BatchEngine {
         ctl(s, OP_DETECT3_BEGIN);
         launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, jobs, s, 0);
+        launch(K_OTHER, k_wis_table<T, true>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs, s, 0);
         for (int i : sel) {
@@ -1196,6 +1220,7 @@ class BatchEngine {
         ctl(s, OP_DETECT3_JOIN_BEGIN);
         launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, jobs, s, 0);
+        launch(K_OTHER, k_wis_table<T, false>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs, s, 0);
         for (int i : sel) slots_[i].pc = PC_FINAL_DETECT;
@@ -1258,9 +1283,13 @@ class BatchEngine {
     J.maxima = A.take<int>(nmax);
     J.minima = A.take<int>(nmin);
     J.orow2 = A.take<int>((long long)ns2 * kRowStride);
+    J.orm2 = A.take<int4>(ns2);
+    J.oend2 = A.take<int4>(ns2);
     J.drow2 = A.take<int>((long long)ns2 * 2);
     J.ocnt2 = A.take<uint8_t>(ns2);
     J.orow1 = A.take<int>((long long)ns1 * kRowStride);
+    J.orm1 = A.take<int4>(ns1);
+    J.oend1 = A.take<int4>(ns1);
     J.drow1 = A.take<int>((long long)ns1 * 2);
     J.ocnt1 = A.take<uint8_t>(ns1);
     J.has2 = A.take<uint8_t>(ns2);

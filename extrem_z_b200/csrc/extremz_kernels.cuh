@@ -60,6 +60,8 @@ struct Job {
 
   int* sad2; int* sad1; int* maxima; int* minima;
   int* orow2; int* orow1;  // original rows of kRowStride ints
+  int4* orm2; int4* orm1;  // per row: its first four entries as extremum indices (-1 past the count)
+  int4* oend2; int4* oend1;  // per row: first and last entry, then both as extremum indices
   int* drow2; int* drow1;  // decompressed rows: 2 persistent slots per row, see k_saddle_pass
   int* largest; int* smallest;  // per maximum / minimum
   int* first1; int* flag2;      // per maximum: wrong_index_max arbitration
@@ -74,7 +76,8 @@ struct Job {
   int tma_f, tma_g;
   int iter_cap;  // device-side limit of pointer jumping and path walks
   int pass_chunk; // 1024-id blocks per saddle-pass work item (a tuning knob)
-  int wn_lockstep; // wrong neighbours by the lockstep resolution (k_wn_step)
+  int wn_lockstep; // wrong neighbours by the lockstep resolution (k_wn_step, the
+                   // default), else in ascending saddle order (k_wn_vote / commit / resolve)
 };
 
 // Jobs served by one launch.  Every per-round kernel takes the device array of
@@ -107,6 +110,7 @@ enum Ctr : int {
   C_WNROUND,   // wrong-neighbour arbitration round (vote high word)
   C_WNSMALL,   // this side's candidate list is small: the block completion does it all
   C_MFFIRST,   // the manifold round being computed is the job's first: every input is new
+  C_TLIST,     // tiles listed for this manifold round's steepest pointers (k_tile_list)
   C_COUNT
 };
 // Error bits in ctr[C_ERROR].
@@ -174,18 +178,20 @@ __device__ __forceinline__ void mark_tiles(uint8_t* tdirty, const Dims& g, int x
 // Halo tile: TMA box (one bulk tensor copy, zero fill outside the grid) when
 // the field's row stride allows it, else plain loads with every thread's loads
 // issued before its first shared store.  Outside-grid entries are never read.
+// A block that loads several tiles initialises the barrier once (init) and
+// waits on alternating phases (parity = loads issued before this one, mod 2).
 template <class T>
 __device__ __forceinline__ bool load_tile(Tile<T>& s, uint64_t* bar, const CUtensorMap* map,
                                           bool tma, const T* __restrict__ a, const Dims& g, int bx,
-                                          int by, int bz) {
+                                          int by, int bz, unsigned parity = 0, bool init = true) {
   if (tma) {
     if (threadIdx.x == 0) {
-      mbar_init(bar, 1);
+      if (init) mbar_init(bar, 1);
       mbar_expect_tx(bar, (unsigned)sizeof(Tile<T>));
       tma_load_3d(&s.v[0][0][0], map, bx - kXOff, by - 1, bz - 1, bar);
     }
     __syncthreads();
-    return mbar_wait(bar, 0, 1ll << 26);
+    return mbar_wait(bar, parity, 1ll << 26);
   }
   constexpr int HX = TX + 2;
   constexpr int kTotal = HX * SY * SZ;
@@ -532,28 +538,25 @@ __device__ __forceinline__ int follow(const int16_t* nxt, const int* exit_gid, i
   return (bx + cx) + (by + cy) * W + (bz + cz) * WH;
 }
 
-// kDec = false: f into ds / as (setup); true: g into dds / das.
+// Steepest pointers of one tile, compressed to the tile's exits: every voxel's
+// pointer is the first vertex outside the tile on its steepest path, or the
+// path's root inside the tile.  kDec = false: f into ds / as (setup); true: g
+// into pdd / pda.  Returns false when the tile's load did not complete.
 template <class T, bool kDec>
-__global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jobs,
-                                                   const __grid_constant__ Sel sel) {
-  __shared__ Tile<T> s;
-  __shared__ uint64_t bar;
-  __shared__ int16_t hnext[TZ * TY * TX], lnext[TZ * TY * TX];
-  __shared__ int hexit[TZ * TY * TX], lexit[TZ * TY * TX];
-  int bx, by, bz, tile;
-  const Job<T>& J = tile_job(jobs, sel, bx, by, bz, &tile);
-  if (kDec && J.ctr[C_MFSKIP]) return;  // same inputs as the last manifold round
-  if (kDec && !J.tdirty[tile]) return;  // tile and halo unchanged: pointers stand
+__device__ __noinline__ bool direction_tile(const Job<T>& J, Tile<T>& s, uint64_t* bar,
+                                               int16_t* hnext, int16_t* lnext, int* hexit,
+                                               int* lexit, int bx, int by, int bz,
+                                               unsigned parity, bool init) {
   const Dims g = J.dim;
   const int WH = g.W * g.H;
   const T* a = kDec ? J.g : J.f;
   int* ds = kDec ? J.pdd : J.ds;
   int* as = kDec ? J.pda : J.as;
   // The block decides together: its threads meet at a barrier further on.
-  if (!__syncthreads_and(load_tile<T>(s, &bar, kDec ? J.map_g : J.map_f, kDec ? J.tma_g : J.tma_f,
-                                      a, g, bx, by, bz))) {
+  if (!__syncthreads_and(load_tile<T>(s, bar, kDec ? J.map_g : J.map_f, kDec ? J.tma_g : J.tma_f,
+                                      a, g, bx, by, bz, parity, init))) {
     if (threadIdx.x == 0) atomicOr(J.ctr + C_ERROR, kErrTile);
-    return;
+    return false;
   }
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   for (int tz = 0; tz < TZ; ++tz) {
@@ -579,7 +582,77 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
     ds[v] = follow(hnext, hexit, li, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
     as[v] = follow(lnext, lexit, li, bx, by, bz, g.W, WH, J.ctr + C_ERROR);
   }
+  return true;
+}
+
+// Setup: every tile of the original field, one block per tile.
+template <class T, bool kDec>
+__global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jobs,
+                                                   const __grid_constant__ Sel sel) {
+  __shared__ Tile<T> s;
+  __shared__ uint64_t bar;
+  __shared__ int16_t hnext[TZ * TY * TX], lnext[TZ * TY * TX];
+  __shared__ int hexit[TZ * TY * TX], lexit[TZ * TY * TX];
+  int bx, by, bz, tile;
+  const Job<T>& J = tile_job(jobs, sel, bx, by, bz, &tile);
+  if (kDec && J.ctr[C_MFSKIP]) return;  // same inputs as the last manifold round
+  if (kDec && !J.tdirty[tile]) return;  // tile and halo unchanged: pointers stand
+  if (!direction_tile<T, kDec>(J, s, &bar, hnext, lnext, hexit, lexit, bx, by, bz, 0, true))
+    return;
   if (kDec && threadIdx.x == 0) J.tdirty[tile] = 0;
+}
+
+// The tiles of each selected job whose tile or halo changed since their
+// pointers were computed (every tile in a job's first round), into the
+// job's tile list (cand_next, free at this point of a manifold round;
+// count C_TLIST, zeroed when the round begins).
+template <class T>
+__global__ void __launch_bounds__(256) k_tile_list(const Job<T>* __restrict__ jobs,
+                                                   const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+    const Job<T>& J = jobs[sel.idx[jk]];
+    if (J.ctr[C_MFSKIP]) continue;
+    const int nt = ((J.dim.W + TX - 1) / TX) * ((J.dim.H + TY - 1) / TY) *
+                   ((J.dim.D + TZ - 1) / TZ);
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < nt; base += stride) {  // uniform per warp
+      const int t = base + threadIdx.x;
+      const bool dirty = t < nt && J.tdirty[t];
+      const int slot = warp_append(J.ctr + C_TLIST, dirty, 0xffffffffu);
+      if (slot >= 0) J.cand_next[slot] = t;
+    }
+  }
+}
+
+// A manifold round's steepest pointers of the decompressed field: a fixed
+// grid whose blocks take the listed tiles of every selected job in turn, so
+// that a round with few changed tiles launches few blocks' worth of work
+// instead of one block per tile of the field.
+template <class T>
+__global__ void __launch_bounds__(256, 3) k_direction_list(const Job<T>* __restrict__ jobs,
+                                                        const __grid_constant__ Sel sel) {
+  __shared__ Tile<T> s;
+  __shared__ uint64_t bar;
+  __shared__ int16_t hnext[TZ * TY * TX], lnext[TZ * TY * TX];
+  __shared__ int hexit[TZ * TY * TX], lexit[TZ * TY * TX];
+  unsigned loads = 0;  // TMA loads issued by this block: the barrier's phase
+  for (int jk = 0; jk < sel.n; ++jk) {
+    const Job<T>& J = jobs[sel.idx[jk]];
+    if (J.ctr[C_MFSKIP]) continue;
+    const int n = J.ctr[C_TLIST];
+    const int ntx = (J.dim.W + TX - 1) / TX, nty = (J.dim.H + TY - 1) / TY;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+      const int t = J.cand_next[k];
+      const int bx = (t % ntx) * TX, by = ((t / ntx) % nty) * TY, bz = (t / (ntx * nty)) * TZ;
+      __syncthreads();  // every thread is done with the shared tile of the last one
+      const bool tma = J.tma_g != 0;
+      if (!direction_tile<T, true>(J, s, &bar, hnext, lnext, hexit, lexit, bx, by, bz,
+                                   loads & 1u, loads == 0))
+        return;
+      loads += tma;
+      if (threadIdx.x == 0) J.tdirty[t] = 0;
+    }
+  }
 }
 
 // Global pointer jumping of both label arrays (ComputeDescendingManifold /
@@ -590,8 +663,11 @@ __global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jo
 // to original 2-saddles, the only places they are read).  Iterations are
 // capped; hitting the cap sets the error word instead of spinning.  On the
 // decompressed field it also writes each vertex's label-mismatch bits
-// and changed-input bytes for the saddle pass.
-template <class T, bool kDec>
+// and changed-input bytes for the saddle pass.  kLater (decompressed field,
+// a job's rounds after its first): the label-mismatch bits of a group change
+// only with its labels, so the original roots are loaded only for groups
+// whose labels changed, after the chase.
+template <class T, bool kDec, bool kLater = false>
 __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ jobs,
                                                const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
@@ -673,12 +749,14 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
           const int4 B = *reinterpret_cast<const int4*>(b + v0);
           const int4 O1 = *reinterpret_cast<const int4*>(ra + v0);
           const int4 O2 = *reinterpret_cast<const int4*>(rb + v0);
-          const int4 R1 = *reinterpret_cast<const int4*>(ods + v0);
-          const int4 R2 = *reinterpret_cast<const int4*>(oas + v0);
+          int4 R1 = make_int4(0, 0, 0, 0), R2 = make_int4(0, 0, 0, 0);
+          if constexpr (!kLater) {
+            R1 = *reinterpret_cast<const int4*>(ods + v0);
+            R2 = *reinterpret_cast<const int4*>(oas + v0);
+          }
           const unsigned cw = vchg[v0 >> 5] >> (v0 & 31);
           int u1[4] = {A.x, A.y, A.z, A.w}, u2[4] = {B.x, B.y, B.z, B.w};
           const int o1[4] = {O1.x, O1.y, O1.z, O1.w}, o2[4] = {O2.x, O2.y, O2.z, O2.w};
-          const int r1[4] = {R1.x, R1.y, R1.z, R1.w}, r2[4] = {R2.x, R2.y, R2.z, R2.w};
           // One hop of every unfinished chain per iteration: the eight loads
           // depend only on their own chain, so they are all in flight at once.
           bool more = true;
@@ -699,7 +777,7 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
             }
           }
           if (it == cap_j && more) atomicOr(err, kErrJump);
-          unsigned dv = 0, mv = 0;
+          unsigned dv = 0;
           bool n1 = false, n2 = false;
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
@@ -708,17 +786,27 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
             n1 |= o1[k] != u1[k];
             n2 |= o2[k] != u2[k];
             const unsigned d = (o1[k] != u1[k]) | (o2[k] != u2[k]) | ((cw >> k | c1 | c2) & 1u);
-            const unsigned m = (u1[k] != r1[k]) | (u2[k] != r2[k]) << 1;
             dv |= d << (8 * k);
-            mv |= m << (8 * k);
           }
           *reinterpret_cast<unsigned*>(dirtyv + v0) = dv;
           // Stores that would rewrite the stored value are skipped.  The
           // mismatch bits follow the labels alone (the original roots are
-          // fixed), so with dv == 0 (no label and no change bit) last round's
-          // bits stand; the first round of a job, whose change bitset is
-          // full, writes every group.
-          if (dv) *reinterpret_cast<unsigned*>(mis + v0) = mv;
+          // fixed), so a group whose labels did not change keeps last round's
+          // bits.  A job's first round writes every group (its change bitset
+          // starts full, so dv is set everywhere; the stored labels may be
+          // another job's).
+          if (kLater ? (n1 || n2) : dv != 0) {
+            if constexpr (kLater) {
+              R1 = *reinterpret_cast<const int4*>(ods + v0);
+              R2 = *reinterpret_cast<const int4*>(oas + v0);
+            }
+            const int r1[4] = {R1.x, R1.y, R1.z, R1.w}, r2[4] = {R2.x, R2.y, R2.z, R2.w};
+            unsigned mv = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+              mv |= ((unsigned)(u1[k] != r1[k]) | (unsigned)(u2[k] != r2[k]) << 1) << (8 * k);
+            *reinterpret_cast<unsigned*>(mis + v0) = mv;
+          }
           if (n1) *reinterpret_cast<int4*>(ra + v0) = make_int4(u1[0], u1[1], u1[2], u1[3]);
           if (n2) *reinterpret_cast<int4*>(rb + v0) = make_int4(u2[0], u2[1], u2[2], u2[3]);
           if (dv || (v0 & (kCpBlockJ - 1)) == 0) {
@@ -933,8 +1021,11 @@ __global__ void k_extreme_saddle(Job<T> J, int pass) {
     const int s = sad[i];
     const K key = KeyOf<T>::enc(J.f[s] + T(0));  // -0 and +0 compare equal
     const int* row = rows + (long long)i * kRowStride;
+    // The first four entries as extremum indices from the compact copy
+    // (k_row_counts), longer rows' tails through the index map.
+    const int4 m4 = (kMax ? J.orm2 : J.orm1)[i];
     for (int p = 0; p < cnt; ++p) {
-      const int m = J.ext[row[p]];
+      const int m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : J.ext[row[p]];
       if (pass == 0) {
         if (kMax) atomicMax(J.ext_key + m, key);
         else atomicMin(J.ext_key + m, key);
@@ -1357,15 +1448,27 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
   }
 }
 
-// Compact copy of the original rows' counts (the only field of a row most
-// passes need).
+// Compact copies of the original rows, so that the per-round scans read a
+// few bytes per saddle instead of a 64-byte row: the count; the first four
+// entries as extremum indices (the wrong-saddle scans); the first and the last
+// entry, as labels and as extremum indices (the wrong-extremum scans).
 template <class T>
 __global__ void k_row_counts(Job<T> J) {
   const int n2 = J.ctr[C_NS2], n1 = J.ctr[C_NS1];
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2 + n1; i += stride) {
-    if (i < n2) J.ocnt2[i] = (uint8_t)J.orow2[(long long)i * kRowStride + 14];
-    else J.ocnt1[i - n2] = (uint8_t)J.orow1[(long long)(i - n2) * kRowStride + 14];
+    const bool two = i < n2;
+    const int k = two ? i : i - n2;
+    const int* row = (two ? J.orow2 : J.orow1) + (long long)k * kRowStride;
+    const int cnt = row[14];
+    (two ? J.ocnt2 : J.ocnt1)[k] = (uint8_t)cnt;
+    int m[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) m[p] = p < cnt ? J.ext[row[p]] : -1;
+    (two ? J.orm2 : J.orm1)[k] = make_int4(m[0], m[1], m[2], m[3]);
+    const int first = cnt > 0 ? row[0] : -1, last = cnt > 0 ? row[cnt - 1] : -1;
+    (two ? J.oend2 : J.oend1)[k] =
+        make_int4(first, last, cnt > 0 ? m[0] : -1, cnt > 0 ? J.ext[last] : -1);
   }
 }
 
@@ -1632,7 +1735,7 @@ __global__ void __launch_bounds__(256) k_wim_scan(const Job<T>* __restrict__ job
   for (int jk = 0; jk < sel.n; ++jk) {
   const Job<T>& J = jobs[sel.idx[jk]];
   const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
-  const int* orow = kMax ? J.orow2 : J.orow1;
+  const int4* oend = kMax ? J.oend2 : J.oend1;
   const int* drow = kMax ? J.drow2 : J.drow1;
   int* first = kMax ? J.first1 : J.first_min1;
   int* flag = kMax ? J.flag2 : J.flag_min2;
@@ -1640,11 +1743,12 @@ __global__ void __launch_bounds__(256) k_wim_scan(const Job<T>* __restrict__ job
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
     const int cnt = (kMax ? J.ocnt2 : J.ocnt1)[i];
     if (cnt == 0) continue;
-    const int* o = orow + (long long)i * kRowStride;
-    const int* d = drow + 2ll * i;  // slots: entry 0, entry (count - 1)
-    if (o[0] != d[0]) atomicMin(first + J.ext[o[0]], i);
-    const int k = cnt - 1;
-    if (o[k] != d[1]) flag[J.ext[o[k]]] = 1;
+    // Original entries 0 and count - 1 (labels, extremum indices) against the
+    // decompressed row slots: entry 0, entry (count - 1).
+    const int4 o = oend[i];
+    const int2 d = *reinterpret_cast<const int2*>(drow + 2ll * i);
+    if (o.x != d.x) atomicMin(first + o.z, i);
+    if (o.y != d.y) flag[o.w] = 1;
   }
   }
 }
@@ -1712,9 +1816,8 @@ __global__ void __launch_bounds__(256) k_wim_min2_scan(const Job<T>* __restrict_
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
     const int cnt = J.ocnt1[i];
     if (cnt == 0) continue;
-    const int* o = J.orow1 + (long long)i * kRowStride;
-    const int k = cnt - 1;
-    if (o[k] != J.drow1[2ll * i + 1]) atomicMin(J.first_sj + J.ext[o[k]], i);
+    const int4 o = J.oend1[i];
+    if (o.y != J.drow1[2ll * i + 1]) atomicMin(J.first_sj + o.w, i);
   }
   }
 }
@@ -1741,6 +1844,28 @@ __global__ void __launch_bounds__(256) k_wim_min2_collect(const Job<T>* __restri
 // largest (smallest) saddle in the decompressed field -- and
 // fix_wrong_index_saddle (:3415-3463).
 // ---------------------------------------------------------------------------
+// Per extremum, the current value of its true largest (smallest) saddle, into
+// the extremum-indexed scratch ext_key (free after the setup), so that the
+// scan below reads it from one compact table instead of through two dependent
+// gathers per row entry.  Rebuilt before every scan: the values change between
+// rounds.
+template <class T, bool kMax>
+__global__ void __launch_bounds__(256) k_wis_table(const Job<T>* __restrict__ jobs,
+                                                   const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+    const Job<T>& J = jobs[sel.idx[jk]];
+    const int next = J.ctr[kMax ? C_NMAX : C_NMIN];
+    const int* best = kMax ? J.largest : J.smallest;
+    T* val = reinterpret_cast<T*>(J.ext_key);
+    const int N = J.dim.N;
+    const int stride = gridDim.x * blockDim.x;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < next; m += stride) {
+      const int t = best[m];  // no saddle: -1 or kInf, never read by the scan
+      val[m] = (t >= 0 && t < N) ? J.g[t] : T(0);
+    }
+  }
+}
+
 template <class T, bool kMax>
 __global__ void __launch_bounds__(256) k_wis_scan(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
@@ -1748,8 +1873,10 @@ __global__ void __launch_bounds__(256) k_wis_scan(const Job<T>* __restrict__ job
   const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
   const int* sad = kMax ? J.sad2 : J.sad1;
   const int* rows = kMax ? J.orow2 : J.orow1;
+  const int4* orm = kMax ? J.orm2 : J.orm1;
   const uint8_t* ocnt = kMax ? J.ocnt2 : J.ocnt1;
   const int* best = kMax ? J.largest : J.smallest;
+  const T* val = reinterpret_cast<const T*>(J.ext_key);
   int* first = kMax ? J.first_s : J.first_sj;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
@@ -1757,27 +1884,24 @@ __global__ void __launch_bounds__(256) k_wis_scan(const Job<T>* __restrict__ job
     if (cnt == 0) continue;
     const int s = sad[i];
     const T gs = J.g[s];
-    // Rows hold 2-3 entries typically: the first four entries go through
-    // their three dependent gathers (extremum index, its true largest /
-    // smallest saddle, that saddle's value) stage by stage, so the four
-    // chains overlap; longer rows finish entry by entry.
-    const int* row = rows + (long long)i * kRowStride;
-    const int4 r4 = *reinterpret_cast<const int4*>(row);
-    const int r0[4] = {r4.x, r4.y, r4.z, r4.w};
-    int m[4], tb[4];
+    // Rows hold 2-3 entries typically: the first four entries come as
+    // extremum indices from the compact copy, their true largest / smallest
+    // saddle's value from the per-extremum table (k_wis_table), all loads
+    // independent; the saddle's id is needed only on a tie of values.
+    // Longer rows finish entry by entry.
+    const int4 m4 = orm[i];
+    const int m[4] = {m4.x, m4.y, m4.z, m4.w};
     T gt[4];
 #pragma unroll
-    for (int p = 0; p < 4; ++p) m[p] = p < cnt ? J.ext[r0[p]] : 0;
-#pragma unroll
-    for (int p = 0; p < 4; ++p) tb[p] = p < cnt ? best[m[p]] : 0;
-#pragma unroll
-    for (int p = 0; p < 4; ++p) gt[p] = p < cnt ? J.g[tb[p]] : T(0);
+    for (int p = 0; p < 4; ++p) gt[p] = p < cnt ? val[m[p]] : T(0);
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
       if (p >= cnt) break;
-      const bool wrong = kMax ? above(gs, s, gt[p], tb[p]) : below(gs, s, gt[p], tb[p]);
+      const bool wrong = kMax ? (gs > gt[p] || (gs == gt[p] && s > best[m[p]]))
+                              : (gs < gt[p] || (gs == gt[p] && s < best[m[p]]));
       if (wrong) atomicMin(first + m[p], i * kRowStride + p);
     }
+    const int* row = rows + (long long)i * kRowStride;
     for (int p = 4; p < cnt; ++p) {
       const int mp = J.ext[row[p]];
       const int tp = best[mp];
@@ -1883,7 +2007,7 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
       if (c[C_MFSKIP]) break;
       c[C_WNSTAMP] += 1;  // next flag stamp; flagged and candidate counts to zero
       c[C_NFC] = c[C_NFC1] = 0;
-      c[C_CAND] = c[C_CANDJ] = c[C_CAND_NEXT] = 0;
+      c[C_CAND] = c[C_CANDJ] = c[C_CAND_NEXT] = c[C_TLIST] = 0;
       break;
     case OP_ZERO_TOUCHED:
       c[C_TOUCHED] = 0;

@@ -90,14 +90,16 @@ typedef struct {
  * W * sizeof(value) is a multiple of 16 bytes). */
 #define EXTREMZ_FLAG_NO_TMA 2
 /* flags: resolve the wrong-neighbour flags (get_wrong_split_neighbors /
- * get_wrong_join_neighbors, src/ExtreM_cuda.cu:2400-2513) in lockstep order --
- * a neighbour two saddles share goes to the saddle that meets it at the
- * earlier neighbour index, as the reference's concurrent launch does when its
- * threads advance in step -- instead of the default canonical order
- * (saddles in ascending id, sequentially).  The reference's check-then-set is
- * a race, so its runs can differ; its runs on the 256^3 benchmark field give
- * the lockstep result, its runs on the 512^3 field the result of both. */
-#define EXTREMZ_FLAG_WN_LOCKSTEP 4
+ * get_wrong_join_neighbors, src/ExtreM_cuda.cu:2400-2513) sequentially in
+ * ascending saddle id instead of the default lockstep order.  The reference
+ * flags with a check-then-set from concurrent threads, so its runs can differ.
+ * By default a neighbour two saddles share goes to the saddle that meets it at
+ * the earlier neighbour index, which is what the reference's launch does when
+ * its threads advance through their neighbour loops in step: its output on
+ * the 256^3 and 512^3 benchmark fields and on every pinned test field whose
+ * runs agree.  The ascending order gives the same result wherever no two
+ * saddles contend for a neighbour. */
+#define EXTREMZ_FLAG_WN_ASCENDING 4
 
 /* Kernel classes of extremz_report.prof_*: 0 setup (classification, labels and
  * rows of the original field), 1 fused classification + mismatch detection,
@@ -397,7 +399,7 @@ long long extremz_job_footprint(int dtype, int width, int height, int depth);
  * in main() (src/ExtreM_cuda.cu:4997-5185).
  *
  * The whole workspace is a static device array sized for at most
- * EXTREMZ_NOALLOC_MAX_VOXELS voxels (about 21 MB, held by every GPU that loads
+ * EXTREMZ_NOALLOC_MAX_VOXELS voxels (about 26 MB, held by every GPU that loads
  * the library until the process exits); larger fields return
  * EXTREMZ_TOO_LARGE without touching the device.  The call makes no
  * cudaMalloc, cudaFree or other allocating call.  Inputs and outputs are the

@@ -11,7 +11,11 @@
 //     ascending vertex id, which fixes the triplet row order and the
 //     max->saddle CSR order (:4806-4888).
 //   * get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513) flag a
-//     neighbour with check-then-set; here saddles are visited in ascending id.
+//     neighbour with check-then-set from concurrent threads; here by default
+//     in lockstep order (every saddle examines its j-th neighbour at step j,
+//     so a shared neighbour goes to the saddle meeting it at the earlier
+//     step: the reference's own outcome on the fields its runs were pinned
+//     on), or with saddles visited sequentially in ascending id.
 //   * get_wrong_index_max / _min (:3113-3171) keep one (true, false) pair per
 //     extremum with check-then-set; here the lowest saddle row wins.
 // The stale read in get_wrong_index_max (:3128-3130: the decompressed row is
@@ -267,9 +271,10 @@ struct oracle_params {
   int max_cloop_rounds;  // cap on rounds of one c_loops call
   int final_join;        // run the final saddle_loops_join (:5997)
   int preserve_join;     // preserve_join_tree (:4969, false in the reference)
-  int wn_lag;            // wrong-neighbour flagging: < 0 canonical (ascending
-                         // saddle id, sequential); k >= 0 the lockstep model of
-                         // the reference's concurrent launch (see wrong_neighbors)
+  int wn_lag;            // wrong-neighbour flagging: k >= 0 the lockstep model of
+                         // the reference's concurrent launch (0: the default, see
+                         // wrong_neighbors_lockstep); < 0 ascending saddle id,
+                         // sequentially
 };
 struct oracle_report {
   int status;        // 0 ok, 1 round cap hit
@@ -310,7 +315,7 @@ struct Corrector {
   T* a;  // decompressed field, corrected in place
   T bound, thr;
   int q, edit_type;
-  int wn_lag = -1;
+  int wn_lag = 0;
   T sentinel;
 
   std::vector<int8_t> otype;
@@ -597,8 +602,8 @@ struct Corrector {
     }
   }
 
-  // get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513), with
-  // saddles visited in ascending id.
+  // get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513): the
+  // lockstep resolution above, or saddles visited sequentially in ascending id.
   void wrong_neighbors() {
     for (int v : wn_ds_list) wn_ds[v] = 0;
     for (int v : wn_as_list) wn_as[v] = 0;
@@ -1383,7 +1388,7 @@ int oracle_correct(const void* f, void* decp, int dtype, int W, int H, int D,
 // Mismatch census of `decp` against the original `f` (Corrector::census):
 // out receives the eleven loop-test counters.
 int oracle_census(const void* f, const void* decp, int dtype, int W, int H, int D, double thr,
-                  int32_t* out) {
+                  int wn_lag, int32_t* out) {
   if (!dims_ok(W, H, D) || !out) return -1;
   auto run = [&](auto* tag) {
     using T = std::remove_pointer_t<decltype(tag)>;
@@ -1397,6 +1402,7 @@ int oracle_census(const void* f, const void* decp, int dtype, int W, int H, int 
     c.thr = (T)thr;
     c.q = 1;
     c.edit_type = 1;
+    c.wn_lag = wn_lag;
     c.sentinel = T(0);
     c.trace = nullptr;
     c.trace_cap = 0;

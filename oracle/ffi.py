@@ -72,7 +72,7 @@ def lib():
                                               vp, ctypes.c_longlong, vp, vp,
                                               ctypes.POINTER(ctypes.c_longlong),
                                               ctypes.POINTER(ctypes.c_longlong)]
-        L.oracle_census.argtypes = [vp, vp, i32, i32, i32, i32, ctypes.c_double, vp]
+        L.oracle_census.argtypes = [vp, vp, i32, i32, i32, i32, ctypes.c_double, i32, vp]
         L.oracle_encode.argtypes = [vp, vp, vp, vp, i32, ctypes.c_longlong, ctypes.c_double,
                                     i32, i32, vp, ctypes.c_longlong, vp, ctypes.c_longlong,
                                     ctypes.POINTER(EditReport)]
@@ -130,17 +130,20 @@ def roots(f: np.ndarray):
 def correct(f: np.ndarray, decp: np.ndarray, bound: float, *, thr: float = 0.0, q: int = 4,
             edit_type: int = 1, max_outer: int = 500, max_cloop_rounds: int = 100000,
             final_join: bool = True, preserve_join: bool = False, trace_cap: int = 0,
-            counter_out: np.ndarray = None, wn_lag: int = -1):
+            counter_out: np.ndarray = None, wn_order: str = "lockstep", wn_lag: int = None):
     """Run the oracle correction; returns (corrected copy, report dict, trace).
 
     counter_out (optional, int32 of the field's size) receives the final edit
-    counters (the reference's delta_counter)."""
+    counters (the reference's delta_counter).  wn_order: the resolution of the
+    reference's wrong-neighbour race, "lockstep" (default) or "ascending";
+    wn_lag (>= 0) selects the lockstep model with that visibility lag."""
     f = np.ascontiguousarray(f)
     out = np.ascontiguousarray(decp).copy()
     assert f.dtype == out.dtype and f.shape == out.shape
     w, h, d = _dims(f)
     p = Params(bound, thr, q, edit_type, max_outer, max_cloop_rounds,
-               int(final_join), int(preserve_join), int(wn_lag))
+               int(final_join), int(preserve_join),
+               int(WN_ORDERS[wn_order] if wn_lag is None else wn_lag))
     r = Report()
     tr = np.zeros(max(trace_cap, 1) * 4, dtype=np.int32)
     rc = lib().oracle_correct(f.ctypes.data, out.ctypes.data, _dtype_code(f), w, h, d,
@@ -162,7 +165,10 @@ COUNTER_NAMES = ("wrong_split_nbrs", "wrong_join_nbrs", "false_max", "false_min"
                  "wrong_saddle_join")
 
 
-def census(f: np.ndarray, decp: np.ndarray, *, thr: float = 0.0):
+WN_ORDERS = {"lockstep": 0, "ascending": -1}
+
+
+def census(f: np.ndarray, decp: np.ndarray, *, thr: float = 0.0, wn_order: str = "lockstep"):
     """Mismatch census of decp against f: the eleven loop-test counters
     (order of ``Report.counters``) evaluated once, no edit."""
     f = np.ascontiguousarray(f)
@@ -171,7 +177,7 @@ def census(f: np.ndarray, decp: np.ndarray, *, thr: float = 0.0):
     w, h, d = _dims(f)
     out = np.zeros(11, dtype=np.int32)
     rc = lib().oracle_census(f.ctypes.data, g.ctypes.data, _dtype_code(f), w, h, d, float(thr),
-                             out.ctypes.data)
+                             WN_ORDERS[wn_order], out.ctypes.data)
     if rc != 0:
         raise ValueError(f"oracle_census returned {rc}")
     return [int(x) for x in out]

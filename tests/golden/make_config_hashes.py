@@ -16,9 +16,11 @@ Cases (both with and without the final join-saddle pass, q 4, edit_type 1):
   plain256_f32  the same field in float32
   plain512_f64  512^3 float64, 4096 Gaussians + k^-5/3 noise, seed 2, eb 1e-5 rel
   mixed64       the 64 fields of the mixed batch (seeds 100-163), one digest each
-Existing entries of the JSON file are kept unless recomputed.  --lockstep adds,
-for the named float64 fields, the digest of the correction with the
-wrong-neighbour race resolved in lockstep order (entry lockstep_final_join_1).
+The wrong-neighbour race of the reference is resolved in the default
+(lockstep) order.  Existing entries of the JSON file are kept unless
+recomputed.  --ascending adds, for the named fields, the digest of the
+correction with the race resolved in ascending saddle order (entry
+ascending_final_join_1).
 """
 
 from __future__ import annotations
@@ -55,15 +57,16 @@ def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def digest(fld, final_join: bool, trace: bool = True, wn_lag: int = -1):
+def digest(fld, final_join: bool, trace: bool = True, wn_order: str = "lockstep"):
     t0 = time.perf_counter()
     fixed, rep, tr = ffi.correct(fld.f, fld.decp, fld.eb, final_join=final_join,
-                                 trace_cap=TRACE_CAP if trace else 0, wn_lag=wn_lag, **PARAMS)
+                                 trace_cap=TRACE_CAP if trace else 0, wn_order=wn_order,
+                                 **PARAMS)
     secs = time.perf_counter() - t0
     out = {"fixed_sha256": sha(fixed), "status": rep["status"],
            "outer_iters": rep["outer_iters"], "cloop_rounds": rep["cloop_rounds"],
            "manifold_rounds": rep["manifold_rounds"], "edited": rep["edited"],
-           "counters": rep["counters"], "census": ffi.census(fld.f, fixed),
+           "counters": rep["counters"], "census": ffi.census(fld.f, fixed, wn_order=wn_order),
            "oracle_seconds": round(secs, 2)}
     if trace:
         out["trace_sha256"] = sha(tr.astype(np.int32))
@@ -75,18 +78,18 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*", default=None)
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
-    ap.add_argument("--lockstep", nargs="*", default=None)
+    ap.add_argument("--ascending", nargs="*", default=None)
     args = ap.parse_args()
     ffi.set_threads(args.threads)
     data = {}
     if os.path.exists(OUT):
         with open(OUT) as fh:
             data = json.load(fh)
-    if args.lockstep:
-        for name in args.lockstep:
+    if args.ascending:
+        for name in args.ascending:
             fld = PLAIN[name]()
-            data[name]["lockstep_final_join_1"] = digest(fld, True, wn_lag=0)
-            print(name, "lockstep", data[name]["lockstep_final_join_1"], flush=True)
+            data[name]["ascending_final_join_1"] = digest(fld, True, wn_order="ascending")
+            print(name, "ascending", data[name]["ascending_final_join_1"], flush=True)
             with open(OUT, "w") as fh:
                 json.dump(data, fh, indent=1, sort_keys=True)
                 fh.write("\n")
@@ -95,7 +98,7 @@ def main():
     for name in names:
         if args.only and name not in args.only:
             continue
-        entry = {"params": PARAMS}
+        entry = dict(data.get(name, {}), params=PARAMS)  # other entries stay
         if name in PLAIN:
             fld = PLAIN[name]()
             entry["eb"] = fld.eb

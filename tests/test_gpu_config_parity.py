@@ -104,14 +104,13 @@ with open(os.path.join(HERE, "golden", "ref_gpu_cases.json")) as _fh:
     REF_RUNS = json.load(_fh)
 
 
-@pytest.mark.parametrize("name,lockstep", [("plain256_f64", True), ("plain512_f64", False),
-                                           ("plain512_f64", True)])
-def test_benchmark_fields_equal_the_reference_gpu_output(name, lockstep):
+@pytest.mark.parametrize("name,order", [("plain256_f64", "lockstep"), ("plain512_f64", "lockstep"),
+                                        ("plain512_f64", "ascending")])
+def test_benchmark_fields_equal_the_reference_gpu_output(name, order):
     """The reference's own GPU correction of the 256^3 and 512^3 float64
     benchmark fields (its runs agree with one another): the library's output
-    is byte-identical to it, with the wrong-neighbour race resolved in
-    lockstep order at 256^3 (the resolution the reference's runs took) and in
-    either order at 512^3."""
+    is byte-identical to it with the default (lockstep) resolution of the
+    wrong-neighbour race, and at 512^3 with the ascending one as well."""
     import torch
     from extrem_z_b200 import api
     fld = field(name)
@@ -120,7 +119,7 @@ def test_benchmark_fields_equal_the_reference_gpu_output(name, lockstep):
     f = torch.from_numpy(fld.f).cuda()
     g = torch.from_numpy(fld.decp).cuda()
     rep, _ = api.context(0).correct_device(f, g, fld.eb, q=4, edit_type=1, max_outer=1000,
-                                           final_join=True, wn_lockstep=lockstep)
+                                           final_join=True, wn_order=order)
     assert rep.status == 0
     assert sha(g.cpu().numpy()) == runs[0]
     del f, g

@@ -172,17 +172,18 @@ def test_round_cap_returns_status(max_outer):
 
 @pytest.mark.parametrize("case", [("cube64_s0", 64, 64, 64, 64, 0, 1e-3),
                                   ("box48x40x24_s12", 48, 40, 24, 24, 12, 3e-3)])
-def test_lockstep_resolution_bit_exact(case):
-    """EXTREMZ_FLAG_WN_LOCKSTEP against the oracle's lockstep resolution of
+def test_ascending_resolution_bit_exact(case):
+    """EXTREMZ_FLAG_WN_ASCENDING against the oracle's ascending resolution of
     the wrong-neighbour race: same trace, same bytes (float64 fields on which
-    the two resolutions differ)."""
+    it differs from the default lockstep resolution)."""
     from oracle import ffi
     _, w, h, d, g, seed, rel = case
     fld = synth.make_field(w, h, d, n_gauss=g, seed=seed, rel=rel)
-    ref, rrep, rtrace = ffi.correct(fld.f, fld.decp, fld.eb, trace_cap=200000, wn_lag=0, **KW)
-    canon, _, _ = ffi.correct(fld.f, fld.decp, fld.eb, **KW)
-    assert not np.array_equal(ref.view(np.uint8), canon.view(np.uint8))
-    out, rep, trace = gpu_correct(fld.f, fld.decp, fld.eb, wn_lockstep=True, **KW)
+    ref, rrep, rtrace = ffi.correct(fld.f, fld.decp, fld.eb, trace_cap=200000,
+                                    wn_order="ascending", **KW)
+    lock, _, _ = ffi.correct(fld.f, fld.decp, fld.eb, **KW)
+    assert not np.array_equal(ref.view(np.uint8), lock.view(np.uint8))
+    out, rep, trace = gpu_correct(fld.f, fld.decp, fld.eb, wn_order="ascending", **KW)
     assert np.array_equal(trace, rtrace), first_divergence(trace, rtrace)
     assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
     assert rep.status == rrep["status"] == 0

@@ -6,18 +6,18 @@ B200 by tests/golden/make_ref_fixtures.py) on seeded float64 fields, including
 the 256^3 and 512^3 benchmark fields.  The reference is not deterministic:
 get_wrong_split_neighbors / get_wrong_join_neighbors (:2400-2513) flag with
 check-then-set from concurrent threads, so its runs can differ from one
-another.  The oracle resolves that site sequentially in ascending saddle id
-(the canonical order the CUDA path reproduces), and, as an option, in a
-lockstep model of the concurrent launch (every saddle thread examines its
-j-th neighbour at step j, so the saddle that meets a shared candidate at the
-earlier step flags it).
+another.  The oracle (and the CUDA path) resolve that race by default in
+lockstep order -- every saddle thread examines its j-th neighbour at step j,
+so the saddle that meets a shared candidate at the earlier step flags it --
+and optionally with saddles visited sequentially in ascending id.
 
 Pinned here, byte for byte:
-  * every case whose reference runs agree, the 512^3 benchmark field among
-    them, equals the canonical oracle;
-  * cases whose runs disagree: each run that either resolution reproduces is
-    reproduced exactly (both resolutions occur among the reference's runs of
-    the 64^3 seed-0 field).
+  * every case whose reference runs agree, the 256^3 and 512^3 benchmark
+    fields among them, equals the default (lockstep) oracle;
+  * cases whose runs disagree: the runs that either resolution reproduces
+    are reproduced exactly (the 64^3 seed-0 field has runs of both);
+  * the ascending resolution differs from the reference on the 256^3 field
+    and agrees with it on the 512^3 field.
 Run as a script to print the table that DESIGN.md's parity section shows.
 """
 
@@ -29,7 +29,11 @@ import os
 import numpy as np
 import pytest
 
-from oracle import ffi
+if __name__ == "__main__":  # run as a script from the repository root
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+from oracle import ffi  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
@@ -43,55 +47,48 @@ FIX = importlib.util.module_from_spec(_spec)
 _spec.loader.exec_module(FIX)
 
 SMALL = [n for n in FIX.CASES if isinstance(FIX.CASES[n], tuple) and n in REF]
-# Runs of the racy cases reproduced by the lockstep resolution.
-LOCKSTEP_RUNS = {"cube64_s0_e1": [1, 2], "box48x40x24_s12_e1": [0, 1]}
+# Runs of the racy cases that each resolution reproduces.
+RACY_RUNS = {"cube64_s0_e1": {"lockstep": [1, 2], "ascending": [0]},
+             "box48x40x24_s12_e1": {"lockstep": [0, 1], "ascending": []}}
 
 
 def sha(a) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def oracle_sha(name, lockstep=False):
+def oracle_sha(name, order="lockstep"):
     fld, et, _, _ = FIX.make(name)
     out, rep, _ = ffi.correct(fld.f, fld.decp, fld.eb, q=4, edit_type=et, max_outer=1000,
-                              final_join=True, wn_lag=0 if lockstep else -1)
+                              final_join=True, wn_order=order)
     assert rep["status"] == 0
     return sha(out)
 
 
 @pytest.mark.parametrize("name", [n for n in SMALL if REF[n]["runs_agree"]])
-def test_reference_runs_agree_and_equal_canonical_oracle(name):
+def test_reference_runs_agree_and_equal_the_oracle(name):
     assert oracle_sha(name) == REF[name]["run_sha256"][0]
 
 
-@pytest.mark.skipif("lockstep_final_join_1" not in DIGESTS.get("plain256_f64", {}),
-                    reason="no lockstep digest of the 256^3 field")
-def test_256_field_reference_equals_lockstep_oracle():
-    """256^3 float64 (512 Gaussians, seed 1, eb 1e-4 rel): the reference's runs
-    agree with one another and equal the oracle's lockstep resolution of the
-    wrong-neighbour race (its canonical resolution differs)."""
-    runs = REF["plain256_f64"]["run_sha256"]
-    assert REF["plain256_f64"]["runs_agree"]
-    assert DIGESTS["plain256_f64"]["lockstep_final_join_1"]["fixed_sha256"] == runs[0]
-    assert DIGESTS["plain256_f64"]["final_join_1"]["fixed_sha256"] != runs[0]
+@pytest.mark.parametrize("name", ["plain256_f64", "plain512_f64"])
+def test_benchmark_fields_reference_equals_oracle_digest(name):
+    """256^3 (512 Gaussians, seed 1, eb 1e-4 rel) and 512^3 (4096 Gaussians,
+    k^-5/3 noise, seed 2, eb 1e-5 rel) float64: the reference's runs agree and
+    equal the oracle's digest of the same field; the ascending resolution
+    differs at 256^3 and agrees at 512^3."""
+    runs = REF[name]["run_sha256"]
+    assert REF[name]["runs_agree"]
+    assert DIGESTS[name]["final_join_1"]["fixed_sha256"] == runs[0]
+    asc = DIGESTS[name]["ascending_final_join_1"]["fixed_sha256"]
+    assert (asc == runs[0]) == (name == "plain512_f64")
 
 
-def test_headline_field_reference_equals_oracle():
-    """512^3 float64 (4096 Gaussians, k^-5/3 noise, eb 1e-5 rel): the
-    reference's corrected field equals the oracle's digest of the same field."""
-    assert REF["plain512_f64"]["run_sha256"][0] == \
-        DIGESTS["plain512_f64"]["final_join_1"]["fixed_sha256"]
-
-
-@pytest.mark.parametrize("name", sorted(LOCKSTEP_RUNS))
+@pytest.mark.parametrize("name", sorted(RACY_RUNS))
 def test_racy_runs_are_reproduced_by_a_resolution_of_the_race(name):
     runs = REF[name]["run_sha256"]
     assert not REF[name]["runs_agree"]
-    lock = oracle_sha(name, lockstep=True)
-    assert [i for i, h in enumerate(runs) if h == lock] == LOCKSTEP_RUNS[name]
-    canon = oracle_sha(name)
-    assert [i for i, h in enumerate(runs) if h == canon] == \
-        [i for i in range(len(runs)) if i not in LOCKSTEP_RUNS[name] and runs[i] == canon]
+    for order, want in RACY_RUNS[name].items():
+        h = oracle_sha(name, order)
+        assert [i for i, r in enumerate(runs) if r == h] == want, order
 
 
 def test_stored_edits_rebuild_the_reference_runs():
@@ -105,21 +102,21 @@ def test_stored_edits_rebuild_the_reference_runs():
 
 
 def table() -> str:
-    rows = ["| case (float64, q 4, edit_type) | reference runs agree | runs equal to the canonical "
-            "oracle | runs equal to the lockstep resolution |", "|---|---|---|---|"]
+    rows = ["| case (float64, q 4) | reference runs agree | runs equal to the oracle (lockstep, "
+            "default) | runs equal to the ascending resolution |", "|---|---|---|---|"]
     for name, entry in REF.items():
         runs = entry["run_sha256"]
         if name in DIGESTS:
-            canon = DIGESTS[name]["final_join_1"]["fixed_sha256"]
-            lock = DIGESTS[name].get("lockstep_final_join_1", {}).get("fixed_sha256")
+            lock = DIGESTS[name]["final_join_1"]["fixed_sha256"]
+            asc = DIGESTS[name]["ascending_final_join_1"]["fixed_sha256"]
         else:
-            canon, lock = oracle_sha(name), oracle_sha(name, lockstep=True)
+            lock, asc = oracle_sha(name), oracle_sha(name, "ascending")
         def hits(h):
             return "—" if h is None else (", ".join(str(i) for i, r in enumerate(runs) if r == h)
                                           or "none")
         rows.append(f"| {name} (edit_type {entry['edit_type']}) | "
                     f"{'yes' if entry['runs_agree'] else 'no'} ({len(runs)} runs) | "
-                    f"{hits(canon)} | {hits(lock)} |")
+                    f"{hits(lock)} | {hits(asc)} |")
     return "\n".join(rows)
 
 
