@@ -1065,7 +1065,8 @@ class BatchEngine {
         launch(K_SETUP, k_jump2<T, false>, grid_, 256, jobs, s);
         for (int i : sel) {
           JobHost<T>& j = slots_[i];
-          launch(K_OTHER, k_cp_count, j.nb, kCpBlock, (const int8_t*)j.J.otype, j.J.dim.N, j.bcount);
+          launch(K_OTHER, k_cp_count, (j.nb + kCpWarps - 1) / kCpWarps, 32 * kCpWarps,
+                 (const int8_t*)j.J.otype, j.J.dim.N, j.nb, j.bcount);
           launch(K_OTHER, k_scan_lists, 1, 1024, j.bcount, j.nb, 4, j.J.ctr + C_NS2);
           j.waiting = true;
         }
@@ -1307,7 +1308,8 @@ class BatchEngine {
     J.ext_id = A.take<int>(ne);
     jh.checksum = A.take<unsigned long long>(8);
     if (!jh.checksum || !J.ext_id || !J.ocnt1 || !J.first_sj) return EXTREMZ_OOM;
-    launch(K_OTHER, k_cp_write, jh.nb, kCpBlock, (const int8_t*)J.otype, N, (const int*)jh.bcount,
+    launch(K_OTHER, k_cp_write, (jh.nb + kCpWarps - 1) / kCpWarps, 32 * kCpWarps,
+           (const int8_t*)J.otype, N, jh.nb, (const int*)jh.bcount,
            J.sad2, J.sad1, J.maxima, J.minima);
     launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
     launch(K_SETUP, k_rows<T, true>, grid_, 256, J, J.f, (const int*)J.ds, (const int*)J.sad2,

@@ -837,34 +837,72 @@ __device__ __forceinline__ int cp_bits(int t) {
          (t == 0 ? 8 : 0);
 }
 
-__global__ void __launch_bounds__(kCpBlock) k_cp_count(const int8_t* __restrict__ otype, int N,
-                                                       int* __restrict__ bcount) {
-  __shared__ int cnt[4];
-  if (threadIdx.x < 4) cnt[threadIdx.x] = 0;
-  __syncthreads();
-  const int v = blockIdx.x * kCpBlock + threadIdx.x;
-  const int b = v < N ? cp_bits(otype[v]) : 0;
-  for (int l = 0; l < 4; ++l) {
-    const unsigned m = __ballot_sync(0xffffffffu, (b >> l) & 1);
-    if (lane_id() == 0 && m) atomicAdd(&cnt[l], __popc(m));
+// One warp per 1024-id block, each lane 32 consecutive ids: the types come in
+// as two 16-byte loads per lane (one coalesced kilobyte per warp), where one
+// 1024-thread block per 1024 ids spent its time scheduling blocks.
+constexpr int kCpWarps = 8;  // warps (1024-id blocks) per CTA
+
+// The CP-list membership bits of the lane's 32 ids, one word per list.
+__device__ __forceinline__ void cp_lane_bits(const int8_t* __restrict__ otype, int N, int v0,
+                                             unsigned bits[4]) {
+  int8_t t[32];
+  if (v0 + 32 <= N) {
+    const int4 q0 = *reinterpret_cast<const int4*>(otype + v0);
+    const int4 q1 = *reinterpret_cast<const int4*>(otype + v0 + 16);
+    const int w[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+    for (int k = 0; k < 32; ++k) t[k] = (int8_t)(w[k >> 2] >> (8 * (k & 3)));
+  } else {
+#pragma unroll
+    for (int k = 0; k < 32; ++k) t[k] = v0 + k < N ? otype[v0 + k] : (int8_t)-1;
   }
-  __syncthreads();
-  if (threadIdx.x < 4) bcount[threadIdx.x * gridDim.x + blockIdx.x] = cnt[threadIdx.x];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) bits[l] = 0u;
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const int b = cp_bits(t[k]);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) bits[l] |= (unsigned)((b >> l) & 1) << k;
+  }
+}
+
+__global__ void __launch_bounds__(32 * kCpWarps) k_cp_count(const int8_t* __restrict__ otype,
+                                                           int N, int nb,
+                                                           int* __restrict__ bcount) {
+  const int b = blockIdx.x * kCpWarps + (int)(threadIdx.x >> 5);
+  if (b >= nb) return;  // whole warps leave together
+  unsigned bits[4];
+  cp_lane_bits(otype, N, b * kCpBlock + (int)lane_id() * 32, bits);
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    int c = __popc(bits[l]);
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane_id() == 0) bcount[l * nb + b] = c;
+  }
 }
 
 // Single block: exclusive scan of nlists x nb block counts in place, list
-// totals to totals[0 .. nlists).  The CP lists use totals = ctr + C_NS2.
+// totals to totals[0 .. nlists).  The CP lists use totals = ctr + C_NS2.  Each
+// thread takes eight consecutive counts per pass.
 __global__ void __launch_bounds__(1024) k_scan_lists(int* __restrict__ bcount, int nb, int nlists,
                                                      int* totals) {
+  constexpr int kPer = 8;
   __shared__ int carry;
   __shared__ int warp_sums[32];
   for (int l = 0; l < nlists; ++l) {
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int base = 0; base < nb; base += 1024) {
-      const int i = base + threadIdx.x;
-      const int x = i < nb ? bcount[l * nb + i] : 0;
-      int incl = x;
+    int* c = bcount + (long long)l * nb;
+    for (int base = 0; base < nb; base += 1024 * kPer) {
+      const int i0 = base + (int)threadIdx.x * kPer;
+      int x[kPer];
+      int sum = 0;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        x[k] = i0 + k < nb ? c[i0 + k] : 0;
+        sum += x[k];
+      }
+      int incl = sum;
       for (int o = 1; o < 32; o <<= 1) {
         const int y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane_id() >= (unsigned)o) incl += y;
@@ -880,10 +918,14 @@ __global__ void __launch_bounds__(1024) k_scan_lists(int* __restrict__ bcount, i
         warp_sums[threadIdx.x] = wi - w;
       }
       __syncthreads();
-      const int excl = carry + warp_sums[threadIdx.x / 32] + incl - x;
-      if (i < nb) bcount[l * nb + i] = excl;
+      int run = carry + warp_sums[threadIdx.x / 32] + incl - sum;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        if (i0 + k < nb) c[i0 + k] = run;
+        run += x[k];
+      }
       __syncthreads();
-      if (threadIdx.x == 1023) carry = excl + x;
+      if (threadIdx.x == 1023) carry = run;
       __syncthreads();
     }
     if (threadIdx.x == 0) totals[l] = carry;
@@ -891,37 +933,27 @@ __global__ void __launch_bounds__(1024) k_scan_lists(int* __restrict__ bcount, i
   }
 }
 
-__global__ void __launch_bounds__(kCpBlock) k_cp_write(const int8_t* __restrict__ otype, int N,
-                                                       const int* __restrict__ boff, int* sad2,
-                                                       int* sad1, int* maxima, int* minima) {
-  __shared__ int wcnt[4][32];
-  const int v = blockIdx.x * kCpBlock + threadIdx.x;
-  const int b = v < N ? cp_bits(otype[v]) : 0;
-  const unsigned lt = (1u << lane_id()) - 1u;
-  unsigned m[4];
-  for (int l = 0; l < 4; ++l) {
-    m[l] = __ballot_sync(0xffffffffu, (b >> l) & 1);
-    if (lane_id() == 0) wcnt[l][threadIdx.x / 32] = __popc(m[l]);
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    for (int l = 0; l < 4; ++l) {
-      const int w = wcnt[l][threadIdx.x];
-      int wi = w;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, wi, o);
-        if (lane_id() >= (unsigned)o) wi += y;
-      }
-      wcnt[l][threadIdx.x] = wi - w;
-    }
-  }
-  __syncthreads();
+__global__ void __launch_bounds__(32 * kCpWarps) k_cp_write(const int8_t* __restrict__ otype,
+                                                           int N, int nb,
+                                                           const int* __restrict__ boff,
+                                                           int* sad2, int* sad1, int* maxima,
+                                                           int* minima) {
+  const int b = blockIdx.x * kCpWarps + (int)(threadIdx.x >> 5);
+  if (b >= nb) return;
+  const int v0 = b * kCpBlock + (int)lane_id() * 32;
+  unsigned bits[4];
+  cp_lane_bits(otype, N, v0, bits);
   int* outs[4] = {sad2, sad1, maxima, minima};
+#pragma unroll
   for (int l = 0; l < 4; ++l) {
-    if ((b >> l) & 1) {
-      const int pos = boff[l * gridDim.x + blockIdx.x] + wcnt[l][threadIdx.x / 32] + __popc(m[l] & lt);
-      outs[l][pos] = v;
+    const int c = __popc(bits[l]);
+    int incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane_id() >= (unsigned)o) incl += y;
     }
+    int pos = boff[l * nb + b] + incl - c;
+    for (unsigned m = bits[l]; m; m &= m - 1) outs[l][pos++] = v0 + __ffs(m) - 1;
   }
 }
 
