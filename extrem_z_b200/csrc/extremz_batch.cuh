@@ -1142,18 +1142,34 @@ class BatchEngine {
             launch(K_JUMP, k_jump2<T, true, true>, grid_, 256, jobs, make_sel(later, false));
           launch(K_OTHER, k_clear_changed<T>, grid_, 256, jobs, bs);
           launch(K_ROWS, k_saddle_pass<T>, grid_, 256, jobs, bs);
-          bool vote = false, lockstep = false;
-          for (int i : busy) (slots_[i].J.wn_lockstep ? lockstep : vote) = true;
+          bool vote = false;
+          // Lockstep jobs: the fourteen steps in one block per job when the
+          // job's previous round had short candidate lists (the counts of
+          // that round are still in the host copy of its counters), else one
+          // grid launch per step.  Either is exact for any list length.
+          std::vector<int> lock_small, lock_large;
+          for (int i : busy) {
+            if (!slots_[i].J.wn_lockstep) {
+              vote = true;
+              continue;
+            }
+            const bool small = slots_[i].manifold_rounds > 0 &&
+                               h(i, C_CAND) + h(i, C_CANDJ) <= kWnBlockMax;
+            (small ? lock_small : lock_large).push_back(i);
+          }
           if (vote) {
             wn_rounds<true>(bs);  // its completion brings in the join side's list
             wn_rounds<false>(bs);
           }
-          if (lockstep) {
+          if (!lock_small.empty()) {
+            const Sel ss = make_sel(lock_small, false);
+            launch(K_WRONG_NBR, k_wn_steps_block<T>, ss.n, 1024, jobs, ss);
+          }
+          if (!lock_large.empty()) {
+            const Sel sl = make_sel(lock_large, false);
             const int grid = std::min(grid_, 2 * sms_);
             for (int d = 0; d < kNumDirs; ++d)
-              launch(K_WRONG_NBR, k_wn_step<T, true>, grid, 256, jobs, bs, d);
-            for (int d = 0; d < kNumDirs; ++d)
-              launch(K_WRONG_NBR, k_wn_step<T, false>, grid, 256, jobs, bs, d);
+              launch(K_WRONG_NBR, k_wn_step<T>, grid, 256, jobs, sl, d);
           }
         }
         for (int i : sel) {

@@ -1664,47 +1664,68 @@ __global__ void __launch_bounds__(1024) k_wn_resolve(Job<T>* __restrict__ jobs, 
 }
 
 // Lockstep resolution of the wrong-neighbour flags (jobs with wn_lockstep).
-// Launch d flags, for every saddle of the side's candidate list that no
-// earlier launch resolved, its direction-d neighbour when that neighbour is a
-// candidate (on the side, label differs from the original's) and no earlier
-// launch flagged it.  Two saddles never share their direction-d neighbour, so
-// a launch has no conflict, and the launches in direction order make each see
-// every earlier one.  This is how the reference's concurrent launch resolves
-// its check-then-set when its threads advance through their neighbour loops
-// in step (get_wrong_split_neighbors / _join_, src/ExtreM_cuda.cu:2400-2513):
-// a shared candidate goes to the saddle that meets it at the earlier
-// neighbour index.  A saddle's resolution is marked in claim[] (unused by this
-// mode), per side and per round stamp.
-template <class T, bool kSplit>
+// Step d flags, for every saddle of a side's candidate list that no earlier
+// step resolved, its direction-d neighbour when that neighbour is a candidate
+// (on the side, label differs from the original's) and no earlier step flagged
+// it.  Two saddles never share their direction-d neighbour, so a step has no
+// conflict, and the steps in direction order make each see every earlier one.
+// This is how the reference's concurrent launch resolves its check-then-set
+// when its threads advance through their neighbour loops in step
+// (get_wrong_split_neighbors / _join_, src/ExtreM_cuda.cu:2400-2513): a shared
+// candidate goes to the saddle that meets it at the earlier neighbour index.
+// The two sides flag into separate arrays, as the reference's two kernels do,
+// so one step serves both.  A saddle's resolution is marked in claim[]
+// (unused by this mode), per side and per round stamp.
+template <class T>
+__device__ __forceinline__ void wn_step_entry(const Job<T>& J, int e, int n2, int d, int stamp) {
+  const bool split = e < n2;
+  const int s = split ? J.cand[e] : J.cand_j[e - n2];
+  const Dims g = J.dim;
+  int x, y, z;
+  coords(s, g, x, y, z);
+  if (!dir_valid(d, boundary_code(x, y, z, g.W, g.H, g.D))) return;
+  const unsigned long long done = (1ull << 63) | (split ? 0ull : (1ull << 62)) | (unsigned)stamp;
+  if (J.claim[s] == done) return;
+  const int r = s + ddx(d) + ddy(d) * g.W + ddz(d) * g.W * g.H;
+  const T sv = J.g[s], rv = J.g[r];
+  if (!(split ? above(rv, r, sv, s) : below(rv, r, sv, s))) return;
+  int* taken = split ? J.taken : J.taken1;
+  if ((split ? J.dds[r] == J.ds[r] : J.das[r] == J.as[r]) || taken[r] == stamp) return;
+  taken[r] = stamp;
+  (split ? J.flagged : J.flagged1)[atomicAdd(J.ctr + (split ? C_NFC : C_NFC1), 1)] = r;
+  J.claim[s] = done;
+}
+
+// One step over every selected job's two candidate lists (a large list: one
+// launch per direction).
+template <class T>
 __global__ void __launch_bounds__(256) k_wn_step(const Job<T>* __restrict__ jobs,
                                                  const __grid_constant__ Sel sel, int d) {
   for (int jk = 0; jk < sel.n; ++jk) {
     const Job<T>& J = jobs[sel.idx[jk]];
     if (J.ctr[C_MFSKIP] || !J.wn_lockstep) continue;
     const int stamp = J.ctr[C_WNSTAMP];
-    const unsigned long long done =
-        (1ull << 63) | (kSplit ? 0ull : (1ull << 62)) | (unsigned)stamp;
-    const int n = J.ctr[kSplit ? C_CAND : C_CANDJ];
-    const int* list = kSplit ? J.cand : J.cand_j;
-    int* taken = kSplit ? J.taken : J.taken1;
-    int* flagged = kSplit ? J.flagged : J.flagged1;
-    int* nflag = J.ctr + (kSplit ? C_NFC : C_NFC1);
-    const Dims g = J.dim;
+    const int n2 = J.ctr[C_CAND], n = n2 + J.ctr[C_CANDJ];
     const int stride = gridDim.x * blockDim.x;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
-      const int s = list[e];
-      int x, y, z;
-      coords(s, g, x, y, z);
-      if (!dir_valid(d, boundary_code(x, y, z, g.W, g.H, g.D))) continue;
-      if (J.claim[s] == done) continue;
-      const int r = s + ddx(d) + ddy(d) * g.W + ddz(d) * g.W * g.H;
-      const T sv = J.g[s], rv = J.g[r];
-      if (!(kSplit ? above(rv, r, sv, s) : below(rv, r, sv, s))) continue;
-      if ((kSplit ? J.dds[r] == J.ds[r] : J.das[r] == J.as[r]) || taken[r] == stamp) continue;
-      taken[r] = stamp;
-      flagged[atomicAdd(nflag, 1)] = r;
-      J.claim[s] = done;
-    }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride)
+      wn_step_entry(J, e, n2, d, stamp);
+  }
+}
+
+// All fourteen steps in one block per job, with a barrier between steps (a
+// short list: fourteen grid launches would cost more than the work).  The
+// barrier makes one step's flags and marks visible to the next.
+template <class T>
+__global__ void __launch_bounds__(1024) k_wn_steps_block(const Job<T>* __restrict__ jobs,
+                                                         const __grid_constant__ Sel sel) {
+  if (blockIdx.x >= sel.n) return;
+  const Job<T>& J = jobs[sel.idx[blockIdx.x]];
+  if (J.ctr[C_MFSKIP] || !J.wn_lockstep) return;
+  const int stamp = J.ctr[C_WNSTAMP];
+  const int n2 = J.ctr[C_CAND], n = n2 + J.ctr[C_CANDJ];
+  for (int d = 0; d < kNumDirs; ++d) {
+    for (int e = threadIdx.x; e < n; e += blockDim.x) wn_step_entry(J, e, n2, d, stamp);
+    __syncthreads();
   }
 }
 
