@@ -116,14 +116,15 @@ constexpr long long job_bytes_voxels(long long n, long long ksz) {
          + arr_bytes(n, 4) + arr_bytes(n, 1)                        // cand_j, mis
          + 2 * arr_bytes(n, 4)                                      // pdd, pda
          + arr_bytes((n + 31) / 32, 4) + arr_bytes(n, 1)            // change bitset, dirtyv
-         + arr_bytes(2 * ((n + kCpBlock - 1) / kCpBlock), 1)        // dirtyv per 1024-id block, x2
-         + arr_bytes(n, 1)                                          // tile marks (<= n tiles)
-         + arr_bytes(4 * ((n + kCpBlock - 1) / kCpBlock), 4)        // CP block counts
+         + 4 * arr_bytes((n + 31) / 32, 4)  // wrong-saddle change bitsets, touched roots
+         + 2 * arr_bytes((n + kCpBlock - 1) / kCpBlock, 4)  // dirtyv stamp, seed count per block
+         + arr_bytes(6 * ((n + kCpBlock - 1) / kCpBlock), 4)        // CP block counts
+         + arr_bytes(6 * ((n + kCpBlock - 1) / kCpBlock / 1024 + 1), 4)  // and their chunk sums
          + 4096;
 }
 
 constexpr long long job_bytes_cps(long long ns2, long long ns1, long long nmax, long long nmin,
-                                  long long ksz) {
+                                  long long e2, long long e1, long long ksz) {
   return arr_bytes(ns2, 4) + arr_bytes(ns1, 4) + arr_bytes(nmax, 4) + arr_bytes(nmin, 4)
          + arr_bytes(ns2 * kRowStride, 4) + arr_bytes(ns2 * 2, 4) + arr_bytes(ns2, 1)
          + arr_bytes(ns1 * kRowStride, 4) + arr_bytes(ns1 * 2, 4) + arr_bytes(ns1, 1)
@@ -131,12 +132,23 @@ constexpr long long job_bytes_cps(long long ns2, long long ns1, long long nmax, 
          + arr_bytes(ns2, 1) + arr_bytes(ns1, 1)                    // seed bits
          + 4 * arr_bytes(nmax, 4) + 4 * arr_bytes(nmin, 4)
          + arr_bytes(nmax > nmin ? nmax : nmin, ksz) + arr_bytes(nmax > nmin ? nmax : nmin, 4)
-         + arr_bytes(8, 8) + 4096;
+         + arr_bytes(8, 8)
+         // per-extremum row-entry lists: offsets, entries, stamps; queue, chunk sums
+         + arr_bytes(nmax + 1, 4) + arr_bytes(e2, 4) + arr_bytes(nmax, 4)
+         + arr_bytes(nmin + 1, 4) + arr_bytes(e1, 4) + arr_bytes(nmin, 4)
+         + 2 * arr_bytes(nmax > nmin ? nmax : nmin, 4)
+         + arr_bytes((nmax > nmin ? nmax : nmin) / 1024 + 2, 4) + 4096;
 }
 
-// Worst case (every voxel a critical point of every kind).
+// Per tile: change mark.
+constexpr long long job_bytes_tiles(long long nt) { return arr_bytes(nt, 1); }
+
+// Worst case (every voxel a critical point of every kind; a voxel's upper and
+// lower neighbours, at most 14, give the row entries of both sides; at most
+// one tile per voxel).
 constexpr long long job_bytes_sz(long long n, long long ksz) {
-  return job_bytes_voxels(n, ksz) + job_bytes_cps(n, n, n, n, ksz);
+  return job_bytes_voxels(n, ksz) + job_bytes_tiles(n) +
+         job_bytes_cps(n, n, n, n, 7 * n, 7 * n, ksz);
 }
 template <class T>
 constexpr long long job_bytes(long long n) {
@@ -164,6 +176,7 @@ struct JobHost {
   bool own_arena = false, own_arena2 = false;
   int ntiles = 0, nb = 0;
   int* bcount = nullptr;
+  int* chunk = nullptr;  // chunk sums of the CP block counts
   unsigned long long* checksum = nullptr;
   int32_t* trace = nullptr;
   int trace_cap = 0, trace_len = 0;
@@ -305,7 +318,9 @@ class BatchEngine {
     // copy of the incoming field when an edit stream will be encoded).
     const bool keep_input = (p.flags & kFlagKeepInput) != 0;
     const bool track_edits = (p.flags & kFlagTrackEdits) != 0;
-    const long long need = (storage ? job_bytes<T>(N) : job_bytes_voxels(N, sizeof(K))) +
+    const long long ntiles = (long long)((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);
+    const long long need = (storage ? job_bytes<T>(N)
+                                    : job_bytes_voxels(N, sizeof(K)) + job_bytes_tiles(ntiles)) +
                            (keep_input ? arr_bytes(N, sizeof(T)) : 0) +
                            (track_edits ? arr_bytes((N + 31) / 32, 4) : 0);
     if (storage) {
@@ -358,13 +373,20 @@ class BatchEngine {
     J.pdd = A.take<int>(N);
     J.pda = A.take<int>(N);
     J.vchg = A.take<unsigned>((N + 31) / 32);
+    J.rtouch2 = A.take<unsigned>((N + 31) / 32);
+    J.rtouch1 = A.take<unsigned>((N + 31) / 32);
+    J.wchg2 = A.take<unsigned>((N + 31) / 32);
+    J.wchg1 = A.take<unsigned>((N + 31) / 32);
     J.dirtyv = A.take<uint8_t>(N);
     jh.nb = (N + kCpBlock - 1) / kCpBlock;
-    J.bdirty = A.take<uint8_t>(2ll * jh.nb);
-    jh.bcount = A.take<int>(4ll * jh.nb);
+    J.bdirty = A.take<int>(jh.nb);
+    J.hcnt = A.take<int>(jh.nb);
+    jh.bcount = A.take<int>(6ll * jh.nb);
+    jh.chunk = A.take<int>(6ll * ((jh.nb + 1023) / 1024));
     J.cpoff = jh.bcount;
     jh.ntiles = ((W + TX - 1) / TX) * ((H + TY - 1) / TY) * ((D + TZ - 1) / TZ);
     J.tdirty = A.take<uint8_t>(jh.ntiles);
+
     J.g0 = keep_input ? A.take<T>(N) : nullptr;
     J.edited = track_edits ? A.take<unsigned>((N + 31) / 32) : nullptr;
     if (!J.tdirty || (keep_input && !J.g0) || (track_edits && !J.edited)) {
@@ -1013,9 +1035,9 @@ class BatchEngine {
 
   // The per-critical-point part of a job's workspace: exact size from the
   // counts, or the rest of borrowed storage.
-  int take_cp_storage(JobHost<T>& jh, int ns2, int ns1, int nmax, int nmin) {
+  int take_cp_storage(JobHost<T>& jh, int ns2, int ns1, int nmax, int nmin, int e2, int e1) {
     if (!jh.own_arena) return EXTREMZ_OK;  // borrowed: carve from the same arena
-    const long long need = job_bytes_cps(ns2, ns1, nmax, nmin, sizeof(K));
+    const long long need = job_bytes_cps(ns2, ns1, nmax, nmin, e2, e1, sizeof(K));
     void* base = nullptr;
     const cudaError_t e = pool_mem_ ? cudaMallocFromPoolAsync(&base, (size_t)need, pool_mem_, st_)
                                     : cudaMallocAsync(&base, (size_t)need, st_);
@@ -1066,8 +1088,8 @@ class BatchEngine {
         for (int i : sel) {
           JobHost<T>& j = slots_[i];
           launch(K_OTHER, k_cp_count, (j.nb + kCpWarps - 1) / kCpWarps, 32 * kCpWarps,
-                 (const int8_t*)j.J.otype, j.J.dim.N, j.nb, j.bcount);
-          launch(K_OTHER, k_scan_lists, 1, 1024, j.bcount, j.nb, 4, j.J.ctr + C_NS2);
+                 (const int8_t*)j.J.otype, (const uint16_t*)j.J.olm, j.J.dim, j.nb, j.bcount);
+          EZ_RUN(scan_counts(j.bcount, j.nb, 6, j.J.ctr + C_NS2, j.chunk));
           j.waiting = true;
         }
         return EXTREMZ_OK;
@@ -1187,8 +1209,9 @@ class BatchEngine {
         return EXTREMZ_OK;
       case PC_SADDLE:
         ctl(s, OP_SADDLE_BEGIN);
-        launch(K_OTHER, k_wis_table<T, true>, grid_, 256, jobs, s);
-        launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_mark<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_update<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_long<T, true>, 2 * sms_, 256, jobs, s);
         launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs, s, 1);
         launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
         for (int i : sel) {
@@ -1208,8 +1231,9 @@ class BatchEngine {
       case PC_SADDLE_J:
       case PC_FINAL_JOIN:
         ctl(s, OP_SADDLE_JOIN_BEGIN);
-        launch(K_OTHER, k_wis_table<T, false>, grid_, 256, jobs, s);
-        launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_mark<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_update<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_long<T, false>, 2 * sms_, 256, jobs, s);
         launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs, s, 1);
         launch(K_APPLY, k_apply<T>, grid_, 256, jobs, s);
         for (int i : sel) {
@@ -1225,8 +1249,9 @@ class BatchEngine {
         ctl(s, OP_DETECT3_BEGIN);
         launch(K_OTHER, k_wim_scan<T, true>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wim_collect<T, true>, grid_, 256, jobs, s, 0);
-        launch(K_OTHER, k_wis_table<T, true>, grid_, 256, jobs, s);
-        launch(K_OTHER, k_wis_scan<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_mark<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_update<T, true>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_long<T, true>, 2 * sms_, 256, jobs, s);
         launch(K_OTHER, k_wis_collect<T, true>, grid_, 256, jobs, s, 0);
         for (int i : sel) {
           slots_[i].pending.push_back(PH_DETECT3);
@@ -1237,8 +1262,9 @@ class BatchEngine {
         ctl(s, OP_DETECT3_JOIN_BEGIN);
         launch(K_OTHER, k_wim_scan<T, false>, grid_, 256, jobs, s);
         launch(K_OTHER, k_wim_collect<T, false>, grid_, 256, jobs, s, 0);
-        launch(K_OTHER, k_wis_table<T, false>, grid_, 256, jobs, s);
-        launch(K_OTHER, k_wis_scan<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_mark<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_update<T, false>, grid_, 256, jobs, s);
+        launch(K_OTHER, k_wis_long<T, false>, 2 * sms_, 256, jobs, s);
         launch(K_OTHER, k_wis_collect<T, false>, grid_, 256, jobs, s, 0);
         for (int i : sel) slots_[i].pc = PC_FINAL_DETECT;
         return EXTREMZ_OK;
@@ -1287,13 +1313,31 @@ class BatchEngine {
     launch(K_WRONG_NBR, k_wn_resolve<T, kSplit>, s.n, 1024, jobs_dev_, s);
   }
 
+  // Exclusive scan of nl lists of n counts each (list l at c + l * n), the
+  // list totals into totals[0 .. nl); chunk holds nl * ceil(n / 1024) sums.
+  int scan_counts(int* c, int n, int nl, int* totals, int* chunk) {
+    const int nc = (n + 1023) / 1024;
+    launch(K_OTHER, k_chunk_sums, dim3(nc, nl), 1024, (const int*)c, n, chunk);
+    launch(K_OTHER, k_scan_lists, 1, 1024, chunk, nc, nl, totals);
+    launch(K_OTHER, k_chunk_scan, dim3(nc, nl), 1024, c, n, (const int*)chunk);
+    return EXTREMZ_OK;
+  }
+
+  // Per-extremum entry counts cnt[0 .. n) into offsets (the total into cnt[n])
+  // and a copy of the offsets into cur, the fill cursors.
+  int entry_lists(int* cnt, int* cur, int n, int* chunk) {
+    EZ_RUN(scan_counts(cnt, n, 1, cnt + n, chunk));
+    EZ_CHECK(cudaMemcpyAsync(cur, cnt, (size_t)n * 4, cudaMemcpyDeviceToDevice, st_));
+    return EXTREMZ_OK;
+  }
+
   int setup_b(int slot) {
     JobHost<T>& jh = slots_[slot];
     Job<T>& J = jh.J;
     const int N = J.dim.N;
     const int ns2 = h(slot, C_NS2), ns1 = h(slot, C_NS1), nmax = h(slot, C_NMAX),
-              nmin = h(slot, C_NMIN);
-    EZ_RUN(take_cp_storage(jh, ns2, ns1, nmax, nmin));
+              nmin = h(slot, C_NMIN), e2 = h(slot, C_E2), e1 = h(slot, C_E1);
+    EZ_RUN(take_cp_storage(jh, ns2, ns1, nmax, nmin, e2, e1));
     Arena& A = jh.own_arena2 ? jh.arena2 : jh.arena;
     J.sad2 = A.take<int>(ns2);
     J.sad1 = A.take<int>(ns1);
@@ -1323,16 +1367,24 @@ class BatchEngine {
     J.ext_key = A.take<K>(ne);
     J.ext_id = A.take<int>(ne);
     jh.checksum = A.take<unsigned long long>(8);
-    if (!jh.checksum || !J.ext_id || !J.ocnt1 || !J.first_sj) return EXTREMZ_OOM;
+    J.moff2 = A.take<int>(nmax + 1);
+    J.ment2 = A.take<int>(e2);
+    J.wstamp2 = A.take<int>(nmax);
+    J.moff1 = A.take<int>(nmin + 1);
+    J.ment1 = A.take<int>(e1);
+    J.wstamp1 = A.take<int>(nmin);
+    J.aff = A.take<int>(ne);
+    J.wlong = A.take<int>(ne);
+    int* chunk = A.take<int>(ne / 1024 + 2);
+    if (!jh.checksum || !J.ext_id || !J.ocnt1 || !J.first_sj || !chunk) return EXTREMZ_OOM;
     launch(K_OTHER, k_cp_write, (jh.nb + kCpWarps - 1) / kCpWarps, 32 * kCpWarps,
            (const int8_t*)J.otype, N, jh.nb, (const int*)jh.bcount,
            J.sad2, J.sad1, J.maxima, J.minima);
     launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
     launch(K_SETUP, k_rows<T, true>, grid_, 256, J, J.f, (const int*)J.ds, (const int*)J.sad2,
-           (int)C_NS2, J.orow2);
+           (int)C_NS2, J.orow2, J.ocnt2, J.orm2, J.oend2);
     launch(K_SETUP, k_rows<T, false>, grid_, 256, J, J.f, (const int*)J.as, (const int*)J.sad1,
-           (int)C_NS1, J.orow1);
-    launch(K_SETUP, k_row_counts<T>, grid_, 256, J);
+           (int)C_NS1, J.orow1, J.ocnt1, J.orm1, J.oend1);
     // Decompressed row slots start at zero: the reference's rows are fresh
     // cudaMalloc memory read before first written (:5338-5341, :3128-3130).
     if (ns2) EZ_CHECK(cudaMemsetAsync(J.drow2, 0, (size_t)ns2 * 2 * 4, st_));
@@ -1340,8 +1392,11 @@ class BatchEngine {
     if (nmax) {
       launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, K(0), (long long)nmax);
       launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, -1, (long long)nmax);
+      EZ_CHECK(cudaMemsetAsync(J.moff2, 0, (size_t)(nmax + 1) * 4, st_));
       launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 0);
+      EZ_RUN(entry_lists(J.moff2, J.wstamp2, nmax, chunk));
       launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 1);
+      EZ_CHECK(cudaMemsetAsync(J.wstamp2, 0, (size_t)nmax * 4, st_));
       EZ_CHECK(cudaMemcpyAsync(J.largest, J.ext_id, nmax * 4, cudaMemcpyDeviceToDevice, st_));
       launch(K_OTHER, k_fill<int>, grid_, 256, J.first1, kInf, (long long)nmax);
       launch(K_OTHER, k_fill<int>, grid_, 256, J.first_s, kInf, (long long)nmax);
@@ -1350,15 +1405,23 @@ class BatchEngine {
     if (nmin) {
       launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, ~K(0), (long long)nmin);
       launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, kInf, (long long)nmin);
+      EZ_CHECK(cudaMemsetAsync(J.moff1, 0, (size_t)(nmin + 1) * 4, st_));
       launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 0);
+      EZ_RUN(entry_lists(J.moff1, J.wstamp1, nmin, chunk));
       launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 1);
+      EZ_CHECK(cudaMemsetAsync(J.wstamp1, 0, (size_t)nmin * 4, st_));
       EZ_CHECK(cudaMemcpyAsync(J.smallest, J.ext_id, nmin * 4, cudaMemcpyDeviceToDevice, st_));
+      launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, kInf, (long long)nmin);
       launch(K_OTHER, k_fill<int>, grid_, 256, J.first_min1, kInf, (long long)nmin);
       launch(K_OTHER, k_fill<int>, grid_, 256, J.first_sj, kInf, (long long)nmin);
       EZ_CHECK(cudaMemsetAsync(J.flag_min2, 0, nmin * 4, st_));
     }
     // Every tile's pointers are computed in the first manifold round.
     EZ_CHECK(cudaMemsetAsync(J.tdirty, 1, (size_t)jh.ntiles, st_));
+    // Block stamps start below the first round's; no root is touched.
+    EZ_CHECK(cudaMemsetAsync(J.bdirty, 0, (size_t)jh.nb * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.rtouch2, 0, (size_t)((N + 31) / 32) * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.rtouch1, 0, (size_t)((N + 31) / 32) * 4, st_));
     // Proposal buffer at the sentinel, edit counters at -1 (:5082), stamps 0.
     launch(K_OTHER, k_fill<K>, grid_, 256, J.delta, J.sentinel_key, (long long)N);
     launch(K_OTHER, k_fill<int>, grid_, 256, J.counter, -1, (long long)N);
@@ -1368,6 +1431,8 @@ class BatchEngine {
     EZ_CHECK(cudaMemsetAsync(J.dstamp, 0, (size_t)N * 4, st_));
     EZ_CHECK(cudaMemsetAsync(J.rstamp, 0, (size_t)N * 4, st_));
     EZ_CHECK(cudaMemsetAsync(J.vchg, 0xff, (size_t)((N + 31) / 32) * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.wchg2, 0, (size_t)((N + 31) / 32) * 4, st_));
+    EZ_CHECK(cudaMemsetAsync(J.wchg1, 0, (size_t)((N + 31) / 32) * 4, st_));
     EZ_CHECK(cudaMemcpyAsync(jobs_dev_ + slot, &J, sizeof(J), cudaMemcpyHostToDevice, st_));
     return EXTREMZ_OK;
   }

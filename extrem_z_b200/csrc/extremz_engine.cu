@@ -444,9 +444,9 @@ static int classify_one(BatchEngine<T>& e, cudaStream_t st, const T* field, int 
 constexpr long long kNoAllocMaxVoxels = EXTREMZ_NOALLOC_MAX_VOXELS;
 // Engine arrays (descriptors, tile maps, counters) first, then one job's
 // worst-case workspace (every voxel a critical point of every kind, 8-byte
-// values: 361 bytes per voxel plus per-array alignment).
+// values: 442 bytes per voxel plus per-array alignment).
 constexpr size_t kNoAllocEngineBytes = 1u << 18;
-constexpr size_t kNoAllocScratchBytes = kNoAllocEngineBytes + (size_t)kNoAllocMaxVoxels * 384 + (1u << 20);
+constexpr size_t kNoAllocScratchBytes = kNoAllocEngineBytes + (size_t)kNoAllocMaxVoxels * 448 + (1u << 20);
 // Both engines (float and double) carve their descriptor, tile-map and
 // counter arrays from the first part.
 constexpr size_t kEngineArrayBytes(size_t job) {

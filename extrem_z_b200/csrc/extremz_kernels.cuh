@@ -50,13 +50,17 @@ struct Job {
   unsigned* vchg;     // bitset: vertices whose value changed since the last computed round
   unsigned* edited;   // bitset: vertices whose value changed in this correction (or null)
   uint8_t* dirtyv;    // per vertex: an input of its saddle rows changed this round
-  uint8_t* bdirty;    // 2 x per 1024-id block: some dirtyv byte in it is set (when N % 4 == 0)
+  int* bdirty;        // per 1024-id block: the round stamp when some dirtyv byte in it was
+                      // set (when N % 4 == 0)
   uint8_t* has2; uint8_t* has1;  // per saddle row: its wrong-neighbour seed bit
+  int* hcnt;          // per saddle-pass chunk: seed bits set in it
   int* cpoff;         // per list (2-saddles, 1-saddles, maxima, minima) and
                       // 1024-id block: offset of the block's first entry
   int* pdd; int* pda; // decompressed steepest pointers, tile-compressed (k_direction)
   uint8_t* tdirty;    // per tile: a value in the tile or its halo changed since
                       // the tile's pointers were computed
+  unsigned* rtouch2; unsigned* rtouch1;  // bitsets: labels (of dds / das) of the vertices of
+                                         // the tiles whose pointers this round recomputes
 
   int* sad2; int* sad1; int* maxima; int* minima;
   int* orow2; int* orow1;  // original rows of kRowStride ints
@@ -66,8 +70,15 @@ struct Job {
   int* largest; int* smallest;  // per maximum / minimum
   int* first1; int* flag2;      // per maximum: wrong_index_max arbitration
   int* first_min1; int* flag_min2;
-  int* first_s; int* first_sj;  // per extremum: wrong_index_saddles arbitration
-  K* ext_key; int* ext_id;      // largest / smallest saddle selection scratch
+  int* first_s; int* first_sj;  // per extremum: its first wrong saddle-row entry (kept across scans)
+  int* moff2; int* ment2;       // per maximum: the row entries (i * kRowStride + p) that name it
+  int* moff1; int* ment1;       // per minimum: the same over the 1-saddles' rows
+  int* wstamp2; int* wstamp1;   // per extremum: the wrong-saddle epoch that last queued it
+  int* aff;                     // extrema queued for the wrong-saddle update
+  int* wlong;                   // of those, the ones with long entry lists
+  unsigned* wchg2; unsigned* wchg1;  // bitsets: values changed since the last wrong-saddle scan
+  K* ext_key; int* ext_id;      // largest / smallest saddle selection scratch; ext_id then
+                                // the lowest-row arbitration of get_wrong_index_min (kInf)
 
   int* ctr;  // device counters, see Ctr
   DeviceTables tb;
@@ -96,6 +107,7 @@ struct Sel {
 enum Ctr : int {
   C_MM = 0, C_CMAX, C_CMIN, C_CSAD, C_TOUCHED, C_NFC, C_NFC1, C_CAND, C_CAND_NEXT,
   C_WMC, C_WMC2, C_WSC, C_WMIN, C_WMIN2, C_WSCJ, C_NS2, C_NS1, C_NMAX, C_NMIN,
+  C_E2, C_E1,  // row entries of the 2-saddles' / 1-saddles' original rows (upper bound)
   C_ERROR,
   C_CHANGED,   // some value changed since the last manifold round began
   C_DIRTY, C_MM_NEXT, C_CANDJ,
@@ -111,6 +123,9 @@ enum Ctr : int {
   C_WNSMALL,   // this side's candidate list is small: the block completion does it all
   C_MFFIRST,   // the manifold round being computed is the job's first: every input is new
   C_TLIST,     // tiles listed for this manifold round's steepest pointers (k_tile_list)
+  C_WEP2, C_WEP1,  // wrong-saddle scan epochs (maxima, minima); epoch 1 computes every extremum
+  C_AFF,       // extrema queued for the current wrong-saddle update
+  C_WLONG,     // of those, the ones with long entry lists (wlong)
   C_COUNT
 };
 // Error bits in ctr[C_ERROR].
@@ -627,7 +642,10 @@ __global__ void __launch_bounds__(256) k_tile_list(const Job<T>* __restrict__ jo
 // A manifold round's steepest pointers of the decompressed field: a fixed
 // grid whose blocks take the listed tiles of every selected job in turn, so
 // that a round with few changed tiles launches few blocks' worth of work
-// instead of one block per tile of the field.
+// instead of one block per tile of the field.  It also marks, per side, the
+// current labels of every vertex of a listed tile as touched roots (rtouch2,
+// rtouch1): only vertices with a touched label can change label this round
+// (k_jump2).
 template <class T>
 __global__ void __launch_bounds__(256, 3) k_direction_list(const Job<T>* __restrict__ jobs,
                                                         const __grid_constant__ Sel sel) {
@@ -651,6 +669,16 @@ __global__ void __launch_bounds__(256, 3) k_direction_list(const Job<T>* __restr
         return;
       loads += tma;
       if (threadIdx.x == 0) J.tdirty[t] = 0;
+      const int x = bx + (int)threadIdx.x % TX, y = by + (int)threadIdx.x / TX;
+      if (x < J.dim.W && y < J.dim.H) {
+        for (int tz = 0; tz < TZ && bz + tz < J.dim.D; ++tz) {
+          const int v = x + y * J.dim.W + (bz + tz) * J.dim.W * J.dim.H;
+          const int r2 = J.dds[v], r1 = J.das[v];
+          // Read first: most roots are marked by many vertices.
+          if (!(J.rtouch2[r2 >> 5] >> (r2 & 31) & 1u)) atomicOr(J.rtouch2 + (r2 >> 5), 1u << (r2 & 31));
+          if (!(J.rtouch1[r1 >> 5] >> (r1 & 31) & 1u)) atomicOr(J.rtouch1 + (r1 >> 5), 1u << (r1 & 31));
+        }
+      }
     }
   }
 }
@@ -732,89 +760,99 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
     if ((N & 3) == 0) {
       // Four consecutive vertices per thread: one 16-byte load per array and
       // one 4-byte store per byte array, a quarter of the memory requests of
-      // the vertex-per-thread loop, with eight chains interleaved.
+      // the vertex-per-thread loop, with eight chains interleaved.  A quad
+      // with a changed-input byte stamps its 1024-id block (bdirty, read by
+      // the saddle pass; its address is read where it is used: kept in a
+      // register for the whole loop it costs spills).
+      //
+      // kLater: a vertex's label on a side can change only when its path
+      // crosses a tile whose pointers this round recomputed, and every vertex
+      // of a path carries the path's label.  So a quad none of whose old
+      // labels is a root marked by k_direction_list (rtouch2 / rtouch1: the
+      // old labels of the recomputed tiles' vertices) keeps its labels and
+      // mismatch bits and has no changed input (a changed value, own or of a
+      // root, lies in a recomputed tile too); only its changed-input bytes
+      // are written, as zeros.
+      const int stamp = J.ctr[C_WNSTAMP];
       const int nq = N >> 2;
       const int qstride = gridDim.x * blockDim.x;
-      // Changed-input flags per 1024-id block, in two buffers by round
-      // parity: this round's are set by the threads whose vertices have a
-      // changed-input byte; the other buffer, next round's, is cleared
-      // meanwhile by the thread that takes the block's first vertices.  (The
-      // buffers' address is read where it is used: kept in registers for
-      // the whole loop it costs spills.)
-      const int nbk = (N + kCpBlockJ - 1) / kCpBlockJ;
       for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += qstride) {
-        {
-          const int v0 = q << 2;
-          const int4 A = *reinterpret_cast<const int4*>(a + v0);
-          const int4 B = *reinterpret_cast<const int4*>(b + v0);
-          const int4 O1 = *reinterpret_cast<const int4*>(ra + v0);
-          const int4 O2 = *reinterpret_cast<const int4*>(rb + v0);
-          int4 R1 = make_int4(0, 0, 0, 0), R2 = make_int4(0, 0, 0, 0);
-          if constexpr (!kLater) {
+        const int v0 = q << 2;
+        const int4 O1 = *reinterpret_cast<const int4*>(ra + v0);
+        const int4 O2 = *reinterpret_cast<const int4*>(rb + v0);
+        const int o1[4] = {O1.x, O1.y, O1.z, O1.w}, o2[4] = {O2.x, O2.y, O2.z, O2.w};
+        if constexpr (kLater) {
+          unsigned hit = 0u;
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            hit |= (J.rtouch2[o1[k] >> 5] >> (o1[k] & 31)) | (J.rtouch1[o2[k] >> 5] >> (o2[k] & 31));
+          if (!(hit & 1u)) {
+            *reinterpret_cast<unsigned*>(dirtyv + v0) = 0u;
+            continue;
+          }
+        }
+        const int4 A = *reinterpret_cast<const int4*>(a + v0);
+        const int4 B = *reinterpret_cast<const int4*>(b + v0);
+        int4 R1 = make_int4(0, 0, 0, 0), R2 = make_int4(0, 0, 0, 0);
+        if constexpr (!kLater) {
+          R1 = *reinterpret_cast<const int4*>(ods + v0);
+          R2 = *reinterpret_cast<const int4*>(oas + v0);
+        }
+        const unsigned cw = vchg[v0 >> 5] >> (v0 & 31);
+        int u1[4] = {A.x, A.y, A.z, A.w}, u2[4] = {B.x, B.y, B.z, B.w};
+        // One hop of every unfinished chain per iteration: the eight loads
+        // depend only on their own chain, so they are all in flight at once.
+        bool more = true;
+        int it = 0;
+        for (; it < cap_j && more; ++it) {
+          int w1[4], w2[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            w1[k] = a[u1[k]];
+            w2[k] = b[u2[k]];
+          }
+          more = false;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            more |= (w1[k] != u1[k]) | (w2[k] != u2[k]);
+            u1[k] = w1[k];
+            u2[k] = w2[k];
+          }
+        }
+        if (it == cap_j && more) atomicOr(err, kErrJump);
+        unsigned dv = 0;
+        bool n1 = false, n2 = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const unsigned c1 = vchg[u1[k] >> 5] >> (u1[k] & 31);
+          const unsigned c2 = vchg[u2[k] >> 5] >> (u2[k] & 31);
+          n1 |= o1[k] != u1[k];
+          n2 |= o2[k] != u2[k];
+          const unsigned d = (o1[k] != u1[k]) | (o2[k] != u2[k]) | ((cw >> k | c1 | c2) & 1u);
+          dv |= d << (8 * k);
+        }
+        *reinterpret_cast<unsigned*>(dirtyv + v0) = dv;
+        // Stores that would rewrite the stored value are skipped.  The
+        // mismatch bits follow the labels alone (the original roots are
+        // fixed), so a group whose labels did not change keeps last round's
+        // bits.  A job's first round writes every group (its change bitset
+        // starts full, so dv is set everywhere; the stored labels may be
+        // another job's).
+        if (kLater ? (n1 || n2) : dv != 0) {
+          if constexpr (kLater) {
             R1 = *reinterpret_cast<const int4*>(ods + v0);
             R2 = *reinterpret_cast<const int4*>(oas + v0);
           }
-          const unsigned cw = vchg[v0 >> 5] >> (v0 & 31);
-          int u1[4] = {A.x, A.y, A.z, A.w}, u2[4] = {B.x, B.y, B.z, B.w};
-          const int o1[4] = {O1.x, O1.y, O1.z, O1.w}, o2[4] = {O2.x, O2.y, O2.z, O2.w};
-          // One hop of every unfinished chain per iteration: the eight loads
-          // depend only on their own chain, so they are all in flight at once.
-          bool more = true;
-          int it = 0;
-          for (; it < cap_j && more; ++it) {
-            int w1[4], w2[4];
+          const int r1[4] = {R1.x, R1.y, R1.z, R1.w}, r2[4] = {R2.x, R2.y, R2.z, R2.w};
+          unsigned mv = 0;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              w1[k] = a[u1[k]];
-              w2[k] = b[u2[k]];
-            }
-            more = false;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              more |= (w1[k] != u1[k]) | (w2[k] != u2[k]);
-              u1[k] = w1[k];
-              u2[k] = w2[k];
-            }
-          }
-          if (it == cap_j && more) atomicOr(err, kErrJump);
-          unsigned dv = 0;
-          bool n1 = false, n2 = false;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const unsigned c1 = vchg[u1[k] >> 5] >> (u1[k] & 31);
-            const unsigned c2 = vchg[u2[k] >> 5] >> (u2[k] & 31);
-            n1 |= o1[k] != u1[k];
-            n2 |= o2[k] != u2[k];
-            const unsigned d = (o1[k] != u1[k]) | (o2[k] != u2[k]) | ((cw >> k | c1 | c2) & 1u);
-            dv |= d << (8 * k);
-          }
-          *reinterpret_cast<unsigned*>(dirtyv + v0) = dv;
-          // Stores that would rewrite the stored value are skipped.  The
-          // mismatch bits follow the labels alone (the original roots are
-          // fixed), so a group whose labels did not change keeps last round's
-          // bits.  A job's first round writes every group (its change bitset
-          // starts full, so dv is set everywhere; the stored labels may be
-          // another job's).
-          if (kLater ? (n1 || n2) : dv != 0) {
-            if constexpr (kLater) {
-              R1 = *reinterpret_cast<const int4*>(ods + v0);
-              R2 = *reinterpret_cast<const int4*>(oas + v0);
-            }
-            const int r1[4] = {R1.x, R1.y, R1.z, R1.w}, r2[4] = {R2.x, R2.y, R2.z, R2.w};
-            unsigned mv = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-              mv |= ((unsigned)(u1[k] != r1[k]) | (unsigned)(u2[k] != r2[k]) << 1) << (8 * k);
-            *reinterpret_cast<unsigned*>(mis + v0) = mv;
-          }
-          if (n1) *reinterpret_cast<int4*>(ra + v0) = make_int4(u1[0], u1[1], u1[2], u1[3]);
-          if (n2) *reinterpret_cast<int4*>(rb + v0) = make_int4(u2[0], u2[1], u2[2], u2[3]);
-          if (dv || (v0 & (kCpBlockJ - 1)) == 0) {
-            const int par = J.ctr[C_WNSTAMP] & 1;
-            if (dv) J.bdirty[(size_t)par * nbk + (v0 >> 10)] = 1;
-            if ((v0 & (kCpBlockJ - 1)) == 0) J.bdirty[(size_t)(par ^ 1) * nbk + (v0 >> 10)] = 0;
-          }
+          for (int k = 0; k < 4; ++k)
+            mv |= ((unsigned)(u1[k] != r1[k]) | (unsigned)(u2[k] != r2[k]) << 1) << (8 * k);
+          *reinterpret_cast<unsigned*>(mis + v0) = mv;
         }
+        if (n1) *reinterpret_cast<int4*>(ra + v0) = make_int4(u1[0], u1[1], u1[2], u1[3]);
+        if (n2) *reinterpret_cast<int4*>(rb + v0) = make_int4(u2[0], u2[1], u2[2], u2[3]);
+        if (dv) J.bdirty[v0 >> 10] = stamp;
       }
       continue;
     }
@@ -866,27 +904,53 @@ __device__ __forceinline__ void cp_lane_bits(const int8_t* __restrict__ otype, i
   }
 }
 
+// Also counts the entries the original rows will hold (lists 4 and 5): a
+// 2-saddle's row has one entry per upper neighbour, a 1-saddle's one per lower
+// neighbour (rows keep repeated labels; the persistence filter thr can only
+// drop entries, so with thr > 0 this is an upper bound).
 __global__ void __launch_bounds__(32 * kCpWarps) k_cp_count(const int8_t* __restrict__ otype,
-                                                           int N, int nb,
+                                                           const uint16_t* __restrict__ olm,
+                                                           Dims g, int nb,
                                                            int* __restrict__ bcount) {
   const int b = blockIdx.x * kCpWarps + (int)(threadIdx.x >> 5);
   if (b >= nb) return;  // whole warps leave together
+  const int v0 = b * kCpBlock + (int)lane_id() * 32;
   unsigned bits[4];
-  cp_lane_bits(otype, N, b * kCpBlock + (int)lane_id() * 32, bits);
+  cp_lane_bits(otype, g.N, v0, bits);
+  int e2 = 0, e1 = 0;
+  if ((bits[0] | bits[1]) != 0u) {
+    int x, y, z;
+    coords(v0, g, x, y, z);
+    for (int k = 0; k < 32; ++k) {
+      if (((bits[0] | bits[1]) >> k) & 1u) {
+        const int nvalid = __popc(valid_mask(boundary_code(x, y, z, g.W, g.H, g.D)));
+        const int lower = __popc((unsigned)olm[v0 + k]);
+        if ((bits[0] >> k) & 1u) e2 += nvalid - lower;
+        if ((bits[1] >> k) & 1u) e1 += lower;
+      }
+      if (++x == g.W) {
+        x = 0;
+        if (++y == g.H) {
+          y = 0;
+          ++z;
+        }
+      }
+    }
+  }
+  int c[6] = {__popc(bits[0]), __popc(bits[1]), __popc(bits[2]), __popc(bits[3]), e2, e1};
 #pragma unroll
-  for (int l = 0; l < 4; ++l) {
-    int c = __popc(bits[l]);
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane_id() == 0) bcount[l * nb + b] = c;
+  for (int l = 0; l < 6; ++l) {
+    for (int o = 16; o > 0; o >>= 1) c[l] += __shfl_xor_sync(0xffffffffu, c[l], o);
+    if (lane_id() == 0) bcount[l * nb + b] = c[l];
   }
 }
 
 // Single block: exclusive scan of nlists x nb block counts in place, list
 // totals to totals[0 .. nlists).  The CP lists use totals = ctr + C_NS2.  Each
-// thread takes eight consecutive counts per pass.
+// thread takes 32 consecutive counts per pass.
 __global__ void __launch_bounds__(1024) k_scan_lists(int* __restrict__ bcount, int nb, int nlists,
                                                      int* totals) {
-  constexpr int kPer = 8;
+  constexpr int kPer = 32;
   __shared__ int carry;
   __shared__ int warp_sums[32];
   for (int l = 0; l < nlists; ++l) {
@@ -933,6 +997,55 @@ __global__ void __launch_bounds__(1024) k_scan_lists(int* __restrict__ bcount, i
   }
 }
 
+// Exclusive scan in place of lists of n counts (list l at c + l * n, one per
+// blockIdx.y) for lists too long for one block: the sum of every 1024-count
+// chunk (k_chunk_sums, into sums + l * gridDim.x), a scan of the sums with the
+// list totals (k_scan_lists, one block), then each chunk scanned from its
+// offset (k_chunk_scan).
+__global__ void __launch_bounds__(1024) k_chunk_sums(const int* __restrict__ c, int n,
+                                                     int* __restrict__ sums) {
+  __shared__ int ws[32];
+  c += (long long)blockIdx.y * n;
+  sums += (long long)blockIdx.y * gridDim.x;
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  int x = i < n ? c[i] : 0;
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  if (lane_id() == 0) ws[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int y = ws[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+    if (threadIdx.x == 0) sums[blockIdx.x] = y;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_chunk_scan(int* __restrict__ c, int n,
+                                                     const int* __restrict__ offs) {
+  __shared__ int ws[32];
+  c += (long long)blockIdx.y * n;
+  offs += (long long)blockIdx.y * gridDim.x;
+  const int i = blockIdx.x * 1024 + threadIdx.x;
+  const int x = i < n ? c[i] : 0;
+  int incl = x;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane_id() >= (unsigned)o) incl += y;
+  }
+  if (lane_id() == 31) ws[threadIdx.x >> 5] = incl;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int w = ws[threadIdx.x];
+    int wi = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane_id() >= (unsigned)o) wi += y;
+    }
+    ws[threadIdx.x] = wi - w;
+  }
+  __syncthreads();
+  if (i < n) c[i] = offs[blockIdx.x] + ws[threadIdx.x >> 5] + incl - x;
+}
+
 __global__ void __launch_bounds__(32 * kCpWarps) k_cp_write(const int8_t* __restrict__ otype,
                                                            int N, int nb,
                                                            const int* __restrict__ boff,
@@ -953,7 +1066,11 @@ __global__ void __launch_bounds__(32 * kCpWarps) k_cp_write(const int8_t* __rest
       if (lane_id() >= (unsigned)o) incl += y;
     }
     int pos = boff[l * nb + b] + incl - c;
-    for (unsigned m = bits[l]; m; m &= m - 1) outs[l][pos++] = v0 + __ffs(m) - 1;
+    for (unsigned m = bits[l]; m; m &= m - 1) {
+      const int v = v0 + __ffs(m) - 1;
+      outs[l][pos] = v;
+      ++pos;
+    }
   }
 }
 
@@ -975,10 +1092,24 @@ __global__ void k_ext_index(Job<T> J) {
 // and the count are written, so entries past a shorter row keep their last
 // value, as in the reference.
 // ---------------------------------------------------------------------------
+// A sorting network for 14 entries: Batcher's odd-even merge sort of 16
+// without the comparators of the two highest positions (which would hold
+// the largest keys); the 0-1 principle checks it (every 0/1 input of 14).
+constexpr int kSort14Size = 53;
+__device__ constexpr unsigned char kSort14[kSort14Size][2] = {
+    {0, 1},  {2, 3},   {0, 2},  {1, 3},   {1, 2},   {4, 5},   {6, 7},   {4, 6},  {5, 7},
+    {5, 6},  {0, 4},   {2, 6},  {2, 4},   {1, 5},   {3, 7},   {3, 5},   {1, 2},  {3, 4},
+    {5, 6},  {8, 9},   {10, 11}, {8, 10}, {9, 11},  {9, 10},  {12, 13}, {8, 12}, {10, 12},
+    {9, 13}, {11, 13}, {9, 10}, {11, 12}, {0, 8},   {4, 12},  {4, 8},   {2, 10}, {6, 10},
+    {2, 4},  {6, 8},   {10, 12}, {1, 9},  {5, 13},  {5, 9},   {3, 11},  {7, 11}, {3, 5},
+    {7, 9},  {11, 13}, {1, 2},  {3, 4},   {5, 6},   {7, 8},   {9, 10},  {11, 12}};
+
 template <class T, bool kAsc>
 __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
                                               const int* __restrict__ lab, const int* __restrict__ sad,
-                                              int ns_slot, int* __restrict__ rows) {
+                                              int ns_slot, int* __restrict__ rows,
+                                              uint8_t* __restrict__ ocnt, int4* __restrict__ orm,
+                                              int4* __restrict__ oend) {
   const int ns = J.ctr[ns_slot];
   const int stride = gridDim.x * blockDim.x;
   const Dims g = J.dim;
@@ -1011,25 +1142,72 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
     const int cnt = __popc(keep);
     // The order of insertionSort (:1795-1811, descending) for ascending rows
     // and of reversed_insertionSort (:1813-1829, ascending) for descending
-    // rows, by rank: each entry's position is the number of entries before it,
-    // equal entries (the same label) in direction order as the stable
-    // insertion sort leaves them.  All indices are static, so the entries stay
-    // in registers.
+    // rows: by (value, label), entries with the same label being equal in
+    // both.  So any sort gives the insertion sort's row; a sorting network
+    // over order-preserving integer keys does it with static indices (the
+    // entries stay in registers).  Ascending rows flip the bits of both keys
+    // so that both orders sort ascending; left-out entries take the largest
+    // key and sort last (no finite value encodes to it).
     int* out = rows + (long long)i * kRowStride;
+    int srt[kNumDirs];  // the row in order, left-out entries last
+    using K = typename KeyOf<T>::K;
+    if constexpr (sizeof(K) == 4) {
+      unsigned long long e[kNumDirs];  // key << 32 | label
+#pragma unroll
+      for (int d = 0; d < kNumDirs; ++d) {
+        const K k = KeyOf<T>::enc(val[d] + T(0));  // -0 and +0 compare equal
+        const unsigned long long p = (unsigned long long)k << 32 | (unsigned)lb[d];
+        e[d] = (keep >> d & 1u) ? (kAsc ? ~p : p) : ~0ull;
+      }
+#pragma unroll
+      for (int c = 0; c < kSort14Size; ++c) {
+        const int x = kSort14[c][0], y = kSort14[c][1];
+        const unsigned long long lo = min(e[x], e[y]), hi = max(e[x], e[y]);
+        e[x] = lo;
+        e[y] = hi;
+      }
+#pragma unroll
+      for (int d = 0; d < kNumDirs; ++d) srt[d] = (int)(kAsc ? ~(unsigned)e[d] : (unsigned)e[d]);
+    } else {
+      K k[kNumDirs];
+      unsigned l[kNumDirs];
+#pragma unroll
+      for (int d = 0; d < kNumDirs; ++d) {
+        const K kd = KeyOf<T>::enc(val[d] + T(0));
+        const bool in = keep >> d & 1u;
+        k[d] = in ? (kAsc ? ~kd : kd) : ~K(0);
+        l[d] = in ? (kAsc ? ~(unsigned)lb[d] : (unsigned)lb[d]) : ~0u;
+      }
+#pragma unroll
+      for (int c = 0; c < kSort14Size; ++c) {
+        const int x = kSort14[c][0], y = kSort14[c][1];
+        const bool sw = k[x] > k[y] || (k[x] == k[y] && l[x] > l[y]);
+        const K kx = k[x], ky = k[y];
+        const unsigned lx = l[x], ly = l[y];
+        k[x] = sw ? ky : kx;
+        k[y] = sw ? kx : ky;
+        l[x] = sw ? ly : lx;
+        l[y] = sw ? lx : ly;
+      }
+#pragma unroll
+      for (int d = 0; d < kNumDirs; ++d) srt[d] = (int)(kAsc ? ~l[d] : l[d]);
+    }
+    int last = -1;
 #pragma unroll
     for (int d = 0; d < kNumDirs; ++d) {
-      if (!(keep >> d & 1u)) continue;
-      int rank = 0;
-#pragma unroll
-      for (int e = 0; e < kNumDirs; ++e) {
-        if (!(keep >> e & 1u) || e == d) continue;
-        const bool before = kAsc ? above(val[e], lb[e], val[d], lb[d])
-                                 : below(val[e], lb[e], val[d], lb[d]);
-        rank += before || (lb[e] == lb[d] && e < d);
-      }
-      out[rank] = lb[d];
+      if (d < cnt) out[d] = srt[d];
+      if (d == cnt - 1) last = srt[d];
     }
     out[14] = cnt;
+    // The compact copies the per-round scans read: the count, the first four
+    // entries as extremum indices (-1 past the count), the first and the last
+    // entry as labels and as extremum indices.
+    int m[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) m[p] = p < cnt ? J.ext[srt[p]] : -1;
+    ocnt[i] = (uint8_t)cnt;
+    orm[i] = make_int4(m[0], m[1], m[2], m[3]);
+    oend[i] = make_int4(cnt > 0 ? srt[0] : -1, last, m[0], cnt > 0 ? J.ext[last] : -1);
   }
 }
 
@@ -1040,30 +1218,58 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
 // Pass 1 selects the extreme value key, pass 2 the extreme id at that value.
 // ---------------------------------------------------------------------------
 template <class T, bool kMax>
-__global__ void k_extreme_saddle(Job<T> J, int pass) {
+__global__ void __launch_bounds__(256) k_extreme_saddle(Job<T> J, int pass) {
   using K = typename KeyOf<T>::K;
   const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
   const int* sad = kMax ? J.sad2 : J.sad1;
   const int* rows = kMax ? J.orow2 : J.orow1;
   const uint8_t* ocnt = kMax ? J.ocnt2 : J.ocnt1;
+  int* cnt_or_cur = pass == 0 ? (kMax ? J.moff2 : J.moff1) : (kMax ? J.wstamp2 : J.wstamp1);
+  int* ent = kMax ? J.ment2 : J.ment1;
   const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
-    const int cnt = ocnt[i];
-    if (cnt == 0) continue;
-    const int s = sad[i];
-    const K key = KeyOf<T>::enc(J.f[s] + T(0));  // -0 and +0 compare equal
-    const int* row = rows + (long long)i * kRowStride;
+  // Uniform per warp: the entries of the lanes' rows go through the atomics
+  // together, so that lanes naming the same extremum (neighbouring saddles
+  // usually do) share one atomic.
+  for (int base = blockIdx.x * blockDim.x; base < ns; base += stride) {
+    const int i = base + threadIdx.x;
+    const int cnt = i < ns ? ocnt[i] : 0;
+    const int s = i < ns ? sad[i] : 0;
+    const K key = KeyOf<T>::enc(J.f[i < ns ? s : 0] + T(0));  // -0 and +0 compare equal
+    const int* row = rows + (long long)(i < ns ? i : 0) * kRowStride;
     // The first four entries as extremum indices from the compact copy
-    // (k_row_counts), longer rows' tails through the index map.
-    const int4 m4 = (kMax ? J.orm2 : J.orm1)[i];
-    for (int p = 0; p < cnt; ++p) {
-      const int m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : J.ext[row[p]];
+    // (k_rows), longer rows' tails through the index map.
+    const int4 m4 = i < ns ? (kMax ? J.orm2 : J.orm1)[i] : make_int4(-1, -1, -1, -1);
+    const int pmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
+    int prev = -1;
+    for (int p = 0; p < pmax; ++p) {
+      int m = -1;
+      if (p < cnt) m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : J.ext[row[p]];
+      // Rows are sorted, so a repeated label is the entry before: the
+      // per-extremum lists keep a row's first entry naming the extremum (a
+      // later one has the same saddle and a larger key).
+      const bool fresh = m >= 0 && m != prev;
+      if (m >= 0) prev = m;
+      const unsigned grp = __match_any_sync(0xffffffffu, fresh ? m : -1);
+      const int leader = __ffs(grp) - 1;
+      const unsigned below = grp & ((1u << lane_id()) - 1u);
+      int at = 0;
+      if (fresh && below == 0u) at = atomicAdd(cnt_or_cur + m, __popc(grp));
+      at = __shfl_sync(0xffffffffu, at, leader) + __popc(below);
+      if (m < 0) continue;
+      // Largest (smallest) saddle key per extremum, then the largest
+      // (smallest) id at that key; a read first skips most atomics (the
+      // key only moves one way).
       if (pass == 0) {
-        if (kMax) atomicMax(J.ext_key + m, key);
-        else atomicMin(J.ext_key + m, key);
-      } else if (J.ext_key[m] == key) {
-        if (kMax) atomicMax(J.ext_id + m, s);
-        else atomicMin(J.ext_id + m, s);
+        if (kMax ? key > J.ext_key[m] : key < J.ext_key[m]) {
+          if (kMax) atomicMax(J.ext_key + m, key);
+          else atomicMin(J.ext_key + m, key);
+        }
+      } else {
+        if (J.ext_key[m] == key) {
+          if (kMax) atomicMax(J.ext_id + m, s);
+          else atomicMin(J.ext_id + m, s);
+        }
+        if (fresh) ent[at] = i * kRowStride + p;
       }
     }
   }
@@ -1208,6 +1414,8 @@ __global__ void __launch_bounds__(256) k_apply(const Job<T>* __restrict__ jobs, 
     if (KeyOf<T>::enc(gv) != KeyOf<T>::enc(g0)) {
       J.ctr[C_CHANGED] = 1;
       atomicOr(J.vchg + (v >> 5), 1u << (v & 31));
+      atomicOr(J.wchg2 + (v >> 5), 1u << (v & 31));
+      atomicOr(J.wchg1 + (v >> 5), 1u << (v & 31));
       if (J.edited) atomicOr(J.edited + (v >> 5), 1u << (v & 31));
       int x, y, z;
       coords(v, J.dim, x, y, z);
@@ -1364,7 +1572,11 @@ __global__ void k_clear_changed(const Job<T>* __restrict__ jobs, const __grid_co
     if (J.ctr[C_MFSKIP]) continue;
     const int nw = (J.dim.N + 31) >> 5;
     const int stride = gridDim.x * blockDim.x;
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += stride) J.vchg[w] = 0u;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += stride) {
+      J.vchg[w] = 0u;
+      J.rtouch2[w] = 0u;
+      J.rtouch1[w] = 0u;
+    }
   }
 }
 
@@ -1432,10 +1644,13 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
           const long long off = (long long)(t / 3 - 1) * WH + (long long)(t % 3 - 1) * W;
           const long long lo = max(0ll, (long long)b0 * kCpBlock + off - 1);
           const long long hi = min(N - 1, (long long)b1 * kCpBlock - 1 + off + 1);
-          const uint8_t* bcur = J.bdirty + (size_t)(J.ctr[C_WNSTAMP] & 1) * nb;
-          for (long long b = lo >> 10; b <= (hi >> 10) && lo <= hi; ++b) seen |= bcur[b];
+          const int stamp = J.ctr[C_WNSTAMP];
+          for (long long b = lo >> 10; b <= (hi >> 10) && lo <= hi; ++b)
+            seen |= J.bdirty[b] == stamp;
         }
         if (!__syncthreads_or(seen)) {  // no saddle here has a changed input
+          // Seed bits as computed in an earlier round; none set: nothing to list.
+          if (J.hcnt[c] == 0) continue;
           for (int base = 0; base < n; base += blockDim.x) {
             const int k = base + threadIdx.x;
             const bool split = k < n2;
@@ -1454,6 +1669,7 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
           continue;
         }
       }
+      int nhas = 0;  // seed bits set in the chunk
       for (int base = 0; base < n; base += blockDim.x) {  // uniform in the block
         const int k = base + threadIdx.x;
         const bool split = k < n2;
@@ -1475,32 +1691,10 @@ __global__ void __launch_bounds__(256, 4) k_saddle_pass(const Job<T>* __restrict
         if (slot2 >= 0) J.cand[slot2] = s;
         const int slot1 = warp_append(J.ctr + C_CANDJ, has && !split, 0xffffffffu);
         if (slot1 >= 0) J.cand_j[slot1] = s;
+        nhas += __syncthreads_count(has);
       }
+      if (threadIdx.x == 0) J.hcnt[c] = nhas;
     }
-  }
-}
-
-// Compact copies of the original rows, so that the per-round scans read a
-// few bytes per saddle instead of a 64-byte row: the count; the first four
-// entries as extremum indices (the wrong-saddle scans); the first and the last
-// entry, as labels and as extremum indices (the wrong-extremum scans).
-template <class T>
-__global__ void k_row_counts(Job<T> J) {
-  const int n2 = J.ctr[C_NS2], n1 = J.ctr[C_NS1];
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2 + n1; i += stride) {
-    const bool two = i < n2;
-    const int k = two ? i : i - n2;
-    const int* row = (two ? J.orow2 : J.orow1) + (long long)k * kRowStride;
-    const int cnt = row[14];
-    (two ? J.ocnt2 : J.ocnt1)[k] = (uint8_t)cnt;
-    int m[4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p) m[p] = p < cnt ? J.ext[row[p]] : -1;
-    (two ? J.orm2 : J.orm1)[k] = make_int4(m[0], m[1], m[2], m[3]);
-    const int first = cnt > 0 ? row[0] : -1, last = cnt > 0 ? row[cnt - 1] : -1;
-    (two ? J.oend2 : J.oend1)[k] =
-        make_int4(first, last, cnt > 0 ? m[0] : -1, cnt > 0 ? J.ext[last] : -1);
   }
 }
 
@@ -1675,7 +1869,9 @@ __global__ void __launch_bounds__(1024) k_wn_resolve(Job<T>* __restrict__ jobs, 
 // candidate goes to the saddle that meets it at the earlier neighbour index.
 // The two sides flag into separate arrays, as the reference's two kernels do,
 // so one step serves both.  A saddle's resolution is marked in claim[]
-// (unused by this mode), per side and per round stamp.
+// (unused by this mode) with the round's stamp: the low 32-bit half for the
+// split side, the high half for the join side, so that a saddle on both lists
+// (type 3) keeps one mark per side.
 template <class T>
 __device__ __forceinline__ void wn_step_entry(const Job<T>& J, int e, int n2, int d, int stamp) {
   const bool split = e < n2;
@@ -1684,8 +1880,9 @@ __device__ __forceinline__ void wn_step_entry(const Job<T>& J, int e, int n2, in
   int x, y, z;
   coords(s, g, x, y, z);
   if (!dir_valid(d, boundary_code(x, y, z, g.W, g.H, g.D))) return;
-  const unsigned long long done = (1ull << 63) | (split ? 0ull : (1ull << 62)) | (unsigned)stamp;
-  if (J.claim[s] == done) return;
+  unsigned* mark = reinterpret_cast<unsigned*>(J.claim + s) + (split ? 0 : 1);
+  const unsigned done = (unsigned)stamp | 0x80000000u;  // never the zeroed initial value
+  if (*mark == done) return;
   const int r = s + ddx(d) + ddy(d) * g.W + ddz(d) * g.W * g.H;
   const T sv = J.g[s], rv = J.g[r];
   if (!(split ? above(rv, r, sv, s) : below(rv, r, sv, s))) return;
@@ -1693,7 +1890,7 @@ __device__ __forceinline__ void wn_step_entry(const Job<T>& J, int e, int n2, in
   if ((split ? J.dds[r] == J.ds[r] : J.das[r] == J.as[r]) || taken[r] == stamp) return;
   taken[r] = stamp;
   (split ? J.flagged : J.flagged1)[atomicAdd(J.ctr + (split ? C_NFC : C_NFC1), 1)] = r;
-  J.claim[s] = done;
+  *mark = done;
 }
 
 // One step over every selected job's two candidate lists (a large list: one
@@ -1859,7 +2056,9 @@ __global__ void __launch_bounds__(256) k_wim_collect(const Job<T>* __restrict__ 
 
 // get_wrong_index_min direction 1 (:3157-3168, fix :3393-3410) keeps the pair of
 // the lowest row per minimum and lowers the row's FALSE last entry, so it needs
-// the winning row: one more scan, arbitrating through first_sj as scratch.
+// the winning row: one more scan, arbitrating through ext_id (the setup's
+// scratch, left at kInf; first_sj keeps the wrong-saddle results between
+// scans).
 template <class T>
 __global__ void __launch_bounds__(256) k_wim_min2_scan(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
@@ -1870,7 +2069,7 @@ __global__ void __launch_bounds__(256) k_wim_min2_scan(const Job<T>* __restrict_
     const int cnt = J.ocnt1[i];
     if (cnt == 0) continue;
     const int4 o = J.oend1[i];
-    if (o.y != J.drow1[2ll * i + 1]) atomicMin(J.first_sj + o.w, i);
+    if (o.y != J.drow1[2ll * i + 1]) atomicMin(J.ext_id + o.w, i);
   }
   }
 }
@@ -1881,9 +2080,9 @@ __global__ void __launch_bounds__(256) k_wim_min2_collect(const Job<T>* __restri
   const int next = J.ctr[C_NMIN];
   const int stride = gridDim.x * blockDim.x;
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < next; m += stride) {
-    const int row = J.first_sj[m];
+    const int row = J.ext_id[m];
     if (row == kInf) continue;
-    J.first_sj[m] = kInf;
+    J.ext_id[m] = kInf;
     const int target = J.drow1[2ll * row + 1];
     propose(J, target, step_delta(J, target));
   }
@@ -1897,72 +2096,160 @@ __global__ void __launch_bounds__(256) k_wim_min2_collect(const Job<T>* __restri
 // largest (smallest) saddle in the decompressed field -- and
 // fix_wrong_index_saddle (:3415-3463).
 // ---------------------------------------------------------------------------
-// Per extremum, the current value of its true largest (smallest) saddle, into
-// the extremum-indexed scratch ext_key (free after the setup), so that the
-// scan below reads it from one compact table instead of through two dependent
-// gathers per row entry.  Rebuilt before every scan: the values change between
-// rounds.
+// The scan is incremental.  An extremum's result -- its first row entry
+// (i * kRowStride + p, row order then entry order) whose saddle outranks the
+// extremum's true largest (smallest) saddle in the decompressed field, or kInf
+// -- depends only on the values of the saddles whose rows name it, and the true
+// largest saddle is one of them.  So after the first scan of a correction
+// (epoch 1: every extremum) only the extrema named in the rows of saddles whose
+// value changed since the previous scan are recomputed, each from its list of
+// row entries (moff / ment, built at setup); the others keep their result.
+// k_apply marks changed values in wchg2 / wchg1, one bitset per side.
+
+// Row index of vertex v on the side (its index in sad2 / sad1), or -1: a
+// binary search among the list entries of v's 1024-id block (cpoff).
 template <class T, bool kMax>
-__global__ void __launch_bounds__(256) k_wis_table(const Job<T>* __restrict__ jobs,
-                                                   const __grid_constant__ Sel sel) {
+__device__ __forceinline__ int side_row(const Job<T>& J, int v) {
+  const int t = J.otype[v];
+  if (!(kMax ? (t == 2 || t == 3) : (t == 1 || t == 3))) return -1;
+  const int nb = (J.dim.N + kCpBlock - 1) / kCpBlock, b = v / kCpBlock;
+  const int* off = J.cpoff + (kMax ? 0 : nb);
+  const int* sad = kMax ? J.sad2 : J.sad1;
+  int lo = off[b], hi = (b + 1 < nb ? off[b + 1] : J.ctr[kMax ? C_NS2 : C_NS1]) - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (sad[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Queues the extrema named in the rows of the saddles whose value changed
+// (and clears the bitset).  In epoch 1 every extremum is recomputed, so the
+// bitset is only cleared.
+template <class T, bool kMax>
+__global__ void __launch_bounds__(256) k_wis_mark(const Job<T>* __restrict__ jobs,
+                                                  const __grid_constant__ Sel sel) {
   for (int jk = 0; jk < sel.n; ++jk) {
     const Job<T>& J = jobs[sel.idx[jk]];
-    const int next = J.ctr[kMax ? C_NMAX : C_NMIN];
-    const int* best = kMax ? J.largest : J.smallest;
-    T* val = reinterpret_cast<T*>(J.ext_key);
-    const int N = J.dim.N;
+    const int epoch = J.ctr[kMax ? C_WEP2 : C_WEP1];
+    unsigned* chg = kMax ? J.wchg2 : J.wchg1;
+    const uint8_t* ocnt = kMax ? J.ocnt2 : J.ocnt1;
+    const int4* orm = kMax ? J.orm2 : J.orm1;
+    const int* rows = kMax ? J.orow2 : J.orow1;
+    int* stamp = kMax ? J.wstamp2 : J.wstamp1;
+    const int nw = (J.dim.N + 31) >> 5;
     const int stride = gridDim.x * blockDim.x;
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < next; m += stride) {
-      const int t = best[m];  // no saddle: -1 or kInf, never read by the scan
-      val[m] = (t >= 0 && t < N) ? J.g[t] : T(0);
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += stride) {
+      unsigned bits = chg[w];
+      if (!bits) continue;
+      chg[w] = 0u;
+      if (epoch == 1) continue;
+      for (; bits; bits &= bits - 1) {
+        const int i = side_row<T, kMax>(J, (w << 5) + __ffs(bits) - 1);
+        if (i < 0) continue;
+        const int cnt = ocnt[i];
+        const int4 m4 = orm[i];
+        for (int p = 0; p < cnt; ++p) {
+          const int m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w
+                                                               : J.ext[rows[(long long)i * kRowStride + p]];
+          if (atomicExch(stamp + m, epoch) != epoch) J.aff[atomicAdd(J.ctr + C_AFF, 1)] = m;
+        }
+      }
     }
   }
 }
 
+// The first entry among ent[k0 + i * step], i >= 0, below k1 whose saddle
+// outranks extremum saddle tb (value gt), or kInf.  Four entries at a time:
+// their three dependent loads (entry, saddle, value) go out together.
 template <class T, bool kMax>
-__global__ void __launch_bounds__(256) k_wis_scan(const Job<T>* __restrict__ jobs, const __grid_constant__ Sel sel) {
-  for (int jk = 0; jk < sel.n; ++jk) {
-  const Job<T>& J = jobs[sel.idx[jk]];
-  const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
-  const int* sad = kMax ? J.sad2 : J.sad1;
-  const int* rows = kMax ? J.orow2 : J.orow1;
-  const int4* orm = kMax ? J.orm2 : J.orm1;
-  const uint8_t* ocnt = kMax ? J.ocnt2 : J.ocnt1;
-  const int* best = kMax ? J.largest : J.smallest;
-  const T* val = reinterpret_cast<const T*>(J.ext_key);
-  int* first = kMax ? J.first_s : J.first_sj;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
-    const int cnt = ocnt[i];
-    if (cnt == 0) continue;
-    const int s = sad[i];
-    const T gs = J.g[s];
-    // Rows hold 2-3 entries typically: the first four entries come as
-    // extremum indices from the compact copy, their true largest / smallest
-    // saddle's value from the per-extremum table (k_wis_table), all loads
-    // independent; the saddle's id is needed only on a tie of values.
-    // Longer rows finish entry by entry.
-    const int4 m4 = orm[i];
-    const int m[4] = {m4.x, m4.y, m4.z, m4.w};
-    T gt[4];
+__device__ __forceinline__ int wis_first(const Job<T>& J, const int* sad, const int* ent, int k0,
+                                         int k1, int step, int tb, T gt) {
+  int hit = kInf;
+  for (int k = k0; k < k1; k += 4 * step) {
+    int key[4], s[4];
+    T gs[4];
 #pragma unroll
-    for (int p = 0; p < 4; ++p) gt[p] = p < cnt ? val[m[p]] : T(0);
+    for (int j = 0; j < 4; ++j) key[j] = k + j * step < k1 ? ent[k + j * step] : -1;
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      if (p >= cnt) break;
-      const bool wrong = kMax ? (gs > gt[p] || (gs == gt[p] && s > best[m[p]]))
-                              : (gs < gt[p] || (gs == gt[p] && s < best[m[p]]));
-      if (wrong) atomicMin(first + m[p], i * kRowStride + p);
-    }
-    const int* row = rows + (long long)i * kRowStride;
-    for (int p = 4; p < cnt; ++p) {
-      const int mp = J.ext[row[p]];
-      const int tp = best[mp];
-      const T gp = J.g[tp];
-      const bool wrong = kMax ? above(gs, s, gp, tp) : below(gs, s, gp, tp);
-      if (wrong) atomicMin(first + mp, i * kRowStride + p);
+    for (int j = 0; j < 4; ++j) s[j] = key[j] >= 0 ? sad[key[j] / kRowStride] : 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) gs[j] = key[j] >= 0 ? J.g[s[j]] : T(0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const bool wrong = kMax ? (gs[j] > gt || (gs[j] == gt && s[j] > tb))
+                              : (gs[j] < gt || (gs[j] == gt && s[j] < tb));
+      if (key[j] >= 0 && wrong && key[j] < hit) hit = key[j];
     }
   }
+  return hit;
+}
+
+// Recomputes the queued extrema (every extremum in epoch 1) from their row
+// entries, a thread per extremum; an extremum with more than kWisShort
+// entries goes to the long queue (wlong) for a block of its own
+// (k_wis_long), so that one long list does not hold up the launch.
+constexpr int kWisShort = 48;
+template <class T, bool kMax>
+__global__ void __launch_bounds__(256) k_wis_update(const Job<T>* __restrict__ jobs,
+                                                    const __grid_constant__ Sel sel) {
+  for (int jk = 0; jk < sel.n; ++jk) {
+    const Job<T>& J = jobs[sel.idx[jk]];
+    const bool all = J.ctr[kMax ? C_WEP2 : C_WEP1] == 1;
+    const int n = all ? J.ctr[kMax ? C_NMAX : C_NMIN] : J.ctr[C_AFF];
+    const int* sad = kMax ? J.sad2 : J.sad1;
+    const int* best = kMax ? J.largest : J.smallest;
+    const int* off = kMax ? J.moff2 : J.moff1;
+    const int* ent = kMax ? J.ment2 : J.ment1;
+    int* first = kMax ? J.first_s : J.first_sj;
+    const int N = J.dim.N;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {  // uniform per warp
+      const int e = base + threadIdx.x;
+      bool lng = false;
+      int m = 0;
+      if (e < n) {
+        m = all ? e : J.aff[e];
+        const int tb = best[m];
+        const int k0 = off[m], k1 = off[m + 1];
+        lng = k1 - k0 > kWisShort;
+        // An extremum named by no row has no saddle.
+        if (!lng)
+          first[m] = (tb >= 0 && tb < N) ? wis_first<T, kMax>(J, sad, ent, k0, k1, 1, tb, J.g[tb])
+                                         : kInf;
+      }
+      const int slot = warp_append(J.ctr + C_WLONG, lng, 0xffffffffu);
+      if (slot >= 0) J.wlong[slot] = m;
+    }
+  }
+}
+
+// The long lists of k_wis_update, a block per extremum.
+template <class T, bool kMax>
+__global__ void __launch_bounds__(256) k_wis_long(const Job<T>* __restrict__ jobs,
+                                                  const __grid_constant__ Sel sel) {
+  __shared__ int part[8];
+  for (int jk = 0; jk < sel.n; ++jk) {
+    const Job<T>& J = jobs[sel.idx[jk]];
+    const int n = J.ctr[C_WLONG];
+    const int* sad = kMax ? J.sad2 : J.sad1;
+    const int* ent = kMax ? J.ment2 : J.ment1;
+    const int* off = kMax ? J.moff2 : J.moff1;
+    for (int e = blockIdx.x; e < n; e += gridDim.x) {  // uniform per block
+      const int m = J.wlong[e];
+      const int tb = (kMax ? J.largest : J.smallest)[m];  // valid: the lists are non-empty
+      int hit = wis_first<T, kMax>(J, sad, ent, off[m] + (int)threadIdx.x, off[m + 1], 256, tb,
+                                   J.g[tb]);
+      for (int o = 16; o > 0; o >>= 1) hit = min(hit, __shfl_xor_sync(0xffffffffu, hit, o));
+      if (lane_id() == 0) part[threadIdx.x >> 5] = hit;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; ++w) hit = min(hit, part[w]);
+        (kMax ? J.first_s : J.first_sj)[m] = hit;
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -1979,10 +2266,9 @@ __global__ void __launch_bounds__(256) k_wis_collect(const Job<T>* __restrict__ 
   for (int base = blockIdx.x * blockDim.x; base < next; base += stride) {
     const int m = base + threadIdx.x;
     bool hit = false;
-    if (m < next && first[m] != kInf) {
+    if (m < next && first[m] != kInf) {  // kept: the scan is incremental
       hit = true;
       const int s = sad[first[m] / kRowStride];
-      first[m] = kInf;
       const int t = best[m];
       if (fix) {
         const T gt = J.g[t], gs = J.g[s];
@@ -2070,18 +2356,26 @@ __global__ void k_ctl(Job<T>* jobs, const __grid_constant__ Sel sel, int op) {
       break;
     case OP_SADDLE_BEGIN:
       c[C_WSC] = c[C_TOUCHED] = 0;
+      c[C_WEP2] += 1;  // next wrong-saddle epoch, empty queue
+      c[C_AFF] = c[C_WLONG] = 0;
       break;
     case OP_SLOOPS_JOIN_BEGIN:
       c[C_WMIN] = c[C_WMIN2] = c[C_TOUCHED] = 0;
       break;
     case OP_SADDLE_JOIN_BEGIN:
       c[C_WSCJ] = c[C_TOUCHED] = 0;
+      c[C_WEP1] += 1;
+      c[C_AFF] = c[C_WLONG] = 0;
       break;
     case OP_DETECT3_BEGIN:
       c[C_WMC] = c[C_WMC2] = c[C_WSC] = 0;
+      c[C_WEP2] += 1;
+      c[C_AFF] = c[C_WLONG] = 0;
       break;
     case OP_DETECT3_JOIN_BEGIN:
       c[C_WMIN] = c[C_WMIN2] = c[C_WSCJ] = 0;
+      c[C_WEP1] += 1;
+      c[C_AFF] = c[C_WLONG] = 0;
       break;
     default:
       break;

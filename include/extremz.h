@@ -399,7 +399,7 @@ long long extremz_job_footprint(int dtype, int width, int height, int depth);
  * in main() (src/ExtreM_cuda.cu:4997-5185).
  *
  * The whole workspace is a static device array sized for at most
- * EXTREMZ_NOALLOC_MAX_VOXELS voxels (about 26 MB, held by every GPU that loads
+ * EXTREMZ_NOALLOC_MAX_VOXELS voxels (about 31 MB, held by every GPU that loads
  * the library until the process exits); larger fields return
  * EXTREMZ_TOO_LARGE without touching the device.  The call makes no
  * cudaMalloc, cudaFree or other allocating call.  Inputs and outputs are the
