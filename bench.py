@@ -70,16 +70,20 @@ SERVE_RESERVE_BYTES = 48 << 30
 PARAMS = dict(q=4, edit_type=1, thr=0.0, max_outer=1000, max_cloop_rounds=100000,
               final_join=True)
 
-# Dominant work: the manifold round of the decompressed field, one launch of
-# the steepest directions (k_direction, kernel class "direction") and one of
-# the pointer jumping (k_jump2, class "jump") per computed round.  Its
-# algorithmic bytes are N*(S + 8) per round: read every decompressed value
-# (S bytes) and write its two int32 labels.  Everything else the kernels move
-# (tile-compressed pointers, original roots, change marks, chain hops) is the
-# design's own traffic, not counted.  Rounds whose inputs were unchanged since
-# the previous round are not launched or return at once; they are not counted.
-DOMINANT = ("direction", "jump")
-DOMINANT_KERNEL = "manifold round (k_direction + k_jump2)"
+# Dominant work: the manifold rounds of the decompressed field, the steepest
+# directions (k_direction) and the pointer jumping (k_jump2).  A correction's
+# first round computes every tile and follows every vertex's chains (kernel
+# classes "direction_first" and "jump_first"); its algorithmic bytes are
+# N*(S + 8): read every decompressed value (S bytes) and write its two int32
+# labels.  Everything else the kernels move (tile-compressed pointers, original
+# roots, change marks, chain hops) is the design's own traffic, not counted.
+# The later rounds (classes "direction" and "jump") recompute only the tiles
+# whose values changed and follow only chains whose root was touched, so a
+# full-field byte count does not describe them; they are reported beside it.
+DOMINANT = ("direction_first", "jump_first")
+LATER = ("direction", "jump")
+DOMINANT_KERNEL = ("first manifold round of the decompressed field (k_direction + k_jump2, "
+                   "every tile and vertex)")
 # The next kernel by device time (the saddle pass after each manifold round),
 # timed beside the dominant ones in a few extra steps.
 RUNNER_UP = "rows"
@@ -101,11 +105,13 @@ def jump_design_bytes(n: int, launches: int, corrections: int) -> int:
     return 34 * n * corrections + 25 * n * (launches - corrections)
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one manifold
-# round (k_direction + k_jump2 of a later round, where k_direction recomputes
-# only changed tiles), by workload, from one ncu capture each; None where not
-# captured.  Filled from the profiles/ summaries.
-MEASURED_TRAFFIC = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the first
+# decompressed manifold round (k_direction + k_jump2 over every tile and
+# vertex), by workload: the ncu capture of the 256^3 float64 correction
+# (profiles/manifold_round_256cube_f64.md: 226.3 MB + 482.6 MB), and the same
+# per voxel for the 512^3 field (eight times the voxels; both kernels stream
+# whole arrays once).  Not captured for float32.
+MEASURED_TRAFFIC = {"plain256_f64": 708_900_000, "plain512_f64": 8 * 708_900_000}
 
 
 def measured_peaks():
@@ -343,31 +349,44 @@ def timed_steps(ctx, f, g, g0, field, stream, steps, profile=False, **over):
 
 
 def manifold_roofline(reps, n, s, step_ms, peak, peak_kind, traffic=None):
-    """Roofline of the decompressed manifold rounds of `reps` (corrections
-    run with the "direction" and "jump" classes timed)."""
-    dir_ms = sum(r.prof_ms["direction"] for r in reps)
-    jump_ms = sum(r.prof_ms["jump"] for r in reps)
-    rounds = sum(r.manifold_rounds - r.manifold_reused for r in reps)
+    """Roofline of the first decompressed manifold round of each correction in
+    `reps` (run with the first-round and later-round classes timed), and the
+    later rounds beside it."""
+    dir_ms = sum(r.prof_ms["direction_first"] for r in reps)
+    jump_ms = sum(r.prof_ms["jump_first"] for r in reps)
+    firsts = sum(r.prof_launches["jump_first"] for r in reps)
     ms = dir_ms + jump_ms
-    alg = round_bytes(n, s) * rounds
+    alg = round_bytes(n, s) * firsts
     achieved = alg / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
-    jb = jump_design_bytes(n, rounds, len(reps))
+    jb = jump_design_bytes(n, firsts, firsts)
     jump_gbs = jb / (jump_ms * 1e-3) / 1e9 if jump_ms > 0 else 0.0
+    later = sum(r.manifold_rounds - r.manifold_reused for r in reps) - firsts
+    ldir = sum(r.prof_ms["direction"] for r in reps)
+    ljump = sum(r.prof_ms["jump"] for r in reps)
     return {"bound": "hbm", "kernel": DOMINANT_KERNEL, "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic,
-            "traffic_note": "ncu DRAM bytes of one later manifold round (k_direction + "
-                            "k_jump2), scaled to this field by its voxel count" if traffic else None,
+            "traffic_note": "ncu DRAM bytes of the first manifold round (k_direction + "
+                            "k_jump2) of the 256^3 float64 correction, scaled to this field "
+                            "by its voxel count; the excess over the algorithmic bytes is "
+                            "the design's own arrays (tile pointers, old labels, original "
+                            "roots)" if traffic else None,
             "algorithmic_bytes_per_launch": round_bytes(n, s),
-            "algorithmic_bytes_note": "N*(S+8) per manifold round: the value read and two "
-                                      "int32 label writes per voxel",
-            "launches": rounds, "launches_reused": sum(r.manifold_reused for r in reps),
-            "kernel_ms": ms, "direction_ms": dir_ms, "jump_ms": jump_ms,
+            "algorithmic_bytes_note": "N*(S+8) per round: the value read and two int32 label "
+                                      "writes per voxel",
+            "launches": firsts, "kernel_ms": ms, "direction_ms": dir_ms, "jump_ms": jump_ms,
             "share_of_step": ms / step_ms if step_ms else None,
             "jump_design_bytes": {"kernel": "k_jump2", "bytes": jb, "achieved_gbs": jump_gbs,
                                   "frac": jump_gbs / peak,
-                                  "note": "the bytes k_jump2 itself moves (pointers, labels, "
-                                          "original roots, change marks), a lower bound"}}
+                                  "note": "the bytes k_jump2 itself moves in a first round "
+                                          "(pointers, labels, original roots, change marks, "
+                                          "34 B per voxel), a lower bound"},
+            "later_rounds": {
+                "rounds": later, "reused": sum(r.manifold_reused for r in reps),
+                "direction_ms": ldir, "jump_ms": ljump,
+                "ms_per_round": (ldir + ljump) / later if later else None,
+                "share_of_step": (ldir + ljump) / step_ms if step_ms else None,
+                "note": "changed tiles' directions and touched chains only"}}
 
 
 def census_of(ctx, f, g):
@@ -397,7 +416,8 @@ def measure_secondary(ctx, local, name, steps, peak, peak_kind):
     # Three warm-up corrections: a tick's launches become a CUDA graph at the
     # third sighting, so the timed steps replay graphs as the headline's do.
     correct_steps(ctx, f, g, g0, field, stream, 3)
-    ms, reps = timed_steps(ctx, f, g, g0, field, stream, steps, profile=list(DOMINANT))
+    ms, reps = timed_steps(ctx, f, g, g0, field, stream, steps,
+                           profile=list(DOMINANT) + list(LATER))
     r0 = reps[-1]
     out = {"workload": name, "description": WORKLOADS[name][1], "steps": steps,
            "value": n * steps / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms / steps,
@@ -444,7 +464,8 @@ def run_ours(args, world, rank, local):
     # (ncu --nvtx --nvtx-include "timed/").
     torch.cuda.nvtx.range_push("timed")
     ev0.record(stream)
-    reps = correct_steps(ctx, f, g, g0, field, stream, args.steps, profile=list(DOMINANT))
+    reps = correct_steps(ctx, f, g, g0, field, stream, args.steps,
+                         profile=list(DOMINANT) + list(LATER))
     ev1.record(stream)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()

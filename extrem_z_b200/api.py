@@ -62,7 +62,7 @@ class Report(ctypes.Structure):
                 ("cloop_rounds", ctypes.c_int), ("manifold_rounds", ctypes.c_int),
                 ("counters", ctypes.c_int * 11), ("error_bits", ctypes.c_int),
                 ("kernel_launches", ctypes.c_longlong),
-                ("prof_ms", ctypes.c_float * 10), ("prof_launches", ctypes.c_int * 10),
+                ("prof_ms", ctypes.c_float * 12), ("prof_launches", ctypes.c_int * 12),
                 ("manifold_reused", ctypes.c_int), ("cp_counts", ctypes.c_int * 4),
                 ("graph_launches", ctypes.c_int), ("host_bytes_back", ctypes.c_longlong)]
 
@@ -100,7 +100,7 @@ FLAG_NO_TMA = 2
 FLAG_WN_ASCENDING = 4
 PROFILE_CLASS_SHIFT = 8
 KCLASS_NAMES = ("setup_classify", "classify_detect", "direction", "jump", "propose", "apply",
-                "rows", "wrong_nbr", "fixpath", "other")
+                "rows", "wrong_nbr", "fixpath", "other", "direction_first", "jump_first")
 
 
 @dataclasses.dataclass

@@ -43,7 +43,7 @@ enum Phase : int {
 // Kernel classes for the optional per-class timing (extremz_report.prof_*).
 enum KClass : int {
   K_SETUP = 0, K_DETECT, K_DIRECTION, K_JUMP, K_PROPOSE, K_APPLY, K_ROWS, K_WRONG_NBR,
-  K_FIXPATH, K_OTHER, K_NUM
+  K_FIXPATH, K_OTHER, K_DIRECTION_FIRST, K_JUMP_FIRST, K_NUM
 };
 
 // Program counter of a job, in the order phases run within a tick.
@@ -1148,7 +1148,7 @@ class BatchEngine {
           for (int i : busy) (slots_[i].manifold_rounds == 0 ? fresh : later).push_back(i);
           if (!fresh.empty()) {
             const Sel ft = make_sel(fresh, true);
-            launch(K_DIRECTION, k_direction<T, true>, ft.off[ft.n], 256, jobs, ft);
+            launch(K_DIRECTION_FIRST, k_direction<T, true>, ft.off[ft.n], 256, jobs, ft);
           }
           if (!later.empty()) {
             const Sel ls = make_sel(later, false), lt = make_sel(later, true);
@@ -1159,7 +1159,7 @@ class BatchEngine {
                    256, jobs, ls);
           }
           if (!fresh.empty())
-            launch(K_JUMP, k_jump2<T, true, false>, grid_, 256, jobs, make_sel(fresh, false));
+            launch(K_JUMP_FIRST, k_jump2<T, true, false>, grid_, 256, jobs, make_sel(fresh, false));
           if (!later.empty())
             launch(K_JUMP, k_jump2<T, true, true>, grid_, 256, jobs, make_sel(later, false));
           launch(K_OTHER, k_clear_changed<T>, grid_, 256, jobs, bs);
@@ -1381,21 +1381,21 @@ class BatchEngine {
            (const int8_t*)J.otype, N, jh.nb, (const int*)jh.bcount,
            J.sad2, J.sad1, J.maxima, J.minima);
     launch(K_OTHER, k_ext_index<T>, grid_, 256, J);
-    launch(K_SETUP, k_rows<T, true>, grid_, 256, J, J.f, (const int*)J.ds, (const int*)J.sad2,
-           (int)C_NS2, J.orow2, J.ocnt2, J.orm2, J.oend2);
-    launch(K_SETUP, k_rows<T, false>, grid_, 256, J, J.f, (const int*)J.as, (const int*)J.sad1,
-           (int)C_NS1, J.orow1, J.ocnt1, J.orm1, J.oend1);
-    // Decompressed row slots start at zero: the reference's rows are fresh
-    // cudaMalloc memory read before first written (:5338-5341, :3128-3130).
-    if (ns2) EZ_CHECK(cudaMemsetAsync(J.drow2, 0, (size_t)ns2 * 2 * 4, st_));
-    if (ns1) EZ_CHECK(cudaMemsetAsync(J.drow1, 0, (size_t)ns1 * 2 * 4, st_));
+    // Per side: the rows (with their compact copies, each named extremum's
+    // extreme saddle key and entry count), the entry lists' offsets, then the
+    // extreme saddle ids and the entries.  The sides share the selection
+    // scratch (ext_key, ext_id), so they go one after the other.  Rows name
+    // only extrema, so a side with rows has extrema.
     if (nmax) {
       launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, K(0), (long long)nmax);
       launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, -1, (long long)nmax);
       EZ_CHECK(cudaMemsetAsync(J.moff2, 0, (size_t)(nmax + 1) * 4, st_));
-      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 0);
+    }
+    launch(K_SETUP, k_rows<T, true>, grid_, 256, J, J.f, (const int*)J.ds, (const int*)J.sad2,
+           (int)C_NS2, J.orow2, J.ocnt2, J.orm2, J.oend2);
+    if (nmax) {
       EZ_RUN(entry_lists(J.moff2, J.wstamp2, nmax, chunk));
-      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J, 1);
+      launch(K_OTHER, k_extreme_saddle<T, true>, grid_, 256, J);
       EZ_CHECK(cudaMemsetAsync(J.wstamp2, 0, (size_t)nmax * 4, st_));
       EZ_CHECK(cudaMemcpyAsync(J.largest, J.ext_id, nmax * 4, cudaMemcpyDeviceToDevice, st_));
       launch(K_OTHER, k_fill<int>, grid_, 256, J.first1, kInf, (long long)nmax);
@@ -1406,9 +1406,12 @@ class BatchEngine {
       launch(K_OTHER, k_fill<K>, grid_, 256, J.ext_key, ~K(0), (long long)nmin);
       launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, kInf, (long long)nmin);
       EZ_CHECK(cudaMemsetAsync(J.moff1, 0, (size_t)(nmin + 1) * 4, st_));
-      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 0);
+    }
+    launch(K_SETUP, k_rows<T, false>, grid_, 256, J, J.f, (const int*)J.as, (const int*)J.sad1,
+           (int)C_NS1, J.orow1, J.ocnt1, J.orm1, J.oend1);
+    if (nmin) {
       EZ_RUN(entry_lists(J.moff1, J.wstamp1, nmin, chunk));
-      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J, 1);
+      launch(K_OTHER, k_extreme_saddle<T, false>, grid_, 256, J);
       EZ_CHECK(cudaMemsetAsync(J.wstamp1, 0, (size_t)nmin * 4, st_));
       EZ_CHECK(cudaMemcpyAsync(J.smallest, J.ext_id, nmin * 4, cudaMemcpyDeviceToDevice, st_));
       launch(K_OTHER, k_fill<int>, grid_, 256, J.ext_id, kInf, (long long)nmin);
@@ -1416,6 +1419,10 @@ class BatchEngine {
       launch(K_OTHER, k_fill<int>, grid_, 256, J.first_sj, kInf, (long long)nmin);
       EZ_CHECK(cudaMemsetAsync(J.flag_min2, 0, nmin * 4, st_));
     }
+    // Decompressed row slots start at zero: the reference's rows are fresh
+    // cudaMalloc memory read before first written (:5338-5341, :3128-3130).
+    if (ns2) EZ_CHECK(cudaMemsetAsync(J.drow2, 0, (size_t)ns2 * 2 * 4, st_));
+    if (ns1) EZ_CHECK(cudaMemsetAsync(J.drow1, 0, (size_t)ns1 * 2 * 4, st_));
     // Every tile's pointers are computed in the first manifold round.
     EZ_CHECK(cudaMemsetAsync(J.tdirty, 1, (size_t)jh.ntiles, st_));
     // Block stamps start below the first round's; no root is touched.

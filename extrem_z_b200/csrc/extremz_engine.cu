@@ -442,6 +442,7 @@ static int classify_one(BatchEngine<T>& e, cudaStream_t st, const T* field, int 
 // the library keeps it until the process exits.
 // ---------------------------------------------------------------------------
 constexpr long long kNoAllocMaxVoxels = EXTREMZ_NOALLOC_MAX_VOXELS;
+static_assert(K_NUM == EXTREMZ_NUM_KCLASS, "the report has one timing slot per kernel class");
 // Engine arrays (descriptors, tile maps, counters) first, then one job's
 // worst-case workspace (every voxel a critical point of every kind, 8-byte
 // values: 442 bytes per voxel plus per-array alignment).

@@ -778,8 +778,10 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
       const int qstride = gridDim.x * blockDim.x;
       for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += qstride) {
         const int v0 = q << 2;
-        const int4 O1 = *reinterpret_cast<const int4*>(ra + v0);
-        const int4 O2 = *reinterpret_cast<const int4*>(rb + v0);
+        // A job's first round writes every label (its change bitset starts
+        // full, and the stored labels may be another job's): no old labels.
+        const int4 O1 = kLater ? *reinterpret_cast<const int4*>(ra + v0) : make_int4(-1, -1, -1, -1);
+        const int4 O2 = kLater ? *reinterpret_cast<const int4*>(rb + v0) : make_int4(-1, -1, -1, -1);
         const int o1[4] = {O1.x, O1.y, O1.z, O1.w}, o2[4] = {O2.x, O2.y, O2.z, O2.w};
         if constexpr (kLater) {
           unsigned hit = 0u;
@@ -1114,11 +1116,13 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
   const int stride = gridDim.x * blockDim.x;
   const Dims g = J.dim;
   const int WH = g.W * g.H;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
-    const int s = sad[i];
+  for (int base = blockIdx.x * blockDim.x; base < ns; base += stride) {  // uniform per warp
+    const int i = base + threadIdx.x;
+    const bool act = i < ns;
+    const int s = act ? sad[i] : 0;
     int x, y, z;
     coords(s, g, x, y, z);
-    const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
+    const int valid = act ? valid_mask(boundary_code(x, y, z, g.W, g.H, g.D)) : 0;
     const T sv = a[s];
     // Neighbour values, then the side's labels, then their values: three
     // batches of independent loads; the sort below compares cached values.
@@ -1195,19 +1199,44 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
     int last = -1;
 #pragma unroll
     for (int d = 0; d < kNumDirs; ++d) {
-      if (d < cnt) out[d] = srt[d];
+      if (act && d < cnt) out[d] = srt[d];
       if (d == cnt - 1) last = srt[d];
     }
-    out[14] = cnt;
     // The compact copies the per-round scans read: the count, the first four
     // entries as extremum indices (-1 past the count), the first and the last
     // entry as labels and as extremum indices.
     int m[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) m[p] = p < cnt ? J.ext[srt[p]] : -1;
-    ocnt[i] = (uint8_t)cnt;
-    orm[i] = make_int4(m[0], m[1], m[2], m[3]);
-    oend[i] = make_int4(cnt > 0 ? srt[0] : -1, last, m[0], cnt > 0 ? J.ext[last] : -1);
+    if (act) {
+      out[14] = cnt;
+      ocnt[i] = (uint8_t)cnt;
+      orm[i] = make_int4(m[0], m[1], m[2], m[3]);
+      oend[i] = make_int4(cnt > 0 ? srt[0] : -1, last, m[0], cnt > 0 ? J.ext[last] : -1);
+    }
+    // The first pass of findLargestSaddlePerMax / findSmallestSaddlePerMin
+    // (:4890-4940) over this row: each named extremum's largest (smallest)
+    // saddle key, and the number of entries naming it (a row's first entry
+    // per extremum: rows are sorted, so a repeated label is the entry
+    // before), for the per-extremum entry lists of the incremental
+    // wrong-saddle scan (filled by k_extreme_saddle).  Lanes naming the same
+    // extremum share one atomic; a read first skips most key atomics (the
+    // key only moves one way).
+    using KK = typename KeyOf<T>::K;
+    const KK key = KeyOf<T>::enc(sv + T(0));  // -0 and +0 compare equal
+    int* mcount = kAsc ? J.moff2 : J.moff1;
+#pragma unroll
+    for (int p = 0; p < kNumDirs; ++p) {
+      if (!__any_sync(0xffffffffu, p < cnt)) break;
+      const int mp = p < cnt ? (p < 4 ? m[p] : J.ext[srt[p]]) : -1;
+      const bool fresh = mp >= 0 && (p == 0 || srt[p] != srt[p > 0 ? p - 1 : 0]);
+      const unsigned grp = __match_any_sync(0xffffffffu, fresh ? mp : -1);
+      if (fresh && (grp & ((1u << lane_id()) - 1u)) == 0u) atomicAdd(mcount + mp, __popc(grp));
+      if (mp >= 0 && (kAsc ? key > J.ext_key[mp] : key < J.ext_key[mp])) {
+        if (kAsc) atomicMax(J.ext_key + mp, key);
+        else atomicMin(J.ext_key + mp, key);
+      }
+    }
   }
 }
 
@@ -1215,26 +1244,27 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
 // Largest saddle per maximum / smallest per minimum on the ORIGINAL field
 // (findLargestSaddlePerMax / findSmallestSaddlePerMin :4890-4940): the CSR
 // max->saddle table is never materialised; every (row, entry) pair votes.
-// Pass 1 selects the extreme value key, pass 2 the extreme id at that value.
+// k_rows selects the extreme value key per extremum (and counts the entries
+// naming it); this pass selects the extreme id at that key and files the
+// entries into the per-extremum lists (cursors start at the scanned offsets).
 // ---------------------------------------------------------------------------
 template <class T, bool kMax>
-__global__ void __launch_bounds__(256) k_extreme_saddle(Job<T> J, int pass) {
+__global__ void __launch_bounds__(256) k_extreme_saddle(Job<T> J) {
   using K = typename KeyOf<T>::K;
   const int ns = J.ctr[kMax ? C_NS2 : C_NS1];
   const int* sad = kMax ? J.sad2 : J.sad1;
   const int* rows = kMax ? J.orow2 : J.orow1;
   const uint8_t* ocnt = kMax ? J.ocnt2 : J.ocnt1;
-  int* cnt_or_cur = pass == 0 ? (kMax ? J.moff2 : J.moff1) : (kMax ? J.wstamp2 : J.wstamp1);
+  int* cur = kMax ? J.wstamp2 : J.wstamp1;
   int* ent = kMax ? J.ment2 : J.ment1;
   const int stride = gridDim.x * blockDim.x;
-  // Uniform per warp: the entries of the lanes' rows go through the atomics
-  // together, so that lanes naming the same extremum (neighbouring saddles
-  // usually do) share one atomic.
+  // Uniform per warp: lanes naming the same extremum (neighbouring saddles
+  // usually do) share one cursor atomic.
   for (int base = blockIdx.x * blockDim.x; base < ns; base += stride) {
     const int i = base + threadIdx.x;
     const int cnt = i < ns ? ocnt[i] : 0;
     const int s = i < ns ? sad[i] : 0;
-    const K key = KeyOf<T>::enc(J.f[i < ns ? s : 0] + T(0));  // -0 and +0 compare equal
+    const K key = KeyOf<T>::enc(J.f[s] + T(0));  // -0 and +0 compare equal
     const int* row = rows + (long long)(i < ns ? i : 0) * kRowStride;
     // The first four entries as extremum indices from the compact copy
     // (k_rows), longer rows' tails through the index map.
@@ -1244,33 +1274,21 @@ __global__ void __launch_bounds__(256) k_extreme_saddle(Job<T> J, int pass) {
     for (int p = 0; p < pmax; ++p) {
       int m = -1;
       if (p < cnt) m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : J.ext[row[p]];
-      // Rows are sorted, so a repeated label is the entry before: the
-      // per-extremum lists keep a row's first entry naming the extremum (a
-      // later one has the same saddle and a larger key).
+      // A row's first entry per extremum only, as counted by k_rows.
       const bool fresh = m >= 0 && m != prev;
       if (m >= 0) prev = m;
       const unsigned grp = __match_any_sync(0xffffffffu, fresh ? m : -1);
       const int leader = __ffs(grp) - 1;
       const unsigned below = grp & ((1u << lane_id()) - 1u);
       int at = 0;
-      if (fresh && below == 0u) at = atomicAdd(cnt_or_cur + m, __popc(grp));
+      if (fresh && below == 0u) at = atomicAdd(cur + m, __popc(grp));
       at = __shfl_sync(0xffffffffu, at, leader) + __popc(below);
       if (m < 0) continue;
-      // Largest (smallest) saddle key per extremum, then the largest
-      // (smallest) id at that key; a read first skips most atomics (the
-      // key only moves one way).
-      if (pass == 0) {
-        if (kMax ? key > J.ext_key[m] : key < J.ext_key[m]) {
-          if (kMax) atomicMax(J.ext_key + m, key);
-          else atomicMin(J.ext_key + m, key);
-        }
-      } else {
-        if (J.ext_key[m] == key) {
-          if (kMax) atomicMax(J.ext_id + m, s);
-          else atomicMin(J.ext_id + m, s);
-        }
-        if (fresh) ent[at] = i * kRowStride + p;
+      if (J.ext_key[m] == key) {
+        if (kMax) atomicMax(J.ext_id + m, s);
+        else atomicMin(J.ext_id + m, s);
       }
+      if (fresh) ent[at] = i * kRowStride + p;
     }
   }
 }

@@ -103,10 +103,13 @@ typedef struct {
 
 /* Kernel classes of extremz_report.prof_*: 0 setup (classification, labels and
  * rows of the original field), 1 fused classification + mismatch detection,
- * 2 steepest directions and 3 pointer jumping of the decompressed field,
+ * 2 steepest directions and 3 pointer jumping of the decompressed field in the
+ * manifold rounds after a correction's first (changed tiles, touched chains),
  * 4 proposals, 5 apply, 6 saddle pass (decompressed rows and wrong-neighbour
- * seeds), 7 wrong-neighbour resolution, 8 path walks, 9 everything else. */
-#define EXTREMZ_NUM_KCLASS 10
+ * seeds), 7 wrong-neighbour resolution, 8 path walks, 9 everything else,
+ * 10 steepest directions and 11 pointer jumping of the decompressed field in
+ * a correction's first manifold round (every tile, every vertex). */
+#define EXTREMZ_NUM_KCLASS 12
 
 /* Outcome of one correction. counters[] are the eleven host counters of the
  * reference's loop test (:5603-5605) at exit: wrong split / join neighbours,
