@@ -445,7 +445,7 @@ constexpr long long kNoAllocMaxVoxels = EXTREMZ_NOALLOC_MAX_VOXELS;
 static_assert(K_NUM == EXTREMZ_NUM_KCLASS, "the report has one timing slot per kernel class");
 // Engine arrays (descriptors, tile maps, counters) first, then one job's
 // worst-case workspace (every voxel a critical point of every kind, 8-byte
-// values: 442 bytes per voxel plus per-array alignment).
+// values: 443 bytes per voxel plus per-array alignment).
 constexpr size_t kNoAllocEngineBytes = 1u << 18;
 constexpr size_t kNoAllocScratchBytes = kNoAllocEngineBytes + (size_t)kNoAllocMaxVoxels * 448 + (1u << 20);
 // Both engines (float and double) carve their descriptor, tile-map and

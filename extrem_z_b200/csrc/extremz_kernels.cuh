@@ -49,7 +49,8 @@ struct Job {
   uint8_t* mis;       // per vertex: 1 if dds != ds, 2 if das != as
   unsigned* vchg;     // bitset: vertices whose value changed since the last computed round
   unsigned* edited;   // bitset: vertices whose value changed in this correction (or null)
-  uint8_t* dirtyv;    // per vertex: an input of its saddle rows changed this round
+  uint8_t* dirtyv;    // per vertex: the round stamp's low byte when an input of its saddle
+                      // rows changed in that round
   int* bdirty;        // per 1024-id block: the round stamp when some dirtyv byte in it was
                       // set (when N % 4 == 0)
   uint8_t* has2; uint8_t* has1;  // per saddle row: its wrong-neighbour seed bit
@@ -63,7 +64,8 @@ struct Job {
                                          // the tiles whose pointers this round recomputes
 
   int* sad2; int* sad1; int* maxima; int* minima;
-  int* orow2; int* orow1;  // original rows of kRowStride ints
+  int* orow2; int* orow1;  // original rows of kRowStride ints: entries 4 .. count-1 as
+                           // extremum indices (the first four are in orm2 / orm1)
   int4* orm2; int4* orm1;  // per row: its first four entries as extremum indices (-1 past the count)
   int4* oend2; int4* oend1;  // per row: first and last entry, then both as extremum indices
   int* drow2; int* drow1;  // decompressed rows: 2 persistent slots per row, see k_saddle_pass
@@ -237,17 +239,16 @@ __device__ __forceinline__ void tile_masks(const Tile<T>& s, int tx, int ty, int
                                            int& lm, int& um) {
   const T c = s.v[tz + 1][ty + 1][tx + kXOff];
   lm = 0;
-  um = 0;
 #pragma unroll
   for (int d = 0; d < kNumDirs; ++d) {
     const T nv = s.v[tz + 1 + dir_z(d)][ty + 1 + dir_y(d)][tx + kXOff + dir_x(d)];
     const bool lower = dir_neighbour_is_before(d) ? (nv <= c) : (nv < c);
-    const bool upper = dir_neighbour_is_before(d) ? (nv > c) : (nv >= c);
     lm |= (int)lower << d;
-    um |= (int)upper << d;
   }
+  // Values and ids order the vertices totally: a valid neighbour is upper
+  // exactly when it is not lower.
   lm &= valid;
-  um &= valid;
+  um = valid & ~lm;
 }
 
 // Vertex type from the masks (classifyVertex_CUDA :3835-3853): maximum when no
@@ -325,13 +326,16 @@ __global__ void __launch_bounds__(256) k_classify(const Job<T>* __restrict__ job
   }
   if (kDetect) __syncthreads();
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  // A tile off the field's faces has every direction valid at every voxel.
+  const bool interior = bx > 0 && by > 0 && bz > 0 && bx + TX < g.W && by + TY < g.H &&
+                        bz + TZ < g.D;
   for (int tz = 0; tz < TZ; ++tz) {
     const int x = bx + tx, y = by + ty, z = bz + tz;
     const bool in = x < g.W && y < g.H && z < g.D;
     if (in) {
       const int v = x + y * g.W + z * g.W * g.H;
-      const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
-      const int valid = valid_mask(bc);
+      const int bc = interior ? 0 : boundary_code(x, y, z, g.W, g.H, g.D);
+      const int valid = interior ? (1 << kNumDirs) - 1 : valid_mask(bc);
       int lm, um;
       tile_masks(s, tx, ty, tz, valid, lm, um);
       const int t = type_from_masks(lm, um, valid, bc, J.tb);
@@ -520,20 +524,8 @@ __device__ __forceinline__ void steepest_dirs(const Tile<T>& s, int tx, int ty, 
   }
 }
 
-// Next step of a path in tile terms: the local index of the next voxel when
-// it lies in the tile, kExit when the path leaves the tile (the global id of
-// the first outside vertex goes to *exit_gid), kRoot when the voxel is a root.
+// Next-step codes of the in-tile path following (besides local indices).
 constexpr int kExit = -1, kRoot = -2;
-__device__ __forceinline__ int next_in_tile(int d, int tx, int ty, int tz, int v, int W, int WH,
-                                            int* exit_gid) {
-  if (d < 0) return kRoot;
-  const int dx = ddx(d), dy = ddy(d), dz = ddz(d);
-  const int nx = tx + dx, ny = ty + dy, nz = tz + dz;
-  if ((unsigned)nx < (unsigned)TX && (unsigned)ny < (unsigned)TY && (unsigned)nz < (unsigned)TZ)
-    return (nz * TY + ny) * TX + nx;
-  *exit_gid = v + dx + dy * W + dz * WH;
-  return kExit;
-}
 
 // Follows next-pointers inside the tile from local voxel li to the path's
 // exit (global id of the first outside vertex) or root.
@@ -574,19 +566,36 @@ __device__ __noinline__ bool direction_tile(const Job<T>& J, Tile<T>& s, uint64_
     return false;
   }
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  // A tile off the field's faces has every direction valid at every voxel.
+  const bool interior = bx > 0 && by > 0 && bz > 0 && bx + TX < g.W && by + TY < g.H &&
+                        bz + TZ < g.D;
   for (int tz = 0; tz < TZ; ++tz) {
     const int li = (tz * TY + ty) * TX + tx;
     const int x = bx + tx, y = by + ty, z = bz + tz;
     int hd = -1, ld = -1;
     const bool in = x < g.W && y < g.H && z < g.D;
-    if (in) {
+    if (interior) {
+      steepest_dirs<T, true>(s, tx, ty, tz, (1 << kNumDirs) - 1, hd, ld);
+    } else if (in) {
       const int bc = boundary_code(x, y, z, g.W, g.H, g.D);
       if (bc == 0) steepest_dirs<T, true>(s, tx, ty, tz, (1 << kNumDirs) - 1, hd, ld);
       else steepest_dirs<T, false>(s, tx, ty, tz, valid_mask(bc), hd, ld);
     }
     const int v = x + y * g.W + z * WH;
-    hnext[li] = (int16_t)(in ? next_in_tile(hd, tx, ty, tz, v, g.W, WH, &hexit[li]) : kRoot);
-    lnext[li] = (int16_t)(in ? next_in_tile(ld, tx, ty, tz, v, g.W, WH, &lexit[li]) : kRoot);
+    // Next step in tile terms: the local index when it stays in the tile,
+    // kExit (the first outside vertex to the exit slot) when it leaves it,
+    // kRoot at a root.
+    auto step = [&](int d, int* exit_gid) {
+      if (d < 0) return kRoot;
+      const int dx = ddx(d), dy = ddy(d), dz = ddz(d);
+      const int nx = tx + dx, ny = ty + dy, nz = tz + dz;
+      if ((unsigned)nx < (unsigned)TX && (unsigned)ny < (unsigned)TY && (unsigned)nz < (unsigned)TZ)
+        return (nz * TY + ny) * TX + nx;
+      *exit_gid = v + dx + dy * g.W + dz * WH;
+      return kExit;
+    };
+    hnext[li] = (int16_t)(in ? step(hd, &hexit[li]) : kRoot);
+    lnext[li] = (int16_t)(in ? step(ld, &lexit[li]) : kRoot);
   }
   __syncthreads();
   for (int tz = 0; tz < TZ; ++tz) {
@@ -602,7 +611,7 @@ __device__ __noinline__ bool direction_tile(const Job<T>& J, Tile<T>& s, uint64_
 
 // Setup: every tile of the original field, one block per tile.
 template <class T, bool kDec>
-__global__ void __launch_bounds__(256) k_direction(const Job<T>* __restrict__ jobs,
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 4 : 6) k_direction(const Job<T>* __restrict__ jobs,
                                                    const __grid_constant__ Sel sel) {
   __shared__ Tile<T> s;
   __shared__ uint64_t bar;
@@ -750,7 +759,8 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
       // value, either label, or the value of either label's root).  The
       // change bitset starts full, so the first round marks every vertex.
       const unsigned c1 = vchg[u1 >> 5] >> (u1 & 31), c2 = vchg[u2 >> 5] >> (u2 & 31);
-      dirtyv[v] = (uint8_t)((o1 != u1) | (o2 != u2) | ((c0 | c1 | c2) & 1u));
+      dirtyv[v] = ((o1 != u1) | (o2 != u2) | ((c0 | c1 | c2) & 1u)) ? (uint8_t)J.ctr[C_WNSTAMP]
+                                                                    : (uint8_t)0;
       mis[v] = (uint8_t)((u1 != r1) | (u2 != r2) << 1);
     }
     ra[v] = u1;
@@ -763,7 +773,9 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
       // the vertex-per-thread loop, with eight chains interleaved.  A quad
       // with a changed-input byte stamps its 1024-id block (bdirty, read by
       // the saddle pass; its address is read where it is used: kept in a
-      // register for the whole loop it costs spills).
+      // register for the whole loop it costs spills).  Changed-input bytes
+      // are round stamps (low byte): a quad that is not followed leaves its
+      // bytes, which then read as unchanged.
       //
       // kLater: a vertex's label on a side can change only when its path
       // crosses a tile whose pointers this round recomputed, and every vertex
@@ -771,26 +783,30 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
       // labels is a root marked by k_direction_list (rtouch2 / rtouch1: the
       // old labels of the recomputed tiles' vertices) keeps its labels and
       // mismatch bits and has no changed input (a changed value, own or of a
-      // root, lies in a recomputed tile too); only its changed-input bytes
-      // are written, as zeros.
+      // root, lies in a recomputed tile too).
       const int stamp = J.ctr[C_WNSTAMP];
-      const int nq = N >> 2;
-      const int qstride = gridDim.x * blockDim.x;
-      for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += qstride) {
-        const int v0 = q << 2;
+      const unsigned st8 = (unsigned)stamp & 0xffu;
+      // Returns the quad's labels through u1 / u2 (the old ones when it is
+      // not followed) and the old ones through o1 / o2 (-1 in a first round).
+      auto quad = [&](int v0, int* u1, int* u2, int* o1, int* o2) {
         // A job's first round writes every label (its change bitset starts
         // full, and the stored labels may be another job's): no old labels.
         const int4 O1 = kLater ? *reinterpret_cast<const int4*>(ra + v0) : make_int4(-1, -1, -1, -1);
         const int4 O2 = kLater ? *reinterpret_cast<const int4*>(rb + v0) : make_int4(-1, -1, -1, -1);
-        const int o1[4] = {O1.x, O1.y, O1.z, O1.w}, o2[4] = {O2.x, O2.y, O2.z, O2.w};
+        o1[0] = O1.x; o1[1] = O1.y; o1[2] = O1.z; o1[3] = O1.w;
+        o2[0] = O2.x; o2[1] = O2.y; o2[2] = O2.z; o2[3] = O2.w;
         if constexpr (kLater) {
           unsigned hit = 0u;
 #pragma unroll
           for (int k = 0; k < 4; ++k)
             hit |= (J.rtouch2[o1[k] >> 5] >> (o1[k] & 31)) | (J.rtouch1[o2[k] >> 5] >> (o2[k] & 31));
           if (!(hit & 1u)) {
-            *reinterpret_cast<unsigned*>(dirtyv + v0) = 0u;
-            continue;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              u1[k] = o1[k];
+              u2[k] = o2[k];
+            }
+            return;
           }
         }
         const int4 A = *reinterpret_cast<const int4*>(a + v0);
@@ -801,7 +817,8 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
           R2 = *reinterpret_cast<const int4*>(oas + v0);
         }
         const unsigned cw = vchg[v0 >> 5] >> (v0 & 31);
-        int u1[4] = {A.x, A.y, A.z, A.w}, u2[4] = {B.x, B.y, B.z, B.w};
+        u1[0] = A.x; u1[1] = A.y; u1[2] = A.z; u1[3] = A.w;
+        u2[0] = B.x; u2[1] = B.y; u2[2] = B.z; u2[3] = B.w;
         // One hop of every unfinished chain per iteration: the eight loads
         // depend only on their own chain, so they are all in flight at once.
         bool more = true;
@@ -831,16 +848,14 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
           n1 |= o1[k] != u1[k];
           n2 |= o2[k] != u2[k];
           const unsigned d = (o1[k] != u1[k]) | (o2[k] != u2[k]) | ((cw >> k | c1 | c2) & 1u);
-          dv |= d << (8 * k);
+          dv |= (d ? st8 : 0u) << (8 * k);
         }
         *reinterpret_cast<unsigned*>(dirtyv + v0) = dv;
         // Stores that would rewrite the stored value are skipped.  The
         // mismatch bits follow the labels alone (the original roots are
         // fixed), so a group whose labels did not change keeps last round's
-        // bits.  A job's first round writes every group (its change bitset
-        // starts full, so dv is set everywhere; the stored labels may be
-        // another job's).
-        if (kLater ? (n1 || n2) : dv != 0) {
+        // bits.
+        if (kLater ? (n1 || n2) : true) {
           if constexpr (kLater) {
             R1 = *reinterpret_cast<const int4*>(ods + v0);
             R2 = *reinterpret_cast<const int4*>(oas + v0);
@@ -855,6 +870,12 @@ __global__ void __launch_bounds__(256, 4) k_jump2(const Job<T>* __restrict__ job
         if (n1) *reinterpret_cast<int4*>(ra + v0) = make_int4(u1[0], u1[1], u1[2], u1[3]);
         if (n2) *reinterpret_cast<int4*>(rb + v0) = make_int4(u2[0], u2[1], u2[2], u2[3]);
         if (dv) J.bdirty[v0 >> 10] = stamp;
+      };
+      const int nq = N >> 2;
+      const int qstride = gridDim.x * blockDim.x;
+      for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += qstride) {
+        int u1[4], u2[4], o1[4], o2[4];
+        quad(q << 2, u1, u2, o1, o2);
       }
       continue;
     }
@@ -1107,7 +1128,7 @@ __device__ constexpr unsigned char kSort14[kSort14Size][2] = {
     {7, 9},  {11, 13}, {1, 2},  {3, 4},   {5, 6},   {7, 8},   {9, 10},  {11, 12}};
 
 template <class T, bool kAsc>
-__global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
+__global__ void __launch_bounds__(256, 4) k_rows(Job<T> J, const T* __restrict__ a,
                                               const int* __restrict__ lab, const int* __restrict__ sad,
                                               int ns_slot, int* __restrict__ rows,
                                               uint8_t* __restrict__ ocnt, int4* __restrict__ orm,
@@ -1198,18 +1219,17 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
     }
     int last = -1;
 #pragma unroll
-    for (int d = 0; d < kNumDirs; ++d) {
-      if (act && d < cnt) out[d] = srt[d];
+    for (int d = 0; d < kNumDirs; ++d)
       if (d == cnt - 1) last = srt[d];
-    }
     // The compact copies the per-round scans read: the count, the first four
     // entries as extremum indices (-1 past the count), the first and the last
-    // entry as labels and as extremum indices.
+    // entry as labels and as extremum indices.  The row itself keeps only the
+    // entries from the fifth on, as extremum indices (below): nothing reads
+    // the others from it.
     int m[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) m[p] = p < cnt ? J.ext[srt[p]] : -1;
     if (act) {
-      out[14] = cnt;
       ocnt[i] = (uint8_t)cnt;
       orm[i] = make_int4(m[0], m[1], m[2], m[3]);
       oend[i] = make_int4(cnt > 0 ? srt[0] : -1, last, m[0], cnt > 0 ? J.ext[last] : -1);
@@ -1229,6 +1249,7 @@ __global__ void __launch_bounds__(256) k_rows(Job<T> J, const T* __restrict__ a,
     for (int p = 0; p < kNumDirs; ++p) {
       if (!__any_sync(0xffffffffu, p < cnt)) break;
       const int mp = p < cnt ? (p < 4 ? m[p] : J.ext[srt[p]]) : -1;
+      if (p >= 4 && mp >= 0) out[p] = mp;
       const bool fresh = mp >= 0 && (p == 0 || srt[p] != srt[p > 0 ? p - 1 : 0]);
       const unsigned grp = __match_any_sync(0xffffffffu, fresh ? mp : -1);
       if (fresh && (grp & ((1u << lane_id()) - 1u)) == 0u) atomicAdd(mcount + mp, __popc(grp));
@@ -1267,13 +1288,13 @@ __global__ void __launch_bounds__(256) k_extreme_saddle(Job<T> J) {
     const K key = KeyOf<T>::enc(J.f[s] + T(0));  // -0 and +0 compare equal
     const int* row = rows + (long long)(i < ns ? i : 0) * kRowStride;
     // The first four entries as extremum indices from the compact copy
-    // (k_rows), longer rows' tails through the index map.
+    // (k_rows), longer rows' tails from the row (stored as extremum indices).
     const int4 m4 = i < ns ? (kMax ? J.orm2 : J.orm1)[i] : make_int4(-1, -1, -1, -1);
     const int pmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
     int prev = -1;
     for (int p = 0; p < pmax; ++p) {
       int m = -1;
-      if (p < cnt) m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : J.ext[row[p]];
+      if (p < cnt) m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : row[p];
       // A row's first entry per extremum only, as counted by k_rows.
       const bool fresh = m >= 0 && m != prev;
       if (m >= 0) prev = m;
@@ -1595,6 +1616,7 @@ __global__ void k_clear_changed(const Job<T>* __restrict__ jobs, const __grid_co
       J.rtouch2[w] = 0u;
       J.rtouch1[w] = 0u;
     }
+
   }
 }
 
@@ -1606,11 +1628,13 @@ __device__ __forceinline__ bool saddle_inputs_changed(const Job<T>& J, int s) {
   int x, y, z;
   coords(s, g, x, y, z);
   const int valid = valid_mask(boundary_code(x, y, z, g.W, g.H, g.D));
-  int d = J.dirtyv[s];
+  // Changed-input bytes hold the low byte of the round stamp that set them.
+  const uint8_t st8 = (uint8_t)J.ctr[C_WNSTAMP];
+  bool d = J.dirtyv[s] == st8;
 #pragma unroll
   for (int k = 0; k < kNumDirs; ++k)
-    if (valid >> k & 1) d |= J.dirtyv[s + dir_x(k) + dir_y(k) * g.W + dir_z(k) * g.W * g.H];
-  return d != 0;
+    if (valid >> k & 1) d |= J.dirtyv[s + dir_x(k) + dir_y(k) * g.W + dir_z(k) * g.W * g.H] == st8;
+  return d;
 }
 
 // Fused pass over the original saddles after a manifold round, both sides in
@@ -2170,7 +2194,7 @@ __global__ void __launch_bounds__(256) k_wis_mark(const Job<T>* __restrict__ job
         const int4 m4 = orm[i];
         for (int p = 0; p < cnt; ++p) {
           const int m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w
-                                                               : J.ext[rows[(long long)i * kRowStride + p]];
+                                                               : rows[(long long)i * kRowStride + p];
           if (atomicExch(stamp + m, epoch) != epoch) J.aff[atomicAdd(J.ctr + C_AFF, 1)] = m;
         }
       }
