@@ -65,8 +65,10 @@ struct Job {
 
   int* sad2; int* sad1; int* maxima; int* minima;
   int* orow2; int* orow1;  // original rows of kRowStride ints: entries 4 .. count-1 as
-                           // extremum indices (the first four are in orm2 / orm1)
-  int4* orm2; int4* orm1;  // per row: its first four entries as extremum indices (-1 past the count)
+                           // extremum indices, -1 for a repeated label (the first four
+                           // are in orm2 / orm1)
+  int4* orm2; int4* orm1;  // per row: its first four entries as extremum indices (-1 past the
+                           // count and for a repeated label; rows are in direction order)
   int4* oend2; int4* oend1;  // per row: first and last entry, then both as extremum indices
   int* drow2; int* drow1;  // decompressed rows: 2 persistent slots per row, see k_saddle_pass
   int* largest; int* smallest;  // per maximum / minimum
@@ -1115,18 +1117,6 @@ __global__ void k_ext_index(Job<T> J) {
 // and the count are written, so entries past a shorter row keep their last
 // value, as in the reference.
 // ---------------------------------------------------------------------------
-// A sorting network for 14 entries: Batcher's odd-even merge sort of 16
-// without the comparators of the two highest positions (which would hold
-// the largest keys); the 0-1 principle checks it (every 0/1 input of 14).
-constexpr int kSort14Size = 53;
-__device__ constexpr unsigned char kSort14[kSort14Size][2] = {
-    {0, 1},  {2, 3},   {0, 2},  {1, 3},   {1, 2},   {4, 5},   {6, 7},   {4, 6},  {5, 7},
-    {5, 6},  {0, 4},   {2, 6},  {2, 4},   {1, 5},   {3, 7},   {3, 5},   {1, 2},  {3, 4},
-    {5, 6},  {8, 9},   {10, 11}, {8, 10}, {9, 11},  {9, 10},  {12, 13}, {8, 12}, {10, 12},
-    {9, 13}, {11, 13}, {9, 10}, {11, 12}, {0, 8},   {4, 12},  {4, 8},   {2, 10}, {6, 10},
-    {2, 4},  {6, 8},   {10, 12}, {1, 9},  {5, 13},  {5, 9},   {3, 11},  {7, 11}, {3, 5},
-    {7, 9},  {11, 13}, {1, 2},  {3, 4},   {5, 6},   {7, 8},   {9, 10},  {11, 12}};
-
 template <class T, bool kAsc>
 __global__ void __launch_bounds__(256, 4) k_rows(Job<T> J, const T* __restrict__ a,
                                               const int* __restrict__ lab, const int* __restrict__ sad,
@@ -1165,99 +1155,73 @@ __global__ void __launch_bounds__(256, 4) k_rows(Job<T> J, const T* __restrict__
     for (int d = 0; d < kNumDirs; ++d)
       if (lb[d] >= 0 && (!kAsc || tabs(T(val[d] - sv)) >= J.thr)) keep |= 1u << d;
     const int cnt = __popc(keep);
-    // The order of insertionSort (:1795-1811, descending) for ascending rows
-    // and of reversed_insertionSort (:1813-1829, ascending) for descending
-    // rows: by (value, label), entries with the same label being equal in
-    // both.  So any sort gives the insertion sort's row; a sorting network
-    // over order-preserving integer keys does it with static indices (the
-    // entries stay in registers).  Ascending rows flip the bits of both keys
-    // so that both orders sort ascending; left-out entries take the largest
-    // key and sort last (no finite value encodes to it).
-    int* out = rows + (long long)i * kRowStride;
-    int srt[kNumDirs];  // the row in order, left-out entries last
-    using K = typename KeyOf<T>::K;
-    if constexpr (sizeof(K) == 4) {
-      unsigned long long e[kNumDirs];  // key << 32 | label
+    // The reference sorts each row (insertionSort :1795-1811, descending, for
+    // ascending rows; reversed_insertionSort :1813-1829, ascending, for
+    // descending rows) by (value, label).  What is read back from an original
+    // row is its count, its first and last entry in that order
+    // (get_wrong_index_max / _min) and the set of extrema it names
+    // (findLargestSaddlePerMax / _Min, get_wrong_index_saddles(_join), where a
+    // repeated label adds nothing: only the row decides).  So the row is not
+    // sorted: the first and last entry come from one pass, and the entries
+    // are kept in direction order as extremum indices, a repeated label's
+    // entry as -1.
+    int fl = -1, ll = -1;
+    T fv = T(0), lv = T(0);
 #pragma unroll
-      for (int d = 0; d < kNumDirs; ++d) {
-        const K k = KeyOf<T>::enc(val[d] + T(0));  // -0 and +0 compare equal
-        const unsigned long long p = (unsigned long long)k << 32 | (unsigned)lb[d];
-        e[d] = (keep >> d & 1u) ? (kAsc ? ~p : p) : ~0ull;
-      }
-#pragma unroll
-      for (int c = 0; c < kSort14Size; ++c) {
-        const int x = kSort14[c][0], y = kSort14[c][1];
-        const unsigned long long lo = min(e[x], e[y]), hi = max(e[x], e[y]);
-        e[x] = lo;
-        e[y] = hi;
-      }
-#pragma unroll
-      for (int d = 0; d < kNumDirs; ++d) srt[d] = (int)(kAsc ? ~(unsigned)e[d] : (unsigned)e[d]);
-    } else {
-      K k[kNumDirs];
-      unsigned l[kNumDirs];
-#pragma unroll
-      for (int d = 0; d < kNumDirs; ++d) {
-        const K kd = KeyOf<T>::enc(val[d] + T(0));
-        const bool in = keep >> d & 1u;
-        k[d] = in ? (kAsc ? ~kd : kd) : ~K(0);
-        l[d] = in ? (kAsc ? ~(unsigned)lb[d] : (unsigned)lb[d]) : ~0u;
-      }
-#pragma unroll
-      for (int c = 0; c < kSort14Size; ++c) {
-        const int x = kSort14[c][0], y = kSort14[c][1];
-        const bool sw = k[x] > k[y] || (k[x] == k[y] && l[x] > l[y]);
-        const K kx = k[x], ky = k[y];
-        const unsigned lx = l[x], ly = l[y];
-        k[x] = sw ? ky : kx;
-        k[y] = sw ? kx : ky;
-        l[x] = sw ? ly : lx;
-        l[y] = sw ? lx : ly;
-      }
-#pragma unroll
-      for (int d = 0; d < kNumDirs; ++d) srt[d] = (int)(kAsc ? ~l[d] : l[d]);
+    for (int d = 0; d < kNumDirs; ++d) {
+      if (!(keep >> d & 1u)) continue;
+      // Strict comparisons: among equal entries (one label) the first kept
+      // direction stays, so first and last are never a repeat.
+      const bool first = fl < 0 || (kAsc ? above(val[d], lb[d], fv, fl) : below(val[d], lb[d], fv, fl));
+      const bool last = ll < 0 || (kAsc ? below(val[d], lb[d], lv, ll) : above(val[d], lb[d], lv, ll));
+      if (first) { fv = val[d]; fl = lb[d]; }
+      if (last) { lv = val[d]; ll = lb[d]; }
     }
-    int last = -1;
+    unsigned dup = 0u;  // kept entries whose label an earlier kept entry has
 #pragma unroll
-    for (int d = 0; d < kNumDirs; ++d)
-      if (d == cnt - 1) last = srt[d];
-    // The compact copies the per-round scans read: the count, the first four
-    // entries as extremum indices (-1 past the count), the first and the last
-    // entry as labels and as extremum indices.  The row itself keeps only the
-    // entries from the fifth on, as extremum indices (below): nothing reads
-    // the others from it.
-    int m[4];
+    for (int d = 1; d < kNumDirs; ++d)
 #pragma unroll
-    for (int p = 0; p < 4; ++p) m[p] = p < cnt ? J.ext[srt[p]] : -1;
+      for (int e = 0; e < d; ++e)
+        if ((keep >> e & keep >> d & 1u) && lb[e] == lb[d]) dup |= 1u << d;
+    int* out = rows + (long long)i * kRowStride;
     if (act) {
       ocnt[i] = (uint8_t)cnt;
-      orm[i] = make_int4(m[0], m[1], m[2], m[3]);
-      oend[i] = make_int4(cnt > 0 ? srt[0] : -1, last, m[0], cnt > 0 ? J.ext[last] : -1);
+      oend[i] = make_int4(fl, ll, fl >= 0 ? J.ext[fl] : -1, ll >= 0 ? J.ext[ll] : -1);
     }
-    // The first pass of findLargestSaddlePerMax / findSmallestSaddlePerMin
-    // (:4890-4940) over this row: each named extremum's largest (smallest)
-    // saddle key, and the number of entries naming it (a row's first entry
-    // per extremum: rows are sorted, so a repeated label is the entry
-    // before), for the per-extremum entry lists of the incremental
-    // wrong-saddle scan (filled by k_extreme_saddle).  Lanes naming the same
-    // extremum share one atomic; a read first skips most key atomics (the
-    // key only moves one way).
+    // Per kept entry, at its position among the kept ones: the first four in
+    // the compact copy, the rest in the row.  And the first pass of
+    // findLargestSaddlePerMax / findSmallestSaddlePerMin (:4890-4940) over
+    // the row: each named extremum's largest (smallest) saddle key, and the
+    // number of rows naming it, for the per-extremum entry lists of the
+    // incremental wrong-saddle scan (filled by k_extreme_saddle).  Lanes
+    // naming the same extremum share one atomic; a read first skips most key
+    // atomics (the key only moves one way).
     using KK = typename KeyOf<T>::K;
     const KK key = KeyOf<T>::enc(sv + T(0));  // -0 and +0 compare equal
     int* mcount = kAsc ? J.moff2 : J.moff1;
+    int m0 = -1, m1 = -1, m2 = -1, m3 = -1;
+    int pos = 0;
 #pragma unroll
-    for (int p = 0; p < kNumDirs; ++p) {
-      if (!__any_sync(0xffffffffu, p < cnt)) break;
-      const int mp = p < cnt ? (p < 4 ? m[p] : J.ext[srt[p]]) : -1;
-      if (p >= 4 && mp >= 0) out[p] = mp;
-      const bool fresh = mp >= 0 && (p == 0 || srt[p] != srt[p > 0 ? p - 1 : 0]);
-      const unsigned grp = __match_any_sync(0xffffffffu, fresh ? mp : -1);
+    for (int d = 0; d < kNumDirs; ++d) {
+      const bool kd = keep >> d & 1u;
+      const bool fresh = kd && !(dup >> d & 1u);
+      const int mp = fresh ? J.ext[lb[d]] : -1;
+      const unsigned grp = __match_any_sync(0xffffffffu, mp);
       if (fresh && (grp & ((1u << lane_id()) - 1u)) == 0u) atomicAdd(mcount + mp, __popc(grp));
-      if (mp >= 0 && (kAsc ? key > J.ext_key[mp] : key < J.ext_key[mp])) {
+      if (fresh && (kAsc ? key > J.ext_key[mp] : key < J.ext_key[mp])) {
         if (kAsc) atomicMax(J.ext_key + mp, key);
         else atomicMin(J.ext_key + mp, key);
       }
+      if (kd) {
+        m0 = pos == 0 ? mp : m0;
+        m1 = pos == 1 ? mp : m1;
+        m2 = pos == 2 ? mp : m2;
+        m3 = pos == 3 ? mp : m3;
+        if (pos >= 4) out[pos] = mp;
+        ++pos;
+      }
     }
+    if (act) orm[i] = make_int4(m0, m1, m2, m3);
   }
 }
 
@@ -1295,7 +1259,8 @@ __global__ void __launch_bounds__(256) k_extreme_saddle(Job<T> J) {
     for (int p = 0; p < pmax; ++p) {
       int m = -1;
       if (p < cnt) m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : row[p];
-      // A row's first entry per extremum only, as counted by k_rows.
+      // A row's first entry per extremum only (a repeat is -1), as counted
+      // by k_rows.
       const bool fresh = m >= 0 && m != prev;
       if (m >= 0) prev = m;
       const unsigned grp = __match_any_sync(0xffffffffu, fresh ? m : -1);
@@ -2195,6 +2160,7 @@ __global__ void __launch_bounds__(256) k_wis_mark(const Job<T>* __restrict__ job
         for (int p = 0; p < cnt; ++p) {
           const int m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w
                                                                : rows[(long long)i * kRowStride + p];
+          if (m < 0) continue;  // a repeated label
           if (atomicExch(stamp + m, epoch) != epoch) J.aff[atomicAdd(J.ctr + C_AFF, 1)] = m;
         }
       }
