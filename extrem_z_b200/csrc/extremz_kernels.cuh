@@ -1199,29 +1199,42 @@ __global__ void __launch_bounds__(256, 4) k_rows(Job<T> J, const T* __restrict__
     using KK = typename KeyOf<T>::K;
     const KK key = KeyOf<T>::enc(sv + T(0));  // -0 and +0 compare equal
     int* mcount = kAsc ? J.moff2 : J.moff1;
+    // The extremum indices of the fresh entries first, all gathers in flight
+    // together (loads after an atomic would wait for it).
+    int mp[kNumDirs];
+#pragma unroll
+    for (int d = 0; d < kNumDirs; ++d)
+      mp[d] = (keep >> d & ~dup >> d & 1u) ? J.ext[lb[d]] : -1;
     int m0 = -1, m1 = -1, m2 = -1, m3 = -1;
     int pos = 0;
 #pragma unroll
     for (int d = 0; d < kNumDirs; ++d) {
       const bool kd = keep >> d & 1u;
-      const bool fresh = kd && !(dup >> d & 1u);
-      const int mp = fresh ? J.ext[lb[d]] : -1;
-      const unsigned grp = __match_any_sync(0xffffffffu, mp);
-      if (fresh && (grp & ((1u << lane_id()) - 1u)) == 0u) atomicAdd(mcount + mp, __popc(grp));
-      if (fresh && (kAsc ? key > J.ext_key[mp] : key < J.ext_key[mp])) {
-        if (kAsc) atomicMax(J.ext_key + mp, key);
-        else atomicMin(J.ext_key + mp, key);
-      }
+      const unsigned grp = __match_any_sync(0xffffffffu, mp[d]);
+      if (mp[d] >= 0 && (grp & ((1u << lane_id()) - 1u)) == 0u) atomicAdd(mcount + mp[d], __popc(grp));
       if (kd) {
-        m0 = pos == 0 ? mp : m0;
-        m1 = pos == 1 ? mp : m1;
-        m2 = pos == 2 ? mp : m2;
-        m3 = pos == 3 ? mp : m3;
-        if (pos >= 4) out[pos] = mp;
+        m0 = pos == 0 ? mp[d] : m0;
+        m1 = pos == 1 ? mp[d] : m1;
+        m2 = pos == 2 ? mp[d] : m2;
+        m3 = pos == 3 ? mp[d] : m3;
+        if (pos >= 4) out[pos] = mp[d];
         ++pos;
       }
     }
     if (act) orm[i] = make_int4(m0, m1, m2, m3);
+    // Then the key reads, seven at a time, and the atomics they call for.
+#pragma unroll
+    for (int h = 0; h < kNumDirs; h += 7) {
+      KK cur[7];
+#pragma unroll
+      for (int d = 0; d < 7; ++d) cur[d] = mp[h + d] >= 0 ? J.ext_key[mp[h + d]] : KK(0);
+#pragma unroll
+      for (int d = 0; d < 7; ++d) {
+        if (mp[h + d] < 0 || !(kAsc ? key > cur[d] : key < cur[d])) continue;
+        if (kAsc) atomicMax(J.ext_key + mp[h + d], key);
+        else atomicMin(J.ext_key + mp[h + d], key);
+      }
+    }
   }
 }
 
@@ -1255,26 +1268,40 @@ __global__ void __launch_bounds__(256) k_extreme_saddle(Job<T> J) {
     // (k_rows), longer rows' tails from the row (stored as extremum indices).
     const int4 m4 = i < ns ? (kMax ? J.orm2 : J.orm1)[i] : make_int4(-1, -1, -1, -1);
     const int pmax = __reduce_max_sync(0xffffffffu, (unsigned)cnt);
-    int prev = -1;
-    for (int p = 0; p < pmax; ++p) {
-      int m = -1;
-      if (p < cnt) m = p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : row[p];
-      // A row's first entry per extremum only (a repeat is -1), as counted
-      // by k_rows.
-      const bool fresh = m >= 0 && m != prev;
-      if (m >= 0) prev = m;
-      const unsigned grp = __match_any_sync(0xffffffffu, fresh ? m : -1);
-      const int leader = __ffs(grp) - 1;
-      const unsigned below = grp & ((1u << lane_id()) - 1u);
-      int at = 0;
-      if (fresh && below == 0u) at = atomicAdd(cur + m, __popc(grp));
-      at = __shfl_sync(0xffffffffu, at, leader) + __popc(below);
-      if (m < 0) continue;
-      if (J.ext_key[m] == key) {
-        if (kMax) atomicMax(J.ext_id + m, s);
-        else atomicMin(J.ext_id + m, s);
+    // Seven entries at a time, each step's loads and atomics issued together
+    // (a load after an atomic would wait for it).  A row names an extremum in
+    // one entry only (a repeat is -1), as counted by k_rows.
+#pragma unroll
+    for (int h = 0; h < kNumDirs; h += 7) {
+      if (h >= pmax) break;
+      int m[7];
+#pragma unroll
+      for (int q = 0; q < 7; ++q) {
+        const int p = h + q;
+        m[q] = p >= cnt ? -1 : p == 0 ? m4.x : p == 1 ? m4.y : p == 2 ? m4.z : p == 3 ? m4.w : row[p];
       }
-      if (fresh) ent[at] = i * kRowStride + p;
+      unsigned grp[7];
+#pragma unroll
+      for (int q = 0; q < 7; ++q) grp[q] = __match_any_sync(0xffffffffu, m[q]);
+      int at[7];
+#pragma unroll
+      for (int q = 0; q < 7; ++q)
+        at[q] = (m[q] >= 0 && (grp[q] & ((1u << lane_id()) - 1u)) == 0u)
+                    ? atomicAdd(cur + m[q], __popc(grp[q])) : 0;
+      K ek[7];
+#pragma unroll
+      for (int q = 0; q < 7; ++q) ek[q] = m[q] >= 0 ? J.ext_key[m[q]] : K(0);
+#pragma unroll
+      for (int q = 0; q < 7; ++q) {
+        const unsigned below = grp[q] & ((1u << lane_id()) - 1u);
+        const int pos = __shfl_sync(0xffffffffu, at[q], __ffs(grp[q]) - 1) + __popc(below);
+        if (m[q] < 0) continue;
+        if (ek[q] == key) {
+          if (kMax) atomicMax(J.ext_id + m[q], s);
+          else atomicMin(J.ext_id + m[q], s);
+        }
+        ent[pos] = i * kRowStride + h + q;
+      }
     }
   }
 }
