@@ -96,13 +96,13 @@ def round_bytes(n: int, s: int) -> int:
     return n * (s + 8)
 
 
-def jump_design_bytes(n: int, launches: int, corrections: int) -> int:
-    """Bytes k_jump2 itself must move in `launches` computed rounds over
-    `corrections` corrections: per voxel the two tile-compressed pointers, the
-    two current labels and the two original roots (24 B) plus the change bit,
-    and the changed-input byte (1 B); a correction's first computed round also
-    writes both labels and the mismatch byte (9 B)."""
-    return 34 * n * corrections + 25 * n * (launches - corrections)
+def jump_design_bytes(n: int, rounds: int) -> int:
+    """Bytes k_jump2 itself must move in `rounds` first (full) manifold rounds:
+    per voxel it reads the two tile-compressed pointers and the two original
+    roots (16 B; a first round needs no old labels) and writes both labels,
+    the mismatch byte and the changed-input byte (10 B); the change bits
+    (N / 8 bytes) are not counted."""
+    return 26 * n * rounds
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the first
@@ -358,7 +358,7 @@ def manifold_roofline(reps, n, s, step_ms, peak, peak_kind, traffic=None):
     ms = dir_ms + jump_ms
     alg = round_bytes(n, s) * firsts
     achieved = alg / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
-    jb = jump_design_bytes(n, firsts, firsts)
+    jb = jump_design_bytes(n, firsts)
     jump_gbs = jb / (jump_ms * 1e-3) / 1e9 if jump_ms > 0 else 0.0
     later = sum(r.manifold_rounds - r.manifold_reused for r in reps) - firsts
     ldir = sum(r.prof_ms["direction"] for r in reps)
@@ -379,8 +379,9 @@ def manifold_roofline(reps, n, s, step_ms, peak, peak_kind, traffic=None):
             "jump_design_bytes": {"kernel": "k_jump2", "bytes": jb, "achieved_gbs": jump_gbs,
                                   "frac": jump_gbs / peak,
                                   "note": "the bytes k_jump2 itself moves in a first round "
-                                          "(pointers, labels, original roots, change marks, "
-                                          "34 B per voxel), a lower bound"},
+                                          "(pointers and original roots read, labels, mismatch "
+                                          "and changed-input bytes written: 26 B per voxel), "
+                                          "a lower bound"},
             "later_rounds": {
                 "rounds": later, "reused": sum(r.manifold_reused for r in reps),
                 "direction_ms": ldir, "jump_ms": ljump,

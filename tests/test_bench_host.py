@@ -16,14 +16,12 @@ def test_manifold_round_bytes_are_value_read_plus_two_label_writes():
     assert bench.round_bytes(n, 4) == 12 * n
 
 
-def test_jump_design_bytes_first_round_full_later_rounds_lower_bound():
+def test_jump_design_bytes_of_first_rounds():
     n = 256 ** 3
-    # One correction: the first computed round reads 24 B and writes 10 B per
-    # voxel; later rounds read 24 B and write the changed-input byte.
-    assert bench.jump_design_bytes(n, 1, 1) == 34 * n
-    assert bench.jump_design_bytes(n, 13, 1) == 34 * n + 12 * 25 * n
-    # Thirty corrections of twelve computed rounds each.
-    assert bench.jump_design_bytes(n, 360, 30) == 30 * 34 * n + 330 * 25 * n
+    # A first round reads pointers and original roots (16 B per voxel) and
+    # writes labels, mismatch and changed-input bytes (10 B).
+    assert bench.jump_design_bytes(n, 1) == 26 * n
+    assert bench.jump_design_bytes(n, 30) == 30 * 26 * n
 
 
 class _Proc:
