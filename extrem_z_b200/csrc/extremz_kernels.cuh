@@ -1546,16 +1546,25 @@ __device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
   const T* __restrict__ gv = J.g;
   const int* __restrict__ lab = kSplit ? J.dds : J.das;
   const T sv = __ldg(gv + s);
-  T val[kNumDirs];
-#pragma unroll
-  for (int d = 0; d < kNumDirs; ++d)
-    val[d] = (valid >> d & 1) ? __ldg(gv + s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH) : T(0);
+  // Neighbour values, then the side's labels and mismatch bytes, then the
+  // labels' values: batches of independent gathers, values seven at a time
+  // (fourteen live values spill at 64 registers).
   unsigned side = 0;
 #pragma unroll
-  for (int d = 0; d < kNumDirs; ++d) {
-    const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
-    if ((valid >> d & 1) && (kSplit ? above(val[d], r, sv, s) : below(val[d], r, sv, s)))
-      side |= 1u << d;
+  for (int h = 0; h < kNumDirs; h += 7) {
+    T val[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+      const int d = h + q;
+      val[q] = (valid >> d & 1) ? __ldg(gv + s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH) : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+      const int d = h + q;
+      const int r = s + dir_x(d) + dir_y(d) * g.W + dir_z(d) * WH;
+      if ((valid >> d & 1) && (kSplit ? above(val[q], r, sv, s) : below(val[q], r, sv, s)))
+        side |= 1u << d;
+    }
   }
   int ml[kNumDirs];
   int mb = 0;
@@ -1565,18 +1574,22 @@ __device__ __forceinline__ bool saddle_row(const Job<T>& J, int i, int s) {
     ml[d] = (side >> d & 1) ? __ldg(lab + r) : -1;
     mb |= (side >> d & 1) ? __ldg(J.mis + r) : 0;
   }
-#pragma unroll
-  for (int d = 0; d < kNumDirs; ++d) val[d] = ml[d] >= 0 ? __ldg(gv + ml[d]) : T(0);
   T fv = T(0), lv = T(0);
   int cnt = 0, fm = -1, lm = -1;
 #pragma unroll
-  for (int d = 0; d < kNumDirs; ++d) {
-    const int m = ml[d];
-    const T v = val[d];
-    if (m >= 0 && (!kSplit || tabs(T(v - sv)) >= J.thr)) {
-      if (cnt == 0 || row_first<T, kSplit>(v, m, fv, fm)) { fv = v; fm = m; }
-      if (cnt == 0 || row_first<T, kSplit>(lv, lm, v, m)) { lv = v; lm = m; }
-      ++cnt;
+  for (int h = 0; h < kNumDirs; h += 7) {
+    T val[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) val[q] = ml[h + q] >= 0 ? __ldg(gv + ml[h + q]) : T(0);
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+      const int m = ml[h + q];
+      const T v = val[q];
+      if (m >= 0 && (!kSplit || tabs(T(v - sv)) >= J.thr)) {
+        if (cnt == 0 || row_first<T, kSplit>(v, m, fv, fm)) { fv = v; fm = m; }
+        if (cnt == 0 || row_first<T, kSplit>(lv, lm, v, m)) { lv = v; lm = m; }
+        ++cnt;
+      }
     }
   }
   const int oc = (kSplit ? J.ocnt2 : J.ocnt1)[i];
