@@ -108,7 +108,7 @@ def jump_design_bytes(n: int, rounds: int) -> int:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the first
 # decompressed manifold round (k_direction + k_jump2 over every tile and
 # vertex), by workload: the ncu capture of the 256^3 float64 correction
-# (profiles/manifold_round_256cube_f64.md: 226.2 MB + 458.4 MB), and the same
+# (226.2 MB for k_direction + 458.4 MB for k_jump2 per first round), and the same
 # per voxel for the 512^3 field (eight times the voxels; both kernels stream
 # whole arrays once).  Not captured for float32.
 MEASURED_TRAFFIC = {"plain256_f64": 684_600_000, "plain512_f64": 8 * 684_600_000}

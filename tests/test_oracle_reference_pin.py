@@ -18,7 +18,8 @@ Pinned here, byte for byte:
     are reproduced exactly (the 64^3 seed-0 field has runs of both);
   * the ascending resolution differs from the reference on the 256^3 field
     and agrees with it on the 512^3 field.
-Run as a script to print the table that DESIGN.md's parity section shows.
+Run as a script to print the table of the pins (case, agreeing runs, runs equal to
+each resolution).
 """
 
 import hashlib
