@@ -108,10 +108,10 @@ def jump_design_bytes(n: int, rounds: int) -> int:
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the first
 # decompressed manifold round (k_direction + k_jump2 over every tile and
 # vertex), by workload: the ncu capture of the 256^3 float64 correction
-# (226.2 MB for k_direction + 458.4 MB for k_jump2 per first round), and the same
+# (226.3 MB for k_direction + 458.0 MB for k_jump2 per first round), and the same
 # per voxel for the 512^3 field (eight times the voxels; both kernels stream
 # whole arrays once).  Not captured for float32.
-MEASURED_TRAFFIC = {"plain256_f64": 684_600_000, "plain512_f64": 8 * 684_600_000}
+MEASURED_TRAFFIC = {"plain256_f64": 684_300_000, "plain512_f64": 8 * 684_300_000}
 
 
 def measured_peaks():

@@ -1155,7 +1155,7 @@ class BatchEngine {
             const int ntiles = lt.off[lt.n];
             launch(K_DIRECTION, k_tile_list<T>,
                    std::max(1, std::min((ntiles + 255) / 256, 2 * sms_)), 256, jobs, ls);
-            launch(K_DIRECTION, k_direction_list<T>, std::max(1, std::min(ntiles, 3 * sms_)),
+            launch(K_DIRECTION, k_direction_list<T>, std::max(1, std::min(ntiles, 4 * sms_)),
                    256, jobs, ls);
           }
           if (!fresh.empty())

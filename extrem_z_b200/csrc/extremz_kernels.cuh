@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(256) k_tile_list(const Job<T>* __restrict__ jo
 // rtouch1): only vertices with a touched label can change label this round
 // (k_jump2).
 template <class T>
-__global__ void __launch_bounds__(256, 3) k_direction_list(const Job<T>* __restrict__ jobs,
+__global__ void __launch_bounds__(256, 4) k_direction_list(const Job<T>* __restrict__ jobs,
                                                         const __grid_constant__ Sel sel) {
   __shared__ Tile<T> s;
   __shared__ uint64_t bar;
