@@ -1082,7 +1082,6 @@ class BatchEngine {
     const Job<T>* jobs = jobs_dev_;
     switch (ph) {
       case PC_SETUP_A:
-        launch(K_SETUP, k_classify<T, false>, st.off[st.n], 256, jobs, st);
         launch(K_SETUP, k_direction<T, false>, st.off[st.n], 256, jobs, st);
         launch(K_SETUP, k_jump2<T, false>, grid_, 256, jobs, s);
         for (int i : sel) {

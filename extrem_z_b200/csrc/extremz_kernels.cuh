@@ -549,8 +549,9 @@ __device__ __forceinline__ int follow(const int16_t* nxt, const int* exit_gid, i
 
 // Steepest pointers of one tile, compressed to the tile's exits: every voxel's
 // pointer is the first vertex outside the tile on its steepest path, or the
-// path's root inside the tile.  kDec = false: f into ds / as (setup); true: g
-// into pdd / pda.  Returns false when the tile's load did not complete.
+// path's root inside the tile.  kDec = false: f into ds / as (setup), with the
+// original classification (otype, olm) from the same tile load; true: g into
+// pdd / pda.  Returns false when the tile's load did not complete.
 template <class T, bool kDec>
 __device__ __noinline__ bool direction_tile(const Job<T>& J, Tile<T>& s, uint64_t* bar,
                                                int16_t* hnext, int16_t* lnext, int* hexit,
@@ -584,6 +585,17 @@ __device__ __noinline__ bool direction_tile(const Job<T>& J, Tile<T>& s, uint64_
       else steepest_dirs<T, false>(s, tx, ty, tz, valid_mask(bc), hd, ld);
     }
     const int v = x + y * g.W + z * WH;
+    if (!kDec && in) {
+      // The original field's classification from the same tile
+      // (classifyVertex_CUDA, the type = 0 call :5289): type and lower-star
+      // direction mask.
+      const int bc = interior ? 0 : boundary_code(x, y, z, g.W, g.H, g.D);
+      const int valid = interior ? (1 << kNumDirs) - 1 : valid_mask(bc);
+      int lm, um;
+      tile_masks(s, tx, ty, tz, valid, lm, um);
+      J.otype[v] = (int8_t)type_from_masks(lm, um, valid, bc, J.tb);
+      J.olm[v] = (uint16_t)lm;
+    }
     // Next step in tile terms: the local index when it stays in the tile,
     // kExit (the first outside vertex to the exit slot) when it leaves it,
     // kRoot at a root.
