@@ -16,6 +16,31 @@ def test_manifold_round_bytes_are_value_read_plus_two_label_writes():
     assert bench.round_bytes(n, 4) == 12 * n
 
 
+class _Rep:
+    """The fields of api.CorrectionReport that the roofline reads."""
+
+    def __init__(self, rounds, reused, ms, launches):
+        self.manifold_rounds, self.manifold_reused = rounds, reused
+        self.prof_ms, self.prof_launches = ms, launches
+
+
+def test_roofline_is_the_first_full_round_with_later_rounds_beside_it():
+    n, s = 512 ** 3, 8
+    ms = {"direction_first": 2.0, "jump_first": 1.2, "direction": 1.5, "jump": 3.5}
+    reps = [_Rep(13, 5, ms, {"jump_first": 1}) for _ in range(2)]
+    r = bench.manifold_roofline(reps, n, s, step_ms=2 * 34.0, peak=6539.2, peak_kind="measured",
+                                traffic=5.47e9)
+    # Two corrections, one first round each: 2 x N*(S+8) bytes over 2 x 3.2 ms.
+    assert r["launches"] == 2
+    assert abs(r["achieved"] - 2 * 16 * n / (6.4e-3) / 1e9) < 1e-6
+    assert abs(r["frac"] - r["achieved"] / 6539.2) < 1e-12
+    assert r["algorithmic_bytes_per_launch"] == 16 * n and r["traffic"] == 5.47e9
+    later = r["later_rounds"]
+    assert later["rounds"] == 2 * (13 - 5) - 2 and later["reused"] == 10
+    assert abs(later["ms_per_round"] - 10.0 / 14) < 1e-12
+    assert abs(r["jump_design_bytes"]["bytes"] - 2 * 26 * n) == 0
+
+
 def test_jump_design_bytes_of_first_rounds():
     n = 256 ** 3
     # A first round reads pointers and original roots (16 B per voxel) and
