@@ -84,3 +84,52 @@ def correct_batch_sharded(ctx, items, voxels: Sequence[int], *, rank: int, world
     if any(r is None for r in out):
         raise RuntimeError("a field of the batch has no report")
     return out, parts, launches
+
+
+class Router:
+    """Requests over several devices' servers, each to the one with the fewest
+    outstanding voxels (``route``).
+
+    servers: one ``api.Server`` per device (or any object with the same
+    ``submit(f, decp, bound, **kw) -> ticket`` / ``poll(ticket)`` /
+    ``wait(ticket, timeout_ms)`` calls).  A request's tensors must live on
+    the device of the server it goes to, so the caller asks ``pick`` first and
+    places the request there; ``submit`` then queues it.  Tickets are the
+    router's own, (server index, server ticket) inside.
+    """
+
+    def __init__(self, servers):
+        if not servers:
+            raise ValueError("no servers")
+        self.servers = list(servers)
+        self.outstanding = [0] * len(self.servers)
+        self._open = {}  # router ticket -> (server, server ticket, voxels)
+        self._next = 0
+
+    def pick(self, voxels: int) -> int:
+        """The server index the next request of ``voxels`` voxels goes to."""
+        return route(self.outstanding)
+
+    def submit(self, index: int, f, decp, bound: float, **kw) -> int:
+        voxels = int(f.numel())
+        t = self.servers[index].submit(f, decp, bound, **kw)
+        self.outstanding[index] += voxels
+        tk = self._next
+        self._next += 1
+        self._open[tk] = (index, t, voxels)
+        return tk
+
+    def _done(self, tk, res):
+        if res is not None:
+            index, _, voxels = self._open.pop(tk)
+            self.outstanding[index] -= voxels
+        return res
+
+    def poll(self, tk: int):
+        """None while pending, else the server's (report, latency ms)."""
+        index, t, _ = self._open[tk]
+        return self._done(tk, self.servers[index].poll(t))
+
+    def wait(self, tk: int, timeout_ms: int = -1):
+        index, t, _ = self._open[tk]
+        return self._done(tk, self.servers[index].wait(t, timeout_ms))

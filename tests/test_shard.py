@@ -2,9 +2,11 @@
 
 The plan must give every field to exactly one rank, the same plan on every
 rank, and a makespan within the longest-processing-time bound; the sharded
-batch must gather every field's report in batch order.  The multi-rank gather
-runs on two CPU ranks (gloo) with a stand-in for the correction context that
-records which fields it was handed.
+batch must gather every field's report in batch order; the request router
+must send each request to the server with the fewest outstanding voxels and
+release them on completion.  The multi-rank gather runs on two CPU ranks
+(gloo) with a stand-in for the correction context that records which fields
+it was handed; the router runs over stand-in servers.
 """
 
 import os
@@ -119,3 +121,49 @@ def test_sharded_batch_gathers_reports_in_batch_order_on_gloo():
         assert ranks == [owner[i] for i in range(len(vox))]
         assert got == parts
         assert launches == 7 * len(parts[rank])
+
+
+class _FakeTensor:
+    def __init__(self, n):
+        self.n = n
+
+    def numel(self):
+        return self.n
+
+
+class _FakeServer:
+    """Completes a request when told to; reports the voxels it saw."""
+
+    def __init__(self):
+        self.jobs, self.done = {}, set()
+
+    def submit(self, f, decp, bound, **kw):
+        t = len(self.jobs)
+        self.jobs[t] = f.numel()
+        return t
+
+    def poll(self, t):
+        return ({"voxels": self.jobs[t]}, 1.0) if t in self.done else None
+
+    def wait(self, t, timeout_ms=-1):
+        self.done.add(t)
+        return self.poll(t)
+
+
+def test_router_balances_outstanding_voxels_and_releases_them():
+    srv = [_FakeServer(), _FakeServer(), _FakeServer()]
+    router = shard.Router(srv)
+    tickets = []
+    for n in (900, 500, 400, 300, 300):
+        i = router.pick(n)
+        tickets.append((router.submit(i, _FakeTensor(n), None, 0.1), i, n))
+    # 900 -> 0, 500 -> 1, 400 -> 2, 300 -> 2 (400 < 500), 300 -> 1 (500 < 700).
+    assert [i for _, i, _ in tickets] == [0, 1, 2, 2, 1]
+    assert router.outstanding == [900, 800, 700]
+    tk, i, n = tickets[0]
+    assert router.poll(tk) is None
+    rep, ms = router.wait(tk)
+    assert rep["voxels"] == 900 and router.outstanding == [0, 800, 700]
+    assert router.pick(100) == 0
+    with pytest.raises(ValueError):
+        shard.Router([])
