@@ -25,6 +25,8 @@ _lib = None
 _lock = threading.Lock()
 
 OK, ROUND_CAP, BAD_ARG, OOM, CUDA_ERR, DEVICE_TIMEOUT, NO_DEVICE, TOO_LARGE, PENDING = range(9)
+# EXTREMZ_ABI_VERSION of include/extremz.h that the structures below follow.
+ABI_VERSION = 2
 F32, F64 = 0, 1
 
 # Every entry point declared in include/extremz.h.
@@ -151,6 +153,9 @@ def load(build_if_missing: bool = True):
         L = ctypes.CDLL(path)
         vp, i32 = ctypes.c_void_p, ctypes.c_int
         L.extremz_version.restype = i32
+        if L.extremz_version() != ABI_VERSION:  # the report layout would not match
+            raise ExtremzError(BAD_ARG, f"{path} has ABI version {L.extremz_version()}, "
+                                        f"this binding {ABI_VERSION}: rebuild it")
         L.extremz_default_params.argtypes = [ctypes.POINTER(Params)]
         L.extremz_ctx_create.argtypes = [i32, ctypes.POINTER(vp)]
         L.extremz_ctx_create.restype = i32

@@ -24,7 +24,9 @@
 extern "C" {
 #endif
 
-#define EXTREMZ_ABI_VERSION 1
+/* 2: extremz_report times twelve kernel classes (the first manifold round's
+ * directions and jumps apart from the later rounds'). */
+#define EXTREMZ_ABI_VERSION 2
 
 typedef enum {
   EXTREMZ_OK = 0,

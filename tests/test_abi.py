@@ -41,7 +41,7 @@ def test_default_params_are_the_reference_defaults():
 
 
 def test_version():
-    assert api.load().extremz_version() == 1
+    assert api.load().extremz_version() == api.ABI_VERSION == 2
 
 
 def test_status_strings():
